@@ -1,0 +1,132 @@
+/* lrc.h - the C ABI of little_renderer's CUDA backend (B200, sm_100a).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes. It replaces the
+ * WebGPU-typed private layer of the reference's GPU path tracer (engine/gpu/gpu_internal.h:
+ * 260-313, gpu_trace_*) so that a `cuda` backend implementing the public, WebGPU-free headers
+ * engine/gpu/gpu.h:17-71 and engine/gpu/view_gpu.h:49-176 drops in beside the WebGPU/Vulkan one
+ * (as NOGPU=1 swaps in stubs, engine/gpu/view_gpu.c:5-46).
+ *
+ * Status codes follow the reference's conventions (view_gpu.h:65-74): 0 = done; > 0 = this
+ * cannot be held now, retry after a change (as gpu_view_trace_start's 0); < 0 = failed for good
+ * (as gpu_view_trace_failed). No exception crosses the ABI. lrc_message() says why.
+ *
+ * Memory: unless LRC_DEVICE is given, every array argument is host memory, copied in and out
+ * inside the call. With LRC_DEVICE every array argument is a device pointer of the context's
+ * device and nothing is copied.
+ */
+#ifndef LRC_H
+#define LRC_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LRC_OK 0
+#define LRC_RETRY 1            /* refusable: out of device memory for this size; retry after a change */
+#define LRC_E_INVALID (-1)     /* a bad argument */
+#define LRC_E_CUDA (-2)        /* a CUDA error (lrc_message has it); the context may be lost */
+#define LRC_E_TIMEOUT (-3)     /* a bounded device wait ran out (the device status word says which) */
+#define LRC_E_STACK (-4)       /* a traversal stack would have overflowed (never dropped silently) */
+#define LRC_E_NODEVICE (-5)    /* no CUDA device (the caller then path traces on the CPU, gpu.h:32-35) */
+
+#define LRC_DEVICE 1u          /* flag: array arguments are device pointers */
+
+typedef struct lrc_ctx lrc_ctx;
+
+/* ---- device and context: replaces gpu_create / gpu_state / gpu_wait / gpu_message /
+ * gpu_destroy (engine/gpu/gpu.h:17-71) ------------------------------------------------------- */
+/* A context on CUDA device `device`, with its own stream. */
+int lrc_open(int device, lrc_ctx **out);
+void lrc_close(lrc_ctx *ctx);
+/* the last error's text (gpu_message, gpu.h) */
+const char *lrc_message(const lrc_ctx *ctx);
+/* waits for the context's work (gpu_wait, gpu.h) */
+int lrc_sync(lrc_ctx *ctx);
+/* later work goes to this CUDA stream (a cudaStream_t; NULL: the context's own) */
+int lrc_set_stream(lrc_ctx *ctx, void *cuda_stream);
+/* the device status word: bits of bounded waits that ran out (1 sort, 2 PLOC, 8 grid barrier)
+ * and of a traversal stack that would have overflowed (4). Read and cleared. */
+uint32_t lrc_status(lrc_ctx *ctx);
+/* the CUDA device's SM count (for callers sizing their own work) */
+int lrc_num_sms(const lrc_ctx *ctx);
+/* GPU time by stage (gpu_set_timing, gpu.h; the reference's GpuTimer stages, trace_gpu.c:330-333):
+ * on = 1 records CUDA events around each stage of later calls */
+#define LRC_TS_BOXES 0       /* triangle boxes and the mesh box */
+#define LRC_TS_MORTON 1      /* Morton codes and the radix histograms */
+#define LRC_TS_SORT 2        /* the radix sort's passes */
+#define LRC_TS_HIERARCHY 3   /* LBVH hierarchy and boxes, or PLOC */
+#define LRC_TS_TRACE 4       /* ray queries */
+#define LRC_TS_SHADE 5       /* path tracing */
+#define LRC_NUM_STAGES 8
+int lrc_set_timing(lrc_ctx *ctx, int on);
+/* milliseconds of each stage (ms[LRC_NUM_STAGES]) and launches of each (optional) since the last
+ * call; waits for the context's work */
+int lrc_timings(lrc_ctx *ctx, double *ms, int *launches);
+
+/* ---- the BVH builder: replaces build_queue + gpu_trace_build (engine/gpu/trace_gpu.c:587-764;
+ * shaders trace_build.wgsl and trace_ploc.wgsl) ----------------------------------------------- */
+typedef struct {
+    uint32_t n;          /* items (boxes) */
+    uint32_t node0;      /* the tree's root goes to nodes[node0]; internal i at node0 + i, leaf j at
+                            node0 + n - 1 + j (LBVH); PLOC: internal k's children at node0 + 1 + 2k, + 2 + 2k */
+    uint32_t ref0;       /* leaf j's entry in aux: ref0 + j */
+    uint32_t ref_add;    /* aux[ref0 + j] = item + ref_add */
+    float lo[3];         /* the bounds' low corner (BuildParams.lo) */
+    float ext[3];        /* 1 / the bounds' size per axis, 0 on a flat axis (BuildParams.ext) */
+    int32_t key_bits;    /* 30: the reference's Morton codes (10 bits per axis); 63: 21 bits per axis */
+    int32_t builder;     /* 0 LBVH (Karras), 1 PLOC */
+} lrc_build_params;
+
+/* build_queue's parameters from a bounds box (trace_gpu.c:605-611): lo, and ext = 1 / size in float */
+void lrc_params_from_bounds(const float lo[3], const float hi[3], lrc_build_params *p);
+/* Builds a BVH over n boxes (8 floats each: lo.xyz, -, hi.xyz, -, as build_queue's boxes) into
+ * nodes (8 words each: node0 + 2n - 1 of them) and aux (ref0 + n words), node for node and bit
+ * for bit the tree the reference's builders make. PLOC needs n >= 3 (as build_queue). */
+int lrc_build(lrc_ctx *ctx, const lrc_build_params *p, const float *boxes, uint32_t *nodes, uint32_t *aux,
+              unsigned flags);
+/* The device scratch memory lrc_build uses for n items (it is the context's, grown as needed). */
+size_t lrc_build_scratch_bytes(uint32_t n, int key_bits, int builder);
+
+/* triangle_bounds (engine/scene/scene.c:65-74) of n triangles in the reference's GPU layout
+ * (12 words each: q.xyz, n0, u.xyz, n1, v.xyz, material << 26 | n2; put_tris, trace_gpu.c:898-911)
+ * into boxes (8 floats each), and the mesh box of their corners (SceneMesh.box, scene.c:638-646)
+ * into bounds6 (lo.xyz, hi.xyz). */
+int lrc_triangle_boxes(lrc_ctx *ctx, const uint32_t *tris, uint32_t n, float *boxes, float *bounds6, unsigned flags);
+
+/* ---- a scene resident on the device: replaces GpuTrace's buffers and uploads
+ * (gpu_trace_sync, trace_gpu.c:1571; upload_tris :913, build_queue for meshes :1497-1512) ---- */
+typedef struct lrc_scene lrc_scene;
+int lrc_scene_create(lrc_ctx *ctx, lrc_scene **out);
+void lrc_scene_destroy(lrc_scene *s);
+/* the scene's triangles (12 words each, the reference GPU layout). Replaces what it held. */
+int lrc_scene_set_triangles(lrc_scene *s, const uint32_t *tris, uint32_t n, unsigned flags);
+/* Builds the scene's BVH over its triangles on the device: boxes = triangle_bounds, bounds = the
+ * mesh box (as upload_instances queues a dynamic mesh, trace_gpu.c:1497-1512), builder 0 LBVH /
+ * 1 PLOC, key_bits 30 or 63. */
+int lrc_scene_build(lrc_scene *s, int builder, int key_bits);
+/* the scene's nodes (2n - 1) and aux (n) copied out (host), or their device addresses */
+int lrc_scene_tree(lrc_scene *s, uint32_t *nodes, uint32_t *aux, unsigned flags);
+int lrc_scene_tree_device(lrc_scene *s, const uint32_t **nodes, const uint32_t **aux, uint32_t *n);
+
+/* Closest hits of nrays rays (origins, directions: 3 floats each) in (tmin, tmax) through the
+ * scene's BVH: prim = the triangle hit (-1: none), t. The reference's Moller-Trumbore arithmetic
+ * (engine/rt/intersect.h:96-112), bit for bit. Replaces traverse (trace.wgsl:270-392) for
+ * closest hits; the CPU counterpart is scene_intersect (engine/rt/accel.c:252). */
+int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
+                        int32_t *prim, float *t, unsigned flags);
+/* Any hit in (tmin, tmax[i]) (shadow rays; scene_occluded, accel.c:280): out[i] = 1 if blocked */
+int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const float *tmax, uint64_t nrays,
+                       float tmin, uint8_t *out, unsigned flags);
+/* The closest-hit walk of lrc_scene_intersect, counting instead of answering: stats[0] = box tests
+ * (32-byte node records read), stats[1] = triangle tests (48-byte triangles read), over all rays.
+ * The traversal's algorithmic bytes (as the reference's tree statistics, LR_GPU_BVH_CHECK's cost
+ * and depth, trace_gpu.c:768-805, describe a tree). stats: host. */
+int lrc_scene_trace_stats(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
+                          uint64_t *stats, unsigned flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,471 @@
+// api.cu - the C ABI (include/lrc.h) over the builder and traversal kernels.
+//
+// A context owns a CUDA stream, a device status word (bits of bounded waits that ran out and of
+// traversal stacks that would have overflowed) and one growing scratch arena, as the reference's
+// GpuTrace owns its builder's keys/flags/lists buffers (trace_gpu.c:736-741, gpu_buffer_reserve).
+// Calls with host arrays stage them through a second growing device arena, run, copy back and
+// synchronise; calls with LRC_DEVICE only enqueue (lrc_sync waits and reports).
+#include "lrc_internal.cuh"
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <new>
+
+using lrc::Node;
+
+struct lrc_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t own = nullptr, st = nullptr;
+    uint32_t *d_status = nullptr;
+    void *scratch = nullptr;
+    size_t scratch_cap = 0;
+    void *stage = nullptr;
+    size_t stage_cap = 0;
+    lrc::StageTimer timer;
+    std::string msg;
+};
+
+struct lrc_scene {
+    lrc_ctx *ctx = nullptr;
+    uint32_t *d_tris = nullptr;
+    size_t tris_cap = 0;
+    uint32_t ntris = 0;
+    Node *d_nodes = nullptr;
+    uint32_t *d_aux = nullptr;
+    size_t tree_cap = 0;          // items the tree buffers hold
+    uint32_t built_n = 0;         // items of the built tree (0: none)
+    float *d_boxes = nullptr;
+    size_t boxes_cap = 0;
+    uint32_t *d_small = nullptr;  // 6 bound keys, 6 bounds, 6 lo/ext
+};
+
+namespace {
+
+int fail(lrc_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess) {
+    if (c) {
+        c->msg = what;
+        if (e != cudaSuccess) {
+            c->msg += ": ";
+            c->msg += cudaGetErrorString(e);
+        }
+    }
+    return code;
+}
+
+// a CUDA error as a status: out of memory is refusable (retry after a change), the rest fatal
+int cuda_status(lrc_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return LRC_OK;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(c, LRC_RETRY, what, e);
+    }
+    return fail(c, LRC_E_CUDA, what, e);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+// a device buffer of at least `bytes` (grown by a quarter more; contents not kept)
+cudaError_t reserve(void **p, size_t *cap, size_t bytes) {
+    if (*cap >= bytes && *p) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t want = bytes + bytes / 4 + 4096;
+    cudaError_t e = cudaMalloc(p, want);
+    if (e == cudaSuccess) *cap = want;
+    return e;
+}
+
+// reads and clears the status word (synchronises the stream first)
+int check_status(lrc_ctx *c) {
+    cudaError_t e = cudaStreamSynchronize(c->st);
+    if (e) return cuda_status(c, e, "device work");
+    uint32_t s = 0;
+    e = cudaMemcpy(&s, c->d_status, 4, cudaMemcpyDeviceToHost);
+    if (e) return cuda_status(c, e, "status word");
+    if (s) {
+        cudaMemset(c->d_status, 0, 4);
+        if (s & lrc::ST_STACK_OVERFLOW) return fail(c, LRC_E_STACK, "a traversal stack would have overflowed (tree too deep)");
+        if (s & lrc::ST_BAD_TREE) return fail(c, LRC_E_INVALID, "a tree index out of range was met (not followed)");
+        return fail(c, LRC_E_TIMEOUT, "a bounded device wait ran out (sort look-back, PLOC look-back or grid barrier)");
+    }
+    return LRC_OK;
+}
+
+size_t al(size_t x) { return (x + 255) / 256 * 256; }
+
+// the walk's view of a scene: its tree (root 0), leaves' triangles, and the sizes it checks against
+lrc::TraceTables tables(const lrc_scene *s) {
+    lrc::TraceTables tt{};
+    tt.nodes = s->d_nodes;
+    tt.aux = s->d_aux;
+    tt.tris = reinterpret_cast<const float4 *>(s->d_tris);
+    tt.root = 0;
+    tt.nnodes = 2 * s->built_n - 1;
+    tt.naux = s->built_n;
+    tt.ntris = s->ntris;
+    return tt;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrc_open(int device, lrc_ctx **out) {
+    if (!out) return LRC_E_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        return LRC_E_NODEVICE;
+    }
+    if (device < 0 || device >= count) return LRC_E_INVALID;
+    lrc_ctx *c = new (std::nothrow) lrc_ctx;
+    if (!c) return LRC_RETRY;
+    c->device = device;
+    DeviceGuard g(device);
+    cudaError_t e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (!e) e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+    if (!e) e = cudaMalloc(&c->d_status, 256);
+    if (!e) e = cudaMemset(c->d_status, 0, 256);
+    if (e) {
+        int rc = cuda_status(c, e, "lrc_open");
+        if (c->own) cudaStreamDestroy(c->own);
+        if (c->d_status) cudaFree(c->d_status);
+        delete c;
+        return rc;
+    }
+    c->st = c->own;
+    *out = c;
+    return LRC_OK;
+}
+
+void lrc_close(lrc_ctx *c) {
+    if (!c) return;
+    DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->st);
+    if (c->scratch) cudaFree(c->scratch);
+    if (c->stage) cudaFree(c->stage);
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+}
+
+const char *lrc_message(const lrc_ctx *c) { return c ? c->msg.c_str() : "no context"; }
+
+int lrc_sync(lrc_ctx *c) {
+    if (!c) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    return check_status(c);
+}
+
+int lrc_set_stream(lrc_ctx *c, void *stream) {
+    if (!c) return LRC_E_INVALID;
+    c->st = stream ? reinterpret_cast<cudaStream_t>(stream) : c->own;
+    return LRC_OK;
+}
+
+uint32_t lrc_status(lrc_ctx *c) {
+    if (!c) return 0;
+    DeviceGuard g(c->device);
+    uint32_t s = 0;
+    cudaStreamSynchronize(c->st);
+    cudaMemcpy(&s, c->d_status, 4, cudaMemcpyDeviceToHost);
+    cudaMemset(c->d_status, 0, 4);
+    return s;
+}
+
+int lrc_num_sms(const lrc_ctx *c) { return c ? c->num_sms : 0; }
+
+int lrc_set_timing(lrc_ctx *c, int on) {
+    if (!c) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    c->timer.end(c->st);
+    c->timer.on = on != 0;
+    return LRC_OK;
+}
+
+int lrc_timings(lrc_ctx *c, double *ms, int *launches) {
+    if (!c || !ms) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    c->timer.end(c->st);
+    c->timer.collect();
+    for (int i = 0; i < LRC_NUM_STAGES; i++) {
+        ms[i] = c->timer.ms[i];
+        if (launches) launches[i] = c->timer.launches[i];
+        c->timer.ms[i] = 0;
+        c->timer.launches[i] = 0;
+    }
+    return LRC_OK;
+}
+
+void lrc_params_from_bounds(const float lo[3], const float hi[3], lrc_build_params *p) {
+    for (int k = 0; k < 3; k++) {
+        volatile float e = hi[k] - lo[k];      // v_sub in float
+        p->lo[k] = lo[k];
+        p->ext[k] = e > 0 ? 1.0f / e : 0.0f;   // (float)(1.0 / ext.x): a float division
+    }
+}
+
+size_t lrc_build_scratch_bytes(uint32_t n, int key_bits, int builder) { return lrc::build_scratch_bytes(n, key_bits, builder); }
+
+int lrc_build(lrc_ctx *c, const lrc_build_params *p, const float *boxes, uint32_t *nodes, uint32_t *aux, unsigned flags) {
+    if (!c || !p) return LRC_E_INVALID;
+    if (p->key_bits != 30 && p->key_bits != 63) return fail(c, LRC_E_INVALID, "key_bits must be 30 or 63");
+    if (p->n >= (1u << 30)) return fail(c, LRC_E_INVALID, "more than 2^30 - 1 items");
+    if (p->n == 0) return LRC_OK;
+    if (!boxes || !nodes || !aux) return fail(c, LRC_E_INVALID, "null array");
+    DeviceGuard g(c->device);
+    const uint32_t n = p->n;
+    const size_t need = lrc::build_scratch_bytes(n, p->key_bits, p->builder);
+    cudaError_t e = reserve(&c->scratch, &c->scratch_cap, need);
+    if (e) return cuda_status(c, e, "build scratch");
+    const size_t nnodes = 2 * (size_t)n - 1;
+    if (flags & LRC_DEVICE) {
+        e = lrc::build_device(*p, boxes, reinterpret_cast<Node *>(nodes) + p->node0, aux + p->ref0, c->scratch,
+                              c->scratch_cap, c->d_status, c->num_sms, c->st);
+        return cuda_status(c, e, "lrc_build");
+    }
+    const size_t b_boxes = al((size_t)n * 32), b_nodes = al(nnodes * 32), b_aux = al((size_t)n * 4);
+    e = reserve(&c->stage, &c->stage_cap, b_boxes + b_nodes + b_aux);
+    if (e) return cuda_status(c, e, "build staging");
+    char *s = static_cast<char *>(c->stage);
+    float *d_boxes = reinterpret_cast<float *>(s);
+    Node *d_nodes = reinterpret_cast<Node *>(s + b_boxes);
+    uint32_t *d_aux = reinterpret_cast<uint32_t *>(s + b_boxes + b_nodes);
+    e = cudaMemcpyAsync(d_boxes, boxes, (size_t)n * 32, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = lrc::build_device(*p, d_boxes, d_nodes, d_aux, c->scratch, c->scratch_cap, c->d_status, c->num_sms, c->st);
+    if (!e) e = cudaMemcpyAsync(reinterpret_cast<Node *>(nodes) + p->node0, d_nodes, nnodes * 32, cudaMemcpyDeviceToHost, c->st);
+    if (!e) e = cudaMemcpyAsync(aux + p->ref0, d_aux, (size_t)n * 4, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_build");
+    return check_status(c);
+}
+
+int lrc_triangle_boxes(lrc_ctx *c, const uint32_t *tris, uint32_t n, float *boxes, float *bounds6, unsigned flags) {
+    if (!c || (n && (!tris || !boxes))) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    const size_t b_tris = al((size_t)n * 48), b_boxes = al((size_t)n * 32);
+    cudaError_t e = reserve(&c->stage, &c->stage_cap, b_tris + b_boxes + 256);
+    if (e) return cuda_status(c, e, "staging");
+    char *s = static_cast<char *>(c->stage);
+    uint32_t *keys = reinterpret_cast<uint32_t *>(s + b_tris + b_boxes);
+    float *d_bounds = reinterpret_cast<float *>(keys + 8);
+    const uint32_t *d_tris = tris;
+    float *d_boxes = boxes;
+    if (!(flags & LRC_DEVICE)) {
+        d_tris = reinterpret_cast<uint32_t *>(s);
+        d_boxes = reinterpret_cast<float *>(s + b_tris);
+        e = cudaMemcpyAsync(const_cast<uint32_t *>(d_tris), tris, (size_t)n * 48, cudaMemcpyHostToDevice, c->st);
+        if (e) return cuda_status(c, e, "copy in");
+    }
+    e = lrc::triangle_boxes(d_tris, n, d_boxes, keys, c->st, c->num_sms);
+    if (!e) e = lrc::bounds_params(keys, (flags & LRC_DEVICE) && bounds6 ? bounds6 : d_bounds, nullptr, c->st);
+    if (e) return cuda_status(c, e, "lrc_triangle_boxes");
+    if (flags & LRC_DEVICE) return LRC_OK;
+    e = cudaMemcpyAsync(boxes, d_boxes, (size_t)n * 32, cudaMemcpyDeviceToHost, c->st);
+    if (!e && bounds6) e = cudaMemcpyAsync(bounds6, d_bounds, 24, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "copy out");
+    return check_status(c);
+}
+
+// ---- scenes -------------------------------------------------------------------------------------
+int lrc_scene_create(lrc_ctx *c, lrc_scene **out) {
+    if (!c || !out) return LRC_E_INVALID;
+    *out = nullptr;
+    lrc_scene *s = new (std::nothrow) lrc_scene;
+    if (!s) return LRC_RETRY;
+    s->ctx = c;
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaMalloc(&s->d_small, 256);
+    if (e) {
+        delete s;
+        return cuda_status(c, e, "scene");
+    }
+    *out = s;
+    return LRC_OK;
+}
+
+void lrc_scene_destroy(lrc_scene *s) {
+    if (!s) return;
+    DeviceGuard g(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->st);
+    cudaFree(s->d_tris);
+    cudaFree(s->d_nodes);
+    cudaFree(s->d_aux);
+    cudaFree(s->d_boxes);
+    cudaFree(s->d_small);
+    delete s;
+}
+
+int lrc_scene_set_triangles(lrc_scene *s, const uint32_t *tris, uint32_t n, unsigned flags) {
+    if (!s || (n && !tris)) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    DeviceGuard g(c->device);
+    cudaError_t e = reserve(reinterpret_cast<void **>(&s->d_tris), &s->tris_cap, (size_t)(n ? n : 1) * 48);
+    if (e) return cuda_status(c, e, "triangles");
+    if (n) e = cudaMemcpyAsync(s->d_tris, tris, (size_t)n * 48,
+                               (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->st);
+    if (e) return cuda_status(c, e, "triangles");
+    s->ntris = n;
+    s->built_n = 0;
+    if (!(flags & LRC_DEVICE)) return check_status(c);   // (the host array may be freed on return)
+    return LRC_OK;
+}
+
+int lrc_scene_build(lrc_scene *s, int builder, int key_bits) {
+    if (!s) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (key_bits != 30 && key_bits != 63) return fail(c, LRC_E_INVALID, "key_bits must be 30 or 63");
+    if (s->ntris >= (1u << 30)) return fail(c, LRC_E_INVALID, "more than 2^30 - 1 triangles");
+    DeviceGuard g(c->device);
+    const uint32_t n = s->ntris;
+    s->built_n = 0;
+    if (!n) return LRC_OK;
+    cudaError_t e = reserve(reinterpret_cast<void **>(&s->d_boxes), &s->boxes_cap, (size_t)n * 32);
+    if (!e && s->tree_cap < n) {
+        cudaFree(s->d_nodes);
+        cudaFree(s->d_aux);
+        s->d_nodes = nullptr;
+        s->d_aux = nullptr;
+        s->tree_cap = 0;
+        e = cudaMalloc(&s->d_nodes, (2 * (size_t)n - 1) * 32);
+        if (!e) e = cudaMalloc(&s->d_aux, (size_t)n * 4);
+        if (!e) s->tree_cap = n;
+    }
+    if (!e) e = reserve(&c->scratch, &c->scratch_cap, lrc::build_scratch_bytes(n, key_bits, builder));
+    if (e) return cuda_status(c, e, "scene build memory");
+    uint32_t *keys = s->d_small;
+    float *bounds = reinterpret_cast<float *>(s->d_small + 8), *lo_ext = reinterpret_cast<float *>(s->d_small + 16);
+    c->timer.begin(LRC_TS_BOXES, c->st);
+    e = lrc::triangle_boxes(s->d_tris, n, s->d_boxes, keys, c->st, c->num_sms);
+    if (!e) e = lrc::bounds_params(keys, bounds, lo_ext, c->st);
+    lrc_build_params p{};
+    p.n = n;
+    p.key_bits = key_bits;
+    p.builder = builder;
+    if (!e) e = lrc::build_device_ext(p, s->d_boxes, lo_ext, s->d_nodes, s->d_aux, c->scratch, c->scratch_cap, c->d_status,
+                                      c->num_sms, c->st, nullptr, &c->timer);
+    if (e) return cuda_status(c, e, "lrc_scene_build");
+    s->built_n = n;
+    return LRC_OK;
+}
+
+int lrc_scene_tree(lrc_scene *s, uint32_t *nodes, uint32_t *aux, unsigned flags) {
+    if (!s || !s->built_n) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    DeviceGuard g(c->device);
+    const uint32_t n = s->built_n;
+    cudaMemcpyKind k = (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    cudaError_t e = cudaSuccess;
+    if (nodes) e = cudaMemcpyAsync(nodes, s->d_nodes, (2 * (size_t)n - 1) * 32, k, c->st);
+    if (!e && aux) e = cudaMemcpyAsync(aux, s->d_aux, (size_t)n * 4, k, c->st);
+    if (e) return cuda_status(c, e, "lrc_scene_tree");
+    return check_status(c);
+}
+
+int lrc_scene_tree_device(lrc_scene *s, const uint32_t **nodes, const uint32_t **aux, uint32_t *n) {
+    if (!s) return LRC_E_INVALID;
+    if (nodes) *nodes = reinterpret_cast<const uint32_t *>(s->d_nodes);
+    if (aux) *aux = s->d_aux;
+    if (n) *n = s->built_n;
+    return s->built_n ? LRC_OK : LRC_E_INVALID;
+}
+
+int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
+                        int32_t *prim, float *t, unsigned flags) {
+    if (!s || (nrays && (!orig || !dir || !prim || !t))) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (!s->built_n) return fail(c, LRC_E_INVALID, "the scene has no built BVH (lrc_scene_build)");
+    DeviceGuard g(c->device);
+    lrc::TraceTables tt = tables(s);
+    if (flags & LRC_DEVICE) {
+        c->timer.begin(LRC_TS_TRACE, c->st);
+        cudaError_t e = lrc::intersect_device(tt, orig, dir, nrays, tmin, tmax, prim, t, c->d_status, c->st, c->num_sms);
+        c->timer.end(c->st);
+        return cuda_status(c, e, "lrc_scene_intersect");
+    }
+    const size_t b_ray = al(nrays * 12);
+    cudaError_t e = reserve(&c->stage, &c->stage_cap, 2 * b_ray + 2 * al(nrays * 4));
+    if (e) return cuda_status(c, e, "ray staging");
+    char *st = static_cast<char *>(c->stage);
+    float *d_o = reinterpret_cast<float *>(st), *d_d = reinterpret_cast<float *>(st + b_ray);
+    int32_t *d_p = reinterpret_cast<int32_t *>(st + 2 * b_ray);
+    float *d_t = reinterpret_cast<float *>(st + 2 * b_ray + al(nrays * 4));
+    e = cudaMemcpyAsync(d_o, orig, nrays * 12, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = cudaMemcpyAsync(d_d, dir, nrays * 12, cudaMemcpyHostToDevice, c->st);
+    c->timer.begin(LRC_TS_TRACE, c->st);
+    if (!e) e = lrc::intersect_device(tt, d_o, d_d, nrays, tmin, tmax, d_p, d_t, c->d_status, c->st, c->num_sms);
+    c->timer.end(c->st);
+    if (!e) e = cudaMemcpyAsync(prim, d_p, nrays * 4, cudaMemcpyDeviceToHost, c->st);
+    if (!e) e = cudaMemcpyAsync(t, d_t, nrays * 4, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_scene_intersect");
+    return check_status(c);
+}
+
+int lrc_scene_trace_stats(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
+                          uint64_t *stats, unsigned flags) {
+    if (!s || !stats || (nrays && (!orig || !dir))) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (!s->built_n) return fail(c, LRC_E_INVALID, "the scene has no built BVH (lrc_scene_build)");
+    DeviceGuard g(c->device);
+    lrc::TraceTables tt = tables(s);
+    const size_t b_ray = al(nrays * 12);
+    cudaError_t e = reserve(&c->stage, &c->stage_cap, 2 * b_ray + 256);
+    if (e) return cuda_status(c, e, "ray staging");
+    char *st = static_cast<char *>(c->stage);
+    const float *d_o = orig, *d_d = dir;
+    unsigned long long *d_stats = reinterpret_cast<unsigned long long *>(st + 2 * b_ray);
+    if (!(flags & LRC_DEVICE)) {
+        float *o = reinterpret_cast<float *>(st), *d = reinterpret_cast<float *>(st + b_ray);
+        e = cudaMemcpyAsync(o, orig, nrays * 12, cudaMemcpyHostToDevice, c->st);
+        if (!e) e = cudaMemcpyAsync(d, dir, nrays * 12, cudaMemcpyHostToDevice, c->st);
+        d_o = o;
+        d_d = d;
+    }
+    if (!e) e = lrc::count_device(tt, d_o, d_d, nrays, tmin, tmax, d_stats, c->d_status, c->st);
+    if (!e) e = cudaMemcpyAsync(stats, d_stats, 16, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_scene_trace_stats");
+    return check_status(c);
+}
+
+int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const float *tmax, uint64_t nrays, float tmin,
+                       uint8_t *out, unsigned flags) {
+    if (!s || (nrays && (!orig || !dir || !tmax || !out))) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (!s->built_n) return fail(c, LRC_E_INVALID, "the scene has no built BVH (lrc_scene_build)");
+    DeviceGuard g(c->device);
+    lrc::TraceTables tt = tables(s);
+    if (flags & LRC_DEVICE) {
+        cudaError_t e = lrc::occluded_device(tt, orig, dir, tmax, nrays, tmin, out, c->d_status, c->st);
+        return cuda_status(c, e, "lrc_scene_occluded");
+    }
+    const size_t b_ray = al(nrays * 12);
+    cudaError_t e = reserve(&c->stage, &c->stage_cap, 2 * b_ray + al(nrays * 4) + al(nrays));
+    if (e) return cuda_status(c, e, "ray staging");
+    char *st = static_cast<char *>(c->stage);
+    float *d_o = reinterpret_cast<float *>(st), *d_d = reinterpret_cast<float *>(st + b_ray);
+    float *d_tm = reinterpret_cast<float *>(st + 2 * b_ray);
+    uint8_t *d_out = reinterpret_cast<uint8_t *>(st + 2 * b_ray + al(nrays * 4));
+    e = cudaMemcpyAsync(d_o, orig, nrays * 12, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = cudaMemcpyAsync(d_d, dir, nrays * 12, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = cudaMemcpyAsync(d_tm, tmax, nrays * 4, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = lrc::occluded_device(tt, d_o, d_d, d_tm, nrays, tmin, d_out, c->d_status, c->st);
+    if (!e) e = cudaMemcpyAsync(out, d_out, nrays, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_scene_occluded");
+    return check_status(c);
+}
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+// lrc_internal.cuh - shared device/host definitions of the CUDA backend (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <cuda_runtime.h>
+#include "../../include/lrc.h"
+
+namespace lrc {
+
+// A BVH node as the reference's path tracer reads it (engine/gpu/shaders/trace/trace.wgsl:2
+// `Node`, written by put_nodes, engine/gpu/trace_gpu.c:883-896): box, and children (absolute
+// node indices) or, for a leaf, b = 0x80000000 | count and a = its first entry of aux.
+struct __align__(16) Node {
+    float lo[3];
+    uint32_t a;
+    float hi[3];
+    uint32_t b;
+};
+static_assert(sizeof(Node) == 32, "Node is 32 bytes");
+
+constexpr uint32_t LEAF_BIT = 0x80000000u;
+
+// Device status word bits (ctx->d_status): a bounded wait that ran out, a traversal stack that
+// would have overflowed. The host reads them after a call; nothing traps.
+constexpr uint32_t ST_TIMEOUT_SORT = 1u;
+constexpr uint32_t ST_TIMEOUT_PLOC = 2u;
+constexpr uint32_t ST_STACK_OVERFLOW = 4u;
+constexpr uint32_t ST_TIMEOUT_BARRIER = 8u;
+constexpr uint32_t ST_BAD_TREE = 16u;
+
+// spins before a bounded wait gives up (each ~ a few hundred ns with the back-off): ~1 s
+constexpr uint32_t SPIN_LIMIT = 1u << 22;
+
+// ---- IEEE single-precision arithmetic in the reference's order, never contracted ----------
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+// WGSL min / max (the shaders' builders): e2 if e2 < e1 (> for max), else e1
+__device__ __forceinline__ float wmin(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float wmax(float a, float b) { return b > a ? b : a; }
+// r_fmin / r_fmax (engine/base/lrmath.h): the other number when b is a NaN
+__device__ __forceinline__ float rfmin(float a, float b) { return b != b ? a : (a < b ? a : b); }
+__device__ __forceinline__ float rfmax(float a, float b) { return b != b ? a : (a > b ? a : b); }
+
+// ---- scratch arena: one cudaMalloc'd block per context, carved per call ----------------------
+struct Carve {
+    char *base;
+    size_t off, cap;
+    template <class T>
+    T *take(size_t count, size_t align = 256) {
+        off = (off + align - 1) / align * align;
+        T *p = reinterpret_cast<T *>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+};
+
+// GPU time by stage: CUDA events around each stage when on (lrc_set_timing)
+struct StageTimer {
+    bool on = false;
+    int open = -1;
+    cudaEvent_t open_ev = nullptr;
+    struct Rec { int stage; cudaEvent_t a, b; };
+    Rec recs[256];
+    int nrec = 0;
+    double ms[LRC_NUM_STAGES] = {};
+    int launches[LRC_NUM_STAGES] = {};
+    void begin(int stage, cudaStream_t st) {
+        if (!on) return;
+        end(st);
+        cudaEventCreate(&open_ev);
+        cudaEventRecord(open_ev, st);
+        open = stage;
+    }
+    void end(cudaStream_t st) {
+        if (!on || open < 0) return;
+        cudaEvent_t b;
+        cudaEventCreate(&b);
+        cudaEventRecord(b, st);
+        if (nrec == 256) collect();
+        recs[nrec++] = {open, open_ev, b};
+        open = -1;
+    }
+    void collect() {
+        for (int i = 0; i < nrec; i++) {
+            float t = 0;
+            cudaEventSynchronize(recs[i].b);
+            cudaEventElapsedTime(&t, recs[i].a, recs[i].b);
+            ms[recs[i].stage] += t;
+            launches[recs[i].stage]++;
+            cudaEventDestroy(recs[i].a);
+            cudaEventDestroy(recs[i].b);
+        }
+        nrec = 0;
+    }
+};
+
+// builder internals (build.cu)
+size_t build_scratch_bytes(uint32_t n, int key_bits, int builder);
+// boxes (n x 8 floats, device) -> the tree: d_nodes points at the tree's node node0 and d_aux at
+// aux[ref0] (the values written are absolute: node0 + ..., ref0 + ...). d_lo_ext (6 floats on the
+// device: lo, ext) overrides p.lo / p.ext when given. Scratch: at least build_scratch_bytes.
+cudaError_t build_device(const lrc_build_params &p, const float *d_boxes, Node *d_nodes, uint32_t *d_aux,
+                         void *d_scratch, size_t scratch_bytes, uint32_t *d_status, int num_sms, cudaStream_t st,
+                         uint32_t *d_sorted_codes_out = nullptr);
+cudaError_t build_device_ext(const lrc_build_params &p, const float *d_boxes, const float *d_lo_ext, Node *d_nodes,
+                             uint32_t *d_aux, void *d_scratch, size_t scratch_bytes, uint32_t *d_status, int num_sms,
+                             cudaStream_t st, uint32_t *d_sorted_codes_out, StageTimer *timer = nullptr);
+// triangle_bounds of n triangles (12 words each) into boxes (8 floats each), and the mesh box's
+// order keys into d_bkeys (6 words); bounds_params turns the keys into bounds6 and lo_ext
+cudaError_t triangle_boxes(const uint32_t *d_tris, uint32_t n, float *d_boxes, uint32_t *d_bkeys, cudaStream_t st,
+                           int num_sms);
+cudaError_t bounds_params(const uint32_t *d_bkeys, float *d_bounds6, float *d_lo_ext, cudaStream_t st);
+
+// traversal internals (traverse.cu)
+struct TraceTables {
+    const Node *nodes;
+    const uint32_t *aux;
+    const float4 *tris;      // 3 float4 per triangle (q, u, v; .w holds normals / material bits)
+    uint32_t root;           // absolute node index of the root
+    uint32_t nnodes, naux, ntris;   // sizes: an index out of them is reported (ST_BAD_TREE), not followed
+};
+cudaError_t intersect_device(const TraceTables &tt, const float *d_orig, const float *d_dir, uint64_t nrays,
+                             float tmin, float tmax, int32_t *d_prim, float *d_t, uint32_t *d_status,
+                             cudaStream_t st, int num_sms);
+cudaError_t count_device(const TraceTables &tt, const float *d_orig, const float *d_dir, uint64_t nrays, float tmin,
+                         float tmax, unsigned long long *d_stats, uint32_t *d_status, cudaStream_t st);
+cudaError_t occluded_device(const TraceTables &tt, const float *d_orig, const float *d_dir, const float *d_tmax,
+                            uint64_t nrays, float tmin, uint8_t *d_out, uint32_t *d_status, cudaStream_t st);
+
+}  // namespace lrc

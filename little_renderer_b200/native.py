@@ -1,0 +1,277 @@
+"""Build recipe and ctypes binding of the CUDA backend's C ABI (include/lrc.h).
+
+The library is built in-tree (``little_renderer_b200/liblrc.so``) with nvcc for sm_100a only.
+Loading it never falls back to anything: a missing or unloadable library raises.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "liblrc.so")
+SOURCES = ["api.cu", "build.cu", "traverse.cu"]
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-shared"]
+
+LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
+LRC_DEVICE = 1
+
+
+def nvcc():
+    for p in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if p and (os.path.sep not in p or os.path.exists(p)):
+            return p
+    return "nvcc"
+
+
+def build(force=False, verbose=False):
+    """Compiles liblrc.so for sm_100a when a source is newer than it (or force)."""
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, "lrc_internal.cuh"), os.path.join(ROOT, "include", "lrc.h")]
+    deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
+        return LIB
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB] + srcs
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True, cwd=CSRC)
+    return LIB
+
+
+_lib = None
+
+
+class LrcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"lrc error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """The loaded liblrc.so (raises if it is missing: there is no other path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise RuntimeError(f"{LIB} is not built: the CUDA backend is required (python -c 'import "
+                           "__graft_entry__ as g; g.build()')")
+    L = C.CDLL(LIB)
+    vp, u32, u64, f32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float
+    L.lrc_open.argtypes = [C.c_int, C.POINTER(vp)]
+    L.lrc_close.argtypes = [vp]
+    L.lrc_message.argtypes = [vp]
+    L.lrc_message.restype = C.c_char_p
+    L.lrc_sync.argtypes = [vp]
+    L.lrc_set_stream.argtypes = [vp, vp]
+    L.lrc_status.argtypes = [vp]
+    L.lrc_status.restype = u32
+    L.lrc_num_sms.argtypes = [vp]
+    L.lrc_params_from_bounds.argtypes = [vp, vp, vp]
+    L.lrc_build.argtypes = [vp, vp, vp, vp, vp, C.c_uint]
+    L.lrc_build_scratch_bytes.argtypes = [u32, C.c_int, C.c_int]
+    L.lrc_build_scratch_bytes.restype = C.c_size_t
+    L.lrc_triangle_boxes.argtypes = [vp, vp, u32, vp, vp, C.c_uint]
+    L.lrc_scene_create.argtypes = [vp, C.POINTER(vp)]
+    L.lrc_scene_destroy.argtypes = [vp]
+    L.lrc_scene_set_triangles.argtypes = [vp, vp, u32, C.c_uint]
+    L.lrc_scene_build.argtypes = [vp, C.c_int, C.c_int]
+    L.lrc_scene_tree.argtypes = [vp, vp, vp, C.c_uint]
+    L.lrc_scene_tree_device.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u32)]
+    L.lrc_scene_intersect.argtypes = [vp, vp, vp, u64, f32, f32, vp, vp, C.c_uint]
+    L.lrc_scene_occluded.argtypes = [vp, vp, vp, vp, u64, f32, vp, C.c_uint]
+    L.lrc_scene_trace_stats.argtypes = [vp, vp, vp, u64, f32, f32, vp, C.c_uint]
+    L.lrc_set_timing.argtypes = [vp, C.c_int]
+    L.lrc_timings.argtypes = [vp, vp, vp]
+    _lib = L
+    return L
+
+
+class BuildParams(C.Structure):
+    """lrc_build_params (build_queue's BuildParams, engine/gpu/trace_gpu.c:546)."""
+    _fields_ = [("n", C.c_uint32), ("node0", C.c_uint32), ("ref0", C.c_uint32), ("ref_add", C.c_uint32),
+                ("lo", C.c_float * 3), ("ext", C.c_float * 3), ("key_bits", C.c_int32), ("builder", C.c_int32)]
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray) else C.c_void_p(int(a))
+
+
+class Context:
+    """An lrc context on one CUDA device (lrc_open)."""
+
+    def __init__(self, device=0):
+        self.L = lib()
+        h = C.c_void_p()
+        rc = self.L.lrc_open(device, C.byref(h))
+        if rc:
+            raise LrcError(rc, "lrc_open failed (no CUDA device?)")
+        self.h = h
+
+    def check(self, rc):
+        if rc:
+            raise LrcError(rc, self.L.lrc_message(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.lrc_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        return self.check(self.L.lrc_sync(self.h))
+
+    def set_stream(self, stream_ptr):
+        self.check(self.L.lrc_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def num_sms(self):
+        return self.L.lrc_num_sms(self.h)
+
+    STAGES = ("boxes", "morton", "sort", "hierarchy", "trace", "shade")
+
+    def set_timing(self, on=True):
+        self.check(self.L.lrc_set_timing(self.h, int(on)))
+
+    def timings(self):
+        """{stage: (ms, launches)} since the last call (lrc_timings)."""
+        ms = np.zeros(8, np.float64)
+        cnt = np.zeros(8, np.int32)
+        self.check(self.L.lrc_timings(self.h, _ptr(ms), _ptr(cnt)))
+        return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(self.STAGES)}
+
+    def params(self, n, lo, hi, key_bits=30, builder=0, node0=0, ref0=0, ref_add=0):
+        p = BuildParams()
+        p.n, p.node0, p.ref0, p.ref_add, p.key_bits, p.builder = n, node0, ref0, ref_add, key_bits, builder
+        lo = np.ascontiguousarray(lo, np.float32)
+        hi = np.ascontiguousarray(hi, np.float32)
+        self.L.lrc_params_from_bounds(_ptr(lo), _ptr(hi), C.byref(p))
+        return p
+
+    def build(self, params, boxes, nodes=None, aux=None):
+        """lrc_build with host arrays: returns (nodes (node0 + 2n - 1, 8) u32, aux (ref0 + n) u32)."""
+        n = params.n
+        boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 8)
+        if nodes is None:
+            nodes = np.zeros((params.node0 + max(2 * n - 1, 1), 8), np.uint32)
+        if aux is None:
+            aux = np.zeros(params.ref0 + n, np.uint32)
+        self.check(self.L.lrc_build(self.h, C.byref(params), _ptr(boxes), _ptr(nodes), _ptr(aux), 0))
+        return nodes, aux
+
+    def build_device(self, params, d_boxes, d_nodes, d_aux):
+        """lrc_build with device pointers (ints): enqueued on the context's stream."""
+        self.check(self.L.lrc_build(self.h, C.byref(params), C.c_void_p(d_boxes), C.c_void_p(d_nodes),
+                                    C.c_void_p(d_aux), LRC_DEVICE))
+
+    def triangle_boxes(self, tris12):
+        tris12 = np.ascontiguousarray(tris12, np.uint32).reshape(-1, 12)
+        n = tris12.shape[0]
+        boxes = np.zeros((n, 8), np.float32)
+        bounds = np.zeros(6, np.float32)
+        self.check(self.L.lrc_triangle_boxes(self.h, _ptr(tris12), n, _ptr(boxes), _ptr(bounds), 0))
+        return boxes, bounds
+
+
+class Scene:
+    """A device-resident scene (lrc_scene_*)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(ctx.L.lrc_scene_create(ctx.h, C.byref(h)))
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.lrc_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_triangles(self, tris12, device_ptr=None, n=None):
+        L = self.ctx.L
+        if device_ptr is not None:
+            self.ctx.check(L.lrc_scene_set_triangles(self.h, C.c_void_p(device_ptr), n, LRC_DEVICE))
+            self.n = n
+            return
+        tris12 = np.ascontiguousarray(tris12, np.uint32).reshape(-1, 12)
+        self.n = tris12.shape[0]
+        self.ctx.check(L.lrc_scene_set_triangles(self.h, _ptr(tris12), self.n, 0))
+
+    def build(self, builder=0, key_bits=30):
+        self.ctx.check(self.ctx.L.lrc_scene_build(self.h, builder, key_bits))
+
+    def tree(self):
+        nodes = np.zeros((2 * self.n - 1, 8), np.uint32)
+        aux = np.zeros(self.n, np.uint32)
+        self.ctx.check(self.ctx.L.lrc_scene_tree(self.h, _ptr(nodes), _ptr(aux), 0))
+        return nodes, aux
+
+    def intersect(self, orig, dirs, tmin=0.0, tmax=1e30):
+        orig = np.ascontiguousarray(orig, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        n = orig.shape[0]
+        prim = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        self.ctx.check(self.ctx.L.lrc_scene_intersect(self.h, _ptr(orig), _ptr(dirs), n, tmin, tmax, _ptr(prim),
+                                                      _ptr(t), 0))
+        return prim, t
+
+    def intersect_device(self, d_orig, d_dir, n, d_prim, d_t, tmin=0.0, tmax=1e30):
+        self.ctx.check(self.ctx.L.lrc_scene_intersect(self.h, C.c_void_p(d_orig), C.c_void_p(d_dir), n, tmin, tmax,
+                                                      C.c_void_p(d_prim), C.c_void_p(d_t), LRC_DEVICE))
+
+    def trace_stats(self, orig, dirs, tmin=0.0, tmax=1e30):
+        """(box tests, triangle tests) of the closest-hit walk over these rays (device or host arrays)."""
+        stats = np.zeros(2, np.uint64)
+        if isinstance(orig, np.ndarray):
+            orig = np.ascontiguousarray(orig, np.float32)
+            dirs = np.ascontiguousarray(dirs, np.float32)
+            self.ctx.check(self.ctx.L.lrc_scene_trace_stats(self.h, _ptr(orig), _ptr(dirs), orig.shape[0], tmin, tmax,
+                                                            _ptr(stats), 0))
+        else:
+            n, po, pd = orig
+            self.ctx.check(self.ctx.L.lrc_scene_trace_stats(self.h, C.c_void_p(po), C.c_void_p(pd), n, tmin, tmax,
+                                                            _ptr(stats), LRC_DEVICE))
+        return int(stats[0]), int(stats[1])
+
+    def occluded(self, orig, dirs, tmax, tmin=0.0):
+        orig = np.ascontiguousarray(orig, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        tmax = np.ascontiguousarray(tmax, np.float32)
+        n = orig.shape[0]
+        out = np.zeros(n, np.uint8)
+        self.ctx.check(self.ctx.L.lrc_scene_occluded(self.h, _ptr(orig), _ptr(dirs), _ptr(tmax), n, tmin, _ptr(out),
+                                                     0))
+        return out
+
+
+def pack_tris(quv, mats=None):
+    """(n, 9) q, u, v float32 -> (n, 12) u32 words in the reference's GPU layout (put_tris,
+    engine/gpu/trace_gpu.c:898-911): flat triangles (n0 = 0xffffffff), material in the top 6 bits."""
+    quv = np.ascontiguousarray(quv, np.float32).reshape(-1, 9)
+    n = quv.shape[0]
+    out = np.zeros((n, 12), np.uint32)
+    f = out.view(np.float32)
+    f[:, 0:3] = quv[:, 0:3]
+    f[:, 4:7] = quv[:, 3:6]
+    f[:, 8:11] = quv[:, 6:9]
+    out[:, 3] = 0xFFFFFFFF
+    out[:, 7] = 0
+    m = np.zeros(n, np.uint32) if mats is None else (np.asarray(mats, np.uint32) & 63)
+    out[:, 11] = m << 26
+    return out

@@ -1,0 +1,250 @@
+// ref_bridge.c - TEST INFRASTRUCTURE (the oracle). Compiled together with the reference's own
+// CPU engine (engine/{base,formats,scene,rt}/*.c, by oracle/Makefile) into _ref/libref_f.so
+// (float build) and _ref/libref_d.so (double build, -DLR_DOUBLE). It turns flat arrays into a
+// reference Scene through the reference's public API and runs the reference's own code on it:
+//   closest hit  scene_intersect   (engine/rt/accel.c:252)
+//   any hit      scene_occluded    (engine/rt/accel.c:280)
+//   image        trace_image       (engine/rt/tracer.c:329)
+//   boxes        triangle_bounds   (engine/scene/scene.c:65)
+// and counts the tracer's rays through link-time --wrap of scene_intersect/scene_occluded
+// (no edit of the reference). Nothing of the product path calls this file.
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+#include "scene/scene.h"
+#include "scene/env.h"
+#include "rt/accel.h"
+#include "rt/tracer.h"
+#include "base/sampler.h"
+
+// ---- ray counters: one slot per OpenMP thread, 64 bytes apart ----------------------------
+#define RB_MAX_THREADS 256
+static long long rb_cnt[RB_MAX_THREADS * 8][2];
+
+int __real_scene_intersect(const Scene *s, const Ray *ray, real tmin, real tmax, Hit *h);
+int __real_scene_occluded(const Scene *s, const Ray *ray, real tmin, real tmax);
+
+int __wrap_scene_intersect(const Scene *s, const Ray *ray, real tmin, real tmax, Hit *h){
+    rb_cnt[(omp_get_thread_num() & (RB_MAX_THREADS - 1)) * 8][0]++;
+    return __real_scene_intersect(s, ray, tmin, tmax, h);
+}
+int __wrap_scene_occluded(const Scene *s, const Ray *ray, real tmin, real tmax){
+    rb_cnt[(omp_get_thread_num() & (RB_MAX_THREADS - 1)) * 8][1]++;
+    return __real_scene_occluded(s, ray, tmin, tmax);
+}
+void rb_rays_reset(void){ memset(rb_cnt, 0, sizeof(rb_cnt)); }
+// out[0] closest-hit rays, out[1] shadow rays since the last reset
+void rb_rays(long long *out){
+    out[0] = out[1] = 0;
+    for (int i = 0; i < RB_MAX_THREADS; i++){ out[0] += rb_cnt[i * 8][0]; out[1] += rb_cnt[i * 8][1]; }
+}
+int rb_real_is_double(void){ return sizeof(real) == sizeof(double); }
+int rb_max_threads(void){ return omp_get_max_threads(); }
+void rb_set_threads(int n){ if (n > 0) omp_set_num_threads(n); }
+
+// ---- scenes ---------------------------------------------------------------------------------
+static Vec3 v3f(const float *p){ return vec3(p[0], p[1], p[2]); }
+
+void *rb_scene_new(void){
+    Scene *s = calloc(1, sizeof(Scene));
+    if (s) s->light = -1;
+    return s;
+}
+void rb_scene_free(void *sp){
+    Scene *s = sp;
+    if (!s) return;
+    scene_free(s);
+    free(s);
+}
+
+// a material: type (MatType), albedo, emission, ior, metallic, roughness, transmission
+int rb_add_material(void *sp, int type, const float *albedo, const float *emission, float ior, float metallic,
+                    float roughness, float transmission){
+    Material m;
+    memset(&m, 0, sizeof(m));
+    m.type = (MatType)type;
+    m.albedo = v3f(albedo);
+    m.emission = v3f(emission);
+    m.ior = ior; m.metallic = metallic; m.roughness = roughness; m.transmission = transmission;
+    return scene_add_material(sp, m);
+}
+// the reference's presets (scene.h:48-70), for scene generators that name them
+int rb_add_material_preset(void *sp, int kind, const float *rgb, float a, float b){
+    Vec3 c = v3f(rgb);
+    Material m;
+    switch (kind){
+    case 0: m = material_diffuse(c); break;
+    case 1: m = material_mirror(c); break;
+    case 2: m = material_glass(c, a); break;
+    case 3: m = material_light(c); break;
+    case 4: m = material_pbr(c, a, b, 1.5, 0); break;          // metal: metallic a, roughness b
+    default: m = material_pbr(c, 0, b, a, 1); break;            // rough glass: ior a, roughness b
+    }
+    return scene_add_material(sp, m);
+}
+
+// n triangles by their corners (9 floats each: a, b, c), flat (no vertex normals)
+void rb_add_triangles(void *sp, const float *corners, const int *mats, int n){
+    for (int i = 0; i < n; i++){
+        const float *c = corners + 9 * (size_t)i;
+        scene_add_triangle(sp, v3f(c), v3f(c + 3), v3f(c + 6), NULL, mats[i]);
+    }
+}
+// a quad primitive (make_quad); light = 1 makes it Scene.light. Returns its index.
+int rb_add_quad(void *sp, const float *q, const float *u, const float *v, int mat, int light){
+    Scene *s = sp;
+    int i = scene_add_prim(s, make_quad(v3f(q), v3f(u), v3f(v), mat));
+    if (light) s->light = i;
+    return i;
+}
+int rb_add_sphere(void *sp, const float *c, float r, int mat){ return scene_add_prim(sp, make_sphere(v3f(c), r, mat)); }
+
+// an instanced mesh from corners (9 floats per triangle), flat, material per triangle
+int rb_add_mesh(void *sp, const float *corners, const int *mats, int n){
+    Triangle *t = malloc((size_t)(n ? n : 1) * sizeof(Triangle));
+    Vec3 *nrm = malloc(sizeof(Vec3));
+    for (int i = 0; i < n; i++){
+        const float *c = corners + 9 * (size_t)i;
+        Vec3 a = v3f(c), b = v3f(c + 3), d = v3f(c + 6);
+        t[i].q = a; t[i].u = v_sub(b, a); t[i].v = v_sub(d, a);
+        for (int k = 0; k < 3; k++){ t[i].n[k] = -1; t[i].t[k] = -1; }
+        t[i].material = mats[i];
+    }
+    return scene_add_mesh_arrays(sp, t, n, nrm, 0, NULL, NULL, 0);
+}
+// an instance of mesh `mesh` by its 3x4 row-major transform
+int rb_add_instance(void *sp, int mesh, const float *xf12, int material){
+    Xform x;
+    for (int r = 0; r < 3; r++) for (int k = 0; k < 4; k++) x.m[r][k] = xf12[4 * r + k];
+    return scene_add_instance(sp, mesh, x, material);
+}
+void rb_move_instance(void *sp, int inst, const float *xf12){
+    Xform x;
+    for (int r = 0; r < 3; r++) for (int k = 0; k < 4; k++) x.m[r][k] = xf12[4 * r + k];
+    scene_move_instance(sp, inst, x);
+}
+// instance i's world box (6 floats) and inverse transform (12)
+void rb_instance_data(const void *sp, int i, float *box6, float *inv12){
+    const Scene *s = sp;
+    const Instance *in = &s->insts[i];
+    box6[0] = in->box.lo.x; box6[1] = in->box.lo.y; box6[2] = in->box.lo.z;
+    box6[3] = in->box.hi.x; box6[4] = in->box.hi.y; box6[5] = in->box.hi.z;
+    for (int r = 0; r < 3; r++) for (int k = 0; k < 4; k++) inv12[4 * r + k] = in->inv.m[r][k];
+}
+void rb_mesh_box(const void *sp, int mesh, float *box6){
+    const Scene *s = sp;
+    const Aabb *b = &s->meshes[mesh].box;
+    box6[0] = b->lo.x; box6[1] = b->lo.y; box6[2] = b->lo.z; box6[3] = b->hi.x; box6[4] = b->hi.y; box6[5] = b->hi.z;
+}
+// a sky from w x h linear RGB floats (copied; the scene owns it)
+int rb_set_env(void *sp, const float *rgb, int w, int h){
+    Scene *s = sp;
+    float *c = malloc(sizeof(float) * 3 * (size_t)w * h);
+    if (!c) return 0;
+    memcpy(c, rgb, sizeof(float) * 3 * (size_t)w * h);
+    s->env = env_from_rgb(c, w, h);
+    return s->env != NULL;
+}
+void rb_set_accel(void *sp){ scene_set_accel(sp, ACCEL_BVH, NULL); }
+
+// the world's triangles as stored (q, u, v: 9 floats each) and their materials
+void rb_tri_data(const void *sp, float *quv, int *mats){
+    const Scene *s = sp;
+    for (int i = 0; i < s->ntris; i++){
+        const Triangle *t = &s->tris[i];
+        float *o = quv + 9 * (size_t)i;
+        o[0] = t->q.x; o[1] = t->q.y; o[2] = t->q.z;
+        o[3] = t->u.x; o[4] = t->u.y; o[5] = t->u.z;
+        o[6] = t->v.x; o[7] = t->v.y; o[8] = t->v.z;
+        if (mats) mats[i] = t->material;
+    }
+}
+int rb_num_tris(const void *sp){ return ((const Scene *)sp)->ntris; }
+int rb_num_prims(const void *sp){ return ((const Scene *)sp)->nprims; }
+
+// triangle_bounds (scene.c:65) of n triangles given as q, u, v (9 floats each): 8 floats per box
+// (lo.xyz, 0, hi.xyz, 0), the GPU builder's input layout
+void rb_triangle_bounds(const float *quv, int n, float *boxes){
+    for (int i = 0; i < n; i++){
+        const float *p = quv + 9 * (size_t)i;
+        Triangle t;
+        memset(&t, 0, sizeof(t));
+        t.q = v3f(p); t.u = v3f(p + 3); t.v = v3f(p + 6);
+        Aabb b = triangle_bounds(&t);
+        float *o = boxes + 8 * (size_t)i;
+        o[0] = b.lo.x; o[1] = b.lo.y; o[2] = b.lo.z; o[3] = 0;
+        o[4] = b.hi.x; o[5] = b.hi.y; o[6] = b.hi.z; o[7] = 0;
+    }
+}
+
+// ---- queries ----------------------------------------------------------------------------------
+// Closest hits of n rays (origins, directions: 3 floats each) in (tmin, tmax): prim = shape id
+// (-1: none), inst, t. OpenMP over the rays.
+void rb_intersect(const void *sp, const float *orig, const float *dir, long long n, float tmin, float tmax,
+                  int *prim, int *inst, float *t){
+    const Scene *s = sp;
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (long long i = 0; i < n; i++){
+        Ray r = {v3f(orig + 3 * i), v3f(dir + 3 * i)};
+        Hit h;
+        if (__real_scene_intersect(s, &r, tmin, tmax, &h)){ prim[i] = h.prim; inst[i] = h.inst; t[i] = (float)h.t; }
+        else { prim[i] = -1; inst[i] = -1; t[i] = -1; }
+    }
+}
+void rb_occluded(const void *sp, const float *orig, const float *dir, long long n, float tmin, float tmax, int *out){
+    const Scene *s = sp;
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (long long i = 0; i < n; i++){
+        Ray r = {v3f(orig + 3 * i), v3f(dir + 3 * i)};
+        out[i] = __real_scene_occluded(s, &r, tmin, tmax);
+    }
+}
+
+// trace_image over rows [y0, y0 + rows) of a w x h image (rows = h: all of it); rgb: rows * w * 3
+// floats (the mean of each pixel's spp samples). cam: from, at, up (9 floats), vfov in degrees.
+void rb_trace_image(const void *sp, const float *cam, float vfov, int w, int h, int y0, int rows, int spp,
+                    unsigned long long seed, int max_depth, int mis, int sampler, float *rgb){
+    const Scene *s = sp;
+    Camera c = camera_make(v3f(cam), v3f(cam + 3), v3f(cam + 6), vfov, (real)w / (real)h);
+    TraceParams tp = trace_default_params();
+    tp.max_depth = max_depth;
+    tp.mis = mis;
+    tp.sampler = sampler;
+    Vec3 *px = malloc(sizeof(Vec3) * (size_t)w * h);
+    if (!px) return;
+    if (rows == h && y0 == 0) trace_image(s, &c, &tp, w, h, spp, seed, 0, px, NULL, NULL);
+    else {
+        // the same pixels as trace_image's (its per-pixel seeding), for a band of rows
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int y = y0; y < y0 + rows; y++)
+            for (int x = 0; x < w; x++){
+                uint64_t pixel = (uint64_t)y * w + x;
+                Rng rng;
+                rng_seed(&rng, 0x853c49e6748fea9bULL ^ (pixel * 0x9E3779B97F4A7C15ULL) ^ (seed * 0xD1B54A32D192ED03ULL), pixel);
+                Vec3 sum = vec3(0, 0, 0);
+                for (int k = 0; k < spp; k++){
+                    Sampler sm = sampler_make(&rng, x, y, (uint32_t)k, (uint32_t)seed * 0x9e3779b9u, tp.sampler);
+                    real jx, jy;
+                    sampler_2d(&sm, SAMPLE_CAMERA, &jx, &jy);
+                    Vec3 col = trace_path_sampled(s, camera_ray(&c, (x + jx) / w, (y + jy) / h), &sm, &tp);
+                    if (!(col.x == col.x && col.y == col.y && col.z == col.z)) continue;
+                    sum = v_add(sum, col);
+                }
+                px[pixel] = v_scale(sum, (real)1 / spp);
+            }
+    }
+    for (int y = y0; y < y0 + rows; y++)
+        for (int x = 0; x < w; x++){
+            const Vec3 *p = &px[(size_t)y * w + x];
+            float *o = rgb + 3 * ((size_t)(y - y0) * w + x);
+            o[0] = (float)p->x; o[1] = (float)p->y; o[2] = (float)p->z;
+        }
+    free(px);
+}
+
+// the blue-noise mask (sampler.c): 64 x 64 ranks
+void rb_blue_noise(uint16_t *out){ memcpy(out, blue_noise_mask(), sizeof(uint16_t) * BLUE_NOISE_SIZE * BLUE_NOISE_SIZE); }
+uint32_t rb_sampler_owen(uint32_t x, uint32_t seed){ return sampler_owen(x, seed); }
+uint32_t rb_sampler_sobol1(uint32_t i){ return sampler_sobol1(i); }
+uint32_t rb_sampler_hash(uint32_t x){ return sampler_hash(x); }
