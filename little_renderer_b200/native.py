@@ -235,8 +235,9 @@ class Scene:
         self.ctx.check(self.ctx.L.lrc_scene_intersect(self.h, C.c_void_p(d_orig), C.c_void_p(d_dir), n, tmin, tmax,
                                                       C.c_void_p(d_prim), C.c_void_p(d_t), LRC_DEVICE))
 
-    def trace_stats(self, orig, dirs, tmin=0.0, tmax=1e30):
-        """(box tests, triangle tests) of the closest-hit walk over these rays (device or host arrays)."""
+    def trace_stats(self, orig, dirs=None, tmin=0.0, tmax=1e30):
+        """(box tests, triangle tests) of the closest-hit walk over these rays: host arrays
+        (orig, dirs), or device rays as orig = (count, origins pointer, directions pointer)."""
         stats = np.zeros(2, np.uint64)
         if isinstance(orig, np.ndarray):
             orig = np.ascontiguousarray(orig, np.float32)
