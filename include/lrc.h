@@ -89,6 +89,24 @@ int lrc_build(lrc_ctx *ctx, const lrc_build_params *p, const float *boxes, uint3
 /* The device scratch memory lrc_build uses for n items (it is the context's, grown as needed). */
 size_t lrc_build_scratch_bytes(uint32_t n, int key_bits, int builder);
 
+/* A build that allocates nothing. It has no counterpart in the reference.
+ * Some callers cannot call cudaMalloc: a host program that gives out all its device memory up
+ * front from its own pool cannot let a library allocate behind its back (the allocation may fail
+ * against that budget), and a frame loop that rebuilds a top-level tree every frame cannot afford
+ * cudaMalloc's implicit device synchronisation. This is lrc_build with LRC_DEVICE (every array a
+ * device pointer of the current device), the same trees bit for bit, its scratch memory in one
+ * fixed device array of LRC_STATIC_SCRATCH_BYTES that every GPU loading the library holds until
+ * the process exits; it calls no allocating routine. n above LRC_STATIC_MAX_ITEMS: LRC_E_TOO_BIG,
+ * nothing done. The first call on a device sets it up (finds the array's device address, sets the
+ * kernels' attributes): make that first call before any stream capture. Every call shares the
+ * array: calls that overlap on the GPU (other streams, other host threads) race and must not be
+ * made. The work goes to cuda_stream (a cudaStream_t; NULL: the default stream) and the call
+ * waits for it, returning LRC_OK, LRC_E_TIMEOUT (a bounded device wait ran out) or LRC_E_CUDA. */
+#define LRC_E_TOO_BIG (-6)
+#define LRC_STATIC_MAX_ITEMS 65536
+#define LRC_STATIC_SCRATCH_BYTES (6u << 20)
+int lrc_build_static(const lrc_build_params *p, const float *boxes, uint32_t *nodes, uint32_t *aux, void *cuda_stream);
+
 /* triangle_bounds (engine/scene/scene.c:65-74) of n triangles in the reference's GPU layout
  * (12 words each: q.xyz, n0, u.xyz, n1, v.xyz, material << 26 | n2; put_tris, trace_gpu.c:898-911)
  * into boxes (8 floats each), and the mesh box of their corners (SceneMesh.box, scene.c:638-646)

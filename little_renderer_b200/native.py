@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -75,6 +75,7 @@ def lib():
     L.lrc_build_scratch_bytes.argtypes = [u32, C.c_int, C.c_int]
     L.lrc_build_scratch_bytes.restype = C.c_size_t
     L.lrc_triangle_boxes.argtypes = [vp, vp, u32, vp, vp, C.c_uint]
+    L.lrc_build_static.argtypes = [vp, vp, vp, vp, vp]
     L.lrc_scene_create.argtypes = [vp, C.POINTER(vp)]
     L.lrc_scene_destroy.argtypes = [vp]
     L.lrc_scene_set_triangles.argtypes = [vp, vp, u32, C.c_uint]
