@@ -32,6 +32,7 @@ extern "C" {
 #define LRC_E_NODEVICE (-5)    /* no CUDA device (the caller then path traces on the CPU, gpu.h:32-35) */
 
 #define LRC_DEVICE 1u          /* flag: array arguments are device pointers */
+#define LRC_SORT_RAYS 2u       /* flag (ray queries): reorder a large batch by a coherence key first */
 
 typedef struct lrc_ctx lrc_ctx;
 
@@ -143,6 +144,51 @@ int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const 
  * and depth, trace_gpu.c:768-805, describe a tree). stats: host. */
 int lrc_scene_trace_stats(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
                           uint64_t *stats, unsigned flags);
+
+/* ---- the world besides its triangles: replaces upload_world / upload_layout's primitives,
+ * normals and the parameters' materials (trace_gpu.c:1098-1171, 1597-1678) ------------------ */
+/* Spheres and quads, 24 floats each as upload_world packs them (trace_gpu.c:1145-1154):
+ * center.xyz, radius | q.xyz, 1 for a quad (0 a sphere) | u.xyz, material | v.xyz, area |
+ * normal.xyz, plane_d | w.xyz, 0. With primitives the world's shapes are numbered as the
+ * reference numbers them (scene.h:101-106): primitives, then triangles; lrc_scene_build builds
+ * over both and lrc_scene_intersect returns shape ids. */
+int lrc_scene_set_prims(lrc_scene *s, const float *prims, uint32_t n, unsigned flags);
+/* vertex normals (3 floats each) that triangles' normal indices (put_tris words 3, 7, 11) refer to */
+int lrc_scene_set_normals(lrc_scene *s, const float *normals, uint32_t n, unsigned flags);
+/* Materials (engine/scene/scene.h:31-51), 16 floats each: albedo.xyz, type (MatType, as the int's
+ * bits) | emission.xyz, 0 | ior, metallic, roughness, transmission | 0, 0, 0, 0. At most 64. Host. */
+int lrc_scene_set_materials(lrc_scene *s, const float *mats, uint32_t n);
+/* Scene.light: the lamp, a quad primitive sampled by next event estimation (-1: none) */
+int lrc_scene_set_light(lrc_scene *s, int32_t prim);
+/* The blue-noise mask (64 x 64 ranks; blue_noise_mask(), engine/base/sampler.c) and the BSDF tables
+ * (2112 floats packed as gpu_bsdf_tables packs scene/brdf_tables.h, engine/gpu/brdf_gpu.c:20-25),
+ * both host. NULL: the ones lrc_default_blue_noise / lrc_default_bsdf_tables make. */
+int lrc_scene_set_tables(lrc_scene *s, const uint16_t *blue_noise, const float *bsdf_tables);
+/* the mask and the tables made here by the reference's published methods (void-and-cluster;
+ * the GGX albedo integrals): the same mask as the reference's, the tables within 1e-6 */
+void lrc_default_blue_noise(uint16_t *out4096);
+void lrc_default_bsdf_tables(float *out2112);
+
+/* ---- the path tracer: replaces gpu_trace_encode + the megakernel `main` / `trace()`
+ * (trace_gpu.c:1935-2031; trace.wgsl:1125-1316); the CPU counterpart is trace_image /
+ * trace_path_sampled (engine/rt/tracer.c:329-545) -------------------------------------------- */
+typedef struct {
+    float origin[3], upper_left[3], horizontal[3], vertical[3];   /* Camera (engine/scene/camera.h:15-20) */
+    int32_t width, height;
+    int32_t max_depth;     /* bounces per path */
+    int32_t mis;           /* next event estimation weighted by the power heuristic */
+    int32_t sampler;       /* 1: Owen-scrambled Sobol + blue noise; 0: plain random (GpuTraceParams.random) */
+    int32_t exact;         /* 1: trace_image's random streams (per pixel, samples in order): the CPU's image
+                              up to transcendental rounding; 0: a stream per sample (faster) */
+    uint64_t seed;         /* the image's seed (trace_image's) */
+    float clamp;           /* largest sample value, 0: none */
+} lrc_trace_params;
+/* Samples [spp0, spp0 + spp) of every pixel of rows [y0, y0 + rows), added into accum (width x
+ * height x 4 floats: the sum of the samples' linear RGB and their count, as gpu_view_trace_read
+ * gives them, view_gpu.h:118-124). exact = 1 needs spp0 = 0 (the streams start at each pixel's
+ * first sample). rays (optional, host): the closest-hit and shadow rays traced. */
+int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0, uint32_t spp,
+              float *accum, uint64_t *rays, unsigned flags);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <string>
 #include <new>
+#include <vector>
 
 using lrc::Node;
 
@@ -39,6 +40,20 @@ struct lrc_scene {
     float *d_boxes = nullptr;
     size_t boxes_cap = 0;
     uint32_t *d_small = nullptr;  // 6 bound keys, 6 bounds, 6 lo/ext
+    // the world besides its triangles (path tracing)
+    float *d_prims = nullptr;     // 24 floats per primitive
+    size_t prims_cap = 0;
+    uint32_t nprims = 0;
+    float *d_normals = nullptr;
+    size_t normals_cap = 0;
+    uint32_t nnormals = 0;
+    float *d_mats = nullptr;      // 64 materials x 16 floats
+    uint32_t nmats = 0;
+    int32_t light = -1;
+    uint16_t *d_mask = nullptr;   // 4096 ranks, then the 2112 table floats
+    float *d_tab = nullptr;
+    bool tables = false;
+    unsigned long long *d_rays = nullptr;
 };
 
 namespace {
@@ -106,6 +121,30 @@ int check_status(lrc_ctx *c) {
 }
 
 size_t al(size_t x) { return (x + 255) / 256 * 256; }
+
+// the BSDF tables' floats (E 32 x 32, B 32 x 32, E_avg 32, B_avg 32)
+constexpr int kBsdfTableFloats = 2112;
+
+// the path tracer's view of a scene
+lrc::PtScene pt_scene(const lrc_scene *s) {
+    lrc::PtScene S{};
+    S.nodes = reinterpret_cast<const float4 *>(s->d_nodes);
+    S.aux = s->d_aux;
+    S.root = 0;
+    S.nnodes = s->built_n ? 2 * s->built_n - 1 : 0;
+    S.naux = s->built_n;
+    S.prims = reinterpret_cast<const float4 *>(s->d_prims);
+    S.nprims = s->nprims;
+    S.tris = reinterpret_cast<const float4 *>(s->d_tris);
+    S.ntris = s->ntris;
+    S.normals = s->nnormals ? s->d_normals : nullptr;
+    S.mats = reinterpret_cast<const float4 *>(s->d_mats);
+    S.nmats = s->nmats;
+    S.light = s->light;
+    S.mask = s->d_mask;
+    S.tab = s->d_tab;
+    return S;
+}
 
 // the walk's view of a scene: its tree (root 0), leaves' triangles, and the sizes it checks against
 lrc::TraceTables tables(const lrc_scene *s) {
@@ -307,6 +346,11 @@ void lrc_scene_destroy(lrc_scene *s) {
     cudaFree(s->d_aux);
     cudaFree(s->d_boxes);
     cudaFree(s->d_small);
+    cudaFree(s->d_prims);
+    cudaFree(s->d_normals);
+    cudaFree(s->d_mats);
+    cudaFree(s->d_mask);
+    cudaFree(s->d_rays);
     delete s;
 }
 
@@ -329,9 +373,10 @@ int lrc_scene_build(lrc_scene *s, int builder, int key_bits) {
     if (!s) return LRC_E_INVALID;
     lrc_ctx *c = s->ctx;
     if (key_bits != 30 && key_bits != 63) return fail(c, LRC_E_INVALID, "key_bits must be 30 or 63");
-    if (s->ntris >= (1u << 30)) return fail(c, LRC_E_INVALID, "more than 2^30 - 1 triangles");
+    if ((uint64_t)s->ntris + s->nprims >= (1u << 30)) return fail(c, LRC_E_INVALID, "more than 2^30 - 1 shapes");
     DeviceGuard g(c->device);
-    const uint32_t n = s->ntris;
+    // the shapes: primitives, then triangles (their ids as the reference's, scene.h:101-106)
+    const uint32_t n = s->ntris + s->nprims;
     s->built_n = 0;
     if (!n) return LRC_OK;
     cudaError_t e = reserve(reinterpret_cast<void **>(&s->d_boxes), &s->boxes_cap, (size_t)n * 32);
@@ -350,7 +395,13 @@ int lrc_scene_build(lrc_scene *s, int builder, int key_bits) {
     uint32_t *keys = s->d_small;
     float *bounds = reinterpret_cast<float *>(s->d_small + 8), *lo_ext = reinterpret_cast<float *>(s->d_small + 16);
     c->timer.begin(LRC_TS_BOXES, c->st);
-    e = lrc::triangle_boxes(s->d_tris, n, s->d_boxes, keys, c->st, c->num_sms);
+    float *tri_boxes = s->d_boxes + 8 * (size_t)s->nprims;
+    e = lrc::triangle_boxes(s->d_tris, s->ntris, tri_boxes, keys, c->st, c->num_sms);
+    if (!e && s->nprims) {
+        // a world with primitives: their boxes (primitive_bounds) first, the bounds over all shapes' boxes
+        e = lrc::pt_prim_boxes(s->d_prims, s->nprims, s->d_boxes, c->st);
+        if (!e) e = lrc::boxes_bounds(s->d_boxes, n, keys, c->st, c->num_sms, true);
+    }
     if (!e) e = lrc::bounds_params(keys, bounds, lo_ext, c->st);
     lrc_build_params p{};
     p.n = n;
@@ -391,9 +442,21 @@ int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint6
     if (!s->built_n) return fail(c, LRC_E_INVALID, "the scene has no built BVH (lrc_scene_build)");
     DeviceGuard g(c->device);
     lrc::TraceTables tt = tables(s);
+    // LRC_SORT_RAYS: the reordering's scratch (large batches); without it the rays go in their order
+    void *sort_scratch = nullptr;
+    if ((flags & LRC_SORT_RAYS) && lrc::intersect_scratch_bytes(nrays)) {
+        if (reserve(&c->scratch, &c->scratch_cap, lrc::intersect_scratch_bytes(nrays)) == cudaSuccess) sort_scratch = c->scratch;
+        else cudaGetLastError();
+    }
+    // a world with primitives walks shape ids (primitives, then triangles); a mesh, triangles alone
+    auto run = [&](const float *o, const float *d, int32_t *p, float *tt_out) {
+        if (s->nprims) return lrc::pt_intersect(pt_scene(s), o, d, nrays, tmin, tmax, p, tt_out, c->d_status, c->st);
+        return lrc::intersect_device(tt, o, d, nrays, tmin, tmax, p, tt_out, c->d_status, c->st, c->num_sms, sort_scratch,
+                                     c->scratch_cap);
+    };
     if (flags & LRC_DEVICE) {
         c->timer.begin(LRC_TS_TRACE, c->st);
-        cudaError_t e = lrc::intersect_device(tt, orig, dir, nrays, tmin, tmax, prim, t, c->d_status, c->st, c->num_sms);
+        cudaError_t e = run(orig, dir, prim, t);
         c->timer.end(c->st);
         return cuda_status(c, e, "lrc_scene_intersect");
     }
@@ -407,7 +470,7 @@ int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint6
     e = cudaMemcpyAsync(d_o, orig, nrays * 12, cudaMemcpyHostToDevice, c->st);
     if (!e) e = cudaMemcpyAsync(d_d, dir, nrays * 12, cudaMemcpyHostToDevice, c->st);
     c->timer.begin(LRC_TS_TRACE, c->st);
-    if (!e) e = lrc::intersect_device(tt, d_o, d_d, nrays, tmin, tmax, d_p, d_t, c->d_status, c->st, c->num_sms);
+    if (!e) e = run(d_o, d_d, d_p, d_t);
     c->timer.end(c->st);
     if (!e) e = cudaMemcpyAsync(prim, d_p, nrays * 4, cudaMemcpyDeviceToHost, c->st);
     if (!e) e = cudaMemcpyAsync(t, d_t, nrays * 4, cudaMemcpyDeviceToHost, c->st);
@@ -466,6 +529,123 @@ int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const 
     if (!e) e = cudaMemcpyAsync(out, d_out, nrays, cudaMemcpyDeviceToHost, c->st);
     if (e) return cuda_status(c, e, "lrc_scene_occluded");
     return check_status(c);
+}
+
+// ---- the world besides its triangles, and the path tracer ---------------------------------------
+int lrc_scene_set_prims(lrc_scene *s, const float *prims, uint32_t n, unsigned flags) {
+    if (!s || (n && !prims)) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    DeviceGuard g(c->device);
+    cudaError_t e = reserve(reinterpret_cast<void **>(&s->d_prims), &s->prims_cap, (size_t)(n ? n : 1) * 96);
+    if (!e && n)
+        e = cudaMemcpyAsync(s->d_prims, prims, (size_t)n * 96, (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            c->st);
+    if (e) return cuda_status(c, e, "primitives");
+    s->nprims = n;
+    s->built_n = 0;
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_scene_set_normals(lrc_scene *s, const float *normals, uint32_t n, unsigned flags) {
+    if (!s || (n && !normals)) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    DeviceGuard g(c->device);
+    cudaError_t e = reserve(reinterpret_cast<void **>(&s->d_normals), &s->normals_cap, (size_t)(n ? n : 1) * 12);
+    if (!e && n)
+        e = cudaMemcpyAsync(s->d_normals, normals, (size_t)n * 12,
+                            (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->st);
+    if (e) return cuda_status(c, e, "normals");
+    s->nnormals = n;
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_scene_set_materials(lrc_scene *s, const float *mats, uint32_t n) {
+    if (!s || n > 64 || (n && !mats)) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaSuccess;
+    if (!s->d_mats) e = cudaMalloc(&s->d_mats, 64 * 64);
+    if (!e && n) e = cudaMemcpyAsync(s->d_mats, mats, (size_t)n * 64, cudaMemcpyHostToDevice, c->st);
+    if (e) return cuda_status(c, e, "materials");
+    s->nmats = n;
+    return check_status(c);
+}
+
+int lrc_scene_set_light(lrc_scene *s, int32_t prim) {
+    if (!s) return LRC_E_INVALID;
+    s->light = prim;
+    return LRC_OK;
+}
+
+int lrc_scene_set_tables(lrc_scene *s, const uint16_t *blue_noise, const float *bsdf_tables) {
+    if (!s) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    DeviceGuard g(c->device);
+    std::vector<uint16_t> mask(4096);
+    std::vector<float> tab(kBsdfTableFloats);
+    if (blue_noise) std::memcpy(mask.data(), blue_noise, 4096 * 2);
+    else lrc::default_blue_noise(mask.data());
+    if (bsdf_tables) std::memcpy(tab.data(), bsdf_tables, tab.size() * 4);
+    else lrc::default_bsdf_tables(tab.data());
+    cudaError_t e = cudaSuccess;
+    if (!s->d_mask) e = cudaMalloc(&s->d_mask, 4096 * 2 + kBsdfTableFloats * 4 + 256);
+    if (e) return cuda_status(c, e, "tables");
+    s->d_tab = reinterpret_cast<float *>(s->d_mask + 4096);
+    e = cudaMemcpyAsync(s->d_mask, mask.data(), 4096 * 2, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = cudaMemcpyAsync(s->d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, c->st);
+    if (e) return cuda_status(c, e, "tables");
+    s->tables = true;
+    return check_status(c);
+}
+
+int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0, uint32_t spp, float *accum,
+              uint64_t *rays, unsigned flags) {
+    if (!s || !p || !accum || p->width <= 0 || p->height <= 0 || y0 < 0 || rows < 0 || y0 + rows > p->height)
+        return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (!s->built_n) return fail(c, LRC_E_INVALID, "the scene has no built BVH (lrc_scene_build)");
+    if (p->exact && spp0 != 0) return fail(c, LRC_E_INVALID, "exact mode starts at each pixel's first sample (spp0 = 0)");
+    if (!s->d_mats || !s->nmats) return fail(c, LRC_E_INVALID, "the scene has no materials (lrc_scene_set_materials)");
+    if (s->light >= (int32_t)s->nprims) return fail(c, LRC_E_INVALID, "the light is not one of the primitives");
+    DeviceGuard g(c->device);
+    if (!s->tables) {
+        int rc = lrc_scene_set_tables(s, nullptr, nullptr);
+        if (rc) return rc;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!s->d_rays) e = cudaMalloc(&s->d_rays, 256);
+    if (!e) e = cudaMemsetAsync(s->d_rays, 0, 8, c->st);
+    if (e) return cuda_status(c, e, "ray counter");
+    lrc::PtParams P{};
+    P.W = p->width; P.H = p->height; P.y0 = y0; P.rows = rows; P.spp0 = (int)spp0; P.spp = (int)spp;
+    P.max_depth = p->max_depth; P.mis = p->mis; P.sampler_on = p->sampler; P.exact = p->exact;
+    int gsz = 1;
+    while (gsz * 2 <= (int)spp && gsz < 16) gsz *= 2;
+    P.group = gsz;
+    P.seed = p->seed;
+    P.clamp = p->clamp;
+    P.origin = {p->origin[0], p->origin[1], p->origin[2]};
+    P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
+    P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
+    P.vertical = {p->vertical[0], p->vertical[1], p->vertical[2]};
+    const size_t bytes = (size_t)p->width * p->height * 16;
+    float *d_acc = accum;
+    if (!(flags & LRC_DEVICE)) {
+        e = reserve(&c->stage, &c->stage_cap, bytes);
+        if (e) return cuda_status(c, e, "image staging");
+        d_acc = static_cast<float *>(c->stage);
+        e = cudaMemcpyAsync(d_acc, accum, bytes, cudaMemcpyHostToDevice, c->st);
+    }
+    c->timer.begin(LRC_TS_SHADE, c->st);
+    if (!e) e = lrc::pt_trace(pt_scene(s), P, d_acc, s->d_rays, c->d_status, c->st);
+    c->timer.end(c->st);
+    if (!e && !(flags & LRC_DEVICE)) e = cudaMemcpyAsync(accum, d_acc, bytes, cudaMemcpyDeviceToHost, c->st);
+    unsigned long long nr = 0;
+    if (!e && rays) e = cudaMemcpyAsync(&nr, s->d_rays, 8, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_trace");
+    int rc = (flags & LRC_DEVICE) && !rays ? LRC_OK : check_status(c);
+    if (rays) *rays = nr;
+    return rc;
 }
 
 }  // extern "C"

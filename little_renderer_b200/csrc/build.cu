@@ -656,10 +656,68 @@ static DevCache &dev_cache() {
     return g_dev_cache[d & 63];
 }
 
+// Every pass of a stable LSD radix sort of n keys (values: the keys' positions to start with), the
+// passes' 256-bin histograms already in hist[pass][256], look-back status words zeroed. On return
+// kin / vin hold the sorted keys and the permutation (the buffers swap roles pass by pass).
+template <typename K>
+static void onesweep_passes(K *&kin, K *&kout, uint32_t *&vin, uint32_t *&vout, uint32_t n, const uint32_t *hist,
+                            uint32_t *status, uint32_t *counters, uint32_t tiles, uint32_t *d_status, cudaStream_t st) {
+    constexpr int P = KeyTraits<K>::PASSES;
+    const size_t smem = sizeof(OsShared<K>);
+    DevCache &dc = dev_cache();
+    if (!dc.os_attr[sizeof(K) == 8]) {
+        cudaFuncSetAttribute(onesweep_kernel<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(onesweep_kernel<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dc.os_attr[sizeof(K) == 8] = true;
+    }
+    for (int pass = 0; pass < P; pass++) {
+        uint32_t *stp = status + (size_t)pass * tiles * 256;
+        if (pass == 0)
+            onesweep_kernel<K, true><<<tiles, OS_THREADS, smem, st>>>(kin, nullptr, kout, vout, n, 8 * pass, hist + pass * 256,
+                                                                      stp, counters + pass, d_status);
+        else
+            onesweep_kernel<K, false><<<tiles, OS_THREADS, smem, st>>>(kin, vin, kout, vout, n, 8 * pass, hist + pass * 256,
+                                                                       stp, counters + pass, d_status);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+}
+
 struct BuildLayout {
     size_t codes_a, codes_b, vals_a, vals_b, hist, status, counters, other, list_a, list_b, stat0, stat1, pstate, total;
     uint32_t tiles;
 };
+static BuildLayout layout_for(uint32_t n, int key_bits, int builder);
+
+// ---- a sort of 32-bit keys for other users (the ray reordering) ----------------------------
+size_t sort_u32_scratch_bytes(uint64_t n) { return layout_for((uint32_t)n, 30, 0).total; }
+
+SortU32 sort_u32_carve(void *scratch, uint64_t n) {
+    BuildLayout L = layout_for((uint32_t)n, 30, 0);
+    char *s = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(scratch) + 255) / 256 * 256);
+    SortU32 r;
+    r.keys = reinterpret_cast<uint32_t *>(s + L.codes_a);
+    r.hist = reinterpret_cast<uint32_t *>(s + L.hist);
+    r.base = s;
+    r.n = (uint32_t)n;
+    return r;
+}
+
+cudaError_t sort_u32_clear(const SortU32 &S, cudaStream_t st) {
+    BuildLayout L = layout_for(S.n, 30, 0);
+    return cudaMemsetAsync(S.base + L.hist, 0, L.counters + 4 * 4 - L.hist, st);
+}
+
+cudaError_t sort_u32_run(const SortU32 &S, uint32_t *d_status, cudaStream_t st, const uint32_t **perm_out) {
+    BuildLayout L = layout_for(S.n, 30, 0);
+    uint32_t *ka = reinterpret_cast<uint32_t *>(S.base + L.codes_a), *kb = reinterpret_cast<uint32_t *>(S.base + L.codes_b);
+    uint32_t *va = reinterpret_cast<uint32_t *>(S.base + L.vals_a), *vb = reinterpret_cast<uint32_t *>(S.base + L.vals_b);
+    onesweep_passes<uint32_t>(ka, kb, va, vb, S.n, reinterpret_cast<uint32_t *>(S.base + L.hist),
+                              reinterpret_cast<uint32_t *>(S.base + L.status), reinterpret_cast<uint32_t *>(S.base + L.counters),
+                              L.tiles, d_status, st);
+    *perm_out = va;
+    return cudaGetLastError();
+}
 
 static BuildLayout layout_for(uint32_t n, int key_bits, int builder) {
     BuildLayout L{};
@@ -716,27 +774,10 @@ static cudaError_t build_typed(const lrc_build_params &p, const float *d_boxes, 
         morton_hist_kernel<K><<<std::max(grid, 1), MH_THREADS, 0, st>>>(
             boxes, n, make_float3(p.lo[0], p.lo[1], p.lo[2]), make_float3(p.ext[0], p.ext[1], p.ext[2]), dlo_ext, ca, hist);
     }
-    const size_t smem = sizeof(OsShared<K>);
-    DevCache &dc = dev_cache();
-    if (!dc.os_attr[sizeof(K) == 8]) {
-        cudaFuncSetAttribute(onesweep_kernel<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(onesweep_kernel<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dc.os_attr[sizeof(K) == 8] = true;
-    }
     if (tm) tm->begin(LRC_TS_SORT, st);
     K *kin = ca, *kout = cb;
     uint32_t *vin = va, *vout = vb;
-    for (int pass = 0; pass < P; pass++) {
-        uint32_t *stp = status + (size_t)pass * L.tiles * 256;
-        if (pass == 0)
-            onesweep_kernel<K, true><<<L.tiles, OS_THREADS, smem, st>>>(kin, nullptr, kout, vout, n, 8 * pass, hist + pass * 256,
-                                                                        stp, counters + pass, d_status);
-        else
-            onesweep_kernel<K, false><<<L.tiles, OS_THREADS, smem, st>>>(kin, vin, kout, vout, n, 8 * pass, hist + pass * 256,
-                                                                         stp, counters + pass, d_status);
-        std::swap(kin, kout);
-        std::swap(vin, vout);
-    }
+    onesweep_passes<K>(kin, kout, vin, vout, n, hist, status, counters, L.tiles, d_status, st);
     // sorted: codes in kin, items in vin
     if (d_sorted_codes_out)
         cudaMemcpyAsync(d_sorted_codes_out, kin, (size_t)n * sizeof(K), cudaMemcpyDeviceToDevice, st);
@@ -756,7 +797,7 @@ static cudaError_t build_typed(const lrc_build_params &p, const float *d_boxes, 
     e = cudaMemsetAsync(scratch + L.stat0, 0, L.pstate + sizeof(PlocState) - L.stat0, st);
     if (e) return e;
     const int psmem = (int)sizeof(PlocShared);
-    int &per_sm = dc.ploc_per_sm;
+    int &per_sm = dev_cache().ploc_per_sm;
     if (per_sm <= 0) {
         cudaFuncSetAttribute(ploc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ploc_kernel, PL_THREADS, psmem);
@@ -805,6 +846,33 @@ cudaError_t triangle_boxes(const uint32_t *d_tris, uint32_t n, float *d_boxes, u
         int grid = (int)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)num_sms * 8);
         tri_boxes_kernel<<<grid, 256, 0, st>>>(reinterpret_cast<const float4 *>(d_tris), n,
                                                reinterpret_cast<float4 *>(d_boxes), d_bkeys);
+    }
+    return cudaGetLastError();
+}
+
+// the union of n boxes (their padded corners) into the bound keys
+__global__ void __launch_bounds__(256) boxes_bounds_kernel(const float4 *__restrict__ boxes, uint32_t n, uint32_t *bkeys) {
+    uint32_t a[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, b[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 lo = __ldg(&boxes[2 * (size_t)i]), hi = __ldg(&boxes[2 * (size_t)i + 1]);
+        a[0] = min(a[0], fkey(lo.x)); a[1] = min(a[1], fkey(lo.y)); a[2] = min(a[2], fkey(lo.z));
+        b[0] = max(b[0], fkey(hi.x)); b[1] = max(b[1], fkey(hi.y)); b[2] = max(b[2], fkey(hi.z));
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            a[k] = min(a[k], __shfl_xor_sync(0xffffffffu, a[k], o));
+            b[k] = max(b[k], __shfl_xor_sync(0xffffffffu, b[k], o));
+        }
+        if ((threadIdx.x & 31) == 0) { atomicMin(&bkeys[k], a[k]); atomicMax(&bkeys[3 + k], b[k]); }
+    }
+}
+
+cudaError_t boxes_bounds(const float *d_boxes, uint32_t n, uint32_t *d_bkeys, cudaStream_t st, int num_sms, bool init) {
+    if (init) bkeys_init_kernel<<<1, 32, 0, st>>>(d_bkeys);
+    if (n) {
+        int grid = (int)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)num_sms * 8);
+        boxes_bounds_kernel<<<grid, 256, 0, st>>>(reinterpret_cast<const float4 *>(d_boxes), n, d_bkeys);
     }
     return cudaGetLastError();
 }

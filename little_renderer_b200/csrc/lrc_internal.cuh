@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cuda_runtime.h>
 #include "../../include/lrc.h"
+#include "pt_math.cuh"
 
 namespace lrc {
 
@@ -112,6 +113,20 @@ cudaError_t triangle_boxes(const uint32_t *d_tris, uint32_t n, float *d_boxes, u
                            int num_sms);
 cudaError_t bounds_params(const uint32_t *d_bkeys, float *d_bounds6, float *d_lo_ext, cudaStream_t st);
 
+// a stable radix sort of 32-bit keys (4 passes of 8 bits) for other kernels' use: carve the
+// scratch, clear the histograms, let a key kernel write S.keys[0..n) and add each key's 4 digits
+// into S.hist[pass][256], then run: the permutation (sorted position -> original index) comes out
+struct SortU32 {
+    uint32_t *keys;
+    uint32_t *hist;
+    char *base;
+    uint32_t n;
+};
+size_t sort_u32_scratch_bytes(uint64_t n);
+SortU32 sort_u32_carve(void *scratch, uint64_t n);
+cudaError_t sort_u32_clear(const SortU32 &S, cudaStream_t st);
+cudaError_t sort_u32_run(const SortU32 &S, uint32_t *d_status, cudaStream_t st, const uint32_t **perm_out);
+
 // traversal internals (traverse.cu)
 struct TraceTables {
     const Node *nodes;
@@ -120,12 +135,49 @@ struct TraceTables {
     uint32_t root;           // absolute node index of the root
     uint32_t nnodes, naux, ntris;   // sizes: an index out of them is reported (ST_BAD_TREE), not followed
 };
+// closest hits; batches of 2^18 rays and more are reordered first when scratch (at least
+// intersect_scratch_bytes) is given
+size_t intersect_scratch_bytes(uint64_t nrays);
 cudaError_t intersect_device(const TraceTables &tt, const float *d_orig, const float *d_dir, uint64_t nrays,
                              float tmin, float tmax, int32_t *d_prim, float *d_t, uint32_t *d_status,
-                             cudaStream_t st, int num_sms);
+                             cudaStream_t st, int num_sms, void *scratch, size_t scratch_bytes);
 cudaError_t count_device(const TraceTables &tt, const float *d_orig, const float *d_dir, uint64_t nrays, float tmin,
                          float tmax, unsigned long long *d_stats, uint32_t *d_status, cudaStream_t st);
 cudaError_t occluded_device(const TraceTables &tt, const float *d_orig, const float *d_dir, const float *d_tmax,
                             uint64_t nrays, float tmin, uint8_t *d_out, uint32_t *d_status, cudaStream_t st);
+
+// the path tracer's view of a scene (pathtrace.cu)
+struct PtScene {
+    const float4 *nodes;        // the world's BVH (shape ids in aux: primitives, then triangles)
+    const uint32_t *aux;
+    uint32_t root, nnodes, naux;
+    const float4 *prims;        // 6 float4 per primitive (upload_world's layout)
+    uint32_t nprims;
+    const float4 *tris;         // 3 float4 per triangle
+    uint32_t ntris;
+    const float *normals;       // vertex normals (3 floats each), or null
+    const float4 *mats;         // 4 float4 per material
+    uint32_t nmats;
+    int32_t light;              // Scene.light: a quad primitive, or -1
+    const uint16_t *mask;       // 64 x 64 blue-noise ranks
+    const float *tab;           // the BSDF's 2112 table floats
+};
+struct PtParams {
+    int W, H, y0, rows, spp0, spp, max_depth, mis, sampler_on, exact, group;
+    uint64_t seed;
+    float clamp;
+    pt::V3 origin, upper_left, horizontal, vertical;   // the Camera (camera.h)
+};
+cudaError_t pt_prim_boxes(const float *d_prims, uint32_t n, float *d_boxes, cudaStream_t st);
+cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsigned long long *d_rays, uint32_t *d_status,
+                     cudaStream_t st);
+cudaError_t pt_intersect(const PtScene &S, const float *d_orig, const float *d_dir, uint64_t n, float tmin, float tmax,
+                         int32_t *d_prim, float *d_t, uint32_t *d_status, cudaStream_t st);
+// min / max over n boxes (8 floats each) into the bound keys (6 words; as triangle_boxes's)
+cudaError_t boxes_bounds(const float *d_boxes, uint32_t n, uint32_t *d_bkeys, cudaStream_t st, int num_sms, bool init);
+
+// the defaults of what the caller may give (host_tables.cu)
+void default_blue_noise(uint16_t *out);
+void default_bsdf_tables(float *out);
 
 }  // namespace lrc

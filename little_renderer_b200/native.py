@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -85,6 +85,14 @@ def lib():
     L.lrc_scene_intersect.argtypes = [vp, vp, vp, u64, f32, f32, vp, vp, C.c_uint]
     L.lrc_scene_occluded.argtypes = [vp, vp, vp, vp, u64, f32, vp, C.c_uint]
     L.lrc_scene_trace_stats.argtypes = [vp, vp, vp, u64, f32, f32, vp, C.c_uint]
+    L.lrc_scene_set_prims.argtypes = [vp, vp, u32, C.c_uint]
+    L.lrc_scene_set_normals.argtypes = [vp, vp, u32, C.c_uint]
+    L.lrc_scene_set_materials.argtypes = [vp, vp, u32]
+    L.lrc_scene_set_light.argtypes = [vp, C.c_int32]
+    L.lrc_scene_set_tables.argtypes = [vp, vp, vp]
+    L.lrc_default_blue_noise.argtypes = [vp]
+    L.lrc_default_bsdf_tables.argtypes = [vp]
+    L.lrc_trace.argtypes = [vp, vp, C.c_int32, C.c_int32, u32, u32, vp, vp, C.c_uint]
     L.lrc_set_timing.argtypes = [vp, C.c_int]
     L.lrc_timings.argtypes = [vp, vp, vp]
     _lib = L
@@ -95,6 +103,24 @@ class BuildParams(C.Structure):
     """lrc_build_params (build_queue's BuildParams, engine/gpu/trace_gpu.c:546)."""
     _fields_ = [("n", C.c_uint32), ("node0", C.c_uint32), ("ref0", C.c_uint32), ("ref_add", C.c_uint32),
                 ("lo", C.c_float * 3), ("ext", C.c_float * 3), ("key_bits", C.c_int32), ("builder", C.c_int32)]
+
+
+class TraceParams(C.Structure):
+    """lrc_trace_params (the Camera of engine/scene/camera.h and GpuTraceParams' numbers)."""
+    _fields_ = [("origin", C.c_float * 3), ("upper_left", C.c_float * 3), ("horizontal", C.c_float * 3),
+                ("vertical", C.c_float * 3), ("width", C.c_int32), ("height", C.c_int32), ("max_depth", C.c_int32),
+                ("mis", C.c_int32), ("sampler", C.c_int32), ("exact", C.c_int32), ("seed", C.c_uint64),
+                ("clamp", C.c_float)]
+
+
+def trace_params(cam12, width, height, max_depth=8, mis=1, sampler=1, exact=0, seed=0, clamp=0.0):
+    p = TraceParams()
+    cam12 = np.asarray(cam12, np.float32).reshape(4, 3)
+    for i, name in enumerate(("origin", "upper_left", "horizontal", "vertical")):
+        getattr(p, name)[:] = cam12[i].tolist()
+    p.width, p.height, p.max_depth, p.mis, p.sampler, p.exact, p.seed, p.clamp = (
+        width, height, max_depth, mis, sampler, exact, seed, clamp)
+    return p
 
 
 def _ptr(a):
@@ -235,6 +261,42 @@ class Scene:
     def intersect_device(self, d_orig, d_dir, n, d_prim, d_t, tmin=0.0, tmax=1e30):
         self.ctx.check(self.ctx.L.lrc_scene_intersect(self.h, C.c_void_p(d_orig), C.c_void_p(d_dir), n, tmin, tmax,
                                                       C.c_void_p(d_prim), C.c_void_p(d_t), LRC_DEVICE))
+
+    def set_prims(self, prims24):
+        prims24 = np.ascontiguousarray(prims24, np.float32).reshape(-1, 24)
+        self.ctx.check(self.ctx.L.lrc_scene_set_prims(self.h, _ptr(prims24), prims24.shape[0], 0))
+
+    def set_normals(self, normals):
+        normals = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        self.ctx.check(self.ctx.L.lrc_scene_set_normals(self.h, _ptr(normals), normals.shape[0], 0))
+
+    def set_materials(self, recs16):
+        recs16 = np.ascontiguousarray(recs16, np.float32).reshape(-1, 16)
+        self.ctx.check(self.ctx.L.lrc_scene_set_materials(self.h, _ptr(recs16), recs16.shape[0]))
+
+    def set_light(self, prim):
+        self.ctx.check(self.ctx.L.lrc_scene_set_light(self.h, prim))
+
+    def set_tables(self, blue_noise=None, bsdf_tables=None):
+        bn = None if blue_noise is None else np.ascontiguousarray(blue_noise, np.uint16)
+        tb = None if bsdf_tables is None else np.ascontiguousarray(bsdf_tables, np.float32)
+        self.ctx.check(self.ctx.L.lrc_scene_set_tables(self.h, None if bn is None else _ptr(bn),
+                                                       None if tb is None else _ptr(tb)))
+
+    def trace(self, params, spp, accum=None, y0=0, rows=None, spp0=0):
+        """lrc_trace with a host image: returns (accum (h, w, 4) sum + count, rays traced)."""
+        rows = params.height if rows is None else rows
+        if accum is None:
+            accum = np.zeros((params.height, params.width, 4), np.float32)
+        rays = C.c_uint64()
+        self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), y0, rows, spp0, spp, _ptr(accum),
+                                            C.byref(rays), 0))
+        return accum, rays.value
+
+    def trace_device(self, params, spp, d_accum, y0=0, rows=None, spp0=0):
+        rows = params.height if rows is None else rows
+        self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), y0, rows, spp0, spp, C.c_void_p(d_accum), None,
+                                            LRC_DEVICE))
 
     def trace_stats(self, orig, dirs=None, tmin=0.0, tmax=1e30):
         """(box tests, triangle tests) of the closest-hit walk over these rays: host arrays

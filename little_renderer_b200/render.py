@@ -1,0 +1,35 @@
+"""A world scene (primitives, triangles, materials, the lamp) on the device, from the dict the
+workload generators return, and the image path tracing through the C ABI gives."""
+import numpy as np
+
+from . import native, workloads as W
+
+
+def world_scene(ctx, sc, builder=1, key_bits=30, blue_noise=None, bsdf_tables=None):
+    """lrc_scene with the scene's triangles, its lamp quad (primitive 0, Scene.light), materials
+    and the path tracer's tables (None: the library's own), its BVH built (PLOC by default)."""
+    s = native.Scene(ctx)
+    quv = W.corners_to_quv(sc["corners"])
+    s.set_triangles(native.pack_tris(quv, sc["tri_mats"]))
+    lamp = sc.get("lamp")
+    if lamp is not None:
+        s.set_prims(W.make_quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"]))
+        s.set_light(0)
+    s.set_materials(W.material_records(sc["materials"]))
+    s.set_tables(blue_noise, bsdf_tables)
+    s.build(builder, key_bits)
+    return s
+
+
+def camera12(sc):
+    return W.camera(sc["camera"], sc["width"] / sc["height"])
+
+
+def render(ctx, scene, sc, spp=None, exact=0, seed=1, max_depth=None, sampler=1):
+    """(mean image (h, w, 3), rays traced): spp samples per pixel."""
+    spp = sc["spp"] if spp is None else spp
+    p = native.trace_params(camera12(sc), sc["width"], sc["height"], sc["max_depth"] if max_depth is None else max_depth,
+                            1, sampler, exact, seed)
+    acc, rays = scene.trace(p, spp)
+    img = acc[..., :3] * (np.float32(1) / np.maximum(acc[..., 3:4], np.float32(1)))
+    return img.astype(np.float32), rays

@@ -55,3 +55,153 @@ def mesh_bounds(quv):
     lo = np.minimum(np.minimum(q.min(0), b.min(0)), c.min(0)).astype(np.float32)
     hi = np.maximum(np.maximum(q.max(0), b.max(0)), c.max(0)).astype(np.float32)
     return lo, hi
+
+
+# ---- the path tracer's scenes ------------------------------------------------------------------
+# material types (engine/scene/scene.h MatType) and the presets' parameters (scene.h:48-70)
+MAT_DIFFUSE, MAT_MIRROR, MAT_GLASS, MAT_LIGHT, MAT_PBR = 0, 1, 2, 3, 4
+
+
+def material(type_, albedo=(0, 0, 0), emission=(0, 0, 0), ior=1.5, metallic=0.0, roughness=1.0, transmission=0.0):
+    return {"type": type_, "albedo": tuple(float(x) for x in albedo), "emission": tuple(float(x) for x in emission),
+            "ior": float(ior), "metallic": float(metallic), "roughness": float(roughness),
+            "transmission": float(transmission)}
+
+
+def diffuse(c):
+    return material(MAT_DIFFUSE, albedo=c, ior=1.5, roughness=1.0)
+
+
+def glass(tint, ior):
+    return material(MAT_GLASS, albedo=tint, ior=ior, roughness=0.0, transmission=1.0)
+
+
+def light(e):
+    return material(MAT_LIGHT, emission=e, ior=1.0, roughness=1.0)
+
+
+def pbr(base, metallic, roughness, ior, transmission):
+    return material(MAT_PBR, albedo=base, ior=ior, metallic=metallic, roughness=roughness, transmission=transmission)
+
+
+def icosphere(subdiv=2):
+    """Unit icosphere: (20 * 4^subdiv, 3, 3) corners, counter-clockwise seen from outside."""
+    t = (1.0 + 5 ** 0.5) / 2
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    tri = np.array([[v[a], v[b], v[c]] for a, b, c in f], np.float64)
+    tri /= np.linalg.norm(tri, axis=2, keepdims=True)
+    for _ in range(subdiv):
+        a, b, c = tri[:, 0], tri[:, 1], tri[:, 2]
+        ab, bc, ca = a + b, b + c, c + a
+        ab /= np.linalg.norm(ab, axis=1, keepdims=True)
+        bc /= np.linalg.norm(bc, axis=1, keepdims=True)
+        ca /= np.linalg.norm(ca, axis=1, keepdims=True)
+        tri = np.concatenate([np.stack(s, 1) for s in ((a, ab, ca), (ab, b, bc), (ca, bc, c), (ab, bc, ca))])
+    return tri
+
+
+def cornell_spheres(seed=7, n_spheres=64, width=256, height=256):
+    """The plain render: a box 555 units on a side, open at the front (5 walls of 2 triangles),
+    a lamp quad under the ceiling (emission 15, white; Scene.light), and 64 icospheres of
+    subdivision 2 (320 flat triangles each) with centres uniform in the box and radii uniform in
+    [0.05, 0.15] x 555; each sphere's material one of Lambert (albedo U[0.2, 0.9]^3), GGX metal
+    (roughness U[0.05, 0.5]) or dielectric (ior 1.5), at most 60 distinct (MAX_MATS is 64).
+    The camera looks into the box from (278, 278, -800), vertical field of view 40 degrees."""
+    S = 555.0
+    rng = np.random.default_rng(seed)
+    mats = [diffuse((0.73, 0.73, 0.73)), diffuse((0.65, 0.05, 0.05)), diffuse((0.12, 0.45, 0.15)),
+            light((15.0, 15.0, 15.0))]
+    corners, tmat = [], []
+
+    def quad(a, b, c, d, m):
+        corners.extend([[a, b, c], [a, c, d]])
+        tmat.extend([m, m])
+
+    quad((0, 0, 0), (S, 0, 0), (S, 0, S), (0, 0, S), 0)            # floor
+    quad((0, S, 0), (0, S, S), (S, S, S), (S, S, 0), 0)            # ceiling
+    quad((0, 0, S), (S, 0, S), (S, S, S), (0, S, S), 0)            # back
+    quad((0, 0, 0), (0, 0, S), (0, S, S), (0, S, 0), 1)            # left
+    quad((S, 0, 0), (S, S, 0), (S, S, S), (S, 0, S), 2)            # right
+    kinds = rng.integers(0, 3, n_spheres)
+    sphere_mats = []
+    for i in range(min(n_spheres, 60)):
+        k = kinds[i]
+        if k == 0:
+            sphere_mats.append(diffuse(rng.uniform(0.2, 0.9, 3)))
+        elif k == 1:
+            sphere_mats.append(pbr(rng.uniform(0.5, 0.95, 3), 1.0, rng.uniform(0.05, 0.5), 1.5, 0.0))
+        else:
+            sphere_mats.append(glass((1.0, 1.0, 1.0), 1.5))
+    base = len(mats)
+    mats.extend(sphere_mats)
+    unit = icosphere(2)
+    for i in range(n_spheres):
+        r = rng.uniform(0.05, 0.15) * S
+        c = rng.uniform(0.0, S, 3)
+        tri = c + r * unit
+        corners.extend(tri.tolist())
+        tmat.extend([base + i % len(sphere_mats)] * len(unit))
+    corners = np.asarray(corners, np.float32).reshape(-1, 3, 3)
+    return {"corners": corners, "tri_mats": np.asarray(tmat, np.int32), "materials": mats,
+            "lamp": {"q": (213.0, 554.0, 227.0), "u": (130.0, 0.0, 0.0), "v": (0.0, 0.0, 105.0), "material": 3},
+            "camera": {"from": (278.0, 278.0, -800.0), "at": (278.0, 278.0, 0.0), "up": (0.0, 1.0, 0.0), "vfov": 40.0},
+            "width": width, "height": height, "spp": 16, "max_depth": 8}
+
+
+def material_records(mats):
+    """Materials as the device reads them: 16 floats each (albedo.xyz, type as int bits |
+    emission.xyz, 0 | ior, metallic, roughness, transmission | 0)."""
+    out = np.zeros((len(mats), 16), np.float32)
+    for i, m in enumerate(mats):
+        out[i, 0:3] = m["albedo"]
+        out[i, 3] = np.array([m["type"]], np.int32).view(np.float32)[0]
+        out[i, 4:7] = m["emission"]
+        out[i, 8:12] = (m["ior"], m["metallic"], m["roughness"], m["transmission"])
+    return out
+
+
+def make_quad(q, u, v, material):
+    """make_quad (engine/scene/scene.c:26-39) in float: the 24 floats the device reads
+    (upload_world's layout, engine/gpu/trace_gpu.c:1145-1154)."""
+    f = np.float32
+    q, u, v = (np.asarray(x, f) for x in (q, u, v))
+    n = np.array([u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]], f)
+    dot = lambda a, b: f(f(f(a[0] * b[0]) + f(a[1] * b[1])) + f(a[2] * b[2]))
+    ln = np.sqrt(dot(n, n), dtype=f)
+    normal = (n * (f(1) / ln)).astype(f) if ln > 0 else n
+    w = (n * (f(1) / dot(n, n))).astype(f)
+    out = np.zeros(24, f)
+    out[4:7], out[7] = q, 1.0
+    out[8:11], out[11] = u, f(material)
+    out[12:15], out[15] = v, ln
+    out[16:19], out[19] = normal, dot(normal, q)
+    out[20:23] = w
+    return out
+
+
+def camera(cam, aspect):
+    """camera_make (engine/scene/camera.h:21-36) in float: origin, upper_left, horizontal, vertical."""
+    f = np.float32
+    frm, at, up = (np.asarray(cam[k], f) for k in ("from", "at", "up"))
+    h = np.tan(f(f(f(f(cam["vfov"]) * f(np.pi)) / f(180.0)) / f(2.0)), dtype=f)
+    view_h = f(f(2.0) * h)
+    view_w = f(f(aspect) * view_h)
+
+    def norm(a):
+        ln = np.sqrt(f(f(f(a[0] * a[0]) + f(a[1] * a[1])) + f(a[2] * a[2])), dtype=f)
+        return (a * (f(1) / ln)).astype(f)
+
+    def cross(a, b):
+        return np.array([f(a[1] * b[2]) - f(a[2] * b[1]), f(a[2] * b[0]) - f(a[0] * b[2]), f(a[0] * b[1]) - f(a[1] * b[0])], f)
+
+    w = norm((frm - at).astype(f))
+    u = norm(cross(up, w))
+    v = cross(w, u)
+    hor = (u * view_w).astype(f)
+    ver = (v * view_h).astype(f)
+    ul = (((frm - (hor * f(0.5)).astype(f)).astype(f) + (ver * f(0.5)).astype(f)).astype(f) - w).astype(f)
+    return np.concatenate([frm, ul, hor, ver]).astype(f)

@@ -174,8 +174,31 @@ def ref_lib(double=False):
         lib.rb_sampler_hash.argtypes = [C.c_uint32]
         lib.rb_sampler_hash.restype = C.c_uint32
         lib.rb_set_threads.argtypes = [C.c_int]
+        lib.rb_bsdf_tables.argtypes = [_f32p]
+        lib.rb_prim_data.argtypes = [vp, _f32p]
+        lib.rb_camera.argtypes = [_f32p, C.c_float, C.c_float, _f32p]
         lib._typed = True
     return lib
+
+
+def bsdf_tables():
+    """scene/brdf_tables.h packed as gpu_bsdf_tables packs it (2112 floats)."""
+    out = np.zeros(2112, np.float32)
+    ref_lib().rb_bsdf_tables(out)
+    return out
+
+
+def blue_noise():
+    out = np.zeros(4096, np.uint16)
+    ref_lib().rb_blue_noise(out)
+    return out
+
+
+def camera(from_at_up, vfov, aspect):
+    """camera_make (camera.h:21-36): (origin, upper_left, horizontal, vertical) as 12 floats."""
+    out = np.zeros(12, np.float32)
+    ref_lib().rb_camera(np.ascontiguousarray(from_at_up, np.float32).reshape(-1), vfov, aspect, out)
+    return out
 
 
 def triangle_bounds(quv):
@@ -249,6 +272,12 @@ class RefScene:
 
     def set_accel(self):
         self.lib.rb_set_accel(self.s)
+
+    def prim_data(self):
+        n = self.lib.rb_num_prims(self.s)
+        out = np.zeros((max(n, 1), 24), np.float32)
+        self.lib.rb_prim_data(self.s, out.reshape(-1))
+        return out[:n]
 
     def tri_data(self):
         n = self.lib.rb_num_tris(self.s)

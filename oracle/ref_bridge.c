@@ -17,6 +17,7 @@
 #include "rt/accel.h"
 #include "rt/tracer.h"
 #include "base/sampler.h"
+#include "scene/brdf_tables.h"
 
 // ---- ray counters: one slot per OpenMP thread, 64 bytes apart ----------------------------
 #define RB_MAX_THREADS 256
@@ -241,6 +242,34 @@ void rb_trace_image(const void *sp, const float *cam, float vfov, int w, int h, 
             o[0] = (float)p->x; o[1] = (float)p->y; o[2] = (float)p->z;
         }
     free(px);
+}
+
+// the BSDF's tables (scene/brdf_tables.h) packed as the GPU backend packs them (brdf_gpu.c:20-25)
+void rb_bsdf_tables(float *out){
+    memcpy(out, BRDF_E, sizeof(BRDF_E));
+    memcpy(out + 1024, BRDF_B, sizeof(BRDF_B));
+    memcpy(out + 2048, BRDF_E_AVG, sizeof(BRDF_E_AVG));
+    memcpy(out + 2080, BRDF_B_AVG, sizeof(BRDF_B_AVG));
+}
+// the primitives as upload_world packs them (trace_gpu.c:1145-1154): 24 floats each
+void rb_prim_data(const void *sp, float *out){
+    const Scene *s = sp;
+    for (int i = 0; i < s->nprims; i++){
+        const Primitive *p = &s->prims[i];
+        float *o = out + 24 * (size_t)i;
+        o[0] = p->center.x; o[1] = p->center.y; o[2] = p->center.z; o[3] = p->radius;
+        o[4] = p->q.x; o[5] = p->q.y; o[6] = p->q.z; o[7] = p->type == PRIM_QUAD ? 1.0f : 0.0f;
+        o[8] = p->u.x; o[9] = p->u.y; o[10] = p->u.z; o[11] = (float)p->material;
+        o[12] = p->v.x; o[13] = p->v.y; o[14] = p->v.z; o[15] = p->area;
+        o[16] = p->normal.x; o[17] = p->normal.y; o[18] = p->normal.z; o[19] = p->plane_d;
+        o[20] = p->w.x; o[21] = p->w.y; o[22] = p->w.z; o[23] = 0;
+    }
+}
+// camera_make (camera.h:21-36): origin, upper_left, horizontal, vertical (12 floats)
+void rb_camera(const float *from_at_up, float vfov, float aspect, float *out){
+    Camera c = camera_make(v3f(from_at_up), v3f(from_at_up + 3), v3f(from_at_up + 6), vfov, aspect);
+    Vec3 v[4] = {c.origin, c.upper_left, c.horizontal, c.vertical};
+    for (int k = 0; k < 4; k++){ out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
 }
 
 // the blue-noise mask (sampler.c): 64 x 64 ranks

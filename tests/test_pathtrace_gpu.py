@@ -1,0 +1,97 @@
+"""GPU parity of the path tracer against the reference's own CPU path tracer (trace_image,
+engine/rt/tracer.c:329) on the plain render (box, lamp, 64 icospheres), and of world hits
+(primitives + triangles) against scene_intersect."""
+import numpy as np
+import pytest
+
+import little_renderer_b200 as L
+from little_renderer_b200 import render as R, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def ref_scene(O, sc, double=False):
+    ref = O.RefScene(double)
+    for m in sc["materials"]:
+        ref.material(m["type"], m["albedo"], m["emission"], m["ior"], m["metallic"], m["roughness"], m["transmission"])
+    ref.triangles(sc["corners"], sc["tri_mats"])
+    lamp = sc["lamp"]
+    ref.quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"], light=True)
+    ref.set_accel()
+    return ref
+
+
+def cam9(sc):
+    c = sc["camera"]
+    return np.array([*c["from"], *c["at"], *c["up"]], np.float32)
+
+
+def rel_rmse(x, ref):
+    return float(np.sqrt(((x.astype(np.float64) - ref) ** 2).sum() / (ref.astype(np.float64) ** 2).sum()))
+
+
+@pytest.fixture(scope="module")
+def cornell128(oracle):
+    return W.cornell_spheres(width=128, height=128)
+
+
+@pytest.mark.parametrize("builder", [0, 1])
+def test_world_hits_match_scene_intersect(ctx, oracle, cornell128, builder):
+    sc = cornell128
+    ref = ref_scene(oracle, sc)
+    s = R.world_scene(ctx, sc, builder, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    rng = np.random.default_rng(3)
+    n = 200000
+    o = rng.uniform(5, 550, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    rp, _, rt = ref.intersect(o, d, 2e-3, 1e30)
+    p, t = s.intersect(o, d, 2e-3, 1e30)
+    diff = p != rp
+    assert (rp >= 0).mean() > 0.85                   # (the box is open at the front)
+    assert diff.sum() <= 10
+    assert np.all(np.abs(t[diff] - rt[diff]) <= 1e-6 * np.abs(rt[diff]))
+    assert np.array_equal(t[~diff], rt[~diff])
+
+
+def test_exact_mode_is_the_cpu_image(ctx, oracle, cornell128):
+    """Sample-exact mode: the CPU's random streams; the image equals trace_image's up to the
+    paths where CUDA's and the C library's sinf/cosf round differently."""
+    sc = cornell128
+    spp, seed = 8, 5
+    ref = ref_scene(oracle, sc)
+    cpu, (closest, shadow) = ref.trace_image(cam9(sc), sc["camera"]["vfov"], 128, 128, spp, seed, sc["max_depth"])
+    s = R.world_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    p = L.native.trace_params(oracle.camera(cam9(sc), sc["camera"]["vfov"], 1.0), 128, 128, sc["max_depth"], 1, 1, 1, seed)
+    acc, rays = s.trace(p, spp)
+    gpu = acc[..., :3] * (np.float32(1) / np.float32(spp))
+    exact = np.all(gpu == cpu, axis=2).mean()
+    err = rel_rmse(gpu, cpu)
+    print(f"pixels equal to the bit: {exact:.4f}; relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}")
+    assert exact > 0.5
+    assert err < 0.05
+    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 0.01
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.02
+
+
+def test_fast_mode_mean_matches_cpu(ctx, oracle, cornell128):
+    """Independent per-sample streams: the mean radiance within 1 % of the CPU's (the reference's own
+    GPU criterion), and the image as close to a converged one as the CPU's at the same spp."""
+    sc = cornell128
+    ref = ref_scene(oracle, sc)
+    cpu, _ = ref.trace_image(cam9(sc), sc["camera"]["vfov"], 128, 128, 64, 11, sc["max_depth"])
+    s = R.world_scene(ctx, sc, 1)
+    gpu, _ = R.render(ctx, s, sc, spp=64, exact=0, seed=3)
+    conv, _ = R.render(ctx, s, sc, spp=1024, exact=0, seed=99)
+    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 0.01
+    e_gpu, e_cpu = rel_rmse(gpu, conv), rel_rmse(cpu, conv)
+    print(f"relRMSE to 1024 spp: GPU {e_gpu:.4f} CPU {e_cpu:.4f}")
+    assert e_gpu < 1.15 * e_cpu
+
+
+def test_fast_mode_is_deterministic(ctx, cornell128):
+    sc = cornell128
+    s = R.world_scene(ctx, sc, 1)
+    a, _ = R.render(ctx, s, sc, spp=16, exact=0, seed=4)
+    b, _ = R.render(ctx, s, sc, spp=16, exact=0, seed=4)
+    assert np.array_equal(a, b)
