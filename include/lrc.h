@@ -160,6 +160,31 @@ int lrc_scene_set_normals(lrc_scene *s, const float *normals, uint32_t n, unsign
 int lrc_scene_set_materials(lrc_scene *s, const float *mats, uint32_t n);
 /* Scene.light: the lamp, a quad primitive sampled by next event estimation (-1: none) */
 int lrc_scene_set_light(lrc_scene *s, int32_t prim);
+/* Instanced meshes (SceneMesh, scene.h:181-194): nmeshes meshes of tri_counts[m] triangles each,
+ * their triangles one mesh after another (12 words each, the GPU layout; flat). Replaces the
+ * scene's meshes (and drops their trees: lrc_scene_build_instances builds them again). */
+int lrc_scene_set_meshes(lrc_scene *s, const uint32_t *tris, const uint32_t *tri_counts, uint32_t nmeshes, unsigned flags);
+/* Instances (scene.h:202-209), 32 floats each: the object-to-world transform (3 x 4, row-major),
+ * its inverse (xform_inverse, scene.c:606-623), the world box's lo.xyz and the mesh's index (the
+ * int's bits), its hi.xyz and the material (the int's bits; -1: the triangles' own). Host. */
+int lrc_scene_set_instances(lrc_scene *s, const float *records, uint32_t n, unsigned flags);
+/* Each mesh's BVH (builder 0 LBVH / 1 PLOC, key_bits 30 / 63; built once per lrc_scene_set_meshes)
+ * and the top level over the instances' boxes (LBVH, 30-bit keys, the reference's GPU top level,
+ * trace_gpu.c:459-460, 1462-1463): after moving instances, only the top level is built again. */
+int lrc_scene_build_instances(lrc_scene *s, int mesh_builder, int key_bits);
+/* The sky (Env, env.h:29-53; upload_sky, trace_gpu.c:1522-1569): w x h linear RGB, rows top to
+ * bottom, times scale; its sampling tables (marg: h + 1 floats, cond: h x (w + 1), prob: w x h =
+ * env_pixel_prob) or NULL: made here as env_prepare makes them (env.c:116-167, 341-363). Host.
+ * rgb NULL: no sky. */
+int lrc_scene_set_sky(lrc_scene *s, const float *rgb, int32_t w, int32_t h, const float *marg, const float *cond,
+                      const float *prob, float scale);
+/* The sky's sampling tables as env_prepare makes them (host only, no device): marg h + 1, cond
+ * h x (w + 1), prob w x h. Returns 1, or 0 when no pixel weighs anything. */
+int lrc_sky_tables(const float *rgb, int32_t w, int32_t h, float *marg, float *cond, float *prob);
+/* Closest hits as scene_intersect's Hit (accel.c:252): prim = the world's shape id (primitives,
+ * then triangles) or, on an instance, the triangle's index in its mesh; inst = the instance or -1 */
+int lrc_scene_intersect_ex(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
+                           int32_t *prim, int32_t *inst, float *t, unsigned flags);
 /* The blue-noise mask (64 x 64 ranks; blue_noise_mask(), engine/base/sampler.c) and the BSDF tables
  * (2112 floats packed as gpu_bsdf_tables packs scene/brdf_tables.h, engine/gpu/brdf_gpu.c:20-25),
  * both host. NULL: the ones lrc_default_blue_noise / lrc_default_bsdf_tables make. */

@@ -54,6 +54,25 @@ struct lrc_scene {
     float *d_tab = nullptr;
     bool tables = false;
     unsigned long long *d_rays = nullptr;
+    // instances: meshes' triangles and trees, records, the top level
+    uint32_t *d_mtris = nullptr;
+    uint32_t nmtris = 0;
+    std::vector<uint32_t> mesh_counts;
+    Node *d_mnodes = nullptr;
+    uint32_t *d_maux = nullptr;
+    uint4 *d_mesh_info = nullptr;
+    bool meshes_built = false;
+    float *d_inst = nullptr;
+    size_t inst_cap = 0;
+    uint32_t ninst = 0;
+    Node *d_tlas_nodes = nullptr;
+    uint32_t *d_tlas_aux = nullptr;
+    size_t tlas_cap = 0;
+    uint32_t tlas_n = 0;
+    // the sky
+    float *d_env = nullptr;       // rgbp (w x h float4), cond, marg
+    int env_w = 0, env_h = 0, env_weighted = 0;
+    float env_scale = 1;
 };
 
 namespace {
@@ -143,6 +162,33 @@ lrc::PtScene pt_scene(const lrc_scene *s) {
     S.light = s->light;
     S.mask = s->d_mask;
     S.tab = s->d_tab;
+    if (s->meshes_built && s->tlas_n == s->ninst && s->ninst) {
+        S.inst = reinterpret_cast<const float4 *>(s->d_inst);
+        S.ninst = s->ninst;
+        S.tlas_nodes = reinterpret_cast<const float4 *>(s->d_tlas_nodes);
+        S.tlas_aux = s->d_tlas_aux;
+        S.tlas_nnodes = 2 * s->ninst - 1;
+        S.mtris = reinterpret_cast<const float4 *>(s->d_mtris);
+        S.nmtris = s->nmtris;
+        S.mnodes = reinterpret_cast<const float4 *>(s->d_mnodes);
+        S.maux = s->d_maux;
+        uint32_t nn = 0;
+        for (uint32_t c : s->mesh_counts) nn += c ? 2 * c - 1 : 0;
+        S.mnnodes = nn;
+        S.mnaux = s->nmtris;
+        S.mesh_info = s->d_mesh_info;
+        S.nmeshes = (uint32_t)s->mesh_counts.size();
+    }
+    if (s->d_env) {
+        S.env_rgbp = reinterpret_cast<const float4 *>(s->d_env);
+        S.env_cond = s->d_env + 4 * (size_t)s->env_w * s->env_h;
+        S.env_marg = S.env_cond + (size_t)s->env_h * (s->env_w + 1);
+        S.env_w = s->env_w;
+        S.env_h = s->env_h;
+        S.has_env = 1;
+        S.env_weighted = s->env_weighted;
+        S.env_scale = s->env_scale;
+    }
     return S;
 }
 
@@ -351,6 +397,14 @@ void lrc_scene_destroy(lrc_scene *s) {
     cudaFree(s->d_mats);
     cudaFree(s->d_mask);
     cudaFree(s->d_rays);
+    cudaFree(s->d_mtris);
+    cudaFree(s->d_mnodes);
+    cudaFree(s->d_maux);
+    cudaFree(s->d_mesh_info);
+    cudaFree(s->d_inst);
+    cudaFree(s->d_tlas_nodes);
+    cudaFree(s->d_tlas_aux);
+    cudaFree(s->d_env);
     delete s;
 }
 
@@ -438,6 +492,7 @@ int lrc_scene_tree_device(lrc_scene *s, const uint32_t **nodes, const uint32_t *
 int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
                         int32_t *prim, float *t, unsigned flags) {
     if (!s || (nrays && (!orig || !dir || !prim || !t))) return LRC_E_INVALID;
+    if (s->tlas_n) return lrc_scene_intersect_ex(s, orig, dir, nrays, tmin, tmax, prim, nullptr, t, flags);
     lrc_ctx *c = s->ctx;
     if (!s->built_n) return fail(c, LRC_E_INVALID, "the scene has no built BVH (lrc_scene_build)");
     DeviceGuard g(c->device);
@@ -450,7 +505,7 @@ int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint6
     }
     // a world with primitives walks shape ids (primitives, then triangles); a mesh, triangles alone
     auto run = [&](const float *o, const float *d, int32_t *p, float *tt_out) {
-        if (s->nprims) return lrc::pt_intersect(pt_scene(s), o, d, nrays, tmin, tmax, p, tt_out, c->d_status, c->st);
+        if (s->nprims) return lrc::pt_intersect(pt_scene(s), o, d, nrays, tmin, tmax, p, nullptr, tt_out, c->d_status, c->st);
         return lrc::intersect_device(tt, o, d, nrays, tmin, tmax, p, tt_out, c->d_status, c->st, c->num_sms, sort_scratch,
                                      c->scratch_cap);
     };
@@ -598,12 +653,191 @@ int lrc_scene_set_tables(lrc_scene *s, const uint16_t *blue_noise, const float *
     return check_status(c);
 }
 
+int lrc_scene_set_meshes(lrc_scene *s, const uint32_t *tris, const uint32_t *tri_counts, uint32_t nmeshes, unsigned flags) {
+    if (!s || (nmeshes && !tri_counts)) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    uint64_t total = 0;
+    for (uint32_t m = 0; m < nmeshes; m++) total += tri_counts[m];
+    if (total >= (1u << 30)) return fail(c, LRC_E_INVALID, "more than 2^30 - 1 mesh triangles");
+    if (total && !tris) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    cudaFree(s->d_mtris);
+    cudaFree(s->d_mnodes);
+    cudaFree(s->d_maux);
+    cudaFree(s->d_mesh_info);
+    s->d_mtris = nullptr; s->d_mnodes = nullptr; s->d_maux = nullptr; s->d_mesh_info = nullptr;
+    s->meshes_built = false;
+    s->mesh_counts.assign(tri_counts, tri_counts + nmeshes);
+    s->nmtris = (uint32_t)total;
+    size_t nodes = 0;
+    for (uint32_t m = 0; m < nmeshes; m++) nodes += tri_counts[m] ? 2 * (size_t)tri_counts[m] - 1 : 0;
+    cudaError_t e = cudaMalloc(&s->d_mtris, (size_t)(total ? total : 1) * 48);
+    if (!e) e = cudaMalloc(&s->d_mnodes, (nodes ? nodes : 1) * 32);
+    if (!e) e = cudaMalloc(&s->d_maux, (size_t)(total ? total : 1) * 4);
+    if (!e) e = cudaMalloc(&s->d_mesh_info, (size_t)(nmeshes ? nmeshes : 1) * 16);
+    if (!e && total)
+        e = cudaMemcpyAsync(s->d_mtris, tris, total * 48, (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            c->st);
+    if (e) return cuda_status(c, e, "meshes");
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_scene_set_instances(lrc_scene *s, const float *records, uint32_t n, unsigned flags) {
+    if (!s || (n && !records)) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (n >= (1u << 30)) return fail(c, LRC_E_INVALID, "more than 2^30 - 1 instances");
+    DeviceGuard g(c->device);
+    cudaError_t e = reserve(reinterpret_cast<void **>(&s->d_inst), &s->inst_cap, (size_t)(n ? n : 1) * 128);
+    if (!e && n)
+        e = cudaMemcpyAsync(s->d_inst, records, (size_t)n * 128,
+                            (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->st);
+    if (e) return cuda_status(c, e, "instances");
+    s->ninst = n;
+    s->tlas_n = 0;
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_scene_build_instances(lrc_scene *s, int mesh_builder, int key_bits) {
+    if (!s) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (key_bits != 30 && key_bits != 63) return fail(c, LRC_E_INVALID, "key_bits must be 30 or 63");
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaSuccess;
+    uint32_t *keys = s->d_small;
+    float *bounds = reinterpret_cast<float *>(s->d_small + 8), *lo_ext = reinterpret_cast<float *>(s->d_small + 16);
+    if (!s->meshes_built) {
+        // each mesh's tree as a dynamic mesh's (upload_instances, trace_gpu.c:1497-1512): its triangles'
+        // boxes, its corners' box as the bounds; leaves' aux: the triangles' global indices
+        std::vector<uint4> info(s->mesh_counts.size());
+        uint32_t node0 = 0, tri0 = 0, most = 1;
+        for (uint32_t n : s->mesh_counts) most = n > most ? n : most;
+        e = reserve(reinterpret_cast<void **>(&s->d_boxes), &s->boxes_cap, (size_t)most * 32);
+        if (!e) e = reserve(&c->scratch, &c->scratch_cap, lrc::build_scratch_bytes(most, key_bits, mesh_builder));
+        if (e) return cuda_status(c, e, "mesh build memory");
+        c->timer.begin(LRC_TS_BOXES, c->st);
+        for (size_t m = 0; m < s->mesh_counts.size() && !e; m++) {
+            const uint32_t n = s->mesh_counts[m];
+            info[m] = make_uint4(node0, tri0, n, 0);
+            if (!n) continue;
+            e = lrc::triangle_boxes(s->d_mtris + 12 * (size_t)tri0, n, s->d_boxes, keys, c->st, c->num_sms);
+            if (!e) e = lrc::bounds_params(keys, bounds, lo_ext, c->st);
+            lrc_build_params p{};
+            p.n = n; p.node0 = node0; p.ref0 = tri0; p.ref_add = tri0; p.key_bits = key_bits; p.builder = mesh_builder;
+            if (!e) e = lrc::build_device_ext(p, s->d_boxes, lo_ext, s->d_mnodes + node0, s->d_maux + tri0, c->scratch,
+                                              c->scratch_cap, c->d_status, c->num_sms, c->st, nullptr, &c->timer);
+            node0 += 2 * n - 1;
+            tri0 += n;
+        }
+        if (!e && !info.empty())
+            e = cudaMemcpyAsync(s->d_mesh_info, info.data(), info.size() * 16, cudaMemcpyHostToDevice, c->st);
+        if (e) return cuda_status(c, e, "mesh trees");
+        int rc = check_status(c);                        // (the host vector goes out of scope)
+        if (rc) return rc;
+        s->meshes_built = true;
+    }
+    s->tlas_n = 0;
+    const uint32_t n = s->ninst;
+    if (!n) return LRC_OK;
+    // the top level: LBVH over the instances' world boxes, bounds their union (upload_instances :1415-1463)
+    if (s->tlas_cap < n) {
+        cudaFree(s->d_tlas_nodes);
+        cudaFree(s->d_tlas_aux);
+        s->d_tlas_nodes = nullptr; s->d_tlas_aux = nullptr; s->tlas_cap = 0;
+        e = cudaMalloc(&s->d_tlas_nodes, (2 * (size_t)n - 1) * 32);
+        if (!e) e = cudaMalloc(&s->d_tlas_aux, (size_t)n * 4);
+        if (!e) s->tlas_cap = n;
+    }
+    if (!e) e = reserve(reinterpret_cast<void **>(&s->d_boxes), &s->boxes_cap, (size_t)n * 32);
+    if (!e) e = reserve(&c->scratch, &c->scratch_cap, lrc::build_scratch_bytes(n, 30, 0));
+    if (e) return cuda_status(c, e, "top level memory");
+    c->timer.begin(LRC_TS_BOXES, c->st);
+    e = lrc::pt_inst_boxes(s->d_inst, n, s->d_boxes, c->st);
+    if (!e) e = lrc::boxes_bounds(s->d_boxes, n, keys, c->st, c->num_sms, true);
+    if (!e) e = lrc::bounds_params(keys, bounds, lo_ext, c->st);
+    lrc_build_params p{};
+    p.n = n; p.key_bits = 30; p.builder = 0;
+    if (!e) e = lrc::build_device_ext(p, s->d_boxes, lo_ext, s->d_tlas_nodes, s->d_tlas_aux, c->scratch, c->scratch_cap,
+                                      c->d_status, c->num_sms, c->st, nullptr, &c->timer);
+    if (e) return cuda_status(c, e, "top level");
+    s->tlas_n = n;
+    return LRC_OK;
+}
+
+int lrc_scene_set_sky(lrc_scene *s, const float *rgb, int32_t w, int32_t h, const float *marg, const float *cond,
+                      const float *prob, float scale) {
+    if (!s) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    DeviceGuard g(c->device);
+    cudaFree(s->d_env);
+    s->d_env = nullptr;
+    s->env_w = s->env_h = 0;
+    if (!rgb) return LRC_OK;
+    if (w <= 0 || h <= 0 || h > w) return fail(c, LRC_E_INVALID, "a sky is w x h with h <= w (upload_sky)");
+    const size_t np = (size_t)w * h;
+    std::vector<float> host(4 * np + (size_t)h * (w + 1) + (h + 1));
+    float *rgbp = host.data(), *hc = rgbp + 4 * np, *hm = hc + (size_t)h * (w + 1);
+    std::vector<float> own_prob;
+    int weighted = 1;
+    if (!marg || !cond || !prob) {
+        own_prob.resize(np);
+        weighted = lrc::env_tables(rgb, w, h, hm, hc, own_prob.data()) ? 1 : 0;
+        prob = own_prob.data();
+    } else {
+        std::memcpy(hm, marg, sizeof(float) * (h + 1));
+        std::memcpy(hc, cond, sizeof(float) * (size_t)h * (w + 1));
+        weighted = 0;
+        for (size_t i = 0; i < np && !weighted; i++) weighted = prob[i] > 0;
+    }
+    for (size_t i = 0; i < np; i++) {
+        rgbp[4 * i] = rgb[3 * i];
+        rgbp[4 * i + 1] = rgb[3 * i + 1];
+        rgbp[4 * i + 2] = rgb[3 * i + 2];
+        rgbp[4 * i + 3] = prob[i];
+    }
+    cudaError_t e = cudaMalloc(&s->d_env, host.size() * 4);
+    if (!e) e = cudaMemcpyAsync(s->d_env, host.data(), host.size() * 4, cudaMemcpyHostToDevice, c->st);
+    if (e) return cuda_status(c, e, "sky");
+    s->env_w = w;
+    s->env_h = h;
+    s->env_weighted = weighted;
+    s->env_scale = scale;
+    return check_status(c);
+}
+
+int lrc_scene_intersect_ex(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,
+                           int32_t *prim, int32_t *inst, float *t, unsigned flags) {
+    if (!s || (nrays && (!orig || !dir || !prim || !t))) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (!s->built_n && !(s->meshes_built && s->tlas_n)) return fail(c, LRC_E_INVALID, "the scene has nothing built");
+    DeviceGuard g(c->device);
+    if (flags & LRC_DEVICE) {
+        cudaError_t e = lrc::pt_intersect(pt_scene(s), orig, dir, nrays, tmin, tmax, prim, inst, t, c->d_status, c->st);
+        return cuda_status(c, e, "lrc_scene_intersect_ex");
+    }
+    const size_t b_ray = al(nrays * 12), b_out = al(nrays * 4);
+    cudaError_t e = reserve(&c->stage, &c->stage_cap, 2 * b_ray + 3 * b_out);
+    if (e) return cuda_status(c, e, "ray staging");
+    char *st = static_cast<char *>(c->stage);
+    float *d_o = reinterpret_cast<float *>(st), *d_d = reinterpret_cast<float *>(st + b_ray);
+    int32_t *d_p = reinterpret_cast<int32_t *>(st + 2 * b_ray), *d_i = reinterpret_cast<int32_t *>(st + 2 * b_ray + b_out);
+    float *d_t = reinterpret_cast<float *>(st + 2 * b_ray + 2 * b_out);
+    e = cudaMemcpyAsync(d_o, orig, nrays * 12, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = cudaMemcpyAsync(d_d, dir, nrays * 12, cudaMemcpyHostToDevice, c->st);
+    if (!e) e = lrc::pt_intersect(pt_scene(s), d_o, d_d, nrays, tmin, tmax, d_p, d_i, d_t, c->d_status, c->st);
+    if (!e) e = cudaMemcpyAsync(prim, d_p, nrays * 4, cudaMemcpyDeviceToHost, c->st);
+    if (!e && inst) e = cudaMemcpyAsync(inst, d_i, nrays * 4, cudaMemcpyDeviceToHost, c->st);
+    if (!e) e = cudaMemcpyAsync(t, d_t, nrays * 4, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_scene_intersect_ex");
+    return check_status(c);
+}
+
 int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0, uint32_t spp, float *accum,
               uint64_t *rays, unsigned flags) {
     if (!s || !p || !accum || p->width <= 0 || p->height <= 0 || y0 < 0 || rows < 0 || y0 + rows > p->height)
         return LRC_E_INVALID;
     lrc_ctx *c = s->ctx;
-    if (!s->built_n) return fail(c, LRC_E_INVALID, "the scene has no built BVH (lrc_scene_build)");
+    if (!s->built_n && !s->tlas_n) return fail(c, LRC_E_INVALID, "the scene has nothing built (lrc_scene_build)");
+    if (s->ninst && s->tlas_n != s->ninst) return fail(c, LRC_E_INVALID, "instances changed: lrc_scene_build_instances");
     if (p->exact && spp0 != 0) return fail(c, LRC_E_INVALID, "exact mode starts at each pixel's first sample (spp0 = 0)");
     if (!s->d_mats || !s->nmats) return fail(c, LRC_E_INVALID, "the scene has no materials (lrc_scene_set_materials)");
     if (s->light >= (int32_t)s->nprims) return fail(c, LRC_E_INVALID, "the light is not one of the primitives");

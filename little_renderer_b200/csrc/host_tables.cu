@@ -192,7 +192,77 @@ void default_bsdf_tables(float *out) {
     }
 }
 
+// The sky's importance-sampling tables, as engine/scene/env.c makes them (make_weights :125-162,
+// prepare_base :341-363, pixel_prob :164-167): a pixel's weight is the largest luminance of its
+// 3 x 3 neighbourhood (wrapping across, stopping at the poles) times its row's sin(theta); each row's
+// cumulative distribution and the rows' are summed in double and stored in float; a pixel's
+// probability is its weight over the whole sum.
+bool env_tables(const float *rgb, int w, int h, float *marg, float *cond, float *prob) {
+    std::vector<float> lum((size_t)w * h), wmax((size_t)w * h);
+    std::vector<float> row_sin(h);
+    for (int y = 0; y < h; y++) {
+        const float *p = rgb + 3 * (size_t)y * w;
+        float *l = lum.data() + (size_t)y * w, *o = wmax.data() + (size_t)y * w;
+        for (int x = 0; x < w; x++) {
+            const float *c = p + 3 * x;
+            float a = 0.2126f * c[0];
+            float b = 0.7152f * c[1];
+            float d = 0.0722f * c[2];
+            l[x] = (a + b) + d;
+        }
+        for (int x = 0; x < w; x++) {
+            float a = l[x == 0 ? w - 1 : x - 1], b = l[x], c = l[x + 1 == w ? 0 : x + 1];
+            float m = a > b ? a : b;
+            o[x] = m > c ? m : c;
+        }
+        float arg = ((float)y + 0.5f) * 3.14159265358979323846f;
+        row_sin[y] = sinf(arg / (float)h);
+    }
+    lum = wmax;
+    for (int y = 0; y < h; y++) {
+        const float *a = lum.data() + (size_t)(y > 0 ? y - 1 : y) * w, *b = lum.data() + (size_t)y * w;
+        const float *c = lum.data() + (size_t)(y + 1 < h ? y + 1 : y) * w;
+        float *o = wmax.data() + (size_t)y * w;
+        for (int x = 0; x < w; x++) {
+            float m = a[x] > b[x] ? a[x] : b[x];
+            m = m > c[x] ? m : c[x];
+            o[x] = m > 0 ? m : 0;
+        }
+    }
+    auto weight = [&](int x, int y) { return wmax[(size_t)y * w + x] * row_sin[y]; };
+    std::vector<double> rows(h);
+    double sum = 0;
+    for (int y = 0; y < h; y++) {
+        float *c = cond + (size_t)y * (w + 1);
+        double acc = 0;
+        c[0] = 0;
+        for (int x = 0; x < w; x++) {
+            acc += weight(x, y);
+            c[x + 1] = (float)acc;
+        }
+        rows[y] = acc;
+        for (int x = 1; x <= w; x++) c[x] = acc > 0 ? (float)(c[x] / acc) : (float)x / w;
+        c[w] = 1;
+        sum += acc;
+    }
+    double acc = 0;
+    marg[0] = 0;
+    for (int y = 0; y < h; y++) {
+        acc += rows[y];
+        marg[y + 1] = sum > 0 ? (float)(acc / sum) : (float)(y + 1) / h;
+    }
+    marg[h] = 1;
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) prob[(size_t)y * w + x] = sum > 0 ? (float)(weight(x, y) / sum) : 0.0f;
+    return sum > 0;
+}
+
 }  // namespace lrc
+
+extern "C" int lrc_sky_tables(const float *rgb, int32_t w, int32_t h, float *marg, float *cond, float *prob) {
+    if (!rgb || w <= 0 || h <= 0 || !marg || !cond || !prob) return 0;
+    return lrc::env_tables(rgb, w, h, marg, cond, prob) ? 1 : 0;
+}
 
 extern "C" void lrc_default_blue_noise(uint16_t *out) {
     if (out) lrc::default_blue_noise(out);

@@ -161,6 +161,26 @@ struct PtScene {
     int32_t light;              // Scene.light: a quad primitive, or -1
     const uint16_t *mask;       // 64 x 64 blue-noise ranks
     const float *tab;           // the BSDF's 2112 table floats
+    // instances: records (8 float4 each), the top level over their boxes, the meshes' triangles,
+    // BVHs (one nodes / aux array, each mesh's root at mesh_info.x) and mesh_info (root, first
+    // triangle, triangles, 0)
+    const float4 *inst;
+    uint32_t ninst;
+    const float4 *tlas_nodes;
+    const uint32_t *tlas_aux;
+    uint32_t tlas_nnodes;
+    const float4 *mtris;
+    uint32_t nmtris;
+    const float4 *mnodes;
+    const uint32_t *maux;
+    uint32_t mnnodes, mnaux;
+    const uint4 *mesh_info;
+    uint32_t nmeshes;
+    // the sky: radiance + pixel probability (w x h), each row's distribution, the rows'
+    const float4 *env_rgbp;
+    const float *env_cond, *env_marg;
+    int env_w, env_h, has_env, env_weighted;
+    float env_scale;
 };
 struct PtParams {
     int W, H, y0, rows, spp0, spp, max_depth, mis, sampler_on, exact, group;
@@ -172,7 +192,11 @@ cudaError_t pt_prim_boxes(const float *d_prims, uint32_t n, float *d_boxes, cuda
 cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsigned long long *d_rays, uint32_t *d_status,
                      cudaStream_t st);
 cudaError_t pt_intersect(const PtScene &S, const float *d_orig, const float *d_dir, uint64_t n, float tmin, float tmax,
-                         int32_t *d_prim, float *d_t, uint32_t *d_status, cudaStream_t st);
+                         int32_t *d_prim, int32_t *d_inst, float *d_t, uint32_t *d_status, cudaStream_t st);
+cudaError_t pt_inst_boxes(const float *d_rec, uint32_t n, float *d_boxes, cudaStream_t st);
+// the sky's sampling tables as env_prepare makes them (host_tables.cu): marg h + 1, cond h x (w + 1),
+// prob w x h; returns false when no pixel weighs anything (sum 0)
+bool env_tables(const float *rgb, int w, int h, float *marg, float *cond, float *prob);
 // min / max over n boxes (8 floats each) into the bound keys (6 words; as triangle_boxes's)
 cudaError_t boxes_bounds(const float *d_boxes, uint32_t n, uint32_t *d_bkeys, cudaStream_t st, int num_sms, bool init);
 

@@ -121,35 +121,27 @@ __device__ __forceinline__ float slab(const RayBox &r, float4 lo, float4 hi, flo
     return tn <= tf ? tn : __int_as_float(0x7f800000);
 }
 
-// The closest (ANY = false) or any (ANY = true) shape of one BVH in (tmin, best): the shape id,
-// or -1. A leaf's entries are tested in order; a hit at the same t as the best is not taken
-// (t >= tmax rejects), as the CPU's walk does.
-template <bool ANY>
-__device__ int32_t walk(const PtScene &S, const float4 *nodes, uint32_t root, uint32_t nnodes, const uint32_t *aux,
-                        uint32_t naux, V3 o, V3 d, float tmin, float &best, uint32_t *err) {
+// One BVH walk in (tmin, best): nodes and aux as the reference lays them out, root its root node.
+// leaf(entry) tests one leaf entry (an aux value), lowering best on a hit, and returns true to
+// end the walk (an any-hit found). Entries of a leaf in order; a hit at the same t as the best is
+// not taken (t >= tmax rejects), as the CPU's walk does. Returns true if a leaf ended it.
+template <typename Leaf>
+__device__ bool bvh_walk(const float4 *nodes, uint32_t root, uint32_t nnodes, const uint32_t *aux, uint32_t naux, V3 o,
+                         V3 d, float tmin, float &best, uint32_t *err, Leaf &&leaf) {
     RayBox rb = ray_box(o, d);
     float4 r0 = ld4(&nodes[2 * (size_t)root]), r1 = ld4(&nodes[2 * (size_t)root + 1]);
-    if (!(slab(rb, r0, r1, tmin, best) <= best)) return -1;
+    if (!(slab(rb, r0, r1, tmin, best) <= best)) return false;
     uint2 stack[PT_STACK];
     int sp = 0;
-    int32_t hit = -1;
     uint32_t a = __float_as_uint(r0.w), b = __float_as_uint(r1.w);
     while (true) {
         if (b & LEAF_BIT) {
             const uint32_t count = b & ~LEAF_BIT;
-            if (a >= naux || count > naux - a) { atomicOr(err, ST_BAD_TREE); return -1; }
-            for (uint32_t k = 0; k < count; k++) {
-                uint32_t id = __ldg(&aux[a + k]);
-                if (id >= S.nprims + S.ntris) { atomicOr(err, ST_BAD_TREE); return -1; }
-                float t;
-                if (shape_test(S, id, o, d, tmin, best, t)) {
-                    best = t;
-                    hit = (int32_t)id;
-                    if (ANY) return hit;
-                }
-            }
+            if (a >= naux || count > naux - a) { atomicOr(err, ST_BAD_TREE); return false; }
+            for (uint32_t k = 0; k < count; k++)
+                if (leaf(__ldg(&aux[a + k]))) return true;
         } else {
-            if (a >= nnodes || b >= nnodes) { atomicOr(err, ST_BAD_TREE); return -1; }
+            if (a >= nnodes || b >= nnodes) { atomicOr(err, ST_BAD_TREE); return false; }
             float4 l0 = ld4(&nodes[2 * (size_t)a]), l1 = ld4(&nodes[2 * (size_t)a + 1]);
             float4 h0 = ld4(&nodes[2 * (size_t)b]), h1 = ld4(&nodes[2 * (size_t)b + 1]);
             float t0 = slab(rb, l0, l1, tmin, best), t1 = slab(rb, h0, h1, tmin, best);
@@ -158,7 +150,7 @@ __device__ int32_t walk(const PtScene &S, const float4 *nodes, uint32_t root, ui
                 bool first0 = t0 <= t1;
                 if (sp < PT_STACK) stack[sp++] = first0 ? make_uint2(__float_as_uint(h0.w), __float_as_uint(h1.w))
                                                         : make_uint2(__float_as_uint(l0.w), __float_as_uint(l1.w));
-                else { atomicOr(err, ST_STACK_OVERFLOW); return -1; }
+                else { atomicOr(err, ST_STACK_OVERFLOW); return false; }
                 a = first0 ? __float_as_uint(l0.w) : __float_as_uint(h0.w);
                 b = first0 ? __float_as_uint(l1.w) : __float_as_uint(h1.w);
                 continue;
@@ -171,7 +163,76 @@ __device__ int32_t walk(const PtScene &S, const float4 *nodes, uint32_t root, ui
         a = e.x;
         b = e.y;
     }
+    return false;
+}
+
+// the closest (ANY = false) or any world shape (primitives, then triangles) in (tmin, best), or -1
+template <bool ANY>
+__device__ int32_t walk(const PtScene &S, const float4 *nodes, uint32_t root, uint32_t nnodes, const uint32_t *aux,
+                        uint32_t naux, V3 o, V3 d, float tmin, float &best, uint32_t *err) {
+    int32_t hit = -1;
+    bvh_walk(nodes, root, nnodes, aux, naux, o, d, tmin, best, err, [&](uint32_t id) {
+        if (id >= S.nprims + S.ntris) { atomicOr(err, ST_BAD_TREE); return true; }
+        float t;
+        if (shape_test(S, id, o, d, tmin, best, t)) {
+            best = t;
+            hit = (int32_t)id;
+            return ANY;
+        }
+        return false;
+    });
     return hit;
+}
+
+// ---- instances (scene.h:202-209; intersect_instances, accel.c:77-150) ---------------------------
+// An instance record: 8 float4 (the object -> world transform's rows, the inverse's rows, the
+// world box's lo with the mesh index's bits, hi with the material's bits: -1 the triangles' own)
+__device__ __forceinline__ V3 xpoint(const float4 *m, V3 p) {     // xform_point (scene.h)
+    float4 r0 = ld4(m), r1 = ld4(m + 1), r2 = ld4(m + 2);
+    return v3(add(add(add(mul(r0.x, p.x), mul(r0.y, p.y)), mul(r0.z, p.z)), r0.w),
+              add(add(add(mul(r1.x, p.x), mul(r1.y, p.y)), mul(r1.z, p.z)), r1.w),
+              add(add(add(mul(r2.x, p.x), mul(r2.y, p.y)), mul(r2.z, p.z)), r2.w));
+}
+__device__ __forceinline__ V3 xdir(const float4 *m, V3 d) {       // xform_dir
+    float4 r0 = ld4(m), r1 = ld4(m + 1), r2 = ld4(m + 2);
+    return v3(add(add(mul(r0.x, d.x), mul(r0.y, d.y)), mul(r0.z, d.z)),
+              add(add(mul(r1.x, d.x), mul(r1.y, d.y)), mul(r1.z, d.z)),
+              add(add(mul(r2.x, d.x), mul(r2.y, d.y)), mul(r2.z, d.z)));
+}
+__device__ __forceinline__ V3 xnormal(const float4 *inv, V3 n) {  // xform_normal: by the inverse's transpose
+    float4 r0 = ld4(inv), r1 = ld4(inv + 1), r2 = ld4(inv + 2);
+    return vnorm(v3(add(add(mul(r0.x, n.x), mul(r1.x, n.y)), mul(r2.x, n.z)),
+                    add(add(mul(r0.y, n.x), mul(r1.y, n.y)), mul(r2.y, n.z)),
+                    add(add(mul(r0.z, n.x), mul(r1.z, n.y)), mul(r2.z, n.z))));
+}
+
+// The closest (ANY = false) or any hit on the instances in (tmin, best): the instance and the
+// triangle's index in its mesh; false if none. The top level's leaves are instances; each is
+// entered with the ray in its own space (o' = inv o, d' = inv d: the same t) and its mesh's BVH walked.
+template <bool ANY>
+__device__ bool walk_instances(const PtScene &S, V3 o, V3 d, float tmin, float &best, int &inst, int &tri, uint32_t *err) {
+    bool found = false;
+    bvh_walk(S.tlas_nodes, 0, S.tlas_nnodes, S.tlas_aux, S.ninst, o, d, tmin, best, err, [&](uint32_t i) {
+        if (i >= S.ninst) { atomicOr(err, ST_BAD_TREE); return true; }
+        const float4 *rec = S.inst + 8 * (size_t)i;
+        const uint32_t mesh = __float_as_uint(ld4(rec + 6).w);
+        if (mesh >= S.nmeshes) return false;                       // (shapes: not in these scenes)
+        const uint4 mi = __ldg(&S.mesh_info[mesh]);                // root node, first triangle, triangles
+        V3 ro = xpoint(rec + 3, o), rd = xdir(rec + 3, d);
+        return bvh_walk(S.mnodes, mi.x, S.mnnodes, S.maux, S.mnaux, ro, rd, tmin, best, err, [&](uint32_t g) {
+            if (g >= S.nmtris) { atomicOr(err, ST_BAD_TREE); return true; }
+            float t;
+            if (hit_tri_t(S.mtris + 3 * (size_t)g, ro, rd, tmin, best, t)) {
+                best = t;
+                inst = (int)i;
+                tri = (int)(g - mi.y);
+                found = true;
+                return ANY;
+            }
+            return false;
+        });
+    });
+    return found;
 }
 
 // set_hit (intersect.c): point, the normal facing the ray, front_face
@@ -219,18 +280,133 @@ __device__ __forceinline__ void shape_hit(const PtScene &S, int id, V3 o, V3 d, 
     h.inst = -1;
 }
 
-// scene_intersect: the closest hit in (tmin, tmax)
+// the Hit of an instance's triangle (intersect_instance, accel.c:98-105): made in the instance's
+// space (finish_triangle with the object ray), the point in the world, the normals turned back
+__device__ __forceinline__ void instance_hit(const PtScene &S, int inst, int tri, V3 o, V3 d, float t, Hit &h) {
+    const float4 *rec = S.inst + 8 * (size_t)inst;
+    const uint4 mi = __ldg(&S.mesh_info[__float_as_uint(ld4(rec + 6).w)]);
+    V3 ro = xpoint(rec + 3, o), rd = xdir(rec + 3, d);
+    const float4 *tp = S.mtris + 3 * (size_t)(mi.y + tri);
+    float4 u = ld4(tp + 1), v = ld4(tp + 2);
+    set_hit(h, ro, rd, t, vnorm(vcross(v3(u.x, u.y, u.z), v3(v.x, v.y, v.z))));
+    h.p = vadd(o, vscale(d, t));
+    h.n = xnormal(rec + 3, h.n);
+    h.ng = xnormal(rec + 3, h.ng);
+    h.prim = tri;
+    h.inst = inst;
+}
+
+// scene_intersect (accel.c:252): the world's closest hit, then the instances' closer than it
 __device__ __forceinline__ bool scene_intersect(const PtScene &S, V3 o, V3 d, float tmin, float tmax, Hit &h, uint32_t *err) {
     float best = tmax;
-    int32_t id = walk<false>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err);
-    if (id < 0) return false;
-    shape_hit(S, id, o, d, best, h);
-    return true;
+    bool found = false;
+    if (S.nnodes) {
+        int32_t id = walk<false>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err);
+        if (id >= 0) {
+            shape_hit(S, id, o, d, best, h);
+            found = true;
+        }
+    }
+    if (S.ninst) {
+        int inst = -1, tri = -1;
+        if (walk_instances<false>(S, o, d, tmin, best, inst, tri, err)) {
+            instance_hit(S, inst, tri, o, d, best, h);
+            found = true;
+        }
+    }
+    return found;
 }
-// scene_occluded: any hit in (tmin, tmax)
+// scene_occluded (accel.c:280): any hit in (tmin, tmax), the instances first
 __device__ __forceinline__ bool scene_occluded(const PtScene &S, V3 o, V3 d, float tmin, float tmax, uint32_t *err) {
     float best = tmax;
-    return walk<true>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err) >= 0;
+    if (S.ninst) {
+        int inst, tri;
+        if (walk_instances<true>(S, o, d, tmin, best, inst, tri, err)) return true;
+    }
+    return S.nnodes && walk<true>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err) >= 0;
+}
+
+// ---- the sky (engine/scene/env.c: env_eval, env_sample, env_pdf) --------------------------------
+// rgbp: the map's radiance and each pixel's probability (env_pixel_prob), w x h; cond: each row's
+// cumulative distribution (w + 1 per row); marg: the rows' (h + 1)
+__device__ __forceinline__ void map_uv(V3 d, float &u, float &v) {
+    float y = d.y < -1.0f ? -1.0f : (d.y > 1.0f ? 1.0f : d.y);
+    float uu = add(0.5f, mul(atan2f(d.x, d.z), dvd(0.5f, PIF)));
+    u = sub(uu, floorf(uu));
+    v = mul(acosf(y), dvd(1.0f, PIF));
+}
+__device__ __forceinline__ V3 map_dir(float u, float v) {
+    float ph = mul(sub(u, 0.5f), mul(2.0f, PIF)), th = mul(v, PIF);
+    float st = sinf(th);
+    return v3(mul(st, sinf(ph)), cosf(th), mul(st, cosf(ph)));
+}
+__device__ __forceinline__ V3 env_bilerp(const PtScene &S, float u, float v) {
+    const int w = S.env_w, h = S.env_h;
+    float x = sub(mul(u, (float)w), 0.5f), y = sub(mul(v, (float)h), 0.5f);
+    int x0 = (int)floorf(x), y0 = (int)floorf(y);
+    float fx = sub(x, (float)x0), fy = sub(y, (float)y0);
+    int y1 = y0 + 1;
+    if (y0 < 0) y0 = 0;
+    if (y1 > h - 1) y1 = h - 1;
+    if (y0 > h - 1) y0 = h - 1;
+    int xa = x0 < 0 ? x0 + w : (x0 >= w ? x0 - w : x0);
+    if (xa < 0 || xa >= w) xa = ((xa % w) + w) % w;
+    int xb = xa + 1 == w ? 0 : xa + 1;
+    float4 a = ld4(&S.env_rgbp[(size_t)y0 * w + xa]), b = ld4(&S.env_rgbp[(size_t)y0 * w + xb]);
+    float4 c = ld4(&S.env_rgbp[(size_t)y1 * w + xa]), dd = ld4(&S.env_rgbp[(size_t)y1 * w + xb]);
+    float gx = sub(1.0f, fx), gy = sub(1.0f, fy);
+    return v3(add(mul(gy, add(mul(gx, a.x), mul(fx, b.x))), mul(fy, add(mul(gx, c.x), mul(fx, dd.x)))),
+              add(mul(gy, add(mul(gx, a.y), mul(fx, b.y))), mul(fy, add(mul(gx, c.y), mul(fx, dd.y)))),
+              add(mul(gy, add(mul(gx, a.z), mul(fx, b.z))), mul(fy, add(mul(gx, c.z), mul(fx, dd.z)))));
+}
+__device__ __forceinline__ V3 env_eval(const PtScene &S, V3 d) {
+    float u, v;
+    map_uv(d, u, v);
+    return vscale(env_bilerp(S, u, v), S.env_scale);
+}
+__device__ __forceinline__ int upper_bound(const float *c, int n, float x) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (__ldg(&c[mid]) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ float env_density(const PtScene &S, int x, int y, float st) {
+    float prob = ld4(&S.env_rgbp[(size_t)y * S.env_w + x]).w;
+    return dvd(mul(mul(prob, (float)S.env_w), (float)S.env_h), mul(mul(mul(2.0f, PIF), PIF), st));
+}
+__device__ __forceinline__ V3 env_sample(const PtScene &S, float u1, float u2, V3 &d, float &pdf) {
+    pdf = 0.0f;
+    if (!S.env_weighted) return v3(0, 0, 0);
+    const int w = S.env_w, h = S.env_h;
+    int y = upper_bound(S.env_marg, h, u2);
+    float m0 = __ldg(&S.env_marg[y]), m1 = __ldg(&S.env_marg[y + 1]);
+    float dv = m1 > m0 ? dvd(sub(u2, m0), sub(m1, m0)) : 0.5f;
+    const float *c = S.env_cond + (size_t)y * (w + 1);
+    int x = upper_bound(c, w, u1);
+    float c0 = __ldg(&c[x]), c1 = __ldg(&c[x + 1]);
+    float du = c1 > c0 ? dvd(sub(u1, c0), sub(c1, c0)) : 0.5f;
+    if (dv > 0.9999f) dv = 0.9999f;
+    if (du > 0.9999f) du = 0.9999f;
+    float u = dvd(add((float)x, du), (float)w), v = dvd(add((float)y, dv), (float)h);
+    float st = sinf(mul(v, PIF));
+    if (st < 1e-6f) return v3(0, 0, 0);
+    d = map_dir(u, v);
+    pdf = env_density(S, x, y, st);
+    return env_eval(S, d);
+}
+__device__ __forceinline__ float env_pdf(const PtScene &S, V3 d) {
+    if (!S.env_weighted) return 0.0f;
+    float u, v;
+    map_uv(d, u, v);
+    float st = sinf(mul(v, PIF));
+    if (st < 1e-6f) return 0.0f;
+    int x = (int)mul(u, (float)S.env_w), y = (int)mul(v, (float)S.env_h);
+    if (x > S.env_w - 1) x = S.env_w - 1;
+    if (y > S.env_h - 1) y = S.env_h - 1;
+    return env_density(S, x, y, st);
 }
 
 __device__ __forceinline__ float power_heuristic(float pa, float pb) {
@@ -283,6 +459,37 @@ __device__ __forceinline__ V3 direct_light(const PtScene &S, const Lamp &L, cons
     return vscale(vmul(f, L.le), g);
 }
 
+// sample_direct_env (tracer.c:87-101): a sky direction by its luminance, the light along it if
+// nothing is in the way, weighted against the BSDF's own sampling
+__device__ __forceinline__ V3 direct_env(const PtScene &S, const Hit &h, Bsdf &b, V3 v, int mis, float ua, float ub,
+                                         uint32_t *err, uint32_t &rays) {
+    V3 wi = v3(0, 0, 0);
+    float pdf;
+    V3 le = env_sample(S, ua, ub, wi, pdf);
+    if (!(pdf > 0.0f) || !(vmax3(le) > 0.0f)) return v3(0, 0, 0);
+    float bpdf;
+    V3 f = bsdf_eval(b, h.n, v, wi, bpdf);
+    if (!(vmax3(f) > 0.0f)) return v3(0, 0, 0);
+    rays++;
+    if (scene_occluded(S, h.p, wi, RT_EPS, 1e30f, err)) return v3(0, 0, 0);
+    float g = dvd(fabsf(vdot(h.n, wi)), pdf);
+    if (mis) g = mul(g, power_heuristic(pdf, bpdf));
+    return vscale(vmul(f, le), g);
+}
+
+// the material of what was hit (hit_material, intersect.h:23-25; scene_instance_material)
+__device__ __forceinline__ int hit_material(const PtScene &S, const Hit &h) {
+    if (h.inst >= 0) {
+        const float4 *rec = S.inst + 8 * (size_t)h.inst;
+        int m = __float_as_int(ld4(rec + 7).w);
+        if (m >= 0) return m;
+        const uint4 mi = __ldg(&S.mesh_info[__float_as_uint(ld4(rec + 6).w)]);
+        return (int)(__float_as_uint(ld4(S.mtris + 3 * (size_t)(mi.y + h.prim) + 2).w) >> 26);
+    }
+    if (h.prim < (int)S.nprims) return (int)ld4(S.prims + 6 * (size_t)h.prim + 2).w;
+    return (int)(__float_as_uint(ld4(S.tris + 3 * (size_t)(h.prim - S.nprims) + 2).w) >> 26);
+}
+
 enum { EMIT_FULL, EMIT_NONE, EMIT_MIS };
 
 // trace_path_sampled (tracer.c:364-545) without media, textures, sky and glowing-shape sampling
@@ -300,10 +507,15 @@ __device__ V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Samp
         Hit h;
         rays++;
         bool found = scene_intersect(S, ro, rd, RT_EPS, 1e30f, h, err);
-        if (!found) break;                           // escaped: black without a sky
-        const int mi = h.prim < (int)S.nprims ? (int)ld4(S.prims + 6 * (size_t)h.prim + 2).w
-                                              : (int)(__float_as_uint(ld4(S.tris + 3 * (size_t)(h.prim - S.nprims) + 2).w) >> 26);
-        const Mat m = load_mat(S.mats, mi);
+        if (!found) {                                // escaped: the sky (black without one)
+            if (S.has_env && emit != EMIT_NONE) {
+                V3 le = env_eval(S, rd);
+                if (emit == EMIT_MIS) le = vscale(le, power_heuristic(bounce_pdf, env_pdf(S, rd)));
+                radiance = vadd(radiance, vmul(thr, le));
+            }
+            break;
+        }
+        const Mat m = load_mat(S.mats, hit_material(S, h) & 63);   // (MAX_MATS 64: the buffer's size)
         if (m.type == MAT_LIGHT) {
             if (h.front) {
                 if (emit == EMIT_FULL) {
@@ -322,10 +534,21 @@ __device__ V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Samp
         if (depth >= max_depth) break;
         V3 v = vneg(vnorm(rd));
         Bsdf b = bsdf_make(m, h.front, S.tab);
-        if (bsdf_rough_part(b) && have_lamp) {
+        if (bsdf_rough_part(b)) {
             float la, lb;
-            sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
-            radiance = vadd(radiance, vmul(thr, direct_light(S, L, h, b, v, mis, lb, la, err, rays)));
+            if (have_lamp) {
+                sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
+                radiance = vadd(radiance, vmul(thr, direct_light(S, L, h, b, v, mis, lb, la, err, rays)));
+            }
+            if (S.has_env) {
+                // env_numbers (tracer.c:209-213): the lamp's pair when there is no lamp, else plain ones
+                if (!have_lamp) sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
+                else {
+                    la = rng_real(*sm.rng);
+                    lb = rng_real(*sm.rng);
+                }
+                radiance = vadd(radiance, vmul(thr, direct_env(S, h, b, v, mis, la, lb, err, rays)));
+            }
         }
         bsdf_view(b, vdot(v, h.n));
         float ur = 0.0f, ul = 0.0f, da = 0.0f, db = 0.0f;
@@ -461,13 +684,23 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
 // closest hits over shape ids (primitives, then triangles): lrc_scene_intersect for world scenes
 __global__ void __launch_bounds__(128) shapes_closest_kernel(PtScene S, const float *__restrict__ orig,
                                                              const float *__restrict__ dir, uint64_t n, float tmin, float tmax,
-                                                             int32_t *__restrict__ prim, float *__restrict__ tout, uint32_t *err) {
+                                                             int32_t *__restrict__ prim, int32_t *__restrict__ inst_out,
+                                                             float *__restrict__ tout, uint32_t *err) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     V3 o = v3(orig[3 * i], orig[3 * i + 1], orig[3 * i + 2]), d = v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
     float best = tmax;
-    int32_t id = walk<false>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err);
+    int32_t id = -1, inst = -1;
+    if (S.nnodes) id = walk<false>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err);
+    if (S.ninst) {
+        int ii = -1, tri = -1;
+        if (walk_instances<false>(S, o, d, tmin, best, ii, tri, err)) {
+            id = tri;
+            inst = ii;
+        }
+    }
     prim[i] = id;
+    if (inst_out) inst_out[i] = inst;
     tout[i] = id >= 0 ? best : -1.0f;
 }
 
@@ -520,10 +753,26 @@ cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsign
 }
 
 cudaError_t pt_intersect(const PtScene &S, const float *d_orig, const float *d_dir, uint64_t n, float tmin, float tmax,
-                         int32_t *d_prim, float *d_t, uint32_t *d_status, cudaStream_t st) {
+                         int32_t *d_prim, int32_t *d_inst, float *d_t, uint32_t *d_status, cudaStream_t st) {
     if (!n) return cudaSuccess;
-    pt::shapes_closest_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(S, d_orig, d_dir, n, tmin, tmax, d_prim, d_t,
-                                                                           d_status);
+    pt::shapes_closest_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(S, d_orig, d_dir, n, tmin, tmax, d_prim, d_inst,
+                                                                           d_t, d_status);
+    return cudaGetLastError();
+}
+
+// the instances' world boxes (records' words 24-26, 28-30) as builder boxes (8 floats each)
+__global__ void inst_boxes_kernel(const float4 *__restrict__ rec, uint32_t n, float4 *__restrict__ boxes) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 lo = __ldg(&rec[8 * (size_t)i + 6]), hi = __ldg(&rec[8 * (size_t)i + 7]);
+    boxes[2 * (size_t)i] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+    boxes[2 * (size_t)i + 1] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+}
+
+cudaError_t pt_inst_boxes(const float *d_rec, uint32_t n, float *d_boxes, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    inst_boxes_kernel<<<(n + 127) / 128, 128, 0, st>>>(reinterpret_cast<const float4 *>(d_rec), n,
+                                                       reinterpret_cast<float4 *>(d_boxes));
     return cudaGetLastError();
 }
 

@@ -93,6 +93,12 @@ def lib():
     L.lrc_default_blue_noise.argtypes = [vp]
     L.lrc_default_bsdf_tables.argtypes = [vp]
     L.lrc_trace.argtypes = [vp, vp, C.c_int32, C.c_int32, u32, u32, vp, vp, C.c_uint]
+    L.lrc_scene_set_meshes.argtypes = [vp, vp, vp, u32, C.c_uint]
+    L.lrc_scene_set_instances.argtypes = [vp, vp, u32, C.c_uint]
+    L.lrc_scene_build_instances.argtypes = [vp, C.c_int, C.c_int]
+    L.lrc_scene_set_sky.argtypes = [vp, vp, C.c_int32, C.c_int32, vp, vp, vp, f32]
+    L.lrc_scene_intersect_ex.argtypes = [vp, vp, vp, u64, f32, f32, vp, vp, vp, C.c_uint]
+    L.lrc_sky_tables.argtypes = [vp, C.c_int32, C.c_int32, vp, vp, vp]
     L.lrc_set_timing.argtypes = [vp, C.c_int]
     L.lrc_timings.argtypes = [vp, vp, vp]
     _lib = L
@@ -121,6 +127,17 @@ def trace_params(cam12, width, height, max_depth=8, mis=1, sampler=1, exact=0, s
     p.width, p.height, p.max_depth, p.mis, p.sampler, p.exact, p.seed, p.clamp = (
         width, height, max_depth, mis, sampler, exact, seed, clamp)
     return p
+
+
+def sky_tables(rgb):
+    """lrc_sky_tables (host): (marg, cond, prob) of an (h, w, 3) sky."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    marg = np.zeros(h + 1, np.float32)
+    cond = np.zeros(h * (w + 1), np.float32)
+    prob = np.zeros(w * h, np.float32)
+    lib().lrc_sky_tables(_ptr(rgb), w, h, _ptr(marg), _ptr(cond), _ptr(prob))
+    return marg, cond, prob
 
 
 def _ptr(a):
@@ -282,6 +299,41 @@ class Scene:
         tb = None if bsdf_tables is None else np.ascontiguousarray(bsdf_tables, np.float32)
         self.ctx.check(self.ctx.L.lrc_scene_set_tables(self.h, None if bn is None else _ptr(bn),
                                                        None if tb is None else _ptr(tb)))
+
+    def set_meshes(self, meshes_tris12):
+        """meshes_tris12: a list of (n_m, 12) u32 arrays (the GPU triangle layout)."""
+        counts = np.array([t.shape[0] for t in meshes_tris12], np.uint32)
+        allt = np.ascontiguousarray(np.concatenate(meshes_tris12), np.uint32) if len(meshes_tris12) else np.zeros((1, 12), np.uint32)
+        self.ctx.check(self.ctx.L.lrc_scene_set_meshes(self.h, _ptr(allt), _ptr(counts), counts.shape[0], 0))
+
+    def set_instances(self, records32):
+        records32 = np.ascontiguousarray(records32, np.float32).reshape(-1, 32)
+        self.ctx.check(self.ctx.L.lrc_scene_set_instances(self.h, _ptr(records32), records32.shape[0], 0))
+
+    def build_instances(self, mesh_builder=1, key_bits=30):
+        self.ctx.check(self.ctx.L.lrc_scene_build_instances(self.h, mesh_builder, key_bits))
+
+    def set_sky(self, rgb, scale=1.0, marg=None, cond=None, prob=None):
+        if rgb is None:
+            self.ctx.check(self.ctx.L.lrc_scene_set_sky(self.h, None, 0, 0, None, None, None, 1.0))
+            return
+        rgb = np.ascontiguousarray(rgb, np.float32)
+        h, w = rgb.shape[:2]
+        arr = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (marg, cond, prob)]
+        self.ctx.check(self.ctx.L.lrc_scene_set_sky(self.h, _ptr(rgb), w, h, *[None if a is None else _ptr(a) for a in arr],
+                                                    scale))
+
+    def intersect_ex(self, orig, dirs, tmin=0.0, tmax=1e30):
+        """(prim, inst, t) as scene_intersect's Hit."""
+        orig = np.ascontiguousarray(orig, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        n = orig.shape[0]
+        prim = np.zeros(n, np.int32)
+        inst = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        self.ctx.check(self.ctx.L.lrc_scene_intersect_ex(self.h, _ptr(orig), _ptr(dirs), n, tmin, tmax, _ptr(prim),
+                                                         _ptr(inst), _ptr(t), 0))
+        return prim, inst, t
 
     def trace(self, params, spp, accum=None, y0=0, rows=None, spp0=0):
         """lrc_trace with a host image: returns (accum (h, w, 4) sum + count, rays traced)."""

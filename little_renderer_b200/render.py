@@ -33,3 +33,22 @@ def render(ctx, scene, sc, spp=None, exact=0, seed=1, max_depth=None, sampler=1)
     acc, rays = scene.trace(p, spp)
     img = acc[..., :3] * (np.float32(1) / np.maximum(acc[..., 3:4], np.float32(1)))
     return img.astype(np.float32), rays
+
+
+def instanced_scene(ctx, sc, mesh_builder=1, key_bits=30, blue_noise=None, bsdf_tables=None, sky=True):
+    """lrc_scene of an instanced field: the ground quad (the world's one primitive), the meshes and
+    their trees, the instances and their top level, the sky, no lamp."""
+    s = native.Scene(ctx)
+    g = sc["ground"]
+    s.set_prims(W.make_quad(g["q"], g["u"], g["v"], g["material"]))
+    s.set_light(-1)
+    s.set_materials(W.material_records(sc["materials"]))
+    s.set_tables(blue_noise, bsdf_tables)
+    s.build(1, 30)
+    s.set_meshes([native.pack_tris(W.corners_to_quv(t), np.full(t.shape[0], m, np.int32))
+                  for t, m in zip(sc["meshes"], sc["mesh_mats"])])
+    s.set_instances(W.instance_records(sc))
+    s.build_instances(mesh_builder, key_bits)
+    if sky:
+        s.set_sky(sc["sky"])
+    return s

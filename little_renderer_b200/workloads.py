@@ -205,3 +205,173 @@ def camera(cam, aspect):
     ver = (v * view_h).astype(f)
     ul = (((frm - (hor * f(0.5)).astype(f)).astype(f) + (ver * f(0.5)).astype(f)).astype(f) - w).astype(f)
     return np.concatenate([frm, ul, hor, ver]).astype(f)
+
+
+# ---- the instanced scene -----------------------------------------------------------------------
+def rounded_box(target, rng):
+    """A box with rounded (bevelled) edges: a subdivided cube pushed onto a rounded box."""
+    n = max(2, int(round((target / 12.0) ** 0.5)))
+    g = np.linspace(-1, 1, n + 1)
+    faces = []
+    for axis in range(3):
+        for sgn in (-1.0, 1.0):
+            a, b = np.meshgrid(g, g, indexing="ij")
+            p = np.zeros(a.shape + (3,))
+            p[..., axis] = sgn
+            p[..., (axis + 1) % 3] = a
+            p[..., (axis + 2) % 3] = b
+            q00, q10, q01, q11 = p[:-1, :-1], p[1:, :-1], p[:-1, 1:], p[1:, 1:]
+            t1 = np.stack([q00, q10, q11], -2).reshape(-1, 3, 3)
+            t2 = np.stack([q00, q11, q01], -2).reshape(-1, 3, 3)
+            tri = np.concatenate([t1, t2])
+            if sgn < 0:
+                tri = tri[:, ::-1]
+            faces.append(tri)
+    tri = np.concatenate(faces)
+    half = rng.uniform(0.5, 1.0, 3)
+    rad = 0.25 * half.min()
+    p = tri * half
+    core = np.clip(p, -(half - rad), half - rad)
+    off = p - core
+    ln = np.linalg.norm(off, axis=-1, keepdims=True)
+    return core + off / np.maximum(ln, 1e-12) * rad
+
+
+def convex_hull_mesh(target, rng):
+    from scipy.spatial import ConvexHull
+    npts = max(8, target // 2 + 2)
+    d = rng.normal(size=(npts, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    p = d * rng.uniform(0.6, 1.0, 3) * rng.uniform(0.9, 1.0, (npts, 1))
+    hull = ConvexHull(p)
+    tri = p[hull.simplices]
+    # outward: the normal away from the centre
+    n = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    flip = (n * tri.mean(axis=1)).sum(1) < 0
+    tri[flip] = tri[flip][:, ::-1]
+    return tri
+
+
+def xform_inverse(m):
+    """xform_inverse (engine/scene/scene.c:606-623) in float32, for (n, 3, 4) transforms."""
+    f = np.float32
+    m = np.asarray(m, f)
+    M = lambda i, j: m[:, i, j]
+    det = (M(0, 0) * (M(1, 1) * M(2, 2) - M(1, 2) * M(2, 1)) - M(0, 1) * (M(1, 0) * M(2, 2) - M(1, 2) * M(2, 0))) \
+        + M(0, 2) * (M(1, 0) * M(2, 1) - M(1, 1) * M(2, 0))
+    idt = np.where(det != 0, f(1) / np.where(det != 0, det, f(1)), f(0)).astype(f)
+    r = np.zeros_like(m)
+    r[:, 0, 0] = (M(1, 1) * M(2, 2) - M(1, 2) * M(2, 1)) * idt
+    r[:, 0, 1] = (M(0, 2) * M(2, 1) - M(0, 1) * M(2, 2)) * idt
+    r[:, 0, 2] = (M(0, 1) * M(1, 2) - M(0, 2) * M(1, 1)) * idt
+    r[:, 1, 0] = (M(1, 2) * M(2, 0) - M(1, 0) * M(2, 2)) * idt
+    r[:, 1, 1] = (M(0, 0) * M(2, 2) - M(0, 2) * M(2, 0)) * idt
+    r[:, 1, 2] = (M(0, 2) * M(1, 0) - M(0, 0) * M(1, 2)) * idt
+    r[:, 2, 0] = (M(1, 0) * M(2, 1) - M(1, 1) * M(2, 0)) * idt
+    r[:, 2, 1] = (M(0, 1) * M(2, 0) - M(0, 0) * M(2, 1)) * idt
+    r[:, 2, 2] = (M(0, 0) * M(1, 1) - M(0, 1) * M(1, 0)) * idt
+    for i in range(3):
+        r[:, i, 3] = -((r[:, i, 0] * M(0, 3) + r[:, i, 1] * M(1, 3)) + r[:, i, 2] * M(2, 3))
+    return r
+
+
+def xform_box(m, lo, hi):
+    """xform_box (scene.c:629-636): the world box of a transformed box, float32; m (n, 3, 4), lo/hi (n, 3)."""
+    f = np.float32
+    m = np.asarray(m, f)
+    blo = np.full((m.shape[0], 3), f(1e30), f)
+    bhi = np.full((m.shape[0], 3), f(-1e30), f)
+    for c in range(8):
+        p = np.stack([hi[:, 0] if c & 1 else lo[:, 0], hi[:, 1] if c & 2 else lo[:, 1], hi[:, 2] if c & 4 else lo[:, 2]], 1)
+        w = np.stack([((m[:, r, 0] * p[:, 0] + m[:, r, 1] * p[:, 1]) + m[:, r, 2] * p[:, 2]) + m[:, r, 3] for r in range(3)], 1)
+        blo = np.where(blo < w, blo, w)
+        bhi = np.where(bhi > w, bhi, w)
+    return blo.astype(f), bhi.astype(f)
+
+
+def random_rotations(n, rng):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)], -1),
+                     np.stack([2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)], -1),
+                     np.stack([2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1)], 1)
+
+
+def sky(w, h, seed=3, sun_elev=45.0, sun_azim=30.0, sun_radius_deg=0.5, sun=5e4):
+    """A synthetic HDR equirect sky (rows top to bottom, as env.h): lognormal luminance (mu 0,
+    sigma 1) per pixel, faintly blue, and a sun disc of the given radius at radiance `sun`."""
+    rng = np.random.default_rng(seed)
+    lum = np.exp(rng.normal(0.0, 1.0, (h, w)))
+    rgb = np.stack([lum * 0.8, lum * 0.9, lum * 1.1], -1)
+    u = (np.arange(w) + 0.5) / w
+    v = (np.arange(h) + 0.5) / h
+    ph = (u - 0.5) * 2 * np.pi
+    th = v * np.pi
+    d = np.stack([np.sin(th)[:, None] * np.sin(ph)[None, :], np.cos(th)[:, None] * np.ones((1, w)),
+                  np.sin(th)[:, None] * np.cos(ph)[None, :]], -1)
+    el, az = np.radians(sun_elev), np.radians(sun_azim)
+    s = np.array([np.cos(el) * np.sin(az), np.sin(el), np.cos(el) * np.cos(az)])
+    rgb[(d @ s) > np.cos(np.radians(sun_radius_deg))] = sun
+    return np.ascontiguousarray(rgb, np.float32)
+
+
+def instanced_field(seed=5, n_instances=5000, n_meshes=14, tri_range=(10_000, 100_000), width=1280, height=720,
+                    sky_w=2048, sky_h=1024, spp=64, max_depth=12):
+    """The instanced scene: n_meshes procedural meshes (icospheres, rounded boxes, convex hulls)
+    with triangle counts log-uniform in tri_range, n_instances instances with random rotations at
+    positions uniform over a 40 x 40 ground quad, heights U[0, 3]; one material per mesh (GGX metal,
+    rough glass or Lambert); a grey ground quad; a synthetic sky; no lamp."""
+    rng = np.random.default_rng(seed)
+    mats, meshes = [], []
+    lo_t, hi_t = np.log(tri_range[0]), np.log(tri_range[1])
+    for m in range(n_meshes):
+        target = int(np.exp(rng.uniform(lo_t, hi_t)))
+        kind = m % 3
+        if kind == 0:
+            sub = int(np.clip(np.round(np.log(target / 20.0) / np.log(4.0)), 1, 7))
+            tri = icosphere(sub) * rng.uniform(0.5, 1.0)
+        elif kind == 1:
+            tri = rounded_box(target, rng)
+        else:
+            tri = convex_hull_mesh(target, rng)
+        meshes.append(np.ascontiguousarray(tri, np.float32))
+        mk = rng.integers(0, 3)
+        if mk == 0:
+            mats.append(pbr(rng.uniform(0.5, 0.95, 3), 1.0, rng.uniform(0.05, 0.5), 1.5, 0.0))
+        elif mk == 1:
+            mats.append(pbr(rng.uniform(0.8, 1.0, 3), 0.0, rng.uniform(0.05, 0.3), 1.5, 1.0))
+        else:
+            mats.append(diffuse(rng.uniform(0.2, 0.9, 3)))
+    mats.append(diffuse((0.5, 0.5, 0.5)))                        # the ground
+    mesh_of = rng.integers(0, n_meshes, n_instances)
+    R = random_rotations(n_instances, rng) * rng.uniform(0.4, 1.0, (n_instances, 1, 1))
+    t = np.stack([rng.uniform(0, 40, n_instances), rng.uniform(0, 3, n_instances), rng.uniform(0, 40, n_instances)], 1)
+    xf = np.concatenate([R, t[:, :, None]], 2).astype(np.float32)
+    return {"meshes": meshes, "mesh_mats": list(range(n_meshes)), "materials": mats, "mesh_of": mesh_of.astype(np.int32),
+            "xf": xf, "ground": {"q": (0.0, 0.0, 0.0), "u": (0.0, 0.0, 40.0), "v": (40.0, 0.0, 0.0),
+                                 "material": n_meshes},
+            "sky": sky(sky_w, sky_h), "camera": {"from": (20.0, 14.0, -18.0), "at": (20.0, 0.0, 20.0),
+                                                 "up": (0.0, 1.0, 0.0), "vfov": 40.0},
+            "width": width, "height": height, "spp": spp, "max_depth": max_depth}
+
+
+def instance_records(sc):
+    """32 floats per instance (lrc_scene_set_instances): xf, its inverse, box lo + mesh, box hi + material."""
+    xf = sc["xf"]
+    n = xf.shape[0]
+    inv = xform_inverse(xf)
+    mlo = np.zeros((len(sc["meshes"]), 3), np.float32)
+    mhi = np.zeros((len(sc["meshes"]), 3), np.float32)
+    for m, tri in enumerate(sc["meshes"]):
+        quv = corners_to_quv(tri)
+        mlo[m], mhi[m] = mesh_bounds(quv)
+    lo, hi = xform_box(xf, mlo[sc["mesh_of"]], mhi[sc["mesh_of"]])
+    rec = np.zeros((n, 32), np.float32)
+    rec[:, 0:12] = xf.reshape(n, 12)
+    rec[:, 12:24] = inv.reshape(n, 12)
+    rec[:, 24:27] = lo
+    rec[:, 27] = sc["mesh_of"].view(np.float32)
+    rec[:, 28:31] = hi
+    rec[:, 31] = np.full(n, -1, np.int32).view(np.float32)
+    return rec

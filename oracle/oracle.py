@@ -177,6 +177,7 @@ def ref_lib(double=False):
         lib.rb_bsdf_tables.argtypes = [_f32p]
         lib.rb_prim_data.argtypes = [vp, _f32p]
         lib.rb_camera.argtypes = [_f32p, C.c_float, C.c_float, _f32p]
+        lib.rb_env_tables.argtypes = [vp, _f32p, _f32p, _f32p]
         lib._typed = True
     return lib
 
@@ -269,6 +270,13 @@ class RefScene:
         h, w = rgb.shape[:2]
         if not self.lib.rb_set_env(self.s, rgb.reshape(-1), w, h):
             raise MemoryError("env")
+
+    def env_tables(self, w, h):
+        marg = np.zeros(h + 1, np.float32)
+        cond = np.zeros(h * (w + 1), np.float32)
+        prob = np.zeros(w * h, np.float32)
+        self.lib.rb_env_tables(self.s, marg, cond, prob)
+        return marg, cond, prob
 
     def set_accel(self):
         self.lib.rb_set_accel(self.s)

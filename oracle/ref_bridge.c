@@ -272,6 +272,16 @@ void rb_camera(const float *from_at_up, float vfov, float aspect, float *out){
     for (int k = 0; k < 4; k++){ out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
 }
 
+// the sky's sampling tables (env.h: marg h + 1, cond h x (w + 1)) and each pixel's probability
+void rb_env_tables(const void *sp, float *marg, float *cond, float *prob){
+    const Scene *s = sp;
+    const Env *e = s->env;
+    memcpy(marg, e->marg, sizeof(float) * (size_t)(e->h + 1));
+    memcpy(cond, e->cond, sizeof(float) * (size_t)e->h * (e->w + 1));
+    for (int y = 0; y < e->h; y++)
+        for (int x = 0; x < e->w; x++) prob[(size_t)y * e->w + x] = (float)env_pixel_prob(e, x, y);
+}
+
 // the blue-noise mask (sampler.c): 64 x 64 ranks
 void rb_blue_noise(uint16_t *out){ memcpy(out, blue_noise_mask(), sizeof(uint16_t) * BLUE_NOISE_SIZE * BLUE_NOISE_SIZE); }
 uint32_t rb_sampler_owen(uint32_t x, uint32_t seed){ return sampler_owen(x, seed); }
