@@ -215,6 +215,44 @@ typedef struct {
 int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0, uint32_t spp,
               float *accum, uint64_t *rays, unsigned flags);
 
+/* ---- batches: many jobs over many resident scenes, built and traced together --------------
+ * No counterpart in the reference, which traces one scene per dispatch and sizes its submits by
+ * the band scheduler (gpu_view_trace_more, engine/gpu/view_gpu.c:1081-1190); a batch replaces a
+ * sequence of lrc_trace calls. Every job's samples are the ones lrc_trace draws for the same
+ * arguments and are added into its image in lrc_trace's order: a batched image equals the
+ * lrc_trace image to the bit, in exact and fast mode. Images are device arrays; the scenes and
+ * images a batch names must outlive it (or its lrc_batch_clear). */
+typedef struct lrc_batch lrc_batch;
+#define LRC_BATCH_BUILD 4u    /* build each job's scene first (its builder and key bits; once per scene) */
+#define LRC_BATCH_GRAPH 8u    /* run as one CUDA graph: captured after the first such run (which runs
+                                 uncaptured, sizing every buffer), replayed while nothing it names changed */
+#define LRC_BATCH_ZERO 16u    /* clear each job's band of its image first */
+int lrc_batch_create(lrc_ctx *c, lrc_batch **out);
+void lrc_batch_destroy(lrc_batch *b);
+/* A job: lrc_trace(s, p, y0, rows, spp0, spp, d_accum, ..., LRC_DEVICE) as part of the batch;
+ * builder 0 (LBVH) / 1 (PLOC) with key_bits 30 / 63 builds the scene's world tree in a
+ * LRC_BATCH_BUILD run, -1 traces the tree it has (instanced scenes: -1). */
+int lrc_batch_add(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
+                  uint32_t spp, float *d_accum, int32_t builder, int32_t key_bits);
+int lrc_batch_clear(lrc_batch *b);
+int lrc_batch_jobs(const lrc_batch *b);
+/* Enqueues the run on the context's stream (lrc_sync or lrc_batch_rays wait for it). */
+int lrc_batch_run(lrc_batch *b, unsigned flags);
+/* After a run (synchronises): rays traced per job (in lrc_batch_add order) and in all; either NULL. */
+int lrc_batch_rays(lrc_batch *b, uint64_t *per_job, uint64_t *total);
+/* The trace kernel's launch shapes: shape `variant`'s threads per block, the blocks per SM its
+ * registers are capped for, and the blocks that fit per SM; returns the number of shapes, or -1. */
+int lrc_batch_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm);
+/* Sets the launch shape: variant, grid blocks (0: as many as are resident at once). */
+int lrc_batch_set_shape(lrc_batch *b, int32_t variant, int32_t grid);
+/* The autotuner: times every shape on the first sample_tasks tasks of the queue (0: a sixteenth)
+ * and keeps the fastest; its shape, grid and ns per task come back (each optional). Changes no image. */
+int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_t *grid, double *ns_per_task);
+/* The last prepared run: its tasks ((pixel, lane slot) pairs), pixels, shape, grid and whether it
+ * replayed a graph. */
+int lrc_batch_info(const lrc_batch *b, uint64_t *tasks, uint64_t *pixels, int32_t *variant, int32_t *grid,
+                   int32_t *graph_used);
+
 #ifdef __cplusplus
 }
 #endif

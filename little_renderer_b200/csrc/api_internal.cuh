@@ -1,0 +1,207 @@
+// api_internal.cuh - what the C ABI's translation units share: the context and scene objects
+// behind include/lrc.h's opaque handles, status helpers and the path tracer's view of a scene.
+#pragma once
+#include "lrc_internal.cuh"
+#include <string>
+#include <vector>
+
+using lrc::Node;
+
+struct lrc_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t own = nullptr, st = nullptr;
+    uint32_t *d_status = nullptr;
+    void *scratch = nullptr;
+    size_t scratch_cap = 0;
+    void *stage = nullptr;
+    size_t stage_cap = 0;
+    lrc::StageTimer timer;
+    std::string msg;
+};
+
+struct lrc_scene {
+    lrc_ctx *ctx = nullptr;
+    uint32_t *d_tris = nullptr;
+    size_t tris_cap = 0;
+    uint32_t ntris = 0;
+    Node *d_nodes = nullptr;
+    uint32_t *d_aux = nullptr;
+    size_t tree_cap = 0;          // items the tree buffers hold
+    uint32_t built_n = 0;         // items of the built tree (0: none)
+    float *d_boxes = nullptr;
+    size_t boxes_cap = 0;
+    uint32_t *d_small = nullptr;  // 6 bound keys, 6 bounds, 6 lo/ext
+    // the world besides its triangles (path tracing)
+    float *d_prims = nullptr;     // 24 floats per primitive
+    size_t prims_cap = 0;
+    uint32_t nprims = 0;
+    float *d_normals = nullptr;
+    size_t normals_cap = 0;
+    uint32_t nnormals = 0;
+    float *d_mats = nullptr;      // 64 materials x 16 floats
+    uint32_t nmats = 0;
+    int32_t light = -1;
+    uint16_t *d_mask = nullptr;   // 4096 ranks, then the 2112 table floats
+    float *d_tab = nullptr;
+    bool tables = false;
+    unsigned long long *d_rays = nullptr;
+    // instances: meshes' triangles and trees, records, the top level
+    uint32_t *d_mtris = nullptr;
+    uint32_t nmtris = 0;
+    std::vector<uint32_t> mesh_counts;
+    Node *d_mnodes = nullptr;
+    uint32_t *d_maux = nullptr;
+    uint4 *d_mesh_info = nullptr;
+    bool meshes_built = false;
+    float *d_inst = nullptr;
+    size_t inst_cap = 0;
+    uint32_t ninst = 0;
+    Node *d_tlas_nodes = nullptr;
+    uint32_t *d_tlas_aux = nullptr;
+    size_t tlas_cap = 0;
+    uint32_t tlas_n = 0;
+    // the sky
+    float *d_env = nullptr;       // rgbp (w x h float4), cond, marg
+    int env_w = 0, env_h = 0, env_weighted = 0;
+    float env_scale = 1;
+};
+
+namespace lrcapi {
+
+inline int fail(lrc_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess) {
+    if (c) {
+        c->msg = what;
+        if (e != cudaSuccess) {
+            c->msg += ": ";
+            c->msg += cudaGetErrorString(e);
+        }
+    }
+    return code;
+}
+
+// a CUDA error as a status: out of memory is refusable (retry after a change), the rest fatal
+inline int cuda_status(lrc_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return LRC_OK;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(c, LRC_RETRY, what, e);
+    }
+    return fail(c, LRC_E_CUDA, what, e);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+// a device buffer of at least `bytes` (grown by a quarter more; contents not kept)
+inline cudaError_t reserve(void **p, size_t *cap, size_t bytes) {
+    if (*cap >= bytes && *p) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t want = bytes + bytes / 4 + 4096;
+    cudaError_t e = cudaMalloc(p, want);
+    if (e == cudaSuccess) *cap = want;
+    return e;
+}
+
+// reads and clears the status word (synchronises the stream first)
+inline int check_status(lrc_ctx *c) {
+    cudaError_t e = cudaStreamSynchronize(c->st);
+    if (e) return cuda_status(c, e, "device work");
+    uint32_t s = 0;
+    e = cudaMemcpy(&s, c->d_status, 4, cudaMemcpyDeviceToHost);
+    if (e) return cuda_status(c, e, "status word");
+    if (s) {
+        cudaMemset(c->d_status, 0, 4);
+        if (s & lrc::ST_STACK_OVERFLOW) return fail(c, LRC_E_STACK, "a traversal stack would have overflowed (tree too deep)");
+        if (s & lrc::ST_BAD_TREE) return fail(c, LRC_E_INVALID, "a tree index out of range was met (not followed)");
+        return fail(c, LRC_E_TIMEOUT, "a bounded device wait ran out (sort look-back, PLOC look-back or grid barrier)");
+    }
+    return LRC_OK;
+}
+
+inline size_t al(size_t x) { return (x + 255) / 256 * 256; }
+
+// the BSDF tables' floats (E 32 x 32, B 32 x 32, E_avg 32, B_avg 32)
+constexpr int kBsdfTableFloats = 2112;
+
+// the path tracer's view of a scene
+inline lrc::PtScene pt_scene(const lrc_scene *s) {
+    lrc::PtScene S{};
+    S.nodes = reinterpret_cast<const float4 *>(s->d_nodes);
+    S.aux = s->d_aux;
+    S.root = 0;
+    S.nnodes = s->built_n ? 2 * s->built_n - 1 : 0;
+    S.naux = s->built_n;
+    S.prims = reinterpret_cast<const float4 *>(s->d_prims);
+    S.nprims = s->nprims;
+    S.tris = reinterpret_cast<const float4 *>(s->d_tris);
+    S.ntris = s->ntris;
+    S.normals = s->nnormals ? s->d_normals : nullptr;
+    S.mats = reinterpret_cast<const float4 *>(s->d_mats);
+    S.nmats = s->nmats;
+    S.light = s->light;
+    S.mask = s->d_mask;
+    S.tab = s->d_tab;
+    if (s->meshes_built && s->tlas_n == s->ninst && s->ninst) {
+        S.inst = reinterpret_cast<const float4 *>(s->d_inst);
+        S.ninst = s->ninst;
+        S.tlas_nodes = reinterpret_cast<const float4 *>(s->d_tlas_nodes);
+        S.tlas_aux = s->d_tlas_aux;
+        S.tlas_nnodes = 2 * s->ninst - 1;
+        S.mtris = reinterpret_cast<const float4 *>(s->d_mtris);
+        S.nmtris = s->nmtris;
+        S.mnodes = reinterpret_cast<const float4 *>(s->d_mnodes);
+        S.maux = s->d_maux;
+        uint32_t nn = 0;
+        for (uint32_t c : s->mesh_counts) nn += c ? 2 * c - 1 : 0;
+        S.mnnodes = nn;
+        S.mnaux = s->nmtris;
+        S.mesh_info = s->d_mesh_info;
+        S.nmeshes = (uint32_t)s->mesh_counts.size();
+    }
+    if (s->d_env) {
+        S.env_rgbp = reinterpret_cast<const float4 *>(s->d_env);
+        S.env_cond = s->d_env + 4 * (size_t)s->env_w * s->env_h;
+        S.env_marg = S.env_cond + (size_t)s->env_h * (s->env_w + 1);
+        S.env_w = s->env_w;
+        S.env_h = s->env_h;
+        S.has_env = 1;
+        S.env_weighted = s->env_weighted;
+        S.env_scale = s->env_scale;
+    }
+    return S;
+}
+
+// the walk's view of a scene: its tree (root 0), leaves' triangles, and the sizes it checks against
+inline lrc::TraceTables tables(const lrc_scene *s) {
+    lrc::TraceTables tt{};
+    tt.nodes = s->d_nodes;
+    tt.aux = s->d_aux;
+    tt.tris = reinterpret_cast<const float4 *>(s->d_tris);
+    tt.root = 0;
+    tt.nnodes = 2 * s->built_n - 1;
+    tt.naux = s->built_n;
+    tt.ntris = s->ntris;
+    return tt;
+}
+
+// builds the scene's world tree (triangles and primitives) on stream st with the given scratch
+// arena; with no_alloc set, a buffer too small is an error instead of a cudaMalloc (the batch's
+// graph capture)
+int scene_build_on(lrc_scene *s, int builder, int key_bits, void **scratch, size_t *scratch_cap, cudaStream_t st,
+                   lrc::StageTimer *timer, bool no_alloc);
+
+}  // namespace lrcapi
+

@@ -1,0 +1,459 @@
+// batch.cu - many render jobs (scene, image band, samples) built and traced together.
+//
+// The reference renders one scene at a time: its band scheduler (engine/gpu/view_gpu.c:1081-1190,
+// gpu_view_trace_more) sizes each submit from the measured time of a pass, and every submit is a
+// dispatch of the megakernel over one image. A batch instead holds any number of jobs over any
+// number of resident scenes, and runs them as one queue of (pixel, lane slot) tasks drained by one
+// persistent kernel (pathtrace.cu batch_kernel): the jobs are ordered by the samples a task
+// carries, most first, so the cheap tasks fill the end (longest-processing-time order), and the
+// resolve pass adds every pixel into its image in the plain kernel's order, so a batched image is
+// the plain one to the bit.
+//
+// A run may first rebuild the jobs' scenes (LBVH or PLOC), and may be replayed as one CUDA graph:
+// builds, the counters' reset, the trace kernel and the resolve pass, captured once after a run
+// that sized every buffer. The graph is captured again when a scene's buffers or sizes changed.
+//
+// The project's autotuner (lrc_batch_tune) picks the trace kernel's launch shape - threads per
+// block, the register cap and so the paths each SM keeps in flight - by timing each shape on the
+// same prefix of the queue: the measured ms per task, as the band scheduler uses its measured ms
+// per pass.
+#include "api_internal.cuh"
+#include <algorithm>
+#include <cstddef>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+using namespace lrcapi;
+
+struct lrc_batch {
+    struct Job {
+        lrc_scene *s;
+        lrc_trace_params p;
+        int32_t y0, rows;
+        uint32_t spp0, spp;
+        float *accum;
+        int32_t builder, key_bits;
+    };
+    lrc_ctx *ctx = nullptr;
+    std::vector<Job> jobs;
+    // the device side of the last prepared run
+    lrc::BatchJob *d_jobs = nullptr;
+    size_t jobs_cap = 0;
+    void *d_part = nullptr;               // partial sums, then ray counts, of every task
+    size_t part_cap = 0;
+    unsigned long long *d_ctr = nullptr;  // [0] the queue's next task, [1 + j] job j's rays
+    size_t ctr_cap = 0;
+    void *scratch = nullptr;              // the builds' scratch arena
+    size_t scratch_cap = 0;
+    std::vector<lrc::BatchJob> table;     // in queue order
+    std::vector<uint32_t> order;          // queue position -> job index
+    unsigned long long ntasks = 0, npix = 0;
+    bool prepared = false;
+    // the launch shape (tuned or set)
+    int variant = 0, grid = 0;
+    // the graph of the last GRAPH run and what it was captured for
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned graph_flags = 0;
+    std::vector<unsigned char> graph_sig;
+    int graph_used = 0;
+};
+
+namespace {
+
+constexpr unsigned kBatchFlags = LRC_BATCH_BUILD | LRC_BATCH_GRAPH | LRC_BATCH_ZERO;
+
+int group_for(const lrc_trace_params &p, uint32_t spp) {
+    if (p.exact) return 1;
+    int g = 1;
+    while (g * 2 <= (int)spp && g < 16) g *= 2;   // as lrc_trace: lanes per pixel, a power of 2 <= spp, <= 16
+    return g;
+}
+
+lrc::PtParams params_of(const lrc_batch::Job &J) {
+    lrc::PtParams P{};
+    const lrc_trace_params *p = &J.p;
+    P.W = p->width; P.H = p->height; P.y0 = J.y0; P.rows = J.rows; P.spp0 = (int)J.spp0; P.spp = (int)J.spp;
+    P.max_depth = p->max_depth; P.mis = p->mis; P.sampler_on = p->sampler; P.exact = p->exact;
+    P.group = group_for(*p, J.spp);
+    P.seed = p->seed;
+    P.clamp = p->clamp;
+    P.origin = {p->origin[0], p->origin[1], p->origin[2]};
+    P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
+    P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
+    P.vertical = {p->vertical[0], p->vertical[1], p->vertical[2]};
+    return P;
+}
+
+void destroy_graph(lrc_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->graph_sig.clear();
+}
+
+// what a captured run depends on: every job's scene view and build buffers, its band and image
+std::vector<unsigned char> signature(const lrc_batch *b) {
+    std::vector<unsigned char> sig;
+    auto put = [&](const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        sig.insert(sig.end(), c, c + n);
+    };
+    for (const lrc_batch::Job &J : b->jobs) {
+        lrc::PtScene S = pt_scene(J.s);
+        put(&S, sizeof S);
+        const void *bufs[4] = {J.s->d_boxes, J.s->d_small, J.s->d_nodes, J.s->d_aux};
+        put(bufs, sizeof bufs);
+        const void *ptrs[2] = {J.s, J.accum};
+        put(ptrs, sizeof ptrs);
+        put(&J.p, offsetof(lrc_trace_params, clamp) + sizeof(float));
+        const int32_t w[6] = {J.y0, J.rows, (int32_t)J.spp0, (int32_t)J.spp, J.builder, J.key_bits};
+        put(w, sizeof w);
+    }
+    const void *own[4] = {b->scratch, b->d_jobs, b->d_part, b->d_ctr};
+    put(own, sizeof own);
+    put(&b->variant, sizeof b->variant);
+    put(&b->grid, sizeof b->grid);
+    return sig;
+}
+
+int check_job(lrc_ctx *c, const lrc_batch::Job &J, bool will_build) {
+    lrc_scene *s = J.s;
+    if (!will_build || J.builder < 0) {
+        if (!s->built_n && !s->tlas_n) return fail(c, LRC_E_INVALID, "a job's scene has nothing built");
+    } else if (!s->ntris && !s->nprims) {
+        return fail(c, LRC_E_INVALID, "a job's scene has nothing to build");
+    }
+    if (s->ninst && s->tlas_n != s->ninst) return fail(c, LRC_E_INVALID, "a job's instances changed: lrc_scene_build_instances");
+    if (!s->d_mats || !s->nmats) return fail(c, LRC_E_INVALID, "a job's scene has no materials");
+    if (s->light >= (int32_t)s->nprims) return fail(c, LRC_E_INVALID, "a job's light is not one of its primitives");
+    return LRC_OK;
+}
+
+// the distinct scenes the run builds, each with its first job's builder and key bits
+std::vector<const lrc_batch::Job *> builds_of(const lrc_batch *b) {
+    std::vector<const lrc_batch::Job *> out;
+    for (const lrc_batch::Job &J : b->jobs) {
+        if (J.builder < 0) continue;
+        bool seen = false;
+        for (const lrc_batch::Job *o : out) seen = seen || o->s == J.s;
+        if (!seen) out.push_back(&J);
+    }
+    return out;
+}
+
+// the job table in queue order, the partial buffers and counters sized, the table uploaded
+int prepare(lrc_batch *b) {
+    lrc_ctx *c = b->ctx;
+    const size_t nj = b->jobs.size();
+    b->order.resize(nj);
+    std::iota(b->order.begin(), b->order.end(), 0u);
+    // longest-processing-time order: samples per task, then pixels, most first
+    std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t x, uint32_t y) {
+        const lrc_batch::Job &A = b->jobs[x], &B = b->jobs[y];
+        const double sa = (double)A.spp / group_for(A.p, A.spp), sb = (double)B.spp / group_for(B.p, B.spp);
+        if (sa != sb) return sa > sb;
+        return (uint64_t)A.p.width * A.rows > (uint64_t)B.p.width * B.rows;
+    });
+    b->table.assign(nj, lrc::BatchJob{});
+    unsigned long long task = 0, pix = 0;
+    for (size_t q = 0; q < nj; q++) {
+        const lrc_batch::Job &J = b->jobs[b->order[q]];
+        lrc::BatchJob &T = b->table[q];
+        T.S = pt_scene(J.s);
+        T.P = params_of(J);
+        T.task0 = task;
+        T.pix0 = pix;
+        const unsigned long long np = (unsigned long long)J.p.width * J.rows;
+        T.ntasks = np * T.P.group;
+        task += T.ntasks;
+        pix += np;
+        T.accum = reinterpret_cast<float4 *>(J.accum);
+    }
+    b->ntasks = task;
+    b->npix = pix;
+    cudaError_t e = reserve(&b->d_part, &b->part_cap, al(task * 16) + al(task * 4) + 256);
+    if (!e) e = reserve(reinterpret_cast<void **>(&b->d_ctr), &b->ctr_cap, (nj + 1) * 8 + 256);
+    if (!e) e = reserve(reinterpret_cast<void **>(&b->d_jobs), &b->jobs_cap, nj * sizeof(lrc::BatchJob) + 256);
+    if (e) return cuda_status(c, e, "batch memory");
+    char *part = static_cast<char *>(b->d_part);
+    float4 *partial = reinterpret_cast<float4 *>(part);
+    uint32_t *prays = reinterpret_cast<uint32_t *>(part + al(task * 16));
+    for (size_t q = 0; q < nj; q++) {
+        lrc::BatchJob &T = b->table[q];
+        T.partial = partial + T.task0;
+        T.prays = prays + T.task0;
+        T.rays = b->d_ctr + 1 + b->order[q];
+    }
+    e = cudaMemcpyAsync(b->d_jobs, b->table.data(), nj * sizeof(lrc::BatchJob), cudaMemcpyHostToDevice, c->st);
+    if (!e) e = cudaStreamSynchronize(c->st);   // (the table is a host vector the next prepare rewrites)
+    if (e) return cuda_status(c, e, "batch table");
+    if (b->grid <= 0) {
+        int block = 0, minb = 0;
+        int per_sm = lrc::batch_variant_shape(b->variant, &block, &minb);
+        b->grid = std::max(per_sm, 1) * c->num_sms;
+    }
+    b->prepared = true;
+    return LRC_OK;
+}
+
+// the run's device work on stream st: builds, resets, trace, resolve
+int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing) {
+    lrc_ctx *c = b->ctx;
+    if (flags & LRC_BATCH_BUILD) {
+        for (const lrc_batch::Job *J : builds_of(b)) {
+            int rc = scene_build_on(J->s, J->builder, J->key_bits, &b->scratch, &b->scratch_cap, st, nullptr, capturing);
+            if (rc) return rc;
+        }
+    }
+    const size_t nj = b->jobs.size();
+    cudaError_t e = cudaMemsetAsync(b->d_ctr, 0, (nj + 1) * 8, st);
+    if (!e && (flags & LRC_BATCH_ZERO)) {
+        for (size_t i = 0; i < nj && !e; i++) {
+            const lrc_batch::Job &J = b->jobs[i];
+            e = cudaMemsetAsync(J.accum + (size_t)J.y0 * J.p.width * 4, 0, (size_t)J.rows * J.p.width * 16, st);
+        }
+    }
+    if (!e) e = lrc::batch_trace(b->d_jobs, (uint32_t)nj, b->ntasks, b->d_ctr, c->d_status, b->variant, b->grid, st);
+    if (!e) e = lrc::batch_resolve(b->d_jobs, (uint32_t)nj, b->npix, st);
+    if (e) return cuda_status(c, e, "batch run");
+    return LRC_OK;
+}
+
+int capture(lrc_batch *b, unsigned flags) {
+    lrc_ctx *c = b->ctx;
+    destroy_graph(b);
+    cudaError_t e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+    if (e) return cuda_status(c, e, "batch graph capture");
+    int rc = enqueue(b, flags, c->st, true);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(c->st, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc;
+    }
+    if (e) return cuda_status(c, e, "batch graph capture");
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e) {
+        cudaGraphDestroy(g);
+        return cuda_status(c, e, "batch graph instantiate");
+    }
+    b->graph = g;
+    b->graph_flags = flags;
+    b->graph_sig = signature(b);
+    return LRC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrc_batch_create(lrc_ctx *c, lrc_batch **out) {
+    if (!c || !out) return LRC_E_INVALID;
+    *out = nullptr;
+    lrc_batch *b = new (std::nothrow) lrc_batch;
+    if (!b) return LRC_RETRY;
+    b->ctx = c;
+    *out = b;
+    return LRC_OK;
+}
+
+void lrc_batch_destroy(lrc_batch *b) {
+    if (!b) return;
+    DeviceGuard g(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->st);
+    destroy_graph(b);
+    cudaFree(b->d_jobs);
+    cudaFree(b->d_part);
+    cudaFree(b->d_ctr);
+    cudaFree(b->scratch);
+    delete b;
+}
+
+int lrc_batch_add(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
+                  uint32_t spp, float *d_accum, int32_t builder, int32_t key_bits) {
+    if (!b || !s || !p || !d_accum || s->ctx != b->ctx) return LRC_E_INVALID;
+    lrc_ctx *c = b->ctx;
+    if (p->width <= 0 || p->height <= 0 || y0 < 0 || rows <= 0 || y0 + rows > p->height || spp == 0)
+        return fail(c, LRC_E_INVALID, "a batch job needs a band of rows in the image and spp >= 1");
+    if (p->exact && spp0 != 0) return fail(c, LRC_E_INVALID, "exact mode starts at each pixel's first sample (spp0 = 0)");
+    if ((uint64_t)spp0 + spp >= (1ull << 31)) return fail(c, LRC_E_INVALID, "spp0 + spp must stay below 2^31");
+    if (builder >= 0 && builder != 0 && builder != 1) return fail(c, LRC_E_INVALID, "builder: -1 (none), 0 (LBVH) or 1 (PLOC)");
+    if (builder >= 0 && key_bits != 30 && key_bits != 63) return fail(c, LRC_E_INVALID, "key_bits must be 30 or 63");
+    if (s->ninst && builder >= 0) return fail(c, LRC_E_INVALID, "instanced scenes are built by lrc_scene_build_instances");
+    b->jobs.push_back({s, *p, y0, rows, spp0, spp, d_accum, builder, key_bits});
+    b->prepared = false;
+    return LRC_OK;
+}
+
+int lrc_batch_clear(lrc_batch *b) {
+    if (!b) return LRC_E_INVALID;
+    b->jobs.clear();
+    b->prepared = false;
+    return LRC_OK;
+}
+
+int lrc_batch_jobs(const lrc_batch *b) { return b ? (int)b->jobs.size() : 0; }
+
+int lrc_batch_run(lrc_batch *b, unsigned flags) {
+    if (!b || (flags & ~kBatchFlags)) return LRC_E_INVALID;
+    lrc_ctx *c = b->ctx;
+    if (b->jobs.empty()) return LRC_OK;
+    for (const lrc_batch::Job &J : b->jobs) {
+        int rc = check_job(c, J, (flags & LRC_BATCH_BUILD) != 0);
+        if (rc) return rc;
+    }
+    DeviceGuard g(c->device);
+    for (lrc_batch::Job &J : b->jobs) {
+        if (!J.s->tables) {
+            int rc = lrc_scene_set_tables(J.s, nullptr, nullptr);
+            if (rc) return rc;
+        }
+    }
+    b->graph_used = 0;
+    if ((flags & LRC_BATCH_GRAPH) && b->exec && b->prepared && b->graph_flags == flags && signature(b) == b->graph_sig) {
+        cudaError_t e = cudaGraphLaunch(b->exec, c->st);
+        if (e) return cuda_status(c, e, "batch graph launch");
+        b->graph_used = 1;
+        return LRC_OK;
+    }
+    if (flags & LRC_BATCH_BUILD) {
+        // builds first: they size the trees the table points at
+        for (const lrc_batch::Job *J : builds_of(b)) {
+            int rc = scene_build_on(J->s, J->builder, J->key_bits, &b->scratch, &b->scratch_cap, c->st, nullptr, false);
+            if (rc) return rc;
+        }
+    }
+    int rc = prepare(b);
+    if (rc) return rc;
+    rc = enqueue(b, flags & ~LRC_BATCH_BUILD, c->st, false);
+    if (rc) return rc;
+    if (flags & LRC_BATCH_GRAPH) {
+        // the next run replays this one: captured now, with every buffer sized
+        cudaError_t e = cudaStreamSynchronize(c->st);
+        if (e) return cuda_status(c, e, "batch run");
+        rc = capture(b, flags);
+        if (rc) return rc;
+    }
+    return LRC_OK;
+}
+
+int lrc_batch_rays(lrc_batch *b, uint64_t *per_job, uint64_t *total) {
+    if (!b) return LRC_E_INVALID;
+    lrc_ctx *c = b->ctx;
+    DeviceGuard g(c->device);
+    int rc = check_status(c);
+    if (rc) return rc;
+    const size_t nj = b->jobs.size();
+    std::vector<unsigned long long> r(nj, 0);
+    if (nj && b->prepared) {
+        cudaError_t e = cudaMemcpy(r.data(), b->d_ctr + 1, nj * 8, cudaMemcpyDeviceToHost);
+        if (e) return cuda_status(c, e, "batch rays");
+    }
+    uint64_t t = 0;
+    for (size_t i = 0; i < nj; i++) {
+        if (per_job) per_job[i] = r[i];
+        t += r[i];
+    }
+    if (total) *total = t;
+    return LRC_OK;
+}
+
+int lrc_batch_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm) {
+    int bl = 0, mb = 0;
+    int n = lrc::batch_variant_shape(variant, &bl, &mb);
+    if (n < 0) return -1;
+    if (block) *block = bl;
+    if (minb) *minb = mb;
+    if (per_sm) *per_sm = n;
+    return lrc::batch_variants();
+}
+
+int lrc_batch_set_shape(lrc_batch *b, int32_t variant, int32_t grid) {
+    if (!b || variant < 0 || variant >= lrc::batch_variants() || grid < 0) return LRC_E_INVALID;
+    b->variant = variant;
+    b->grid = grid;
+    if (!grid) {
+        int block = 0, minb = 0;
+        DeviceGuard g(b->ctx->device);
+        b->grid = std::max(lrc::batch_variant_shape(variant, &block, &minb), 1) * b->ctx->num_sms;
+    }
+    return LRC_OK;
+}
+
+int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_t *grid, double *ns_per_task) {
+    if (!b) return LRC_E_INVALID;
+    lrc_ctx *c = b->ctx;
+    if (b->jobs.empty()) return fail(c, LRC_E_INVALID, "an empty batch has nothing to tune on");
+    for (const lrc_batch::Job &J : b->jobs) {
+        int rc = check_job(c, J, false);
+        if (rc) return rc;
+    }
+    DeviceGuard g(c->device);
+    for (lrc_batch::Job &J : b->jobs) {
+        if (!J.s->tables) {
+            int rc = lrc_scene_set_tables(J.s, nullptr, nullptr);
+            if (rc) return rc;
+        }
+    }
+    int rc = b->prepared ? LRC_OK : prepare(b);
+    if (rc) return rc;
+    // the queue's head: the most expensive tasks (the trace kernel writes only partials, which the
+    // next run overwrites, so tuning changes no image)
+    const unsigned long long n = std::min<unsigned long long>(b->ntasks, sample_tasks ? sample_tasks : b->ntasks / 16 + 1);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    int best_v = 0, best_grid = 0;
+    cudaError_t e = cudaSuccess;
+    for (int v = 0; v < lrc::batch_variants() && !e; v++) {
+        int block = 0, minb = 0;
+        const int per_sm = lrc::batch_variant_shape(v, &block, &minb);
+        if (per_sm < 1) continue;
+        const int grid_v = per_sm * c->num_sms;
+        float ms = 0;
+        for (int rep = 0; rep < 2 && !e; rep++) {   // the first launch of a shape pays its module load
+            e = cudaMemsetAsync(b->d_ctr, 0, 8, c->st);
+            if (!e) e = cudaEventRecord(e0, c->st);
+            if (!e) e = lrc::batch_trace(b->d_jobs, (uint32_t)b->jobs.size(), rep ? n : std::min<unsigned long long>(n, 4096),
+                                         b->d_ctr, c->d_status, v, grid_v, c->st);
+            if (!e) e = cudaEventRecord(e1, c->st);
+            if (!e) e = cudaEventSynchronize(e1);
+            if (!e) e = cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (!e && ms < best) {
+            best = ms;
+            best_v = v;
+            best_grid = grid_v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e) return cuda_status(c, e, "batch tune");
+    rc = check_status(c);
+    if (rc) return rc;
+    b->variant = best_v;
+    b->grid = best_grid;
+    if (variant) *variant = best_v;
+    if (grid) *grid = best_grid;
+    if (ns_per_task) *ns_per_task = best * 1e6 / (double)n;
+    return LRC_OK;
+}
+
+int lrc_batch_info(const lrc_batch *b, uint64_t *tasks, uint64_t *pixels, int32_t *variant, int32_t *grid,
+                   int32_t *graph_used) {
+    if (!b) return LRC_E_INVALID;
+    if (tasks) *tasks = b->ntasks;
+    if (pixels) *pixels = b->npix;
+    if (variant) *variant = b->variant;
+    if (grid) *grid = b->grid;
+    if (graph_used) *graph_used = b->graph_used;
+    return LRC_OK;
+}
+
+}  // extern "C"

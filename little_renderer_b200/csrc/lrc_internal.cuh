@@ -194,6 +194,32 @@ cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsign
 cudaError_t pt_intersect(const PtScene &S, const float *d_orig, const float *d_dir, uint64_t n, float tmin, float tmax,
                          int32_t *d_prim, int32_t *d_inst, float *d_t, uint32_t *d_status, cudaStream_t st);
 cudaError_t pt_inst_boxes(const float *d_rec, uint32_t n, float *d_boxes, cudaStream_t st);
+
+// One job of a batch: a band of one image of one scene. Its tasks are (pixel, lane slot) pairs,
+// task0 + p * group + s for pixel p of the band (row-major) and slot s < group; slot s traces
+// samples spp0 + s, spp0 + s + group, ... as lane s of the plain fast kernel does, and leaves
+// its sum and sample count in partial[] and its ray count in prays[]. The resolve pass then adds
+// each pixel's slots in the fast kernel's fixed tree order into accum, so a batched image is the
+// plain one to the bit. Exact jobs have group 1 and the per-pixel stream of trace_image.
+struct BatchJob {
+    PtScene S;
+    PtParams P;
+    unsigned long long task0, ntasks;   // the job's first task in the batch, its tasks (pixels x group)
+    unsigned long long pix0;            // its first pixel among all the batch's bands (resolve pass)
+    float4 *partial;                    // ntasks (sum rgb, samples)
+    uint32_t *prays;                    // ntasks ray counts
+    float4 *accum;                      // the image (W x H)
+    unsigned long long *rays;           // the job's ray count (added to)
+};
+// the persistent trace kernel over the batch's tasks [0, ntasks) in job order (launch shape
+// `variant`, grid blocks), then the resolve pass over its npix pixels
+cudaError_t batch_trace(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, unsigned long long *d_next,
+                        uint32_t *d_status, int variant, int grid, cudaStream_t st);
+cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long long npix, cudaStream_t st);
+// the launch shapes: how many; a shape's threads per block, the blocks per SM its registers are
+// capped for, and the blocks of it that fit on one SM (-1: no such shape)
+int batch_variants();
+int batch_variant_shape(int variant, int *block, int *minb);
 // the sky's sampling tables as env_prepare makes them (host_tables.cu): marg h + 1, cond h x (w + 1),
 // prob w x h; returns false when no pixel weighs anything (sum 0)
 bool env_tables(const float *rgb, int w, int h, float *marg, float *cond, float *prob);

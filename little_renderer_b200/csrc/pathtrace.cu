@@ -492,87 +492,114 @@ __device__ __forceinline__ int hit_material(const PtScene &S, const Hit &h) {
 
 enum { EMIT_FULL, EMIT_NONE, EMIT_MIS };
 
-// trace_path_sampled (tracer.c:364-545) without media, textures, sky and glowing-shape sampling
-// (none in these scenes: each is a step of its own), counting the rays it traces
-__device__ V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err, uint32_t &rays) {
-    const int max_depth = P.max_depth, mis = P.mis;
-    V3 radiance = v3(0, 0, 0), thr = v3(1, 1, 1);
-    int emit = EMIT_FULL;
-    float bounce_pdf = 0.0f;
+// The state trace_path_sampled (tracer.c:364-545) carries from one bounce to the next: the ray,
+// the throughput, the radiance gathered so far, how the next emitter hit counts and the pdf of
+// the bounce that led to it. With the Rng (and the sample index the Sampler is made from) it is
+// all a path needs to resume, so a thread can hold one path per lane and start the next sample
+// the moment its path ends (path regeneration in the batch kernel).
+struct PathState {
+    V3 ro, rd, thr, radiance;
+    float bounce_pdf;
+    int depth, emit;
+};
+
+__device__ __forceinline__ void path_begin(int mis, V3 ro, V3 rd, PathState &ps) {
+    ps.ro = ro;
+    ps.rd = mis ? vnorm(rd) : rd;
+    ps.thr = v3(1, 1, 1);
+    ps.radiance = v3(0, 0, 0);
+    ps.bounce_pdf = 0.0f;
+    ps.depth = 0;
+    ps.emit = EMIT_FULL;
+}
+
+// One pass of trace_path_sampled's bounce loop (without media, textures and glowing-shape
+// sampling: none in these scenes), counting the rays it traces. Returns false when the path has
+// ended; ps.radiance is then its value.
+__device__ __forceinline__ bool path_bounce(const PtScene &S, int max_depth, int mis, PathState &ps, Sampler &sm,
+                                            uint32_t *err, uint32_t &rays) {
+    const int depth = ps.depth;
     const bool have_lamp = S.light >= 0;
-    Lamp L;
-    if (have_lamp) L = load_lamp(S);
-    if (mis) rd = vnorm(rd);
-    for (int depth = 0;; depth++) {
-        Hit h;
-        rays++;
-        bool found = scene_intersect(S, ro, rd, RT_EPS, 1e30f, h, err);
-        if (!found) {                                // escaped: the sky (black without one)
-            if (S.has_env && emit != EMIT_NONE) {
-                V3 le = env_eval(S, rd);
-                if (emit == EMIT_MIS) le = vscale(le, power_heuristic(bounce_pdf, env_pdf(S, rd)));
-                radiance = vadd(radiance, vmul(thr, le));
-            }
-            break;
+    Hit h;
+    rays++;
+    bool found = scene_intersect(S, ps.ro, ps.rd, RT_EPS, 1e30f, h, err);
+    if (!found) {                                    // escaped: the sky (black without one)
+        if (S.has_env && ps.emit != EMIT_NONE) {
+            V3 le = env_eval(S, ps.rd);
+            if (ps.emit == EMIT_MIS) le = vscale(le, power_heuristic(ps.bounce_pdf, env_pdf(S, ps.rd)));
+            ps.radiance = vadd(ps.radiance, vmul(ps.thr, le));
         }
-        const Mat m = load_mat(S.mats, hit_material(S, h) & 63);   // (MAX_MATS 64: the buffer's size)
-        if (m.type == MAT_LIGHT) {
-            if (h.front) {
-                if (emit == EMIT_FULL) {
-                    radiance = vadd(radiance, vmul(thr, m.emission));
-                } else if (emit == EMIT_MIS && h.inst < 0 && h.prim == S.light) {
-                    float cos_light = -vdot(L.normal, rd);
-                    if (cos_light > 0.0f) {
-                        float w = power_heuristic(bounce_pdf, light_pdf(L, mul(h.t, h.t), cos_light));
-                        radiance = vadd(radiance, vmul(thr, vscale(m.emission, w)));
-                    }
-                }
-            }
-            break;
-        }
-        if (glows(m)) radiance = vadd(radiance, vmul(thr, m.emission));   // (no glowing shapes sampled)
-        if (depth >= max_depth) break;
-        V3 v = vneg(vnorm(rd));
-        Bsdf b = bsdf_make(m, h.front, S.tab);
-        if (bsdf_rough_part(b)) {
-            float la, lb;
-            if (have_lamp) {
-                sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
-                radiance = vadd(radiance, vmul(thr, direct_light(S, L, h, b, v, mis, lb, la, err, rays)));
-            }
-            if (S.has_env) {
-                // env_numbers (tracer.c:209-213): the lamp's pair when there is no lamp, else plain ones
-                if (!have_lamp) sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
-                else {
-                    la = rng_real(*sm.rng);
-                    lb = rng_real(*sm.rng);
-                }
-                radiance = vadd(radiance, vmul(thr, direct_env(S, h, b, v, mis, la, lb, err, rays)));
-            }
-        }
-        bsdf_view(b, vdot(v, h.n));
-        float ur = 0.0f, ul = 0.0f, da = 0.0f, db = 0.0f;
-        if (depth >= RR_START || bsdf_nlobes(b) > 1) sampler_2d(sm, SAMPLE_MISC(depth), ur, ul);
-        int lobe = bsdf_pick(b, ul);
-        if (lobe >= 0 && !bsdf_lobe_delta(b, lobe)) sampler_2d(sm, SAMPLE_DIR(depth), da, db);
-        BsdfSample bs;
-        if (!bsdf_sample_lobe(b, lobe, h.n, v, da, db, bs)) break;
-        thr = vmul(thr, bs.w);
-        if (bs.delta) {
-            emit = EMIT_FULL;
-        } else {
-            bounce_pdf = bs.pdf;
-            emit = mis ? EMIT_MIS : EMIT_NONE;
-        }
-        if (depth >= RR_START) {                     // russian_roulette_u
-            float p = rmin(vmax3(thr), 0.95f);
-            if (ur >= p) break;
-            thr = vscale(thr, dvd(1.0f, p));
-        }
-        ro = h.p;
-        rd = mis ? vnorm(bs.l) : bs.l;
+        return false;
     }
-    return radiance;
+    const Mat m = load_mat(S.mats, hit_material(S, h) & 63);   // (MAX_MATS 64: the buffer's size)
+    if (m.type == MAT_LIGHT) {
+        if (h.front) {
+            if (ps.emit == EMIT_FULL) {
+                ps.radiance = vadd(ps.radiance, vmul(ps.thr, m.emission));
+            } else if (ps.emit == EMIT_MIS && h.inst < 0 && h.prim == S.light) {
+                const Lamp L = load_lamp(S);
+                float cos_light = -vdot(L.normal, ps.rd);
+                if (cos_light > 0.0f) {
+                    float w = power_heuristic(ps.bounce_pdf, light_pdf(L, mul(h.t, h.t), cos_light));
+                    ps.radiance = vadd(ps.radiance, vmul(ps.thr, vscale(m.emission, w)));
+                }
+            }
+        }
+        return false;
+    }
+    if (glows(m)) ps.radiance = vadd(ps.radiance, vmul(ps.thr, m.emission));   // (no glowing shapes sampled)
+    if (depth >= max_depth) return false;
+    V3 v = vneg(vnorm(ps.rd));
+    Bsdf b = bsdf_make(m, h.front, S.tab);
+    if (bsdf_rough_part(b)) {
+        float la, lb;
+        if (have_lamp) {
+            const Lamp L = load_lamp(S);
+            sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
+            ps.radiance = vadd(ps.radiance, vmul(ps.thr, direct_light(S, L, h, b, v, mis, lb, la, err, rays)));
+        }
+        if (S.has_env) {
+            // env_numbers (tracer.c:209-213): the lamp's pair when there is no lamp, else plain ones
+            if (!have_lamp) sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
+            else {
+                la = rng_real(*sm.rng);
+                lb = rng_real(*sm.rng);
+            }
+            ps.radiance = vadd(ps.radiance, vmul(ps.thr, direct_env(S, h, b, v, mis, la, lb, err, rays)));
+        }
+    }
+    bsdf_view(b, vdot(v, h.n));
+    float ur = 0.0f, ul = 0.0f, da = 0.0f, db = 0.0f;
+    if (depth >= RR_START || bsdf_nlobes(b) > 1) sampler_2d(sm, SAMPLE_MISC(depth), ur, ul);
+    int lobe = bsdf_pick(b, ul);
+    if (lobe >= 0 && !bsdf_lobe_delta(b, lobe)) sampler_2d(sm, SAMPLE_DIR(depth), da, db);
+    BsdfSample bs;
+    if (!bsdf_sample_lobe(b, lobe, h.n, v, da, db, bs)) return false;
+    ps.thr = vmul(ps.thr, bs.w);
+    if (bs.delta) {
+        ps.emit = EMIT_FULL;
+    } else {
+        ps.bounce_pdf = bs.pdf;
+        ps.emit = mis ? EMIT_MIS : EMIT_NONE;
+    }
+    if (depth >= RR_START) {                         // russian_roulette_u
+        float p = rmin(vmax3(ps.thr), 0.95f);
+        if (ur >= p) return false;
+        ps.thr = vscale(ps.thr, dvd(1.0f, p));
+    }
+    ps.ro = h.p;
+    ps.rd = mis ? vnorm(bs.l) : bs.l;
+    ps.depth = depth + 1;
+    return true;
+}
+
+// trace_path_sampled (tracer.c:364-545): the bounces of one path
+__device__ V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err, uint32_t &rays) {
+    PathState ps;
+    path_begin(P.mis, ro, rd, ps);
+    while (path_bounce(S, P.max_depth, P.mis, ps, sm, err, rays)) {
+    }
+    return ps.radiance;
 }
 
 // camera_ray (camera.h:38-42)
@@ -681,6 +708,150 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
     }
 }
 
+// ---- the batch: one persistent kernel over the tasks of many jobs --------------------------------
+// the job holding task t (jobs in task order; binary search over task0)
+__device__ __forceinline__ uint32_t batch_job_of(const BatchJob *__restrict__ jobs, uint32_t njobs, unsigned long long t) {
+    uint32_t lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&jobs[mid].task0) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Each lane holds one task (a pixel's lane slot) and one path of it at a time. A loop pass is
+// one bounce for every lane with a path; a lane whose path ends adds it to its task's sum and
+// starts the task's next sample, and a lane whose task is done writes it out and takes the next
+// task of the queue (one atomic per warp and pass for all such lanes). The lanes thus stay busy
+// however the path lengths and the samples per task differ, within a job and across jobs, and
+// the grid drains the queue with no launch per job and no tail per job.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__restrict__ jobs, uint32_t njobs,
+                                                      unsigned long long ntasks, unsigned long long *next, uint32_t *err) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    int j = -1;                       // the job of the lane's task (-1: none)
+    unsigned long long task = 0;
+    uint64_t pixel = 0;               // the pixel's index in its image
+    uint32_t x = 0, y = 0, slot = 0, kk = 0, kend = 0, g = 1, rays = 0;
+    V3 c = v3(0, 0, 0);
+    float cnt = 0.0f;
+    bool active = false, done = false;
+    PathState ps;
+    Rng rng;
+    rng.state = 0;
+    rng.inc = 1;
+    for (;;) {
+        if (j >= 0 && !active && kk >= kend) {       // the task is done
+            const BatchJob &J = jobs[j];
+            const unsigned long long l = task - J.task0;
+            J.partial[l] = make_float4(c.x, c.y, c.z, cnt);
+            J.prays[l] = rays;
+            j = -1;
+        }
+        const bool need = !done && j < 0;
+        const uint32_t m = __ballot_sync(0xffffffffu, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(next, (unsigned long long)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                task = base + __popc(m & lt_mask);
+                if (task >= ntasks) {
+                    done = true;
+                } else {
+                    j = (int)batch_job_of(jobs, njobs, task);
+                    const BatchJob &J = jobs[j];
+                    const unsigned long long l = task - J.task0;
+                    g = (uint32_t)J.P.group;
+                    const unsigned long long pl = l / g;
+                    slot = (uint32_t)(l - pl * g);
+                    x = (uint32_t)(pl % (uint32_t)J.P.W);
+                    y = (uint32_t)J.P.y0 + (uint32_t)(pl / (uint32_t)J.P.W);
+                    pixel = (uint64_t)y * (uint32_t)J.P.W + x;
+                    kk = (uint32_t)J.P.spp0 + slot;
+                    kend = (uint32_t)(J.P.spp0 + J.P.spp);
+                    c = v3(0, 0, 0);
+                    cnt = 0.0f;
+                    rays = 0;
+                    if (J.P.exact)                    // trace_image's per-pixel stream, all samples in order
+                        rng_seed(rng, 0x853c49e6748fea9bull ^ (pixel * 0x9E3779B97F4A7C15ull) ^ (J.P.seed * 0xD1B54A32D192ED03ull),
+                                 pixel);
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, done)) break;
+        if (j < 0) continue;                         // (only lanes that ran out of tasks)
+        const BatchJob &J = jobs[j];
+        Sampler sm{&rng, kk, (uint32_t)J.P.seed * 0x9e3779b9u, (int)x, (int)y, J.P.sampler_on, J.S.mask};
+        if (!active) {                               // the task's next sample: its camera ray
+            if (!J.P.exact)
+                rng_seed(rng, mix64(pixel * 0x9E3779B97F4A7C15ull ^ ((uint64_t)kk << 40) ^ J.P.seed), pixel);
+            float jx, jy;
+            sampler_2d(sm, 0, jx, jy);
+            float u = dvd(add((float)x, jx), (float)J.P.W), v = dvd(add((float)y, jy), (float)J.P.H);
+            V3 o, d;
+            camera_ray(J.P, u, v, o, d);
+            path_begin(J.P.mis, o, d, ps);
+            active = true;
+        }
+        if (!path_bounce(J.S, J.P.max_depth, J.P.mis, ps, sm, err, rays)) {
+            V3 s = is_number(ps.radiance) ? clamp_sample(ps.radiance, J.P.clamp) : v3(0, 0, 0);
+            c = vadd(c, s);
+            cnt += 1.0f;
+            active = false;
+            kk += g;
+        }
+    }
+}
+
+// one thread per pixel of all the batch's bands: the pixel's slots summed in the fast kernel's
+// shuffle order (pairs, then pairs of pairs, ...) and added to its image, its rays to its job
+__global__ void __launch_bounds__(128) batch_resolve_kernel(const BatchJob *__restrict__ jobs, uint32_t njobs,
+                                                            unsigned long long npix) {
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t jj = 0xffffffffu;
+    unsigned long long r = 0;
+    if (i < npix) {
+        uint32_t lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(&jobs[mid].pix0) <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        jj = lo;
+        const BatchJob &J = jobs[jj];
+        const unsigned long long pl = i - J.pix0;
+        const uint32_t g = (uint32_t)J.P.group;
+        float4 v[16];
+        for (uint32_t s = 0; s < 16; s++) {
+            if (s < g) {
+                v[s] = J.partial[pl * g + s];
+                r += J.prays[pl * g + s];
+            }
+        }
+        for (uint32_t o = 1; o < 16; o <<= 1)
+            for (uint32_t s = 0; s + o < 16; s += 2 * o)
+                if (s + o < g) {
+                    v[s].x += v[s + o].x;
+                    v[s].y += v[s + o].y;
+                    v[s].z += v[s + o].z;
+                    v[s].w += v[s + o].w;
+                }
+        const uint32_t x = (uint32_t)(pl % (uint32_t)J.P.W), y = (uint32_t)J.P.y0 + (uint32_t)(pl / (uint32_t)J.P.W);
+        float4 *a = J.accum + (uint64_t)y * (uint32_t)J.P.W + x;
+        float4 av = *a;
+        *a = make_float4(av.x + v[0].x, av.y + v[0].y, av.z + v[0].z, av.w + v[0].w);
+    }
+    // the rays of the warp's pixels, one atomic per job present
+    const uint32_t peers = __match_any_sync(0xffffffffu, jj);
+    const uint32_t sum = __reduce_add_sync(peers, (uint32_t)r);
+    if (jj != 0xffffffffu && (threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1) && sum)
+        atomicAdd(jobs[jj].rays, (unsigned long long)sum);
+}
+
 // closest hits over shape ids (primitives, then triangles): lrc_scene_intersect for world scenes
 __global__ void __launch_bounds__(128) shapes_closest_kernel(PtScene S, const float *__restrict__ orig,
                                                              const float *__restrict__ dir, uint64_t n, float tmin, float tmax,
@@ -749,6 +920,46 @@ cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsign
         const uint64_t threads = (uint64_t)P.W * P.rows * P.group;
         pt::fast_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(S, P, acc, d_rays, d_status);
     }
+    return cudaGetLastError();
+}
+
+// the batch kernel's launch shapes: threads per block and the blocks per SM its registers are
+// capped for (65536 / (threads x blocks) registers a thread)
+namespace {
+using BatchFn = void (*)(const BatchJob *, uint32_t, unsigned long long, unsigned long long *, uint32_t *);
+struct BatchVariant {
+    int block, minb;
+    BatchFn fn;
+};
+const BatchVariant kBatchVariants[] = {
+    {128, 4, pt::batch_kernel<128, 4>}, {128, 3, pt::batch_kernel<128, 3>}, {128, 5, pt::batch_kernel<128, 5>},
+    {256, 2, pt::batch_kernel<256, 2>}, {64, 8, pt::batch_kernel<64, 8>},   {256, 3, pt::batch_kernel<256, 3>},
+};
+}  // namespace
+
+int batch_variants() { return (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0])); }
+
+int batch_variant_shape(int v, int *block, int *minb) {
+    if (v < 0 || v >= batch_variants()) return -1;
+    *block = kBatchVariants[v].block;
+    *minb = kBatchVariants[v].minb;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kBatchVariants[v].fn, kBatchVariants[v].block, 0)) return -1;
+    return n;
+}
+
+cudaError_t batch_trace(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, unsigned long long *d_next,
+                        uint32_t *d_status, int variant, int grid, cudaStream_t st) {
+    if (!njobs || !ntasks) return cudaSuccess;
+    if (grid < 1 || variant < 0 || variant >= batch_variants()) return cudaErrorInvalidValue;
+    void *args[] = {(void *)&d_jobs, (void *)&njobs, (void *)&ntasks, (void *)&d_next, (void *)&d_status};
+    return cudaLaunchKernel((const void *)kBatchVariants[variant].fn, dim3(grid), dim3(kBatchVariants[variant].block), args,
+                            0, st);
+}
+
+cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long long npix, cudaStream_t st) {
+    if (!njobs || !npix) return cudaSuccess;
+    pt::batch_resolve_kernel<<<(unsigned)((npix + 127) / 128), 128, 0, st>>>(d_jobs, njobs, npix);
     return cudaGetLastError();
 }
 

@@ -13,12 +13,13 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
 LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
 LRC_DEVICE = 1
+LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO = 4, 8, 16
 
 
 def nvcc():
@@ -101,6 +102,17 @@ def lib():
     L.lrc_sky_tables.argtypes = [vp, C.c_int32, C.c_int32, vp, vp, vp]
     L.lrc_set_timing.argtypes = [vp, C.c_int]
     L.lrc_timings.argtypes = [vp, vp, vp]
+    L.lrc_batch_create.argtypes = [vp, C.POINTER(vp)]
+    L.lrc_batch_destroy.argtypes = [vp]
+    L.lrc_batch_add.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, u32, u32, vp, C.c_int32, C.c_int32]
+    L.lrc_batch_clear.argtypes = [vp]
+    L.lrc_batch_jobs.argtypes = [vp]
+    L.lrc_batch_run.argtypes = [vp, C.c_uint]
+    L.lrc_batch_rays.argtypes = [vp, vp, vp]
+    L.lrc_batch_shape.argtypes = [C.c_int32, vp, vp, vp]
+    L.lrc_batch_set_shape.argtypes = [vp, C.c_int32, C.c_int32]
+    L.lrc_batch_tune.argtypes = [vp, u64, vp, vp, vp]
+    L.lrc_batch_info.argtypes = [vp, vp, vp, vp, vp, vp]
     _lib = L
     return L
 
@@ -390,4 +402,76 @@ def pack_tris(quv, mats=None):
     out[:, 7] = 0
     m = np.zeros(n, np.uint32) if mats is None else (np.asarray(mats, np.uint32) & 63)
     out[:, 11] = m << 26
+    return out
+
+
+class Batch:
+    """A batch of jobs (lrc_batch_*): each job traces a band of one scene's image into a device
+    image; a run drains all of them through one persistent kernel (optionally building the scenes
+    first, optionally as one CUDA graph)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(ctx.L.lrc_batch_create(ctx.h, C.byref(h)))
+        self.h = h
+        self.keep = []        # the scenes and parameters the jobs name
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.lrc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, scene, params, spp, d_accum, y0=0, rows=None, spp0=0, builder=-1, key_bits=30):
+        rows = params.height if rows is None else rows
+        self.ctx.check(self.ctx.L.lrc_batch_add(self.h, scene.h, C.byref(params), y0, rows, spp0, spp,
+                                                C.c_void_p(d_accum), builder, key_bits))
+        self.keep.append((scene, params))
+        return len(self.keep) - 1
+
+    def clear(self):
+        self.ctx.check(self.ctx.L.lrc_batch_clear(self.h))
+        self.keep = []
+
+    def run(self, build=False, graph=False, zero=False):
+        flags = (LRC_BATCH_BUILD if build else 0) | (LRC_BATCH_GRAPH if graph else 0) | (LRC_BATCH_ZERO if zero else 0)
+        self.ctx.check(self.ctx.L.lrc_batch_run(self.h, flags))
+
+    def rays(self):
+        """(rays per job, total) of the last run (waits for it)."""
+        per = np.zeros(max(len(self.keep), 1), np.uint64)
+        tot = C.c_uint64()
+        self.ctx.check(self.ctx.L.lrc_batch_rays(self.h, _ptr(per), C.byref(tot)))
+        return per[:len(self.keep)], tot.value
+
+    def tune(self, sample_tasks=0):
+        v, g, ns = C.c_int32(), C.c_int32(), C.c_double()
+        self.ctx.check(self.ctx.L.lrc_batch_tune(self.h, sample_tasks, C.byref(v), C.byref(g), C.byref(ns)))
+        return v.value, g.value, ns.value
+
+    def set_shape(self, variant, grid=0):
+        self.ctx.check(self.ctx.L.lrc_batch_set_shape(self.h, variant, grid))
+
+    def info(self):
+        t, p, v, g, u = C.c_uint64(), C.c_uint64(), C.c_int32(), C.c_int32(), C.c_int32()
+        self.ctx.check(self.ctx.L.lrc_batch_info(self.h, C.byref(t), C.byref(p), C.byref(v), C.byref(g), C.byref(u)))
+        return {"tasks": t.value, "pixels": p.value, "variant": v.value, "grid": g.value, "graph_used": u.value}
+
+
+def batch_shapes():
+    """[(threads per block, register-cap blocks per SM, resident blocks per SM)] of the batch
+    kernel's launch shapes (needs a device for the last)."""
+    L = lib()
+    out = []
+    b, m, r = C.c_int32(), C.c_int32(), C.c_int32()
+    n = L.lrc_batch_shape(0, C.byref(b), C.byref(m), C.byref(r))
+    for v in range(max(n, 0)):
+        L.lrc_batch_shape(v, C.byref(b), C.byref(m), C.byref(r))
+        out.append((b.value, m.value, r.value))
     return out

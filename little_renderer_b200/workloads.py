@@ -152,6 +152,63 @@ def cornell_spheres(seed=7, n_spheres=64, width=256, height=256):
             "width": width, "height": height, "spp": 16, "max_depth": 8}
 
 
+def box_scene(seed, n_tris, width=256, height=256, spp=16, max_depth=8):
+    """A scene of the plain render's kind with about n_tris triangles: the open box and its lamp,
+    then icospheres and bevelled boxes (a quarter of the objects) with centres uniform in the box.
+    Objects grow finer with the count (icosphere subdivision 1 to 4) and their radii shrink as
+    count^(-1/3), so the box holds the same volume of them as the plain render's 64 spheres.
+    Materials as the plain render's (Lambert, GGX metal, dielectric), at most 60 distinct."""
+    S = 555.0
+    rng = np.random.default_rng(seed)
+    sub = 1 if n_tris < 4_000 else 2 if n_tris < 30_000 else 3 if n_tris < 120_000 else 4
+    unit = icosphere(sub)
+    per = unit.shape[0]
+    n_obj = max(1, (n_tris - 12) // per)
+    base_sc = cornell_spheres(seed=seed, n_spheres=0, width=width, height=height)
+    corners = [base_sc["corners"].astype(np.float64)]
+    tmat = [base_sc["tri_mats"]]
+    mats = base_sc["materials"]
+    kinds = rng.integers(0, 3, min(n_obj, 60))
+    for k in kinds:
+        if k == 0:
+            mats.append(diffuse(rng.uniform(0.2, 0.9, 3)))
+        elif k == 1:
+            mats.append(pbr(rng.uniform(0.5, 0.95, 3), 1.0, rng.uniform(0.05, 0.5), 1.5, 0.0))
+        else:
+            mats.append(glass((1.0, 1.0, 1.0), 1.5))
+    first = 4
+    shrink = (64.0 / n_obj) ** (1.0 / 3.0)
+    box_unit = rounded_box(per, rng)
+    rots = random_rotations(n_obj, rng)
+    radii = rng.uniform(0.05, 0.15, n_obj) * S * shrink
+    centres = rng.uniform(0.0, S, (n_obj, 3))
+    is_box = rng.random(n_obj) < 0.25
+    for i in range(n_obj):
+        shape = box_unit @ rots[i].T if is_box[i] else unit
+        corners.append(centres[i] + radii[i] * shape)
+        tmat.append(np.full(shape.shape[0], first + i % len(kinds), np.int32))
+    base_sc["corners"] = np.concatenate(corners).astype(np.float32)
+    base_sc["tri_mats"] = np.concatenate(tmat).astype(np.int32)
+    base_sc["materials"] = mats
+    base_sc["spp"], base_sc["max_depth"] = spp, max_depth
+    return base_sc
+
+
+def batch_scenes(n_scenes=256, seed=11, tri_range=(1_000, 200_000), resolutions=(128, 256, 512), spps=(8, 32, 128),
+                 max_depth=8):
+    """The multi-scene launch: n_scenes box scenes with triangle counts log-uniform in tri_range,
+    each with a square resolution and spp drawn uniformly from the choices, depth max_depth."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(tri_range[0]), np.log(tri_range[1])
+    out = []
+    for i in range(n_scenes):
+        n = int(np.exp(rng.uniform(lo, hi)))
+        r = int(rng.choice(resolutions))
+        spp = int(rng.choice(spps))
+        out.append(box_scene(seed * 100_003 + i, n, r, r, spp, max_depth))
+    return out
+
+
 def material_records(mats):
     """Materials as the device reads them: 16 floats each (albedo.xyz, type as int bits |
     emission.xyz, 0 | ior, metallic, roughness, transmission | 0)."""
