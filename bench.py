@@ -1,17 +1,25 @@
-"""Benchmark of the hot path: a BVH build (LBVH or PLOC over N triangles) plus one pass of
-closest-hit rays through it, on B200. Prints one JSON line (rank 0).
+"""Benchmarks of the hot path on B200. Prints one JSON line (rank 0).
 
-Workload (the builder + closest-hit configuration, synthetic and seeded): N = 4M triangles with
-centroids uniform in the unit cube, Gaussian edges (sigma = 0.002 N^-1/3), 2 % of them scaled x50;
-16M rays from a sphere of radius 2 toward uniform points of the cube. One step = triangle boxes,
-Morton codes, radix sort, hierarchy (PLOC by default: the reference's builder for meshes), then
-16M closest-hit queries. metric: Mrays/s of the whole step.
+--workload builder (default): a BVH build (LBVH or PLOC over N triangles) plus one pass of
+closest-hit rays through it. N = 4M triangles with centroids uniform in the unit cube, Gaussian
+edges (sigma = 0.002 N^-1/3), 2 % of them scaled x50; 16M rays from a sphere of radius 2 toward
+uniform points of the cube. One step = triangle boxes, Morton codes, radix sort, hierarchy (PLOC
+by default: the reference's builder for meshes), then 16M closest-hit queries. Mrays/s of the step.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--builder ploc|lbvh] [--bits 30|63]
-  python bench.py --impl reference ...   the reference's own CPU path (SAH build + scene_intersect)
+--workload batch: the multi-scene launch. 256 box scenes (icospheres and bevelled boxes in the
+open box with its lamp) with triangle counts log-uniform in [1k, 200k], resolutions from {128^2,
+256^2, 512^2}, spp from {8, 32, 128}, depth 8. One step = every scene built (LBVH, then PLOC) and
+every image traced, all in one CUDA graph of the batch engine (persistent path-regenerating trace
+kernel, launch shape picked by the autotuner). The plain path - per scene two builds and one
+lrc_trace launch, one scene after another - is timed in the same run on the same jobs; its images
+equal the batched ones to the bit (checked every run), so the RMSE is equal by construction.
+Mrays/s (closest-hit + shadow rays, counted on the device) of the step.
 
-Multi-GPU: replicas (each rank builds and traces its own scene; no collective on the data path),
-timed as the max over ranks.
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload builder|batch] ...
+  python bench.py --impl reference ...   the reference's own CPU path on this host's cores
+
+Multi-GPU: replicas (each rank builds and traces its own copy of the workload; no collective on the
+data path), timed as the max over ranks.
 """
 import argparse
 import json
@@ -28,6 +36,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "Mrays/s (build + closest-hit pass over the builder workload)"
+METRIC_BATCH = "Mrays/s (256-scene batched launch: builds + path tracing, closest-hit + shadow rays)"
 
 
 def parse():
@@ -42,7 +51,14 @@ def parse():
     ap.add_argument("--bits", type=int, default=30, choices=[30, 63])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    return ap.parse_args()
+    ap.add_argument("--workload", default="builder", choices=["builder", "batch"])
+    ap.add_argument("--scenes", type=int, default=256, help="batch: scenes (jobs)")
+    ap.add_argument("--plain-steps", type=int, default=1, help="batch: timed passes of the plain path")
+    ap.add_argument("--cpu-scenes", type=int, default=8, help="batch: scenes the CPU baseline samples")
+    ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"], help="batch: the engine")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)      # (at least 3 untimed steps before the timed ones)
+    return a
 
 
 def config(a, world):
@@ -157,10 +173,227 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def batch_config(a, world, jobs):
+    px = sum(sc["width"] * sc["height"] for sc in jobs)
+    paths = sum(sc["width"] * sc["height"] * sc["spp"] for sc in jobs)
+    tris = sum(sc["corners"].shape[0] for sc in jobs)
+    return {"workload": f"batched multi-scene launch: {len(jobs)} box scenes, triangles log-uniform in [1k, 200k] "
+                        f"({tris} in all), resolutions {{128^2, 256^2, 512^2}}, spp {{8, 32, 128}}, depth 8; builds "
+                        "LBVH then PLOC per scene; one CUDA graph", "scenes": len(jobs), "triangles": tris,
+            "pixels": px, "paths": paths, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (all scenes' triangles and trees, images and per-task sums > 126 MB)"}
+
+
+def ref_box_scene(O, sc):
+    ref = O.RefScene()
+    for m in sc["materials"]:
+        ref.material(m["type"], m["albedo"], m["emission"], m["ior"], m["metallic"], m["roughness"], m["transmission"])
+    ref.triangles(sc["corners"], sc["tri_mats"])
+    lamp = sc["lamp"]
+    ref.quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"], light=True)
+    return ref
+
+
+def batch_cpu_sample(a, jobs, seconds=20.0):
+    """The reference's CPU path tracer (scene_set_accel + trace_image, all host cores) on a fixed
+    seeded subset of the jobs: the first cpu_scenes scenes, each built and a band of its rows traced
+    at the job's spp (about 300k paths per scene, fewer once `seconds` are spent). Returns
+    (Mrays/s, cores, sample text)."""
+    from oracle import oracle as O
+    lib = O.ref_lib()
+    cores = lib.rb_max_threads()
+    rays = 0
+    t_all = 0.0
+    done = []
+    for i, sc in enumerate(jobs[:a.cpu_scenes]):
+        if t_all > seconds:
+            break
+        ref = ref_box_scene(O, sc)
+        c = sc["camera"]
+        fau = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
+        w, h, spp = sc["width"], sc["height"], sc["spp"]
+        rows = max(1, min(h, 300_000 // (w * spp)))
+        t0 = time.perf_counter()
+        ref.set_accel()
+        _, (closest, shadow) = ref.trace_image(fau, c["vfov"], w, h, spp, i, sc["max_depth"], y0=h // 2 - rows // 2,
+                                               rows=rows)
+        t_all += time.perf_counter() - t0
+        rays += closest + shadow
+        done.append(f"{sc['corners'].shape[0]} tris {w}x{rows} rows x {spp} spp")
+        ref.close()
+    return rays / t_all / 1e6, cores, (f"the first {len(done)} scenes of the batch (scene_set_accel, 4-wide SAH, + "
+                                       f"trace_image of a central band): " + "; ".join(done) +
+                                       f"; {rays} rays in {t_all:.1f} s; the whole batch extrapolated at that rate")
+
+
+def run_reference_batch(a):
+    """--impl reference --workload batch: the reference's CPU path tracer on this host's cores, each
+    step the bounded sample of batch_cpu_sample (the whole batch would take hours)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from little_renderer_b200 import workloads as W
+    jobs = W.batch_scenes(a.scenes, seed=11)
+    vals = []
+    for step in range(a.warmup + a.steps):
+        v, cores, sample = batch_cpu_sample(a, jobs, seconds=4.0)
+        if step >= a.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    line = {"metric": METRIC_BATCH, "value": v, "unit": "Mrays/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "impl": "reference", "config": batch_config(a, 1, jobs),
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(a):
+    import torch
+    import little_renderer_b200 as L
+    from little_renderer_b200 import render as R, workloads as W
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    jobs = W.batch_scenes(a.scenes, seed=11 + rank)
+    ctx = L.Context(local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    scenes = [R.world_scene(ctx, sc, 0) for sc in jobs]
+    params = [L.native.trace_params(R.camera12(sc), sc["width"], sc["height"], sc["max_depth"], 1, 1, 0, 1000 + i)
+              for i, sc in enumerate(jobs)]
+    imgs = [torch.zeros(sc["height"], sc["width"], 4, device=dev) for sc in jobs]
+    torch.cuda.synchronize()
+
+    def plain_step():
+        for s, p, img, sc in zip(scenes, params, imgs, jobs):
+            s.build(0, 30)
+            s.build(1, 30)
+            s.trace_device(p, sc["spp"], img.data_ptr())
+
+    def timed(fn, n):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.sync()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # the plain path: one pass for its images (and its warm-up), then the timed passes
+    for img in imgs:
+        img.zero_()
+    plain_step()
+    ctx.sync()
+    torch.cuda.synchronize()
+    plain_imgs = [img.cpu() for img in imgs]
+    plain_ms = timed(plain_step, a.plain_steps) / a.plain_steps
+
+    def builds_step():
+        for s in scenes:
+            s.build(0, 30)
+            s.build(1, 30)
+
+    build_ms = timed(builds_step, 1)
+
+    # the batch: every job with LBVH-then-PLOC builds; the autotuner's shape; one graph per step
+    b = L.native.Batch(ctx)
+    b.set_engine(1 if a.engine == "wavefront" else 0)
+    for s, p, img, sc in zip(scenes, params, imgs, jobs):
+        b.add(s, p, sc["spp"], img.data_ptr(), builder=2, key_bits=30)
+    b.run(build=True, zero=True)
+    variant, grid, ns_task = b.tune()
+    shapes = L.native.wavefront_shapes() if a.engine == "wavefront" else L.native.batch_shapes()
+    for _ in range(a.warmup):
+        b.run(build=True, graph=True, zero=True)
+    ctx.sync()
+    torch.cuda.synchronize()
+    batch_imgs = [img.cpu() for img in imgs]
+    same = all(torch.equal(x, y) for x, y in zip(plain_imgs, batch_imgs))
+    per_job, rays = b.rays()
+    clk = Clocks(local)
+    ms = timed(lambda: b.run(build=True, graph=True, zero=True), a.steps)
+    clocks = clk.stop()
+    info = b.info()
+    ms_step = ms / a.steps
+    value = world * rays * a.steps / (ms / 1e3) / 1e6
+    plain_value = world * rays / (plain_ms / 1e3) / 1e6
+
+    # end to end through the public API with host buffers: every scene's triangles copied in from
+    # pinned memory, the batch run (builds + trace), every image copied out, inside each step
+    pins = [torch.from_numpy(L.pack_tris(W.corners_to_quv(sc["corners"]), sc["tri_mats"]).view(np.int32)).pin_memory()
+            for sc in jobs]
+    host_tris = [p.numpy().view(np.uint32) for p in pins]
+    outs = [torch.empty(sc["height"], sc["width"], 4).pin_memory() for sc in jobs]
+
+    def e2e_step():
+        for t, s in zip(host_tris, scenes):
+            s.set_triangles(t)
+        b.run(build=True, graph=True, zero=True)
+        for o, img in zip(outs, imgs):
+            o.copy_(img, non_blocking=True)
+
+    e2e_step()
+    e2e_steps = max(1, min(a.steps, 3))
+    e_ms = timed(e2e_step, e2e_steps) / e2e_steps
+    e2e = {"value": world * rays / (e_ms / 1e3) / 1e6, "unit": "Mrays/s",
+           "h2d_bytes_per_step": int(sum(p.numel() * 4 for p in pins)),
+           "d2h_bytes_per_step": int(sum(o.numel() * 4 for o in outs)), "ms_per_step": e_ms}
+
+    peak, peak_kind = peaks()
+    line = {"metric": METRIC_BATCH, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": batch_config(a, world, jobs),
+            "clocks": clocks, "e2e": e2e,
+            "gpu_launches": a.steps * (len(jobs) * (5 + 4 + 6) + 2),
+            "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_step": plain_ms, "builds_ms": build_ms,
+                      "what": "per scene: LBVH build, PLOC build, one lrc_trace launch; scenes one after another"},
+            "speedup_vs_plain": value / plain_value, "images_equal_plain": bool(same),
+            "rays_per_step": int(rays), "paths_per_step": int(sum(sc["width"] * sc["height"] * sc["spp"] for sc in jobs)),
+            "batch": {"engine": a.engine, "tasks": info["tasks"],
+                      "shape": dict(zip(("block", "minb", "per_sm"), shapes[variant])),
+                      ("paths_in_flight" if a.engine == "wavefront" else "grid"): grid,
+                      "ns_per_task_tuned": ns_task, "graph_replayed": info["graph_used"]},
+            "roofline": {"bound": "hbm", "kernel": "batch_kernel", "achieved": None, "peak": peak, "unit": "GB/s",
+                         "peak_kind": peak_kind, "frac": None, "traffic": None,
+                         "note": "latency-bound traversal over L2-resident scenes; DRAM traffic from the ncu summary"}}
+    if rank == 0 and world == 1 and not a.no_cpu:
+        v, cores, sample = batch_cpu_sample(a, jobs)
+        line["cpu_baseline"] = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "reference", "sample": sample}
+    b.close()
+    for s in scenes:
+        s.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
-        run_reference(a)
+        run_reference_batch(a) if a.workload == "batch" else run_reference(a)
+        return
+    if a.workload == "batch":
+        run_batch(a)
         return
     import torch
     import little_renderer_b200 as L

@@ -230,8 +230,9 @@ typedef struct lrc_batch lrc_batch;
 int lrc_batch_create(lrc_ctx *c, lrc_batch **out);
 void lrc_batch_destroy(lrc_batch *b);
 /* A job: lrc_trace(s, p, y0, rows, spp0, spp, d_accum, ..., LRC_DEVICE) as part of the batch;
- * builder 0 (LBVH) / 1 (PLOC) with key_bits 30 / 63 builds the scene's world tree in a
- * LRC_BATCH_BUILD run, -1 traces the tree it has (instanced scenes: -1). */
+ * builder 0 (LBVH) / 1 (PLOC) / 2 (LBVH, then PLOC: the PLOC tree is traced) with key_bits 30 / 63
+ * builds the scene's world tree in a LRC_BATCH_BUILD run, -1 traces the tree it has (instanced
+ * scenes: -1). A scene in several jobs is built once, by its first job's builder. */
 int lrc_batch_add(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
                   uint32_t spp, float *d_accum, int32_t builder, int32_t key_bits);
 int lrc_batch_clear(lrc_batch *b);
@@ -245,8 +246,20 @@ int lrc_batch_rays(lrc_batch *b, uint64_t *per_job, uint64_t *total);
 int lrc_batch_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm);
 /* Sets the launch shape: variant, grid blocks (0: as many as are resident at once). */
 int lrc_batch_set_shape(lrc_batch *b, int32_t variant, int32_t grid);
-/* The autotuner: times every shape on the first sample_tasks tasks of the queue (0: a sixteenth)
- * and keeps the fastest; its shape, grid and ns per task come back (each optional). Changes no image. */
+/* The engine: 1 (the default) the wavefront - a pool of paths in flight advanced by four kernels
+ * per bounce (advance / closest hit / shade / shadow rays) looped inside one CUDA graph; 0 the
+ * persistent megakernel (one path per lane, the next sample started when a path ends). Both give
+ * the same images. */
+int lrc_batch_set_engine(lrc_batch *b, int32_t engine);
+/* The wavefront's size (paths in flight: a multiple of 256) and its closest-hit / shadow kernels'
+ * launch shape (lrc_batch_wavefront_shape describes them as lrc_batch_shape does). */
+int lrc_batch_set_wavefront(lrc_batch *b, uint32_t slots, int32_t variant);
+int lrc_batch_wavefront_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm);
+int lrc_batch_engine(const lrc_batch *b, int32_t *engine, uint32_t *slots, int32_t *wf_variant);
+/* The autotuner: times the engine's shapes on the first sample_tasks tasks of the queue (0: a
+ * sixteenth) and keeps the fastest - the megakernel's launch shape (variant, grid blocks), or the
+ * wavefront's size and launch shape (variant, grid = paths in flight) - and the ns per task (each
+ * optional). Changes no image. */
 int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_t *grid, double *ns_per_task);
 /* The last prepared run: its tasks ((pixel, lane slot) pairs), pixels, shape, grid and whether it
  * replayed a graph. */

@@ -126,6 +126,7 @@ inline int check_status(lrc_ctx *c) {
         cudaMemset(c->d_status, 0, 4);
         if (s & lrc::ST_STACK_OVERFLOW) return fail(c, LRC_E_STACK, "a traversal stack would have overflowed (tree too deep)");
         if (s & lrc::ST_BAD_TREE) return fail(c, LRC_E_INVALID, "a tree index out of range was met (not followed)");
+        if (s & lrc::ST_LOOP) return fail(c, LRC_E_TIMEOUT, "the wavefront loop ran past its bound (stopped)");
         return fail(c, LRC_E_TIMEOUT, "a bounded device wait ran out (sort look-back, PLOC look-back or grid barrier)");
     }
     return LRC_OK;

@@ -51,8 +51,15 @@ struct lrc_batch {
     std::vector<uint32_t> order;          // queue position -> job index
     unsigned long long ntasks = 0, npix = 0;
     bool prepared = false;
-    // the launch shape (tuned or set)
+    // the engine: 0 the persistent megakernel (launch shape variant, grid blocks), 1 the wavefront
+    // (wf_slots paths in flight, closest-hit / shadow kernels' shape wf_variant); tuned or set
+    int engine = 1;
     int variant = 0, grid = 0;
+    int wf_variant = 0;
+    uint32_t wf_slots = 1u << 20;
+    void *d_wf = nullptr;
+    size_t wf_cap = 0;
+    cudaStream_t body = nullptr;          // the stream the wavefront loop's body is captured on
     // the graph of the last GRAPH run and what it was captured for
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -95,15 +102,28 @@ void destroy_graph(lrc_batch *b) {
     b->graph_sig.clear();
 }
 
+// the path tracer's view of a job's scene once the run's builds are done (a build makes the tree
+// over all its shapes)
+lrc::PtScene view_of(const lrc_batch::Job &J, bool building) {
+    lrc::PtScene S = pt_scene(J.s);
+    if (building && J.builder >= 0) {
+        const uint32_t n = J.s->ntris + J.s->nprims;
+        S.nnodes = n ? 2 * n - 1 : 0;
+        S.naux = n;
+    }
+    return S;
+}
+
 // what a captured run depends on: every job's scene view and build buffers, its band and image
-std::vector<unsigned char> signature(const lrc_batch *b) {
+std::vector<unsigned char> signature(const lrc_batch *b, unsigned flags) {
     std::vector<unsigned char> sig;
     auto put = [&](const void *p, size_t n) {
         const unsigned char *c = static_cast<const unsigned char *>(p);
         sig.insert(sig.end(), c, c + n);
     };
+    put(&flags, sizeof flags);
     for (const lrc_batch::Job &J : b->jobs) {
-        lrc::PtScene S = pt_scene(J.s);
+        lrc::PtScene S = view_of(J, (flags & LRC_BATCH_BUILD) != 0);
         put(&S, sizeof S);
         const void *bufs[4] = {J.s->d_boxes, J.s->d_small, J.s->d_nodes, J.s->d_aux};
         put(bufs, sizeof bufs);
@@ -113,10 +133,10 @@ std::vector<unsigned char> signature(const lrc_batch *b) {
         const int32_t w[6] = {J.y0, J.rows, (int32_t)J.spp0, (int32_t)J.spp, J.builder, J.key_bits};
         put(w, sizeof w);
     }
-    const void *own[4] = {b->scratch, b->d_jobs, b->d_part, b->d_ctr};
+    const void *own[5] = {b->scratch, b->d_jobs, b->d_part, b->d_ctr, b->d_wf};
     put(own, sizeof own);
-    put(&b->variant, sizeof b->variant);
-    put(&b->grid, sizeof b->grid);
+    const int shape[5] = {b->engine, b->variant, b->grid, b->wf_variant, (int)b->wf_slots};
+    put(shape, sizeof shape);
     return sig;
 }
 
@@ -143,6 +163,14 @@ std::vector<const lrc_batch::Job *> builds_of(const lrc_batch *b) {
         if (!seen) out.push_back(&J);
     }
     return out;
+}
+
+// the job's scene built: builder 0 LBVH, 1 PLOC, 2 LBVH and then PLOC (the PLOC tree is kept)
+int build_job(lrc_batch *b, const lrc_batch::Job *J, cudaStream_t st, bool capturing) {
+    const int first = J->builder == 2 ? 0 : J->builder;
+    int rc = scene_build_on(J->s, first, J->key_bits, &b->scratch, &b->scratch_cap, st, nullptr, capturing);
+    if (!rc && J->builder == 2) rc = scene_build_on(J->s, 1, J->key_bits, &b->scratch, &b->scratch_cap, st, nullptr, capturing);
+    return rc;
 }
 
 // the job table in queue order, the partial buffers and counters sized, the table uploaded
@@ -178,6 +206,8 @@ int prepare(lrc_batch *b) {
     cudaError_t e = reserve(&b->d_part, &b->part_cap, al(task * 16) + al(task * 4) + 256);
     if (!e) e = reserve(reinterpret_cast<void **>(&b->d_ctr), &b->ctr_cap, (nj + 1) * 8 + 256);
     if (!e) e = reserve(reinterpret_cast<void **>(&b->d_jobs), &b->jobs_cap, nj * sizeof(lrc::BatchJob) + 256);
+    if (!e && b->engine == 1) e = reserve(&b->d_wf, &b->wf_cap, lrc::wf_bytes(b->wf_slots));
+    if (!e && b->engine == 1 && !b->body) e = cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking);
     if (e) return cuda_status(c, e, "batch memory");
     char *part = static_cast<char *>(b->d_part);
     float4 *partial = reinterpret_cast<float4 *>(part);
@@ -200,52 +230,162 @@ int prepare(lrc_batch *b) {
     return LRC_OK;
 }
 
-// the run's device work on stream st: builds, resets, trace, resolve
-int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing) {
+// a bound on the wavefront's passes for the first `limit` tasks: each slot runs at most
+// ceil(limit / slots) tasks one after another, each of at most (samples a task holds) paths of at
+// most max_depth + 1 bounces, plus one pass to start and one to end each task
+uint32_t max_passes(const lrc_batch *b, unsigned long long limit) {
+    unsigned long long per_task = 1, depth = 1;
+    for (const lrc_batch::Job &J : b->jobs) {
+        const int g = group_for(J.p, J.spp);
+        per_task = std::max<unsigned long long>(per_task, (J.spp + g - 1) / g);
+        depth = std::max<unsigned long long>(depth, (unsigned long long)J.p.max_depth + 1);
+    }
+    const unsigned long long rounds = (limit + b->wf_slots - 1) / b->wf_slots + 1;
+    const unsigned long long bound = rounds * (per_task * (depth + 1) + 2) + 16;
+    return (uint32_t)std::min<unsigned long long>(bound, 0xffffffffull);
+}
+
+// the run's device work on stream st: builds (with_builds), resets, trace, resolve (with_resolve;
+// without it nothing but the per-task sums is written: the autotuner's runs). The wavefront's loop
+// can only be captured (st capturing).
+int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool with_builds, bool with_resolve,
+            unsigned long long limit) {
     lrc_ctx *c = b->ctx;
-    if (flags & LRC_BATCH_BUILD) {
+    if (with_builds && (flags & LRC_BATCH_BUILD)) {
         for (const lrc_batch::Job *J : builds_of(b)) {
-            int rc = scene_build_on(J->s, J->builder, J->key_bits, &b->scratch, &b->scratch_cap, st, nullptr, capturing);
+            int rc = build_job(b, J, st, capturing);
             if (rc) return rc;
         }
     }
     const size_t nj = b->jobs.size();
-    cudaError_t e = cudaMemsetAsync(b->d_ctr, 0, (nj + 1) * 8, st);
-    if (!e && (flags & LRC_BATCH_ZERO)) {
+    cudaError_t e = with_resolve ? cudaMemsetAsync(b->d_ctr, 0, (nj + 1) * 8, st) : cudaSuccess;
+    if (!e && with_resolve && (flags & LRC_BATCH_ZERO)) {
         for (size_t i = 0; i < nj && !e; i++) {
             const lrc_batch::Job &J = b->jobs[i];
             e = cudaMemsetAsync(J.accum + (size_t)J.y0 * J.p.width * 4, 0, (size_t)J.rows * J.p.width * 16, st);
         }
     }
-    if (!e) e = lrc::batch_trace(b->d_jobs, (uint32_t)nj, b->ntasks, b->d_ctr, c->d_status, b->variant, b->grid, st);
-    if (!e) e = lrc::batch_resolve(b->d_jobs, (uint32_t)nj, b->npix, st);
+    if (!e && b->engine == 0)
+        e = lrc::batch_trace(b->d_jobs, (uint32_t)nj, limit, b->d_ctr, c->d_status, b->variant, b->grid, st);
+    if (!e && b->engine == 1) {
+        if (!capturing) return fail(c, LRC_E_INVALID, "the wavefront runs as a captured graph");
+        const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
+        e = lrc::wf_capture_loop(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, c->num_sms,
+                                 max_passes(b, limit), st, b->body);
+    }
+    if (!e && with_resolve) e = lrc::batch_resolve(b->d_jobs, (uint32_t)nj, b->npix, st);
     if (e) return cuda_status(c, e, "batch run");
     return LRC_OK;
 }
 
-int capture(lrc_batch *b, unsigned flags) {
+// captures enqueue(...) into a new executable graph
+int capture_exec(lrc_batch *b, unsigned flags, bool with_builds, bool with_resolve, unsigned long long limit,
+                 cudaGraph_t *g_out, cudaGraphExec_t *x_out) {
     lrc_ctx *c = b->ctx;
-    destroy_graph(b);
+    *g_out = nullptr;
+    *x_out = nullptr;
     cudaError_t e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
     if (e) return cuda_status(c, e, "batch graph capture");
-    int rc = enqueue(b, flags, c->st, true);
+    int rc = enqueue(b, flags, c->st, true, with_builds, with_resolve, limit);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(c->st, &g);
-    if (rc) {
+    if (rc || e) {
         if (g) cudaGraphDestroy(g);
         cudaGetLastError();
-        return rc;
+        return rc ? rc : cuda_status(c, e, "batch graph capture");
     }
-    if (e) return cuda_status(c, e, "batch graph capture");
-    e = cudaGraphInstantiate(&b->exec, g, 0);
+    e = cudaGraphInstantiate(x_out, g, 0);
     if (e) {
         cudaGraphDestroy(g);
         return cuda_status(c, e, "batch graph instantiate");
     }
-    b->graph = g;
-    b->graph_flags = flags;
-    b->graph_sig = signature(b);
+    *g_out = g;
     return LRC_OK;
+}
+
+// the run's graph, kept for replays: builds inside when GRAPH (the megakernel engine captures only
+// GRAPH runs; the wavefront's trace is always a graph, its builds plain launches without GRAPH)
+int capture(lrc_batch *b, unsigned flags) {
+    destroy_graph(b);
+    int rc = capture_exec(b, flags, (flags & LRC_BATCH_GRAPH) != 0, true, b->ntasks, &b->graph, &b->exec);
+    if (rc) return rc;
+    b->graph_flags = flags;
+    b->graph_sig = signature(b, flags);
+    return LRC_OK;
+}
+
+// the wavefront's autotuner: the time of the first n tasks at each wavefront size (paths in
+// flight), then at each closest-hit / shadow launch shape at the best size; keeps the fastest
+int tune_wavefront(lrc_batch *b, unsigned long long n, int32_t *variant, int32_t *slots, double *ns_per_task) {
+    lrc_ctx *c = b->ctx;
+    const uint32_t sizes[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22};
+    uint32_t top = 1u << 18;
+    for (uint32_t m : sizes)
+        if ((unsigned long long)m / 2 < n) top = m;   // (no larger than the tasks need)
+    cudaError_t e = reserve(&b->d_wf, &b->wf_cap, lrc::wf_bytes(top));
+    if (!e && !b->body) e = cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking);
+    if (e) return cuda_status(c, e, "batch tune memory");
+    destroy_graph(b);                                // (its buffers may move)
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int keep_v = b->wf_variant;
+    const uint32_t keep_m = b->wf_slots;
+    auto time_one = [&](uint32_t m, int v, float &ms) -> int {
+        b->wf_slots = m;
+        b->wf_variant = v;
+        cudaGraph_t g;
+        cudaGraphExec_t x;
+        int rc = capture_exec(b, 0, false, false, n, &g, &x);
+        if (rc) return rc;
+        cudaError_t err = cudaSuccess;
+        for (int rep = 0; rep < 2 && !err; rep++) {   // (the first run pays the kernels' module load)
+            err = cudaEventRecord(e0, c->st);
+            if (!err) err = cudaGraphLaunch(x, c->st);
+            if (!err) err = cudaEventRecord(e1, c->st);
+            if (!err) err = cudaEventSynchronize(e1);
+            if (!err) err = cudaEventElapsedTime(&ms, e0, e1);
+        }
+        cudaGraphExecDestroy(x);
+        cudaGraphDestroy(g);
+        return err ? cuda_status(c, err, "batch tune") : LRC_OK;
+    };
+    float best = 3e38f;
+    uint32_t best_m = keep_m;
+    int best_v = keep_v, rc = LRC_OK;
+    for (uint32_t m : sizes) {
+        if (m > top || rc) continue;
+        float ms = 0;
+        rc = time_one(m, keep_v, ms);
+        if (!rc && ms < best) {
+            best = ms;
+            best_m = m;
+        }
+    }
+    for (int v = 0; v < lrc::wf_variants() && !rc; v++) {
+        if (v == keep_v) continue;
+        float ms = 0;
+        rc = time_one(best_m, v, ms);
+        if (!rc && ms < best) {
+            best = ms;
+            best_v = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->wf_slots = rc ? keep_m : best_m;
+    b->wf_variant = rc ? keep_v : best_v;
+    if (rc) return rc;
+    rc = check_status(c);
+    if (rc) return rc;
+    if (variant) *variant = best_v;
+    if (slots) *slots = (int32_t)best_m;
+    if (ns_per_task) *ns_per_task = best * 1e6 / (double)n;
+    return LRC_OK;
+}
+
+void note_built(lrc_batch *b) {   // (what captured builds' host side records)
+    for (const lrc_batch::Job *J : builds_of(b)) J->s->built_n = J->s->ntris + J->s->nprims;
 }
 
 }  // namespace
@@ -271,6 +411,8 @@ void lrc_batch_destroy(lrc_batch *b) {
     cudaFree(b->d_part);
     cudaFree(b->d_ctr);
     cudaFree(b->scratch);
+    cudaFree(b->d_wf);
+    if (b->body) cudaStreamDestroy(b->body);
     delete b;
 }
 
@@ -282,7 +424,8 @@ int lrc_batch_add(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t
         return fail(c, LRC_E_INVALID, "a batch job needs a band of rows in the image and spp >= 1");
     if (p->exact && spp0 != 0) return fail(c, LRC_E_INVALID, "exact mode starts at each pixel's first sample (spp0 = 0)");
     if ((uint64_t)spp0 + spp >= (1ull << 31)) return fail(c, LRC_E_INVALID, "spp0 + spp must stay below 2^31");
-    if (builder >= 0 && builder != 0 && builder != 1) return fail(c, LRC_E_INVALID, "builder: -1 (none), 0 (LBVH) or 1 (PLOC)");
+    if (p->max_depth < 0 || p->max_depth > 0xffff) return fail(c, LRC_E_INVALID, "max_depth must be in [0, 65535]");
+    if (builder < -1 || builder > 2) return fail(c, LRC_E_INVALID, "builder: -1 (none), 0 (LBVH), 1 (PLOC) or 2 (both)");
     if (builder >= 0 && key_bits != 30 && key_bits != 63) return fail(c, LRC_E_INVALID, "key_bits must be 30 or 63");
     if (s->ninst && builder >= 0) return fail(c, LRC_E_INVALID, "instanced scenes are built by lrc_scene_build_instances");
     b->jobs.push_back({s, *p, y0, rows, spp0, spp, d_accum, builder, key_bits});
@@ -315,22 +458,44 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
         }
     }
     b->graph_used = 0;
-    if ((flags & LRC_BATCH_GRAPH) && b->exec && b->prepared && b->graph_flags == flags && signature(b) == b->graph_sig) {
+    const bool cached = b->exec && b->prepared && b->graph_flags == flags && signature(b, flags) == b->graph_sig;
+    if (b->engine == 1) {
+        if (!cached || ((flags & LRC_BATCH_BUILD) && !(flags & LRC_BATCH_GRAPH))) {
+            // builds as plain launches: a first run sizes the buffers a captured build needs
+            if (flags & LRC_BATCH_BUILD)
+                for (const lrc_batch::Job *J : builds_of(b)) {
+                    int rc = build_job(b, J, c->st, false);
+                    if (rc) return rc;
+                }
+        }
+        if (!cached) {
+            int rc = prepare(b);
+            if (!rc) rc = capture(b, flags);
+            if (rc) return rc;
+        }
+        cudaError_t e = cudaGraphLaunch(b->exec, c->st);
+        if (e) return cuda_status(c, e, "batch graph launch");
+        b->graph_used = cached ? 1 : 0;
+        if ((flags & LRC_BATCH_BUILD) && (flags & LRC_BATCH_GRAPH)) note_built(b);
+        return LRC_OK;
+    }
+    if ((flags & LRC_BATCH_GRAPH) && cached) {
         cudaError_t e = cudaGraphLaunch(b->exec, c->st);
         if (e) return cuda_status(c, e, "batch graph launch");
         b->graph_used = 1;
+        if (flags & LRC_BATCH_BUILD) note_built(b);
         return LRC_OK;
     }
     if (flags & LRC_BATCH_BUILD) {
         // builds first: they size the trees the table points at
         for (const lrc_batch::Job *J : builds_of(b)) {
-            int rc = scene_build_on(J->s, J->builder, J->key_bits, &b->scratch, &b->scratch_cap, c->st, nullptr, false);
+            int rc = build_job(b, J, c->st, false);
             if (rc) return rc;
         }
     }
     int rc = prepare(b);
     if (rc) return rc;
-    rc = enqueue(b, flags & ~LRC_BATCH_BUILD, c->st, false);
+    rc = enqueue(b, flags, c->st, false, false, true, b->ntasks);
     if (rc) return rc;
     if (flags & LRC_BATCH_GRAPH) {
         // the next run replays this one: captured now, with every buffer sized
@@ -402,9 +567,10 @@ int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_
     }
     int rc = b->prepared ? LRC_OK : prepare(b);
     if (rc) return rc;
-    // the queue's head: the most expensive tasks (the trace kernel writes only partials, which the
-    // next run overwrites, so tuning changes no image)
+    // the queue's head: the most expensive tasks (the trace kernels write only per-task sums, which
+    // the next run overwrites, so tuning changes no image)
     const unsigned long long n = std::min<unsigned long long>(b->ntasks, sample_tasks ? sample_tasks : b->ntasks / 16 + 1);
+    if (b->engine == 1) return tune_wavefront(b, n, variant, grid, ns_per_task);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -442,6 +608,38 @@ int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_
     if (variant) *variant = best_v;
     if (grid) *grid = best_grid;
     if (ns_per_task) *ns_per_task = best * 1e6 / (double)n;
+    return LRC_OK;
+}
+
+int lrc_batch_set_engine(lrc_batch *b, int32_t engine) {
+    if (!b || (engine != 0 && engine != 1)) return LRC_E_INVALID;
+    b->engine = engine;
+    return LRC_OK;
+}
+
+int lrc_batch_set_wavefront(lrc_batch *b, uint32_t slots, int32_t variant) {
+    if (!b || variant < 0 || variant >= lrc::wf_variants() || slots < 256 || slots % 256 || slots > (1u << 26))
+        return LRC_E_INVALID;
+    b->wf_slots = slots;
+    b->wf_variant = variant;
+    return LRC_OK;
+}
+
+int lrc_batch_wavefront_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm) {
+    int bl = 0, mb = 0;
+    int n = lrc::wf_variant_shape(variant, &bl, &mb);
+    if (n < 0) return -1;
+    if (block) *block = bl;
+    if (minb) *minb = mb;
+    if (per_sm) *per_sm = n;
+    return lrc::wf_variants();
+}
+
+int lrc_batch_engine(const lrc_batch *b, int32_t *engine, uint32_t *slots, int32_t *wf_variant) {
+    if (!b) return LRC_E_INVALID;
+    if (engine) *engine = b->engine;
+    if (slots) *slots = b->wf_slots;
+    if (wf_variant) *wf_variant = b->wf_variant;
     return LRC_OK;
 }
 

@@ -28,6 +28,7 @@ constexpr uint32_t ST_TIMEOUT_PLOC = 2u;
 constexpr uint32_t ST_STACK_OVERFLOW = 4u;
 constexpr uint32_t ST_TIMEOUT_BARRIER = 8u;
 constexpr uint32_t ST_BAD_TREE = 16u;
+constexpr uint32_t ST_LOOP = 32u;          // the wavefront's loop ran past its bound (stopped)
 
 // spins before a bounded wait gives up (each ~ a few hundred ns with the back-off): ~1 s
 constexpr uint32_t SPIN_LIMIT = 1u << 22;
@@ -220,6 +221,47 @@ cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long 
 // capped for, and the blocks of it that fit on one SM (-1: no such shape)
 int batch_variants();
 int batch_variant_shape(int variant, int *block, int *minb);
+
+// The wavefront batch's paths in flight: M slots, each holding one task and the path of its current
+// sample between the kernels of a bounce (advance, closest hit, shade, shadow rays). Arrays of M
+// (vis: 2M) in structure-of-arrays order, so that a warp's slots are read in whole sectors.
+struct WfState {
+    uint32_t M;
+    unsigned long long *task;   // the slot's task (~0: none)
+    uint32_t *job;              // its job (queue order)
+    uint32_t *kk;               // the sample it traces (the Sampler's index)
+    uint32_t *trays;            // rays traced for the task so far
+    uint32_t *flags;            // F_PATH, F_ENDED and the Nee flags of the bounce just shaded
+    uint2 *xy;                  // the task's pixel
+    float4 *sum;                // the task's sum so far (rgb, samples)
+    float4 *ro;                 // the path's ray origin, bounce_pdf
+    float4 *rd;                 // its direction, depth | emit << 16 (int bits)
+    float4 *thr;                // its throughput
+    float4 *rad;                // its radiance so far
+    ulonglong2 *rng;            // its Rng (state, inc)
+    float4 *hit;                // the closest hit: t, world shape, instance, instance triangle (int bits)
+    float4 *nthr, *nvl, *nve;   // the bounce's next event estimation: throughput, lamp and sky values
+    uint8_t *vis;               // 2 per slot: the lamp's / the sky's shadow ray unoccluded
+    uint32_t *rq;               // the ray queue: slots with a path (M)
+    float4 *sq_o, *sq_d;        // the shadow queue (2M): origin + (slot << 1 | kind) bits, direction + tmax
+    uint32_t *ctl;              // [0] rays queued, [1] shadow rays queued, [2] [3] their fetch counters, [4] passes
+    unsigned long long *next;   // the task queue's next task; next[1]: how many tasks this run takes
+};
+// the device bytes of a wavefront of M slots, and its arrays carved from them (256-byte aligned base)
+size_t wf_bytes(uint32_t M);
+WfState wf_carve(void *base, uint32_t M);
+// the wavefront's trace shapes (closest-hit and shadow kernels: threads per block, register-cap
+// blocks per SM, blocks per SM that fit): how many; -1 for none
+int wf_variants();
+int wf_variant_shape(int variant, int *block, int *minb);
+// Captures the wavefront's loop into the graph stream st is capturing: the slots cleared and the
+// task queue set to the first ntasks tasks, then a while node whose body (captured on body_st)
+// runs the advance, closest-hit, shade and shadow kernels until no slot holds a path.
+// The loop stops after max_passes passes whatever is left (ST_LOOP in the status word): a bound well
+// above what the tasks need (a pass per bounce of each slot's tasks).
+cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
+                            uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st,
+                            cudaStream_t body_st);
 // the sky's sampling tables as env_prepare makes them (host_tables.cu): marg h + 1, cond h x (w + 1),
 // prob w x h; returns false when no pixel weighs anything (sum 0)
 bool env_tables(const float *rgb, int w, int h, float *marg, float *cond, float *prob);

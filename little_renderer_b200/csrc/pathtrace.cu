@@ -16,605 +16,12 @@
 //   fast:  one thread per (pixel, sample), each sample its own PCG32 stream (seeded from pixel,
 //          sample and image seed) and the same Owen-Sobol dimensions; a pixel's samples sit in
 //          neighbouring lanes and are summed by warp shuffles in a fixed order (deterministic).
-#include "lrc_internal.cuh"
-#include "bsdf.cuh"
+
+#include "pt_device.cuh"
 #include <algorithm>
 
 namespace lrc {
 namespace pt {
-
-constexpr float RT_EPS = 2e-3f;
-constexpr float RT_SHADOW_MARGIN = 2e-2f;
-constexpr int RR_START = 3;
-constexpr int PT_STACK = 64;
-
-struct Hit {
-    float t;
-    V3 p, n, ng;
-    int front;
-    int prim;
-    int inst;
-};
-
-__device__ __forceinline__ float4 ld4(const float4 *p) { return __ldg(p); }
-
-// ---- shape tests (engine/rt/intersect.h:66-112), rounded as the C code rounds them -----------
-__device__ __forceinline__ bool hit_sphere_t(V3 c, float radius, V3 o, V3 d, float tmin, float tmax, float &tout) {
-    V3 oc = vsub(c, o);
-    float a = vdot(d, d);
-    float hh = vdot(d, oc);
-    float cc = sub(vdot(oc, oc), mul(radius, radius));
-    float disc = sub(mul(hh, hh), mul(a, cc));
-    if (disc < 0.0f) return false;
-    float sq = __fsqrt_rn(disc);
-    float t = dvd(sub(hh, sq), a);
-    if (t <= tmin || t >= tmax) {
-        t = dvd(add(hh, sq), a);
-        if (t <= tmin || t >= tmax) return false;
-    }
-    tout = t;
-    return true;
-}
-__device__ __forceinline__ bool hit_quad_t(const float4 *pr, V3 o, V3 d, float tmin, float tmax, float &tout) {
-    float4 q = ld4(pr + 1), u = ld4(pr + 2), v = ld4(pr + 3), nd = ld4(pr + 4), w = ld4(pr + 5);
-    V3 nrm = v3(nd.x, nd.y, nd.z);
-    float denom = vdot(nrm, d);
-    if (fabsf(denom) < 1e-12f) return false;
-    float t = dvd(sub(nd.w, vdot(nrm, o)), denom);
-    if (t <= tmin || t >= tmax) return false;
-    V3 p = vadd(o, vscale(d, t));
-    V3 rel = vsub(p, v3(q.x, q.y, q.z));
-    V3 ww = v3(w.x, w.y, w.z);
-    float a = vdot(ww, vcross(rel, v3(v.x, v.y, v.z)));
-    float b = vdot(ww, vcross(v3(u.x, u.y, u.z), rel));
-    if (a < 0.0f || a > 1.0f || b < 0.0f || b > 1.0f) return false;
-    tout = t;
-    return true;
-}
-__device__ __forceinline__ bool hit_tri_t(const float4 *tp, V3 o, V3 d, float tmin, float tmax, float &tout) {
-    float4 q = ld4(tp), u = ld4(tp + 1), v = ld4(tp + 2);
-    V3 vv = v3(v.x, v.y, v.z), uu = v3(u.x, u.y, u.z);
-    V3 pvec = vcross(d, vv);
-    float det = vdot(uu, pvec);
-    if (fabsf(det) < 1e-12f) return false;
-    float inv = dvd(1.0f, det);
-    V3 tvec = vsub(o, v3(q.x, q.y, q.z));
-    float b1 = mul(vdot(tvec, pvec), inv);
-    if (b1 < 0.0f || b1 > 1.0f) return false;
-    V3 qvec = vcross(tvec, uu);
-    float b2 = mul(vdot(d, qvec), inv);
-    if (b2 < 0.0f || add(b1, b2) > 1.0f) return false;
-    float t = mul(vdot(vv, qvec), inv);
-    if (t <= tmin || t >= tmax) return false;
-    tout = t;
-    return true;
-}
-
-// shape `id` (primitives, then triangles) against the ray
-__device__ __forceinline__ bool shape_test(const PtScene &S, uint32_t id, V3 o, V3 d, float tmin, float tmax, float &t) {
-    if (id < S.nprims) {
-        const float4 *pr = S.prims + 6 * (size_t)id;
-        float4 c = ld4(pr), qf = ld4(pr + 1);
-        if (qf.w == 0.0f) return hit_sphere_t(v3(c.x, c.y, c.z), c.w, o, d, tmin, tmax, t);
-        return hit_quad_t(pr, o, d, tmin, tmax, t);
-    }
-    return hit_tri_t(S.tris + 3 * (size_t)(id - S.nprims), o, d, tmin, tmax, t);
-}
-
-struct RayBox {
-    float ix, iy, iz, ax, ay, az;
-};
-__device__ __forceinline__ RayBox ray_box(V3 o, V3 d) {
-    auto inv = [](float x) { return 1.0f / (fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x); };
-    RayBox r;
-    r.ix = inv(d.x); r.iy = inv(d.y); r.iz = inv(d.z);
-    r.ax = o.x * r.ix; r.ay = o.y * r.iy; r.az = o.z * r.iz;
-    return r;
-}
-// conservative slab test (boxes are padded by 1e-3): entry distance or +inf
-__device__ __forceinline__ float slab(const RayBox &r, float4 lo, float4 hi, float tmin, float tmax) {
-    float x0 = fmaf(lo.x, r.ix, -r.ax), x1 = fmaf(hi.x, r.ix, -r.ax);
-    float y0 = fmaf(lo.y, r.iy, -r.ay), y1 = fmaf(hi.y, r.iy, -r.ay);
-    float z0 = fmaf(lo.z, r.iz, -r.az), z1 = fmaf(hi.z, r.iz, -r.az);
-    float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-    float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
-    return tn <= tf ? tn : __int_as_float(0x7f800000);
-}
-
-// One BVH walk in (tmin, best): nodes and aux as the reference lays them out, root its root node.
-// leaf(entry) tests one leaf entry (an aux value), lowering best on a hit, and returns true to
-// end the walk (an any-hit found). Entries of a leaf in order; a hit at the same t as the best is
-// not taken (t >= tmax rejects), as the CPU's walk does. Returns true if a leaf ended it.
-template <typename Leaf>
-__device__ bool bvh_walk(const float4 *nodes, uint32_t root, uint32_t nnodes, const uint32_t *aux, uint32_t naux, V3 o,
-                         V3 d, float tmin, float &best, uint32_t *err, Leaf &&leaf) {
-    RayBox rb = ray_box(o, d);
-    float4 r0 = ld4(&nodes[2 * (size_t)root]), r1 = ld4(&nodes[2 * (size_t)root + 1]);
-    if (!(slab(rb, r0, r1, tmin, best) <= best)) return false;
-    uint2 stack[PT_STACK];
-    int sp = 0;
-    uint32_t a = __float_as_uint(r0.w), b = __float_as_uint(r1.w);
-    while (true) {
-        if (b & LEAF_BIT) {
-            const uint32_t count = b & ~LEAF_BIT;
-            if (a >= naux || count > naux - a) { atomicOr(err, ST_BAD_TREE); return false; }
-            for (uint32_t k = 0; k < count; k++)
-                if (leaf(__ldg(&aux[a + k]))) return true;
-        } else {
-            if (a >= nnodes || b >= nnodes) { atomicOr(err, ST_BAD_TREE); return false; }
-            float4 l0 = ld4(&nodes[2 * (size_t)a]), l1 = ld4(&nodes[2 * (size_t)a + 1]);
-            float4 h0 = ld4(&nodes[2 * (size_t)b]), h1 = ld4(&nodes[2 * (size_t)b + 1]);
-            float t0 = slab(rb, l0, l1, tmin, best), t1 = slab(rb, h0, h1, tmin, best);
-            bool c0 = t0 <= best, c1 = t1 <= best;
-            if (c0 && c1) {
-                bool first0 = t0 <= t1;
-                if (sp < PT_STACK) stack[sp++] = first0 ? make_uint2(__float_as_uint(h0.w), __float_as_uint(h1.w))
-                                                        : make_uint2(__float_as_uint(l0.w), __float_as_uint(l1.w));
-                else { atomicOr(err, ST_STACK_OVERFLOW); return false; }
-                a = first0 ? __float_as_uint(l0.w) : __float_as_uint(h0.w);
-                b = first0 ? __float_as_uint(l1.w) : __float_as_uint(h1.w);
-                continue;
-            }
-            if (c0) { a = __float_as_uint(l0.w); b = __float_as_uint(l1.w); continue; }
-            if (c1) { a = __float_as_uint(h0.w); b = __float_as_uint(h1.w); continue; }
-        }
-        if (sp == 0) break;
-        uint2 e = stack[--sp];
-        a = e.x;
-        b = e.y;
-    }
-    return false;
-}
-
-// the closest (ANY = false) or any world shape (primitives, then triangles) in (tmin, best), or -1
-template <bool ANY>
-__device__ int32_t walk(const PtScene &S, const float4 *nodes, uint32_t root, uint32_t nnodes, const uint32_t *aux,
-                        uint32_t naux, V3 o, V3 d, float tmin, float &best, uint32_t *err) {
-    int32_t hit = -1;
-    bvh_walk(nodes, root, nnodes, aux, naux, o, d, tmin, best, err, [&](uint32_t id) {
-        if (id >= S.nprims + S.ntris) { atomicOr(err, ST_BAD_TREE); return true; }
-        float t;
-        if (shape_test(S, id, o, d, tmin, best, t)) {
-            best = t;
-            hit = (int32_t)id;
-            return ANY;
-        }
-        return false;
-    });
-    return hit;
-}
-
-// ---- instances (scene.h:202-209; intersect_instances, accel.c:77-150) ---------------------------
-// An instance record: 8 float4 (the object -> world transform's rows, the inverse's rows, the
-// world box's lo with the mesh index's bits, hi with the material's bits: -1 the triangles' own)
-__device__ __forceinline__ V3 xpoint(const float4 *m, V3 p) {     // xform_point (scene.h)
-    float4 r0 = ld4(m), r1 = ld4(m + 1), r2 = ld4(m + 2);
-    return v3(add(add(add(mul(r0.x, p.x), mul(r0.y, p.y)), mul(r0.z, p.z)), r0.w),
-              add(add(add(mul(r1.x, p.x), mul(r1.y, p.y)), mul(r1.z, p.z)), r1.w),
-              add(add(add(mul(r2.x, p.x), mul(r2.y, p.y)), mul(r2.z, p.z)), r2.w));
-}
-__device__ __forceinline__ V3 xdir(const float4 *m, V3 d) {       // xform_dir
-    float4 r0 = ld4(m), r1 = ld4(m + 1), r2 = ld4(m + 2);
-    return v3(add(add(mul(r0.x, d.x), mul(r0.y, d.y)), mul(r0.z, d.z)),
-              add(add(mul(r1.x, d.x), mul(r1.y, d.y)), mul(r1.z, d.z)),
-              add(add(mul(r2.x, d.x), mul(r2.y, d.y)), mul(r2.z, d.z)));
-}
-__device__ __forceinline__ V3 xnormal(const float4 *inv, V3 n) {  // xform_normal: by the inverse's transpose
-    float4 r0 = ld4(inv), r1 = ld4(inv + 1), r2 = ld4(inv + 2);
-    return vnorm(v3(add(add(mul(r0.x, n.x), mul(r1.x, n.y)), mul(r2.x, n.z)),
-                    add(add(mul(r0.y, n.x), mul(r1.y, n.y)), mul(r2.y, n.z)),
-                    add(add(mul(r0.z, n.x), mul(r1.z, n.y)), mul(r2.z, n.z))));
-}
-
-// The closest (ANY = false) or any hit on the instances in (tmin, best): the instance and the
-// triangle's index in its mesh; false if none. The top level's leaves are instances; each is
-// entered with the ray in its own space (o' = inv o, d' = inv d: the same t) and its mesh's BVH walked.
-template <bool ANY>
-__device__ bool walk_instances(const PtScene &S, V3 o, V3 d, float tmin, float &best, int &inst, int &tri, uint32_t *err) {
-    bool found = false;
-    bvh_walk(S.tlas_nodes, 0, S.tlas_nnodes, S.tlas_aux, S.ninst, o, d, tmin, best, err, [&](uint32_t i) {
-        if (i >= S.ninst) { atomicOr(err, ST_BAD_TREE); return true; }
-        const float4 *rec = S.inst + 8 * (size_t)i;
-        const uint32_t mesh = __float_as_uint(ld4(rec + 6).w);
-        if (mesh >= S.nmeshes) return false;                       // (shapes: not in these scenes)
-        const uint4 mi = __ldg(&S.mesh_info[mesh]);                // root node, first triangle, triangles
-        V3 ro = xpoint(rec + 3, o), rd = xdir(rec + 3, d);
-        return bvh_walk(S.mnodes, mi.x, S.mnnodes, S.maux, S.mnaux, ro, rd, tmin, best, err, [&](uint32_t g) {
-            if (g >= S.nmtris) { atomicOr(err, ST_BAD_TREE); return true; }
-            float t;
-            if (hit_tri_t(S.mtris + 3 * (size_t)g, ro, rd, tmin, best, t)) {
-                best = t;
-                inst = (int)i;
-                tri = (int)(g - mi.y);
-                found = true;
-                return ANY;
-            }
-            return false;
-        });
-    });
-    return found;
-}
-
-// set_hit (intersect.c): point, the normal facing the ray, front_face
-__device__ __forceinline__ void set_hit(Hit &h, V3 o, V3 d, float t, V3 outward) {
-    h.t = t;
-    h.p = vadd(o, vscale(d, t));
-    h.front = vdot(d, outward) < 0.0f;
-    h.n = h.front ? outward : vneg(outward);
-    h.ng = h.n;
-}
-// shape_hit (intersect.c): the Hit of the shape kept
-__device__ __forceinline__ void shape_hit(const PtScene &S, int id, V3 o, V3 d, float t, Hit &h) {
-    if ((uint32_t)id < S.nprims) {
-        const float4 *pr = S.prims + 6 * (size_t)id;
-        float4 c = ld4(pr), qf = ld4(pr + 1);
-        if (qf.w == 0.0f) {
-            V3 p = vadd(o, vscale(d, t));
-            V3 n = vscale(vsub(p, v3(c.x, c.y, c.z)), dvd(1.0f, c.w));
-            set_hit(h, o, d, t, n);
-        } else {
-            float4 nd = ld4(pr + 4);
-            set_hit(h, o, d, t, v3(nd.x, nd.y, nd.z));
-        }
-    } else {
-        const float4 *tp = S.tris + 3 * (size_t)(id - S.nprims);
-        float4 u = ld4(tp + 1), v = ld4(tp + 2), q = ld4(tp);
-        V3 uu = v3(u.x, u.y, u.z), vv = v3(v.x, v.y, v.z);
-        set_hit(h, o, d, t, vnorm(vcross(uu, vv)));
-        uint32_t n0 = __float_as_uint(q.w);
-        if (n0 != 0xffffffffu && S.normals) {
-            // smooth: the vertex normals blended by the barycentrics (finish_triangle)
-            V3 pvec = vcross(d, vv);
-            float inv = dvd(1.0f, vdot(uu, pvec));
-            V3 tvec = vsub(o, v3(q.x, q.y, q.z));
-            float b1 = mul(vdot(tvec, pvec), inv);
-            float b2 = mul(vdot(d, vcross(tvec, uu)), inv);
-            uint32_t n1 = __float_as_uint(u.w), n2 = __float_as_uint(v.w) & 0x03ffffffu;
-            auto N = [&](uint32_t k) { return v3(__ldg(&S.normals[3 * k]), __ldg(&S.normals[3 * k + 1]), __ldg(&S.normals[3 * k + 2])); };
-            V3 ns = vnorm(vadd(vadd(vscale(N(n0), sub(sub(1.0f, b1), b2)), vscale(N(n1), b1)), vscale(N(n2), b2)));
-            if (vdot(ns, h.n) < 0.0f) ns = vneg(ns);
-            if (vdot(ns, ns) > 0.5f) h.n = ns;
-        }
-    }
-    h.prim = id;
-    h.inst = -1;
-}
-
-// the Hit of an instance's triangle (intersect_instance, accel.c:98-105): made in the instance's
-// space (finish_triangle with the object ray), the point in the world, the normals turned back
-__device__ __forceinline__ void instance_hit(const PtScene &S, int inst, int tri, V3 o, V3 d, float t, Hit &h) {
-    const float4 *rec = S.inst + 8 * (size_t)inst;
-    const uint4 mi = __ldg(&S.mesh_info[__float_as_uint(ld4(rec + 6).w)]);
-    V3 ro = xpoint(rec + 3, o), rd = xdir(rec + 3, d);
-    const float4 *tp = S.mtris + 3 * (size_t)(mi.y + tri);
-    float4 u = ld4(tp + 1), v = ld4(tp + 2);
-    set_hit(h, ro, rd, t, vnorm(vcross(v3(u.x, u.y, u.z), v3(v.x, v.y, v.z))));
-    h.p = vadd(o, vscale(d, t));
-    h.n = xnormal(rec + 3, h.n);
-    h.ng = xnormal(rec + 3, h.ng);
-    h.prim = tri;
-    h.inst = inst;
-}
-
-// scene_intersect (accel.c:252): the world's closest hit, then the instances' closer than it
-__device__ __forceinline__ bool scene_intersect(const PtScene &S, V3 o, V3 d, float tmin, float tmax, Hit &h, uint32_t *err) {
-    float best = tmax;
-    bool found = false;
-    if (S.nnodes) {
-        int32_t id = walk<false>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err);
-        if (id >= 0) {
-            shape_hit(S, id, o, d, best, h);
-            found = true;
-        }
-    }
-    if (S.ninst) {
-        int inst = -1, tri = -1;
-        if (walk_instances<false>(S, o, d, tmin, best, inst, tri, err)) {
-            instance_hit(S, inst, tri, o, d, best, h);
-            found = true;
-        }
-    }
-    return found;
-}
-// scene_occluded (accel.c:280): any hit in (tmin, tmax), the instances first
-__device__ __forceinline__ bool scene_occluded(const PtScene &S, V3 o, V3 d, float tmin, float tmax, uint32_t *err) {
-    float best = tmax;
-    if (S.ninst) {
-        int inst, tri;
-        if (walk_instances<true>(S, o, d, tmin, best, inst, tri, err)) return true;
-    }
-    return S.nnodes && walk<true>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err) >= 0;
-}
-
-// ---- the sky (engine/scene/env.c: env_eval, env_sample, env_pdf) --------------------------------
-// rgbp: the map's radiance and each pixel's probability (env_pixel_prob), w x h; cond: each row's
-// cumulative distribution (w + 1 per row); marg: the rows' (h + 1)
-__device__ __forceinline__ void map_uv(V3 d, float &u, float &v) {
-    float y = d.y < -1.0f ? -1.0f : (d.y > 1.0f ? 1.0f : d.y);
-    float uu = add(0.5f, mul(atan2f(d.x, d.z), dvd(0.5f, PIF)));
-    u = sub(uu, floorf(uu));
-    v = mul(acosf(y), dvd(1.0f, PIF));
-}
-__device__ __forceinline__ V3 map_dir(float u, float v) {
-    float ph = mul(sub(u, 0.5f), mul(2.0f, PIF)), th = mul(v, PIF);
-    float st = sinf(th);
-    return v3(mul(st, sinf(ph)), cosf(th), mul(st, cosf(ph)));
-}
-__device__ __forceinline__ V3 env_bilerp(const PtScene &S, float u, float v) {
-    const int w = S.env_w, h = S.env_h;
-    float x = sub(mul(u, (float)w), 0.5f), y = sub(mul(v, (float)h), 0.5f);
-    int x0 = (int)floorf(x), y0 = (int)floorf(y);
-    float fx = sub(x, (float)x0), fy = sub(y, (float)y0);
-    int y1 = y0 + 1;
-    if (y0 < 0) y0 = 0;
-    if (y1 > h - 1) y1 = h - 1;
-    if (y0 > h - 1) y0 = h - 1;
-    int xa = x0 < 0 ? x0 + w : (x0 >= w ? x0 - w : x0);
-    if (xa < 0 || xa >= w) xa = ((xa % w) + w) % w;
-    int xb = xa + 1 == w ? 0 : xa + 1;
-    float4 a = ld4(&S.env_rgbp[(size_t)y0 * w + xa]), b = ld4(&S.env_rgbp[(size_t)y0 * w + xb]);
-    float4 c = ld4(&S.env_rgbp[(size_t)y1 * w + xa]), dd = ld4(&S.env_rgbp[(size_t)y1 * w + xb]);
-    float gx = sub(1.0f, fx), gy = sub(1.0f, fy);
-    return v3(add(mul(gy, add(mul(gx, a.x), mul(fx, b.x))), mul(fy, add(mul(gx, c.x), mul(fx, dd.x)))),
-              add(mul(gy, add(mul(gx, a.y), mul(fx, b.y))), mul(fy, add(mul(gx, c.y), mul(fx, dd.y)))),
-              add(mul(gy, add(mul(gx, a.z), mul(fx, b.z))), mul(fy, add(mul(gx, c.z), mul(fx, dd.z)))));
-}
-__device__ __forceinline__ V3 env_eval(const PtScene &S, V3 d) {
-    float u, v;
-    map_uv(d, u, v);
-    return vscale(env_bilerp(S, u, v), S.env_scale);
-}
-__device__ __forceinline__ int upper_bound(const float *c, int n, float x) {
-    int lo = 0, hi = n;
-    while (hi - lo > 1) {
-        int mid = (lo + hi) / 2;
-        if (__ldg(&c[mid]) <= x) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-__device__ __forceinline__ float env_density(const PtScene &S, int x, int y, float st) {
-    float prob = ld4(&S.env_rgbp[(size_t)y * S.env_w + x]).w;
-    return dvd(mul(mul(prob, (float)S.env_w), (float)S.env_h), mul(mul(mul(2.0f, PIF), PIF), st));
-}
-__device__ __forceinline__ V3 env_sample(const PtScene &S, float u1, float u2, V3 &d, float &pdf) {
-    pdf = 0.0f;
-    if (!S.env_weighted) return v3(0, 0, 0);
-    const int w = S.env_w, h = S.env_h;
-    int y = upper_bound(S.env_marg, h, u2);
-    float m0 = __ldg(&S.env_marg[y]), m1 = __ldg(&S.env_marg[y + 1]);
-    float dv = m1 > m0 ? dvd(sub(u2, m0), sub(m1, m0)) : 0.5f;
-    const float *c = S.env_cond + (size_t)y * (w + 1);
-    int x = upper_bound(c, w, u1);
-    float c0 = __ldg(&c[x]), c1 = __ldg(&c[x + 1]);
-    float du = c1 > c0 ? dvd(sub(u1, c0), sub(c1, c0)) : 0.5f;
-    if (dv > 0.9999f) dv = 0.9999f;
-    if (du > 0.9999f) du = 0.9999f;
-    float u = dvd(add((float)x, du), (float)w), v = dvd(add((float)y, dv), (float)h);
-    float st = sinf(mul(v, PIF));
-    if (st < 1e-6f) return v3(0, 0, 0);
-    d = map_dir(u, v);
-    pdf = env_density(S, x, y, st);
-    return env_eval(S, d);
-}
-__device__ __forceinline__ float env_pdf(const PtScene &S, V3 d) {
-    if (!S.env_weighted) return 0.0f;
-    float u, v;
-    map_uv(d, u, v);
-    float st = sinf(mul(v, PIF));
-    if (st < 1e-6f) return 0.0f;
-    int x = (int)mul(u, (float)S.env_w), y = (int)mul(v, (float)S.env_h);
-    if (x > S.env_w - 1) x = S.env_w - 1;
-    if (y > S.env_h - 1) y = S.env_h - 1;
-    return env_density(S, x, y, st);
-}
-
-__device__ __forceinline__ float power_heuristic(float pa, float pb) {
-    float a = mul(pa, pa), b = mul(pb, pb);
-    return add(a, b) > 0.0f ? dvd(a, add(a, b)) : 0.0f;
-}
-
-// the lamp (Scene.light: a quad primitive) and its emission
-struct Lamp {
-    V3 q, u, v, normal, le;
-    float area;
-    int prim;
-};
-__device__ __forceinline__ Lamp load_lamp(const PtScene &S) {
-    Lamp L;
-    L.prim = S.light;
-    const float4 *pr = S.prims + 6 * (size_t)S.light;
-    float4 q = ld4(pr + 1), u = ld4(pr + 2), v = ld4(pr + 3), nd = ld4(pr + 4);
-    L.q = v3(q.x, q.y, q.z);
-    L.u = v3(u.x, u.y, u.z);
-    L.v = v3(v.x, v.y, v.z);
-    L.normal = v3(nd.x, nd.y, nd.z);
-    L.area = v.w;
-    Mat m = load_mat(S.mats, (int)u.w);
-    L.le = m.emission;
-    return L;
-}
-__device__ __forceinline__ float light_pdf(const Lamp &L, float dist2, float cos_light) {
-    return dvd(dist2, mul(cos_light, L.area));
-}
-
-// sample_direct_light (tracer.c:56-84)
-__device__ __forceinline__ V3 direct_light(const PtScene &S, const Lamp &L, const Hit &h, Bsdf &b, V3 v, int mis, float ua,
-                                           float ub, uint32_t *err, uint32_t &rays) {
-    V3 xl = vadd(L.q, vadd(vscale(L.u, ua), vscale(L.v, ub)));
-    V3 to = vsub(xl, h.p);
-    float dist2 = vdot(to, to);
-    float dist = __fsqrt_rn(dist2);
-    V3 wi = vscale(to, dvd(1.0f, dist));
-    float cos_surf = vdot(h.n, wi);
-    float cos_light = -vdot(L.normal, wi);
-    if (cos_light <= 0.0f) return v3(0, 0, 0);
-    float pdf;
-    V3 f = bsdf_eval(b, h.n, v, wi, pdf);
-    if (!(vmax3(f) > 0.0f)) return v3(0, 0, 0);
-    rays++;
-    if (scene_occluded(S, h.p, wi, RT_EPS, sub(dist, RT_SHADOW_MARGIN), err)) return v3(0, 0, 0);
-    float g = dvd(mul(mul(fabsf(cos_surf), cos_light), L.area), dist2);
-    if (mis) g = mul(g, power_heuristic(light_pdf(L, dist2, cos_light), pdf));
-    return vscale(vmul(f, L.le), g);
-}
-
-// sample_direct_env (tracer.c:87-101): a sky direction by its luminance, the light along it if
-// nothing is in the way, weighted against the BSDF's own sampling
-__device__ __forceinline__ V3 direct_env(const PtScene &S, const Hit &h, Bsdf &b, V3 v, int mis, float ua, float ub,
-                                         uint32_t *err, uint32_t &rays) {
-    V3 wi = v3(0, 0, 0);
-    float pdf;
-    V3 le = env_sample(S, ua, ub, wi, pdf);
-    if (!(pdf > 0.0f) || !(vmax3(le) > 0.0f)) return v3(0, 0, 0);
-    float bpdf;
-    V3 f = bsdf_eval(b, h.n, v, wi, bpdf);
-    if (!(vmax3(f) > 0.0f)) return v3(0, 0, 0);
-    rays++;
-    if (scene_occluded(S, h.p, wi, RT_EPS, 1e30f, err)) return v3(0, 0, 0);
-    float g = dvd(fabsf(vdot(h.n, wi)), pdf);
-    if (mis) g = mul(g, power_heuristic(pdf, bpdf));
-    return vscale(vmul(f, le), g);
-}
-
-// the material of what was hit (hit_material, intersect.h:23-25; scene_instance_material)
-__device__ __forceinline__ int hit_material(const PtScene &S, const Hit &h) {
-    if (h.inst >= 0) {
-        const float4 *rec = S.inst + 8 * (size_t)h.inst;
-        int m = __float_as_int(ld4(rec + 7).w);
-        if (m >= 0) return m;
-        const uint4 mi = __ldg(&S.mesh_info[__float_as_uint(ld4(rec + 6).w)]);
-        return (int)(__float_as_uint(ld4(S.mtris + 3 * (size_t)(mi.y + h.prim) + 2).w) >> 26);
-    }
-    if (h.prim < (int)S.nprims) return (int)ld4(S.prims + 6 * (size_t)h.prim + 2).w;
-    return (int)(__float_as_uint(ld4(S.tris + 3 * (size_t)(h.prim - S.nprims) + 2).w) >> 26);
-}
-
-enum { EMIT_FULL, EMIT_NONE, EMIT_MIS };
-
-// The state trace_path_sampled (tracer.c:364-545) carries from one bounce to the next: the ray,
-// the throughput, the radiance gathered so far, how the next emitter hit counts and the pdf of
-// the bounce that led to it. With the Rng (and the sample index the Sampler is made from) it is
-// all a path needs to resume, so a thread can hold one path per lane and start the next sample
-// the moment its path ends (path regeneration in the batch kernel).
-struct PathState {
-    V3 ro, rd, thr, radiance;
-    float bounce_pdf;
-    int depth, emit;
-};
-
-__device__ __forceinline__ void path_begin(int mis, V3 ro, V3 rd, PathState &ps) {
-    ps.ro = ro;
-    ps.rd = mis ? vnorm(rd) : rd;
-    ps.thr = v3(1, 1, 1);
-    ps.radiance = v3(0, 0, 0);
-    ps.bounce_pdf = 0.0f;
-    ps.depth = 0;
-    ps.emit = EMIT_FULL;
-}
-
-// One pass of trace_path_sampled's bounce loop (without media, textures and glowing-shape
-// sampling: none in these scenes), counting the rays it traces. Returns false when the path has
-// ended; ps.radiance is then its value.
-__device__ __forceinline__ bool path_bounce(const PtScene &S, int max_depth, int mis, PathState &ps, Sampler &sm,
-                                            uint32_t *err, uint32_t &rays) {
-    const int depth = ps.depth;
-    const bool have_lamp = S.light >= 0;
-    Hit h;
-    rays++;
-    bool found = scene_intersect(S, ps.ro, ps.rd, RT_EPS, 1e30f, h, err);
-    if (!found) {                                    // escaped: the sky (black without one)
-        if (S.has_env && ps.emit != EMIT_NONE) {
-            V3 le = env_eval(S, ps.rd);
-            if (ps.emit == EMIT_MIS) le = vscale(le, power_heuristic(ps.bounce_pdf, env_pdf(S, ps.rd)));
-            ps.radiance = vadd(ps.radiance, vmul(ps.thr, le));
-        }
-        return false;
-    }
-    const Mat m = load_mat(S.mats, hit_material(S, h) & 63);   // (MAX_MATS 64: the buffer's size)
-    if (m.type == MAT_LIGHT) {
-        if (h.front) {
-            if (ps.emit == EMIT_FULL) {
-                ps.radiance = vadd(ps.radiance, vmul(ps.thr, m.emission));
-            } else if (ps.emit == EMIT_MIS && h.inst < 0 && h.prim == S.light) {
-                const Lamp L = load_lamp(S);
-                float cos_light = -vdot(L.normal, ps.rd);
-                if (cos_light > 0.0f) {
-                    float w = power_heuristic(ps.bounce_pdf, light_pdf(L, mul(h.t, h.t), cos_light));
-                    ps.radiance = vadd(ps.radiance, vmul(ps.thr, vscale(m.emission, w)));
-                }
-            }
-        }
-        return false;
-    }
-    if (glows(m)) ps.radiance = vadd(ps.radiance, vmul(ps.thr, m.emission));   // (no glowing shapes sampled)
-    if (depth >= max_depth) return false;
-    V3 v = vneg(vnorm(ps.rd));
-    Bsdf b = bsdf_make(m, h.front, S.tab);
-    if (bsdf_rough_part(b)) {
-        float la, lb;
-        if (have_lamp) {
-            const Lamp L = load_lamp(S);
-            sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
-            ps.radiance = vadd(ps.radiance, vmul(ps.thr, direct_light(S, L, h, b, v, mis, lb, la, err, rays)));
-        }
-        if (S.has_env) {
-            // env_numbers (tracer.c:209-213): the lamp's pair when there is no lamp, else plain ones
-            if (!have_lamp) sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
-            else {
-                la = rng_real(*sm.rng);
-                lb = rng_real(*sm.rng);
-            }
-            ps.radiance = vadd(ps.radiance, vmul(ps.thr, direct_env(S, h, b, v, mis, la, lb, err, rays)));
-        }
-    }
-    bsdf_view(b, vdot(v, h.n));
-    float ur = 0.0f, ul = 0.0f, da = 0.0f, db = 0.0f;
-    if (depth >= RR_START || bsdf_nlobes(b) > 1) sampler_2d(sm, SAMPLE_MISC(depth), ur, ul);
-    int lobe = bsdf_pick(b, ul);
-    if (lobe >= 0 && !bsdf_lobe_delta(b, lobe)) sampler_2d(sm, SAMPLE_DIR(depth), da, db);
-    BsdfSample bs;
-    if (!bsdf_sample_lobe(b, lobe, h.n, v, da, db, bs)) return false;
-    ps.thr = vmul(ps.thr, bs.w);
-    if (bs.delta) {
-        ps.emit = EMIT_FULL;
-    } else {
-        ps.bounce_pdf = bs.pdf;
-        ps.emit = mis ? EMIT_MIS : EMIT_NONE;
-    }
-    if (depth >= RR_START) {                         // russian_roulette_u
-        float p = rmin(vmax3(ps.thr), 0.95f);
-        if (ur >= p) return false;
-        ps.thr = vscale(ps.thr, dvd(1.0f, p));
-    }
-    ps.ro = h.p;
-    ps.rd = mis ? vnorm(bs.l) : bs.l;
-    ps.depth = depth + 1;
-    return true;
-}
-
-// trace_path_sampled (tracer.c:364-545): the bounces of one path
-__device__ V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err, uint32_t &rays) {
-    PathState ps;
-    path_begin(P.mis, ro, rd, ps);
-    while (path_bounce(S, P.max_depth, P.mis, ps, sm, err, rays)) {
-    }
-    return ps.radiance;
-}
-
-// camera_ray (camera.h:38-42)
-__device__ __forceinline__ void camera_ray(const PtParams &P, float s, float t, V3 &o, V3 &d) {
-    V3 target = vsub(vadd(P.upper_left, vscale(P.horizontal, s)), vscale(P.vertical, t));
-    o = P.origin;
-    d = vnorm(vsub(target, P.origin));
-}
-
-__device__ __forceinline__ bool is_number(V3 c) { return c.x == c.x && c.y == c.y && c.z == c.z; }
-
-__device__ __forceinline__ V3 clamp_sample(V3 c, float clamp) {
-    if (clamp > 0.0f && vmax3(c) > clamp) c = vscale(c, dvd(clamp, vmax3(c)));
-    return c;
-}
 
 // exact mode: one thread per pixel of rows [y0, y0 + rows), samples [0, spp) in order from the
 // CPU's per-pixel stream (trace_image, tracer.c:337-353)
@@ -649,12 +56,6 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
         for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
         if ((threadIdx.x & 31) == 0 && r) atomicAdd(ray_count, r);
     }
-}
-
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-    return z ^ (z >> 31);
 }
 
 // fast mode: P.group lanes (a power of 2 dividing 32) per pixel, lane s tracing samples s, s + g,
@@ -709,16 +110,6 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
 }
 
 // ---- the batch: one persistent kernel over the tasks of many jobs --------------------------------
-// the job holding task t (jobs in task order; binary search over task0)
-__device__ __forceinline__ uint32_t batch_job_of(const BatchJob *__restrict__ jobs, uint32_t njobs, unsigned long long t) {
-    uint32_t lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) >> 1;
-        if (__ldg(&jobs[mid].task0) <= t) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
 
 // Each lane holds one task (a pixel's lane slot) and one path of it at a time. A loop pass is
 // one bounce for every lane with a path; a lane whose path ends adds it to its task's sum and

@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -113,6 +113,10 @@ def lib():
     L.lrc_batch_set_shape.argtypes = [vp, C.c_int32, C.c_int32]
     L.lrc_batch_tune.argtypes = [vp, u64, vp, vp, vp]
     L.lrc_batch_info.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.lrc_batch_set_engine.argtypes = [vp, C.c_int32]
+    L.lrc_batch_set_wavefront.argtypes = [vp, u32, C.c_int32]
+    L.lrc_batch_wavefront_shape.argtypes = [C.c_int32, vp, vp, vp]
+    L.lrc_batch_engine.argtypes = [vp, vp, vp, vp]
     _lib = L
     return L
 
@@ -458,10 +462,35 @@ class Batch:
     def set_shape(self, variant, grid=0):
         self.ctx.check(self.ctx.L.lrc_batch_set_shape(self.h, variant, grid))
 
+    def set_engine(self, engine):
+        """0: the persistent megakernel, 1: the wavefront (the default)."""
+        self.ctx.check(self.ctx.L.lrc_batch_set_engine(self.h, engine))
+
+    def set_wavefront(self, slots, variant=0):
+        self.ctx.check(self.ctx.L.lrc_batch_set_wavefront(self.h, slots, variant))
+
+    def engine(self):
+        e, m, v = C.c_int32(), C.c_uint32(), C.c_int32()
+        self.ctx.check(self.ctx.L.lrc_batch_engine(self.h, C.byref(e), C.byref(m), C.byref(v)))
+        return {"engine": e.value, "slots": m.value, "wf_variant": v.value}
+
     def info(self):
         t, p, v, g, u = C.c_uint64(), C.c_uint64(), C.c_int32(), C.c_int32(), C.c_int32()
         self.ctx.check(self.ctx.L.lrc_batch_info(self.h, C.byref(t), C.byref(p), C.byref(v), C.byref(g), C.byref(u)))
         return {"tasks": t.value, "pixels": p.value, "variant": v.value, "grid": g.value, "graph_used": u.value}
+
+
+def wavefront_shapes():
+    """[(threads per block, register-cap blocks per SM, resident blocks per SM)] of the wavefront's
+    closest-hit / shadow kernels' launch shapes."""
+    L = lib()
+    out = []
+    b, m, r = C.c_int32(), C.c_int32(), C.c_int32()
+    n = L.lrc_batch_wavefront_shape(0, C.byref(b), C.byref(m), C.byref(r))
+    for v in range(max(n, 0)):
+        L.lrc_batch_wavefront_shape(v, C.byref(b), C.byref(m), C.byref(r))
+        out.append((b.value, m.value, r.value))
+    return out
 
 
 def batch_shapes():

@@ -1,7 +1,8 @@
-"""GPU tests of the batch (lrc_batch_*): many jobs over many scenes through one persistent kernel.
-Each job's image must equal the plain lrc_trace image of the same arguments to the bit (fast and
-exact mode), and its ray count must be the plain count; building the scenes inside the run,
-replaying the run as a CUDA graph, bands, sample offsets and the autotuner must change nothing."""
+"""GPU tests of the batch (lrc_batch_*): many jobs over many scenes through one persistent
+megakernel (engine 0) or the wavefront loop (engine 1). Each job's image must equal the plain
+lrc_trace image of the same arguments to the bit (fast and exact mode), and its ray count must be
+the plain count; building the scenes inside the run, replaying the run as a CUDA graph, bands,
+sample offsets, wavefront sizes and the autotuner must change nothing."""
 import numpy as np
 import pytest
 
@@ -46,11 +47,13 @@ def host(ctx, imgs):
     return [t.cpu().numpy() for t in imgs]
 
 
+@pytest.mark.parametrize("engine", [0, 1])
 @pytest.mark.parametrize("exact", [0, 1])
-def test_batched_images_are_the_plain_ones(ctx, scenes, built, exact):
+def test_batched_images_are_the_plain_ones(ctx, scenes, built, exact, engine):
     want = plain(built, scenes, exact)
     imgs = device_images(scenes)
     b = L.native.Batch(ctx)
+    b.set_engine(engine)
     for s, sc, t in zip(built, scenes, imgs):
         b.add(s, params(sc, exact), sc["spp"], t.data_ptr())
     b.run()
@@ -64,13 +67,15 @@ def test_batched_images_are_the_plain_ones(ctx, scenes, built, exact):
     assert info["pixels"] == sum(sc["width"] * sc["height"] for sc in scenes)
 
 
-def test_graph_replay_with_builds(ctx, oracle, scenes):
-    """Builds (LBVH and PLOC) inside the run, the run replayed as one CUDA graph: every replay
+@pytest.mark.parametrize("engine", [0, 1])
+def test_graph_replay_with_builds(ctx, oracle, scenes, engine):
+    """Builds (LBVH, PLOC, both) inside the run, the run replayed as one CUDA graph: every replay
     gives the plain image of a scene built by the same builder."""
     own = [R.world_scene(ctx, sc, 0, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables()) for sc in scenes]
-    builders = [i % 2 for i in range(len(scenes))]
+    builders = [i % 3 for i in range(len(scenes))]
     imgs = device_images(scenes)
     b = L.native.Batch(ctx)
+    b.set_engine(engine)
     for s, sc, t, bl in zip(own, scenes, imgs, builders):
         b.add(s, params(sc), sc["spp"], t.data_ptr(), builder=bl, key_bits=30)
     used = []
@@ -79,7 +84,7 @@ def test_graph_replay_with_builds(ctx, oracle, scenes):
         got = host(ctx, imgs)
         used.append(b.info()["graph_used"])
         for s, sc, g, bl in zip(own, scenes, got, builders):
-            ref = R.world_scene(ctx, sc, bl, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+            ref = R.world_scene(ctx, sc, min(bl, 1), blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
             acc, _ = ref.trace(params(sc), sc["spp"])
             assert np.array_equal(g, acc)
             ref.close()
@@ -110,6 +115,7 @@ def test_tuner_changes_no_image(ctx, scenes, built):
     want = plain(built, scenes)
     imgs = device_images(scenes)
     b = L.native.Batch(ctx)
+    b.set_engine(0)
     for s, sc, t in zip(built, scenes, imgs):
         b.add(s, params(sc), sc["spp"], t.data_ptr())
     v, grid, ns = b.tune(sample_tasks=20000)
@@ -127,3 +133,47 @@ def test_tuner_changes_no_image(ctx, scenes, built):
         got = host(ctx, imgs)
         for (acc, _), g in zip(want, got):
             assert np.array_equal(g, acc)
+
+
+def test_wavefront_tuner_and_sizes_change_no_image(ctx, scenes, built):
+    want = plain(built, scenes)
+    imgs = device_images(scenes)
+    b = L.native.Batch(ctx)
+    for s, sc, t in zip(built, scenes, imgs):
+        b.add(s, params(sc), sc["spp"], t.data_ptr())
+    assert b.engine()["engine"] == 1
+    v, slots, ns = b.tune(sample_tasks=50000)
+    shapes = L.native.wavefront_shapes()
+    assert 0 <= v < len(shapes) and slots % 256 == 0 and ns > 0
+    assert b.engine() == {"engine": 1, "slots": slots, "wf_variant": v}
+    assert all(not g.any() for g in host(ctx, imgs))     # tuning wrote no image
+    b.run()
+    for (acc, _), g in zip(want, host(ctx, imgs)):
+        assert np.array_equal(g, acc)
+    # tiny pools (paths regenerate in every pass) and every launch shape
+    for slots, v in [(256, 0), (4096, 1), (65536, 2)] + [(1 << 16, k) for k in range(len(shapes))]:
+        b.set_wavefront(slots, v)
+        b.run(zero=True)
+        got = host(ctx, imgs)
+        per, _ = b.rays()
+        for i, ((acc, rays), g) in enumerate(zip(want, got)):
+            assert np.array_equal(g, acc), (slots, v, i)
+            assert int(per[i]) == rays
+
+
+def test_wavefront_instanced_scene_with_sky(ctx, oracle):
+    """The two-level scene (instances, sky, no lamp) through the wavefront, exact and fast mode."""
+    sc = W.instanced_field(n_instances=300, tri_range=(500, 3000), width=40, height=24, sky_w=128, sky_h=64, spp=4,
+                           max_depth=12)
+    s = R.instanced_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    for exact in (0, 1):
+        p = L.native.trace_params(R.camera12(sc), sc["width"], sc["height"], sc["max_depth"], 1, 1, exact, 9)
+        acc, rays = s.trace(p, sc["spp"])
+        img = device_images([sc])[0]
+        b = L.native.Batch(ctx)
+        b.add(s, p, sc["spp"], img.data_ptr())
+        b.run()
+        got = host(ctx, [img])[0]
+        assert np.array_equal(got, acc)
+        assert int(b.rays()[0][0]) == rays
+        b.close()
