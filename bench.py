@@ -37,6 +37,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "Mrays/s (build + closest-hit pass over the builder workload)"
 METRIC_BATCH = "Mrays/s (256-scene batched launch: builds + path tracing, closest-hit + shadow rays)"
+METRIC_SERVE = "Mrays/s and p50/p99 job latency (served request stream, Poisson arrivals)"
 
 
 def parse():
@@ -51,11 +52,17 @@ def parse():
     ap.add_argument("--bits", type=int, default=30, choices=[30, 63])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--workload", default="builder", choices=["builder", "batch"])
+    ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve"])
+    ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
+    ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
+    ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
+    ap.add_argument("--wave-paths", type=int, default=8 << 20, help="serve: paths per wave")
     ap.add_argument("--scenes", type=int, default=256, help="batch: scenes (jobs)")
     ap.add_argument("--plain-steps", type=int, default=1, help="batch: timed passes of the plain path")
     ap.add_argument("--cpu-scenes", type=int, default=8, help="batch: scenes the CPU baseline samples")
     ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"], help="batch: the engine")
+    ap.add_argument("--stepped", action="store_true",
+                    help="batch: wavefront passes launched from the host (for ncu, which cannot see into graph loops)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)      # (at least 3 untimed steps before the timed ones)
     return a
@@ -321,15 +328,21 @@ def run_batch(a):
     b.run(build=True, zero=True)
     variant, grid, ns_task = b.tune()
     shapes = L.native.wavefront_shapes() if a.engine == "wavefront" else L.native.batch_shapes()
+    def batch_step():
+        if a.stepped:
+            b.run(build=True, zero=True, stepped=True)
+        else:
+            b.run(build=True, graph=True, zero=True)
+
     for _ in range(a.warmup):
-        b.run(build=True, graph=True, zero=True)
+        batch_step()
     ctx.sync()
     torch.cuda.synchronize()
     batch_imgs = [img.cpu() for img in imgs]
     same = all(torch.equal(x, y) for x, y in zip(plain_imgs, batch_imgs))
     per_job, rays = b.rays()
     clk = Clocks(local)
-    ms = timed(lambda: b.run(build=True, graph=True, zero=True), a.steps)
+    ms = timed(batch_step, a.steps)
     clocks = clk.stop()
     info = b.info()
     ms_step = ms / a.steps
@@ -387,13 +400,169 @@ def run_batch(a):
         print(json.dumps(line), flush=True)
 
 
+def serve_jobs(n, rate, seed, scenes, inst_ids):
+    """n jobs with Poisson arrivals at `rate`/s: (arrival s, scene index, width, height, spp, motion
+    frame or None); a tenth of them move the instances of an instanced scene."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    res = [(256, 256), (1280, 720), (1920, 1080)]
+    out = []
+    for i in range(n):
+        w, h = res[rng.integers(0, 3)]
+        spp = int(rng.choice([4, 16, 64]))
+        if rng.random() < 0.1:
+            out.append((float(t[i]), int(rng.choice(inst_ids)), w, h, spp, float(rng.uniform(1, 30))))
+        else:
+            out.append((float(t[i]), int(rng.integers(0, len(scenes))), w, h, spp, None))
+    return out
+
+
+def run_serve(a):
+    """--workload serve: 64 resident scenes (56 box scenes, triangles log-uniform in [1k, 2M], and 8
+    instanced boxes of 2000 instances), jobs (scene, resolution in {256^2, 720p, 1080p}, spp in {4,
+    16, 64}; a tenth move their scene's 2000 instances: the top level refit first) arriving as a
+    Poisson stream, served in waves by lrc_server under an HBM budget; then the same stream through
+    the plain path, one job at a time (lrc_trace per job). Latency = end - arrival (host clock)."""
+    import torch
+    import little_renderer_b200 as L
+    from little_renderer_b200 import render as R, workloads as W
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(17)
+    lo, hi = np.log(1_000), np.log(2_000_000)
+    counts = [int(np.exp(rng.uniform(lo, hi))) for _ in range(56)]
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    scenes, dicts = [], []
+    for i, n in enumerate(counts):
+        sc = W.box_scene(5000 + i, n, 256, 256, 16)
+        dicts.append(sc)
+        scenes.append(R.world_scene(ctx, sc, 1))
+    inst_ids = []
+    for i in range(8):
+        sc = W.instanced_box(6000 + i, n_instances=2000)
+        dicts.append(sc)
+        inst_ids.append(len(scenes))
+        scenes.append(R.instanced_box_scene(ctx, sc, 1))
+    motions = {k: W.rigid_motion(2000, 7000 + k) for k in inst_ids}
+    originals = {k: W.instance_records(dicts[k]) for k in inst_ids}
+    ctx.sync()
+    tris = sum(counts) + sum(len(dicts[k]["corners"]) for k in inst_ids)
+
+    def records(job):
+        k, frame = job[1], job[5]
+        return W.instance_records(dict(dicts[k], xf=W.moved_xf(dicts[k]["xf"], motions[k], frame)))
+
+    def params(job, idx):
+        sc = dicts[job[1]]
+        return L.native.trace_params(W.camera(sc["camera"], job[2] / job[3]), job[2], job[3], 8, 1, 1, 0, 9000 + idx)
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x), q))
+
+    results = {}
+    check = {}
+    clk = Clocks(0)
+    for rate in [float(r) for r in a.rates.split(",")]:
+        jobs = serve_jobs(a.jobs, rate, int(rate), scenes, inst_ids)
+        recs = [records(j) if j[5] is not None else None for j in jobs]
+        # served: submit each job at its arrival, step waves while any job is held
+        sv = L.native.Server(ctx, int(a.budget_gb * 2**30), a.wave_paths)
+        lat, rays_s, ids = [], 0, {}
+        nxt, done = 0, 0
+        t0 = L.native.clock_ms()
+        while done < len(jobs):
+            now = (L.native.clock_ms() - t0) / 1e3
+            while nxt < len(jobs) and jobs[nxt][0] <= now:
+                j = jobs[nxt]
+                ids[sv.submit(scenes[j[1]], params(j, nxt), j[4], recs[nxt], 0)] = nxt
+                nxt += 1
+            st = sv.state()
+            if st["queued"] + st["active"] == 0:
+                if nxt < len(jobs):
+                    time.sleep(max(0.0, min(0.002, jobs[nxt][0] - now)))
+                continue
+            if sv.step():
+                for jid, k in list(ids.items()):
+                    r = sv.result(jid)
+                    if r is None:
+                        continue
+                    lat.append(r[4] - (t0 + jobs[k][0] * 1e3))
+                    rays_s += r[1]
+                    if rate == float(a.rates.split(",")[0]) and k < 6:
+                        check[k] = sv.image(jid)
+                    sv.release(jid)
+                    del ids[jid]
+                    done += 1
+        span_s = (L.native.clock_ms() - t0) / 1e3
+        sv.close()
+        # plain: one job at a time, in arrival order, each traced alone
+        lat_p, rays_p = [], 0
+        imgs = {}
+        t0 = L.native.clock_ms()
+        for k, j in enumerate(jobs):
+            now = (L.native.clock_ms() - t0) / 1e3
+            if j[0] > now:
+                time.sleep(j[0] - now)
+            s = scenes[j[1]]
+            if recs[k] is not None:
+                s.move_instances(recs[k], 0)
+            img = torch.zeros(j[3], j[2], 4, device=dev)
+            s.trace_device(params(j, k), j[4], img.data_ptr())
+            ctx.sync()
+            lat_p.append(L.native.clock_ms() - (t0 + j[0] * 1e3))
+            if rate == float(a.rates.split(",")[0]) and k < 6:
+                imgs[k] = img.cpu().numpy()
+        span_p = (L.native.clock_ms() - t0) / 1e3
+        for k in inst_ids:
+            scenes[k].move_instances(originals[k], 1)
+        # rays of the plain pass: the served count (the same samples; checked on the first jobs' images)
+        rays_p = rays_s
+        results[str(int(rate))] = {
+            "served": {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mrays_s": rays_s / span_s / 1e6, "span_s": span_s},
+            "plain": {"p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99), "mrays_s": rays_p / span_p / 1e6,
+                      "span_s": span_p},
+            "jobs": len(jobs), "motion_jobs": sum(1 for j in jobs if j[5] is not None),
+            "paths": int(sum(j[2] * j[3] * j[4] for j in jobs)), "rays": int(rays_s)}
+        if imgs:
+            results[str(int(rate))]["images_equal_plain"] = all(np.array_equal(check[k], imgs[k]) for k in imgs)
+    clocks = clk.stop()
+    mid = results[sorted(results, key=float)[len(results) // 2]]
+    line = {"metric": METRIC_SERVE, "value": mid["served"]["mrays_s"], "unit": "Mrays/s", "n_gpus": 1,
+            "steps": len(results), "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"served request stream: 64 resident scenes ({tris} triangles; 8 with 2000 moving "
+                                   "instances), jobs {256^2, 720p, 1080p} x spp {4, 16, 64}, depth 8, Poisson arrivals",
+                       "rates": a.rates, "jobs_per_rate": a.jobs, "budget_gb": a.budget_gb,
+                       "wave_paths": a.wave_paths, "parallelism": "one GPU"},
+            "clocks": clocks, "rates": results}
+    for s in scenes:
+        s.close()
+    ctx.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
-        run_reference_batch(a) if a.workload == "batch" else run_reference(a)
+        if a.workload == "serve":
+            print(json.dumps({"impl": "reference", "metric": METRIC_SERVE, "unavailable":
+                              "the reference has no request server: its latency baseline is the plain one-job-at-a-time "
+                              "CUDA path timed beside the served one in --workload serve"}), flush=True)
+        elif a.workload == "batch":
+            run_reference_batch(a)
+        else:
+            run_reference(a)
         return
     if a.workload == "batch":
         run_batch(a)
+        return
+    if a.workload == "serve":
+        run_serve(a)
         return
     import torch
     import little_renderer_b200 as L

@@ -172,6 +172,23 @@ int lrc_scene_set_instances(lrc_scene *s, const float *records, uint32_t n, unsi
  * and the top level over the instances' boxes (LBVH, 30-bit keys, the reference's GPU top level,
  * trace_gpu.c:459-460, 1462-1463): after moving instances, only the top level is built again. */
 int lrc_scene_build_instances(lrc_scene *s, int mesh_builder, int key_bits);
+/* Moved instances (scene_update_instances, engine/rt/accel.c:197-207; the reference's top level
+ * follows them in build_tlas, accel.c:154-173): new records for the same n instances (host, or
+ * device with LRC_DEVICE), and the top level made again for them - LRC_TLAS_REFIT: the built
+ * tree's boxes from its leaves up (bvh_refit_boxes, engine/rt/bvh.c:471-485); LRC_TLAS_REBUILD:
+ * built again (LBVH); LRC_TLAS_AUTO: refit while the tree's SAH cost stays within 1.1x of its cost
+ * as built, else built again (the reference's TLAS_REFIT_GROWTH policy). */
+#define LRC_TLAS_REFIT 0
+#define LRC_TLAS_REBUILD 1
+#define LRC_TLAS_AUTO 2
+int lrc_scene_move_instances(lrc_scene *s, const float *records, uint32_t n, int mode, unsigned flags);
+/* The top level's SAH cost (bvh_cost, bvh.c:463-468: the nodes' surface areas over the root's). */
+int lrc_scene_tlas_cost(lrc_scene *s, double *cost);
+/* The bottom-up refit of any tree these builders made (root at nodes[0], node0 = 0): every box made
+ * again from the n items' new boxes (8 floats each, as lrc_build's), the topology kept; boxes to
+ * the bit bvh_refit_boxes' on that topology. Host arrays, or device ones with LRC_DEVICE. */
+int lrc_refit(lrc_ctx *ctx, uint32_t *nodes, const uint32_t *aux, uint32_t n, uint32_t ref_add, const float *boxes,
+              unsigned flags);
 /* The sky (Env, env.h:29-53; upload_sky, trace_gpu.c:1522-1569): w x h linear RGB, rows top to
  * bottom, times scale; its sampling tables (marg: h + 1 floats, cond: h x (w + 1), prob: w x h =
  * env_pixel_prob) or NULL: made here as env_prepare makes them (env.c:116-167, 341-363). Host.
@@ -227,6 +244,8 @@ typedef struct lrc_batch lrc_batch;
 #define LRC_BATCH_GRAPH 8u    /* run as one CUDA graph: captured after the first such run (which runs
                                  uncaptured, sizing every buffer), replayed while nothing it names changed */
 #define LRC_BATCH_ZERO 16u    /* clear each job's band of its image first */
+#define LRC_BATCH_STEPPED 32u /* wavefront: launch each pass's kernels from the host, no graph (slower;
+                                 for profilers that cannot see into a graph's loop); not with GRAPH */
 int lrc_batch_create(lrc_ctx *c, lrc_batch **out);
 void lrc_batch_destroy(lrc_batch *b);
 /* A job: lrc_trace(s, p, y0, rows, spp0, spp, d_accum, ..., LRC_DEVICE) as part of the batch;
@@ -265,6 +284,42 @@ int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_
  * replayed a graph. */
 int lrc_batch_info(const lrc_batch *b, uint64_t *tasks, uint64_t *pixels, int32_t *variant, int32_t *grid,
                    int32_t *graph_used);
+
+/* ---- a render server: jobs admitted as they arrive, traced together in waves --------------
+ * No counterpart in the reference (its GPU view traces one scene at a time, paced by the band
+ * scheduler, engine/gpu/view_gpu.c:1081-1190). Jobs are admitted in arrival order while their
+ * device bytes (the image; for moved instances, their own records and top level) fit the budget;
+ * each wave traces the next band of rows of every admitted job as one batch (the wavefront), the
+ * wave's paths shared evenly, so jobs that arrive join at the next wave and small jobs finish in a
+ * wave or two. A band holds all of its pixels' samples: a job's image is the lrc_trace image of it
+ * alone, to the bit. One host thread drives a server. */
+typedef struct lrc_server lrc_server;
+int lrc_server_create(lrc_ctx *c, uint64_t hbm_budget_bytes, uint64_t wave_paths, lrc_server **out);
+void lrc_server_destroy(lrc_server *sv);
+/* Queues a job: the whole image p (fast mode) of scene s at spp samples per pixel. records (host, n
+ * x 32 floats as lrc_scene_set_instances's; n = the scene's instance count) moves its instances for
+ * this job only: the job gets its own copy of the instance layer, its top level refit
+ * (LRC_TLAS_REFIT) or built again (LRC_TLAS_REBUILD) on the device when admitted; NULL: the scene
+ * as it is. A job larger than the whole budget: LRC_E_TOO_BIG. */
+int lrc_server_submit(lrc_server *sv, lrc_scene *s, const lrc_trace_params *p, uint32_t spp, const float *records,
+                      uint32_t n, int tlas_mode, uint64_t *id);
+/* One wave: admission, the next band of every admitted job traced in one batch run, waited for;
+ * *finished: the jobs it finished. */
+int lrc_server_step(lrc_server *sv, int32_t *finished);
+/* A finished job (LRC_RETRY while not): its image (device, W x H x 4 floats: sum and count), its
+ * rays, and the server clock's times (ms) of its submit, admission and end. */
+int lrc_server_result(lrc_server *sv, uint64_t id, const float **d_image, uint64_t *rays, double *t_submit,
+                      double *t_admit, double *t_done);
+/* A finished job's image copied to host memory (W x H x 4 floats; gpu_view_trace_read's sum and
+ * count, view_gpu.h:118-124); waits. LRC_RETRY while the job is not finished. */
+int lrc_server_read(lrc_server *sv, uint64_t id, float *out);
+/* Frees a finished job (its image) and its bytes in the budget. */
+int lrc_server_release(lrc_server *sv, uint64_t id);
+int lrc_server_state(const lrc_server *sv, int32_t *queued, int32_t *active, int32_t *finished, uint64_t *bytes);
+/* The server's clock (ms; monotonic). */
+double lrc_server_clock(void);
+/* The batch a server runs its waves with (to set its engine or wavefront size; do not add jobs). */
+lrc_batch *lrc_server_batch(lrc_server *sv);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,23 @@ int scene_build_on(lrc_scene *s, int builder, int key_bits, void **scratch, size
     return LRC_OK;
 }
 
+// the top level over n instances (records at d_inst): LBVH over their world boxes, 30-bit keys,
+// bounds their union (upload_instances, trace_gpu.c:1415-1463) into d_nodes / d_aux; d_boxes
+// (n x 8 floats) and d_small (64 words) are scratch, as is the build scratch
+cudaError_t build_tlas_on(lrc_ctx *c, const float *d_inst, uint32_t n, Node *d_nodes, uint32_t *d_aux, float *d_boxes,
+                          uint32_t *d_small, void *scratch, size_t scratch_cap, cudaStream_t st, lrc::StageTimer *timer) {
+    uint32_t *keys = d_small;
+    float *bounds = reinterpret_cast<float *>(d_small + 8), *lo_ext = reinterpret_cast<float *>(d_small + 16);
+    cudaError_t e = lrc::pt_inst_boxes(d_inst, n, d_boxes, st);
+    if (!e) e = lrc::boxes_bounds(d_boxes, n, keys, st, c->num_sms, true);
+    if (!e) e = lrc::bounds_params(keys, bounds, lo_ext, st);
+    lrc_build_params p{};
+    p.n = n; p.key_bits = 30; p.builder = 0;
+    if (!e) e = lrc::build_device_ext(p, d_boxes, lo_ext, d_nodes, d_aux, scratch, scratch_cap, c->d_status, c->num_sms,
+                                      st, nullptr, timer);
+    return e;
+}
+
 }  // namespace lrcapi
 
 extern "C" {
@@ -563,7 +580,6 @@ int lrc_scene_build_instances(lrc_scene *s, int mesh_builder, int key_bits) {
     s->tlas_n = 0;
     const uint32_t n = s->ninst;
     if (!n) return LRC_OK;
-    // the top level: LBVH over the instances' world boxes, bounds their union (upload_instances :1415-1463)
     if (s->tlas_cap < n) {
         cudaFree(s->d_tlas_nodes);
         cudaFree(s->d_tlas_aux);
@@ -576,16 +592,89 @@ int lrc_scene_build_instances(lrc_scene *s, int mesh_builder, int key_bits) {
     if (!e) e = reserve(&c->scratch, &c->scratch_cap, lrc::build_scratch_bytes(n, 30, 0));
     if (e) return cuda_status(c, e, "top level memory");
     c->timer.begin(LRC_TS_BOXES, c->st);
-    e = lrc::pt_inst_boxes(s->d_inst, n, s->d_boxes, c->st);
-    if (!e) e = lrc::boxes_bounds(s->d_boxes, n, keys, c->st, c->num_sms, true);
-    if (!e) e = lrc::bounds_params(keys, bounds, lo_ext, c->st);
-    lrc_build_params p{};
-    p.n = n; p.key_bits = 30; p.builder = 0;
-    if (!e) e = lrc::build_device_ext(p, s->d_boxes, lo_ext, s->d_tlas_nodes, s->d_tlas_aux, c->scratch, c->scratch_cap,
-                                      c->d_status, c->num_sms, c->st, nullptr, &c->timer);
+    e = build_tlas_on(c, s->d_inst, n, s->d_tlas_nodes, s->d_tlas_aux, s->d_boxes, s->d_small, c->scratch, c->scratch_cap,
+                      c->st, &c->timer);
     if (e) return cuda_status(c, e, "top level");
     s->tlas_n = n;
+    s->tlas_cost = -1.0;
     return LRC_OK;
+}
+
+int lrc_scene_move_instances(lrc_scene *s, const float *records, uint32_t n, int mode, unsigned flags) {
+    if (!s || !records) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (mode < LRC_TLAS_REFIT || mode > LRC_TLAS_AUTO) return fail(c, LRC_E_INVALID, "mode: refit, rebuild or auto");
+    if (!s->tlas_n || n != s->ninst) return fail(c, LRC_E_INVALID, "moves the built instances only (same count)");
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaMemcpyAsync(s->d_inst, records, (size_t)n * 128,
+                                    (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->st);
+    if (e) return cuda_status(c, e, "instances");
+    if (mode == LRC_TLAS_REBUILD) {
+        s->tlas_n = 0;
+        e = reserve(&c->scratch, &c->scratch_cap, lrc::build_scratch_bytes(n, 30, 0));
+        if (!e) e = build_tlas_on(c, s->d_inst, n, s->d_tlas_nodes, s->d_tlas_aux, s->d_boxes, s->d_small, c->scratch,
+                                  c->scratch_cap, c->st, &c->timer);
+        if (e) return cuda_status(c, e, "top level");
+        s->tlas_n = n;
+        s->tlas_cost = -1.0;
+        return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+    }
+    if (mode == LRC_TLAS_AUTO && s->tlas_cost < 0) {        // (the cost the refits are held against)
+        int rc = lrc_scene_tlas_cost(s, &s->tlas_cost);
+        if (rc) return rc;
+    }
+    e = reserve(&c->scratch, &c->scratch_cap, lrc::refit_scratch_bytes(n));
+    if (!e) e = lrc::refit_device(s->d_tlas_nodes, s->d_tlas_aux, n, 0, s->d_inst, 8, 6, c->scratch, c->scratch_cap,
+                                  c->d_status, c->st);
+    if (e) return cuda_status(c, e, "top level refit");
+    if (mode == LRC_TLAS_AUTO) {
+        double cost = 0;
+        int rc = lrc_scene_tlas_cost(s, &cost);
+        if (rc) return rc;
+        if (cost > 1.1 * s->tlas_cost) return lrc_scene_move_instances(s, s->d_inst, n, LRC_TLAS_REBUILD, LRC_DEVICE);
+    }
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_scene_tlas_cost(lrc_scene *s, double *cost) {
+    if (!s || !cost) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (!s->tlas_n) return fail(c, LRC_E_INVALID, "the scene has no top level");
+    DeviceGuard g(c->device);
+    double *d = reinterpret_cast<double *>(s->d_small + 32);
+    cudaError_t e = lrc::tree_cost_device(s->d_tlas_nodes, s->tlas_n, d, c->st);
+    if (!e) e = cudaMemcpyAsync(cost, d, 8, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "top level cost");
+    return check_status(c);
+}
+
+int lrc_refit(lrc_ctx *c, uint32_t *nodes, const uint32_t *aux, uint32_t n, uint32_t ref_add, const float *boxes,
+              unsigned flags) {
+    if (!c || !nodes || !aux || !boxes) return LRC_E_INVALID;
+    if (!n) return LRC_OK;
+    if (n >= (1u << 30)) return fail(c, LRC_E_INVALID, "more than 2^30 - 1 items");
+    DeviceGuard g(c->device);
+    const size_t b_nodes = (2 * (size_t)n - 1) * 32, b_aux = (size_t)n * 4, b_boxes = (size_t)n * 32;
+    cudaError_t e = reserve(&c->scratch, &c->scratch_cap, lrc::refit_scratch_bytes(n));
+    if (e) return cuda_status(c, e, "refit scratch");
+    Node *d_nodes = reinterpret_cast<Node *>(nodes);
+    const uint32_t *d_aux = aux;
+    const float *d_boxes = boxes;
+    if (!(flags & LRC_DEVICE)) {
+        e = reserve(&c->stage, &c->stage_cap, al(b_nodes) + al(b_aux) + al(b_boxes));
+        if (e) return cuda_status(c, e, "refit staging");
+        char *st = static_cast<char *>(c->stage);
+        d_nodes = reinterpret_cast<Node *>(st);
+        d_aux = reinterpret_cast<const uint32_t *>(st + al(b_nodes));
+        d_boxes = reinterpret_cast<const float *>(st + al(b_nodes) + al(b_aux));
+        e = cudaMemcpyAsync(d_nodes, nodes, b_nodes, cudaMemcpyHostToDevice, c->st);
+        if (!e) e = cudaMemcpyAsync(const_cast<uint32_t *>(d_aux), aux, b_aux, cudaMemcpyHostToDevice, c->st);
+        if (!e) e = cudaMemcpyAsync(const_cast<float *>(d_boxes), boxes, b_boxes, cudaMemcpyHostToDevice, c->st);
+    }
+    if (!e) e = lrc::refit_device(d_nodes, d_aux, n, ref_add, d_boxes, 2, 0, c->scratch, c->scratch_cap, c->d_status, c->st);
+    if (!e && !(flags & LRC_DEVICE)) e = cudaMemcpyAsync(nodes, d_nodes, b_nodes, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_refit");
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 
 int lrc_scene_set_sky(lrc_scene *s, const float *rgb, int32_t w, int32_t h, const float *marg, const float *cond,

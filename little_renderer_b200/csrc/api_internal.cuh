@@ -61,6 +61,7 @@ struct lrc_scene {
     uint32_t *d_tlas_aux = nullptr;
     size_t tlas_cap = 0;
     uint32_t tlas_n = 0;
+    double tlas_cost = -1.0;      // its SAH cost as built (-1: not yet reckoned)
     // the sky
     float *d_env = nullptr;       // rgbp (w x h float4), cond, marg
     int env_w = 0, env_h = 0, env_weighted = 0;
@@ -203,6 +204,17 @@ inline lrc::TraceTables tables(const lrc_scene *s) {
 // graph capture)
 int scene_build_on(lrc_scene *s, int builder, int key_bits, void **scratch, size_t *scratch_cap, cudaStream_t st,
                    lrc::StageTimer *timer, bool no_alloc);
+// a batch job's own instances: records and their top level (nodes, aux) in place of the scene's
+struct InstView {
+    const float *inst;
+    const void *tlas_nodes;
+    const uint32_t *tlas_aux;
+};
+// lrc_batch_add (no build) with the job's own instances (a server's moving-instance job)
+int batch_add_view(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
+                   uint32_t spp, float *d_accum, const InstView &view);
+cudaError_t build_tlas_on(lrc_ctx *c, const float *d_inst, uint32_t n, Node *d_nodes, uint32_t *d_aux, float *d_boxes,
+                          uint32_t *d_small, void *scratch, size_t scratch_cap, cudaStream_t st, lrc::StageTimer *timer);
 
 }  // namespace lrcapi
 

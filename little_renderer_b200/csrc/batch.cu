@@ -35,6 +35,7 @@ struct lrc_batch {
         uint32_t spp0, spp;
         float *accum;
         int32_t builder, key_bits;
+        InstView view;                    // the job's own instances (moved), or none: the scene's
     };
     lrc_ctx *ctx = nullptr;
     std::vector<Job> jobs;
@@ -70,7 +71,7 @@ struct lrc_batch {
 
 namespace {
 
-constexpr unsigned kBatchFlags = LRC_BATCH_BUILD | LRC_BATCH_GRAPH | LRC_BATCH_ZERO;
+constexpr unsigned kBatchFlags = LRC_BATCH_BUILD | LRC_BATCH_GRAPH | LRC_BATCH_ZERO | LRC_BATCH_STEPPED;
 
 int group_for(const lrc_trace_params &p, uint32_t spp) {
     if (p.exact) return 1;
@@ -106,6 +107,11 @@ void destroy_graph(lrc_batch *b) {
 // over all its shapes)
 lrc::PtScene view_of(const lrc_batch::Job &J, bool building) {
     lrc::PtScene S = pt_scene(J.s);
+    if (J.view.inst) {
+        S.inst = reinterpret_cast<const float4 *>(J.view.inst);
+        S.tlas_nodes = reinterpret_cast<const float4 *>(J.view.tlas_nodes);
+        S.tlas_aux = J.view.tlas_aux;
+    }
     if (building && J.builder >= 0) {
         const uint32_t n = J.s->ntris + J.s->nprims;
         S.nnodes = n ? 2 * n - 1 : 0;
@@ -191,7 +197,7 @@ int prepare(lrc_batch *b) {
     for (size_t q = 0; q < nj; q++) {
         const lrc_batch::Job &J = b->jobs[b->order[q]];
         lrc::BatchJob &T = b->table[q];
-        T.S = pt_scene(J.s);
+        T.S = view_of(J, false);
         T.P = params_of(J);
         T.task0 = task;
         T.pix0 = pix;
@@ -267,7 +273,11 @@ int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool 
     }
     if (!e && b->engine == 0)
         e = lrc::batch_trace(b->d_jobs, (uint32_t)nj, limit, b->d_ctr, c->d_status, b->variant, b->grid, st);
-    if (!e && b->engine == 1) {
+    if (!e && b->engine == 1 && !capturing && (flags & LRC_BATCH_STEPPED)) {
+        const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
+        e = lrc::wf_run_stepped(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, c->num_sms,
+                                max_passes(b, limit), st);
+    } else if (!e && b->engine == 1) {
         if (!capturing) return fail(c, LRC_E_INVALID, "the wavefront runs as a captured graph");
         const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
         e = lrc::wf_capture_loop(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, c->num_sms,
@@ -318,7 +328,7 @@ int capture(lrc_batch *b, unsigned flags) {
 // flight), then at each closest-hit / shadow launch shape at the best size; keeps the fastest
 int tune_wavefront(lrc_batch *b, unsigned long long n, int32_t *variant, int32_t *slots, double *ns_per_task) {
     lrc_ctx *c = b->ctx;
-    const uint32_t sizes[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22};
+    const uint32_t sizes[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22, 1u << 23};
     uint32_t top = 1u << 18;
     for (uint32_t m : sizes)
         if ((unsigned long long)m / 2 < n) top = m;   // (no larger than the tasks need)
@@ -390,6 +400,17 @@ void note_built(lrc_batch *b) {   // (what captured builds' host side records)
 
 }  // namespace
 
+namespace lrcapi {
+int batch_add_view(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
+                   uint32_t spp, float *d_accum, const InstView &view) {
+    int rc = lrc_batch_add(b, s, p, y0, rows, spp0, spp, d_accum, -1, 30);
+    if (rc) return rc;
+    if (view.inst && !s->tlas_n) return fail(b->ctx, LRC_E_INVALID, "own instances for a scene without instances");
+    b->jobs.back().view = view;
+    return LRC_OK;
+}
+}  // namespace lrcapi
+
 extern "C" {
 
 int lrc_batch_create(lrc_ctx *c, lrc_batch **out) {
@@ -428,7 +449,7 @@ int lrc_batch_add(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t
     if (builder < -1 || builder > 2) return fail(c, LRC_E_INVALID, "builder: -1 (none), 0 (LBVH), 1 (PLOC) or 2 (both)");
     if (builder >= 0 && key_bits != 30 && key_bits != 63) return fail(c, LRC_E_INVALID, "key_bits must be 30 or 63");
     if (s->ninst && builder >= 0) return fail(c, LRC_E_INVALID, "instanced scenes are built by lrc_scene_build_instances");
-    b->jobs.push_back({s, *p, y0, rows, spp0, spp, d_accum, builder, key_bits});
+    b->jobs.push_back({s, *p, y0, rows, spp0, spp, d_accum, builder, key_bits, InstView{}});
     b->prepared = false;
     return LRC_OK;
 }
@@ -444,6 +465,7 @@ int lrc_batch_jobs(const lrc_batch *b) { return b ? (int)b->jobs.size() : 0; }
 
 int lrc_batch_run(lrc_batch *b, unsigned flags) {
     if (!b || (flags & ~kBatchFlags)) return LRC_E_INVALID;
+    if ((flags & LRC_BATCH_STEPPED) && (flags & LRC_BATCH_GRAPH)) return fail(b->ctx, LRC_E_INVALID, "STEPPED is not GRAPH");
     lrc_ctx *c = b->ctx;
     if (b->jobs.empty()) return LRC_OK;
     for (const lrc_batch::Job &J : b->jobs) {
@@ -458,6 +480,16 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
         }
     }
     b->graph_used = 0;
+    if (b->engine == 1 && (flags & LRC_BATCH_STEPPED)) {   // (plain launches, pass by pass)
+        if (flags & LRC_BATCH_BUILD)
+            for (const lrc_batch::Job *J : builds_of(b)) {
+                int rc = build_job(b, J, c->st, false);
+                if (rc) return rc;
+            }
+        int rc = prepare(b);
+        if (!rc) rc = enqueue(b, flags, c->st, false, false, true, b->ntasks);
+        return rc;
+    }
     const bool cached = b->exec && b->prepared && b->graph_flags == flags && signature(b, flags) == b->graph_sig;
     if (b->engine == 1) {
         if (!cached || ((flags & LRC_BATCH_BUILD) && !(flags & LRC_BATCH_GRAPH))) {

@@ -128,6 +128,15 @@ SortU32 sort_u32_carve(void *scratch, uint64_t n);
 cudaError_t sort_u32_clear(const SortU32 &S, cudaStream_t st);
 cudaError_t sort_u32_run(const SortU32 &S, uint32_t *d_status, cudaStream_t st, const uint32_t **perm_out);
 
+// refit (refit.cu): the boxes of a built tree (root at node 0, leaves' aux = item + ref_add) made
+// again from the items' boxes up - item k's lo at boxes float4 [k * stride4 + lo_at], hi at the
+// next - and the tree's SAH cost (nodes' areas over the root's, in double, in a fixed order)
+size_t refit_scratch_bytes(uint32_t n);
+cudaError_t refit_device(Node *d_nodes, const uint32_t *d_aux, uint32_t n, uint32_t ref_add, const float *d_boxes,
+                         uint32_t stride4, uint32_t lo_at, void *scratch, size_t scratch_bytes, uint32_t *d_status,
+                         cudaStream_t st);
+cudaError_t tree_cost_device(const Node *d_nodes, uint32_t n, double *d_out, cudaStream_t st);
+
 // traversal internals (traverse.cu)
 struct TraceTables {
     const Node *nodes;
@@ -262,6 +271,10 @@ int wf_variant_shape(int variant, int *block, int *minb);
 cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
                             uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st,
                             cudaStream_t body_st);
+// The same loop with each pass's kernels launched from the host (no graph; the host reads the
+// queued count after every pass): for profilers that cannot see into a graph's loop.
+cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
+                           uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st);
 // the sky's sampling tables as env_prepare makes them (host_tables.cu): marg h + 1, cond h x (w + 1),
 // prob w x h; returns false when no pixel weighs anything (sum 0)
 bool env_tables(const float *rgb, int w, int h, float *marg, float *cond, float *prob);

@@ -1,0 +1,308 @@
+// serve.cu - a render server: jobs (scene, image, spp, optionally moved instances) admitted as
+// they arrive, by an HBM byte budget, and traced together in waves through the batch's wavefront.
+//
+// No counterpart in the reference, whose GPU view traces one scene at a time and paces its submits
+// by the band scheduler (gpu_view_trace_more, engine/gpu/view_gpu.c:1081-1190: rows x repeats per
+// submit from the measured ms per pass). Here every wave takes the next band of rows of EVERY
+// admitted job - the band sized so that the wave's paths are shared evenly among them - and runs
+// them as one batch: jobs that arrive while others are on the GPU join at the next wave (continuous
+// batching), a small job is done after a wave or two however large the others are, and the
+// device's paths in flight are always full. A band traces all of its pixels' samples, so a job's
+// image is the one lrc_trace makes of it alone, to the bit, whatever else shares its waves.
+//
+// Admission holds a job's bytes - its image, and for moved instances its own records and top level -
+// against the budget, in arrival order; a job larger than the whole budget is refused at submit.
+// A moved-instance job gets its own copy of the scene's instance layer (records and top level, the
+// meshes' trees shared), its top level refit (bvh_refit_boxes's bottom-up refit) or built again on
+// the device when admitted, so jobs of the same scene at different frames run side by side.
+#include "api_internal.cuh"
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <new>
+#include <unordered_map>
+#include <vector>
+
+using namespace lrcapi;
+
+struct lrc_server {
+    struct Job {
+        uint64_t id = 0;
+        lrc_scene *s = nullptr;
+        lrc_trace_params p{};
+        uint32_t spp = 0;
+        std::vector<float> records;     // moved instances (32 floats each), or none
+        int tlas_mode = 0;
+        float *d_img = nullptr;         // W x H float4 (sum, count)
+        float *d_inst = nullptr;        // the job's instance records
+        Node *d_tlas = nullptr;         // and their top level
+        uint32_t *d_tlas_aux = nullptr;
+        size_t bytes = 0;
+        int32_t next_row = 0, band = 0;
+        uint64_t rays = 0;
+        double t_submit = 0, t_admit = 0, t_done = 0;
+        int state = 0;                  // 0 queued, 1 admitted, 2 finished
+    };
+    lrc_ctx *ctx = nullptr;
+    lrc_batch *batch = nullptr;
+    uint64_t budget = 0, wave_paths = 0, in_use = 0;
+    uint64_t next_id = 1;
+    std::deque<Job *> queued;
+    std::vector<Job *> active;
+    std::unordered_map<uint64_t, Job *> jobs;
+    int32_t finished = 0;
+    // scratch for the jobs' top levels (build / refit)
+    void *scratch = nullptr;
+    size_t scratch_cap = 0;
+    float *d_boxes = nullptr;
+    size_t boxes_cap = 0;
+    uint32_t *d_small = nullptr;
+};
+
+namespace {
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+size_t job_bytes(const lrc_server::Job &J) {
+    size_t b = (size_t)J.p.width * J.p.height * 16;
+    const size_t n = J.records.size() / 32;
+    if (n) b += n * 128 + (2 * n - 1) * 32 + n * 4;
+    return b;
+}
+
+void free_job(lrc_server *sv, lrc_server::Job *J) {
+    lrc_ctx *c = sv->ctx;
+    if (J->d_img) cudaFreeAsync(J->d_img, c->st);
+    if (J->d_inst) cudaFreeAsync(J->d_inst, c->st);
+    if (J->d_tlas) cudaFreeAsync(J->d_tlas, c->st);
+    if (J->d_tlas_aux) cudaFreeAsync(J->d_tlas_aux, c->st);
+    J->d_img = nullptr;
+    J->d_inst = nullptr;
+    J->d_tlas = nullptr;
+    J->d_tlas_aux = nullptr;
+}
+
+// the job's device memory: its image (cleared) and, for moved instances, its records and top level
+int admit(lrc_server *sv, lrc_server::Job *J) {
+    lrc_ctx *c = sv->ctx;
+    const size_t img = (size_t)J->p.width * J->p.height * 16;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&J->d_img), img, c->st);
+    if (!e) e = cudaMemsetAsync(J->d_img, 0, img, c->st);
+    const uint32_t n = (uint32_t)(J->records.size() / 32);
+    if (!e && n) {
+        lrc_scene *s = J->s;
+        e = cudaMallocAsync(reinterpret_cast<void **>(&J->d_inst), (size_t)n * 128, c->st);
+        if (!e) e = cudaMallocAsync(reinterpret_cast<void **>(&J->d_tlas), (2 * (size_t)n - 1) * 32, c->st);
+        if (!e) e = cudaMallocAsync(reinterpret_cast<void **>(&J->d_tlas_aux), (size_t)n * 4, c->st);
+        if (!e) e = cudaMemcpyAsync(J->d_inst, J->records.data(), (size_t)n * 128, cudaMemcpyHostToDevice, c->st);
+        if (!e && J->tlas_mode == LRC_TLAS_REBUILD) {
+            e = reserve(reinterpret_cast<void **>(&sv->d_boxes), &sv->boxes_cap, (size_t)n * 32);
+            if (!e) e = reserve(&sv->scratch, &sv->scratch_cap, lrc::build_scratch_bytes(n, 30, 0));
+            if (!e) e = build_tlas_on(c, J->d_inst, n, J->d_tlas, J->d_tlas_aux, sv->d_boxes, sv->d_small, sv->scratch,
+                                      sv->scratch_cap, c->st, nullptr);
+        } else if (!e) {
+            // the scene's top level, refit for the job's boxes (its topology as built)
+            e = cudaMemcpyAsync(J->d_tlas, s->d_tlas_nodes, (2 * (size_t)n - 1) * 32, cudaMemcpyDeviceToDevice, c->st);
+            if (!e) e = cudaMemcpyAsync(J->d_tlas_aux, s->d_tlas_aux, (size_t)n * 4, cudaMemcpyDeviceToDevice, c->st);
+            if (!e) e = reserve(&sv->scratch, &sv->scratch_cap, lrc::refit_scratch_bytes(n));
+            if (!e) e = lrc::refit_device(J->d_tlas, J->d_tlas_aux, n, 0, J->d_inst, 8, 6, sv->scratch, sv->scratch_cap,
+                                          c->d_status, c->st);
+        }
+    }
+    if (e) {
+        free_job(sv, J);
+        return cuda_status(c, e, "server admission");
+    }
+    J->state = 1;
+    J->t_admit = now_ms();
+    sv->in_use += J->bytes;
+    return LRC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+double lrc_server_clock(void) { return now_ms(); }
+
+int lrc_server_create(lrc_ctx *c, uint64_t hbm_budget_bytes, uint64_t wave_paths, lrc_server **out) {
+    if (!c || !out || !hbm_budget_bytes || !wave_paths) return LRC_E_INVALID;
+    *out = nullptr;
+    lrc_server *sv = new (std::nothrow) lrc_server;
+    if (!sv) return LRC_RETRY;
+    sv->ctx = c;
+    sv->budget = hbm_budget_bytes;
+    sv->wave_paths = wave_paths;
+    DeviceGuard g(c->device);
+    int rc = lrc_batch_create(c, &sv->batch);
+    cudaError_t e = rc ? cudaSuccess : cudaMalloc(&sv->d_small, 256);
+    if (rc || e) {
+        if (sv->batch) lrc_batch_destroy(sv->batch);
+        delete sv;
+        return rc ? rc : cuda_status(c, e, "server");
+    }
+    *out = sv;
+    return LRC_OK;
+}
+
+void lrc_server_destroy(lrc_server *sv) {
+    if (!sv) return;
+    DeviceGuard g(sv->ctx->device);
+    lrc_batch_destroy(sv->batch);
+    for (auto &kv : sv->jobs) {
+        free_job(sv, kv.second);
+        delete kv.second;
+    }
+    cudaStreamSynchronize(sv->ctx->st);
+    cudaFree(sv->scratch);
+    cudaFree(sv->d_boxes);
+    cudaFree(sv->d_small);
+    delete sv;
+}
+
+int lrc_server_submit(lrc_server *sv, lrc_scene *s, const lrc_trace_params *p, uint32_t spp, const float *records,
+                      uint32_t n, int tlas_mode, uint64_t *id) {
+    if (!sv || !s || !p || s->ctx != sv->ctx || (n && !records)) return LRC_E_INVALID;
+    lrc_ctx *c = sv->ctx;
+    if (p->width <= 0 || p->height <= 0 || spp == 0 || spp >= (1u << 31))
+        return fail(c, LRC_E_INVALID, "a job is a whole image with spp >= 1");
+    if (p->exact) return fail(c, LRC_E_INVALID, "served jobs trace in fast mode");
+    if (n && (n != s->ninst || !s->tlas_n)) return fail(c, LRC_E_INVALID, "moved instances: the scene's instances, built");
+    if (n && (tlas_mode < LRC_TLAS_REFIT || tlas_mode > LRC_TLAS_REBUILD))
+        return fail(c, LRC_E_INVALID, "a job's top level is refit or rebuilt");
+    lrc_server::Job *J = new (std::nothrow) lrc_server::Job;
+    if (!J) return LRC_RETRY;
+    J->id = sv->next_id++;
+    J->s = s;
+    J->p = *p;
+    J->spp = spp;
+    if (n) J->records.assign(records, records + (size_t)n * 32);
+    J->tlas_mode = tlas_mode;
+    J->bytes = job_bytes(*J);
+    if (J->bytes > sv->budget) {
+        delete J;
+        return fail(c, LRC_E_TOO_BIG, "the job needs more device memory than the whole budget");
+    }
+    J->t_submit = now_ms();
+    sv->queued.push_back(J);
+    sv->jobs[J->id] = J;
+    if (id) *id = J->id;
+    return LRC_OK;
+}
+
+int lrc_server_step(lrc_server *sv, int32_t *finished) {
+    if (!sv) return LRC_E_INVALID;
+    lrc_ctx *c = sv->ctx;
+    DeviceGuard g(c->device);
+    if (finished) *finished = 0;
+    // admission, in arrival order, while the budget holds
+    while (!sv->queued.empty() && sv->in_use + sv->queued.front()->bytes <= sv->budget) {
+        lrc_server::Job *J = sv->queued.front();
+        int rc = admit(sv, J);
+        if (rc) return rc;
+        sv->queued.pop_front();
+        sv->active.push_back(J);
+    }
+    if (sv->active.empty()) return LRC_OK;
+    // the wave: the next band of every admitted job, the paths shared evenly
+    const uint64_t share = sv->wave_paths / sv->active.size() + 1;
+    int rc = lrc_batch_clear(sv->batch);
+    for (lrc_server::Job *J : sv->active) {
+        const uint64_t row_paths = (uint64_t)J->p.width * J->spp;
+        int32_t rows = (int32_t)std::max<uint64_t>(1, share / row_paths);
+        rows = std::min(rows, J->p.height - J->next_row);
+        J->band = rows;
+        InstView v{J->d_inst, J->d_tlas, J->d_tlas_aux};
+        if (!rc) rc = batch_add_view(sv->batch, J->s, &J->p, J->next_row, rows, 0, J->spp, J->d_img, v);
+    }
+    if (!rc) rc = lrc_batch_run(sv->batch, 0);
+    std::vector<uint64_t> rays(sv->active.size());
+    if (!rc) rc = lrc_batch_rays(sv->batch, rays.data(), nullptr);   // (waits for the wave)
+    if (rc) return rc;
+    const double t = now_ms();
+    std::vector<lrc_server::Job *> still;
+    for (size_t i = 0; i < sv->active.size(); i++) {
+        lrc_server::Job *J = sv->active[i];
+        J->rays += rays[i];
+        J->next_row += J->band;
+        if (J->next_row >= J->p.height) {
+            J->state = 2;
+            J->t_done = t;
+            sv->finished++;
+            if (finished) (*finished)++;
+            if (J->d_inst) {                            // (its instances are done with; its image stays)
+                cudaFreeAsync(J->d_inst, c->st);
+                cudaFreeAsync(J->d_tlas, c->st);
+                cudaFreeAsync(J->d_tlas_aux, c->st);
+                J->d_inst = nullptr;
+                J->d_tlas = nullptr;
+                J->d_tlas_aux = nullptr;
+                sv->in_use -= J->bytes - (size_t)J->p.width * J->p.height * 16;
+                J->bytes = (size_t)J->p.width * J->p.height * 16;
+            }
+        } else {
+            still.push_back(J);
+        }
+    }
+    sv->active.swap(still);
+    return LRC_OK;
+}
+
+int lrc_server_result(lrc_server *sv, uint64_t id, const float **d_image, uint64_t *rays, double *t_submit,
+                      double *t_admit, double *t_done) {
+    if (!sv) return LRC_E_INVALID;
+    auto it = sv->jobs.find(id);
+    if (it == sv->jobs.end()) return fail(sv->ctx, LRC_E_INVALID, "no such job");
+    const lrc_server::Job *J = it->second;
+    if (J->state != 2) return LRC_RETRY;
+    if (d_image) *d_image = J->d_img;
+    if (rays) *rays = J->rays;
+    if (t_submit) *t_submit = J->t_submit;
+    if (t_admit) *t_admit = J->t_admit;
+    if (t_done) *t_done = J->t_done;
+    return LRC_OK;
+}
+
+int lrc_server_read(lrc_server *sv, uint64_t id, float *out) {
+    if (!sv || !out) return LRC_E_INVALID;
+    auto it = sv->jobs.find(id);
+    if (it == sv->jobs.end()) return fail(sv->ctx, LRC_E_INVALID, "no such job");
+    const lrc_server::Job *J = it->second;
+    if (J->state != 2) return LRC_RETRY;
+    DeviceGuard g(sv->ctx->device);
+    cudaError_t e = cudaMemcpyAsync(out, J->d_img, (size_t)J->p.width * J->p.height * 16, cudaMemcpyDeviceToHost,
+                                    sv->ctx->st);
+    if (e) return cuda_status(sv->ctx, e, "server read");
+    return check_status(sv->ctx);
+}
+
+int lrc_server_release(lrc_server *sv, uint64_t id) {
+    if (!sv) return LRC_E_INVALID;
+    auto it = sv->jobs.find(id);
+    if (it == sv->jobs.end()) return fail(sv->ctx, LRC_E_INVALID, "no such job");
+    lrc_server::Job *J = it->second;
+    if (J->state != 2) return fail(sv->ctx, LRC_E_INVALID, "the job is not finished");
+    DeviceGuard g(sv->ctx->device);
+    free_job(sv, J);
+    sv->in_use -= J->bytes;
+    sv->finished--;
+    sv->jobs.erase(it);
+    delete J;
+    return LRC_OK;
+}
+
+lrc_batch *lrc_server_batch(lrc_server *sv) { return sv ? sv->batch : nullptr; }
+
+int lrc_server_state(const lrc_server *sv, int32_t *queued, int32_t *active, int32_t *finished, uint64_t *bytes) {
+    if (!sv) return LRC_E_INVALID;
+    if (queued) *queued = (int32_t)sv->queued.size();
+    if (active) *active = (int32_t)sv->active.size();
+    if (finished) *finished = sv->finished;
+    if (bytes) *bytes = sv->in_use;
+    return LRC_OK;
+}
+
+}  // extern "C"

@@ -180,10 +180,12 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
     }
 }
 
-// the closest hit of every queued ray; sets the loop's condition (another pass while rays are queued)
+// the closest hit of every queued ray (warps fetch 32 rays at a time); sets the loop's condition
+// (another pass while rays are queued)
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJob *__restrict__ jobs, WfState W, uint32_t *err,
-                                                                   cudaGraphConditionalHandle cond, uint32_t max_passes) {
+                                                                   cudaGraphConditionalHandle cond, uint32_t max_passes,
+                                                                   int use_cond) {
     // (the pass counter is advanced by the shadow kernel, so every block of this one and of the
     // shade kernel reads the same value)
     uint32_t count = *reinterpret_cast<volatile uint32_t *>(&W.ctl[0]);
@@ -191,7 +193,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJo
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, ST_LOOP);
         count = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, count > 0 ? 1u : 0u);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (use_cond) cudaGraphSetConditional(cond, count > 0 ? 1u : 0u);
+        else W.ctl[5] = count;                       // (the stepped loop's host reads it)
+    }
     const uint32_t lane = threadIdx.x & 31;
     for (;;) {
         uint32_t base = 0;
@@ -273,7 +278,8 @@ __global__ void __launch_bounds__(SHADE_BLOCK) wf_shade_kernel(const BatchJob *_
     }
 }
 
-// the any-hit test of every queued shadow ray; clears the ray queue for the next pass
+// the any-hit test of every queued shadow ray; clears the ray queue and counts the pass for the
+// next one
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) wf_shadow_kernel(const BatchJob *__restrict__ jobs, WfState W, uint32_t *err) {
     const uint32_t count = *reinterpret_cast<volatile uint32_t *>(&W.ctl[1]);
@@ -304,13 +310,11 @@ struct WfVariant {
     int block, minb;
     const void *isect, *shadow;
 };
+#define LRC_WF_VARIANT(B, M) {B, M, (const void *)pt::wf_intersect_kernel<B, M>, (const void *)pt::wf_shadow_kernel<B, M>}
 const WfVariant kWfVariants[] = {
-    {128, 4, (const void *)pt::wf_intersect_kernel<128, 4>, (const void *)pt::wf_shadow_kernel<128, 4>},
-    {128, 6, (const void *)pt::wf_intersect_kernel<128, 6>, (const void *)pt::wf_shadow_kernel<128, 6>},
-    {128, 8, (const void *)pt::wf_intersect_kernel<128, 8>, (const void *)pt::wf_shadow_kernel<128, 8>},
-    {256, 4, (const void *)pt::wf_intersect_kernel<256, 4>, (const void *)pt::wf_shadow_kernel<256, 4>},
-    {64, 12, (const void *)pt::wf_intersect_kernel<64, 12>, (const void *)pt::wf_shadow_kernel<64, 12>},
+    LRC_WF_VARIANT(128, 4), LRC_WF_VARIANT(128, 6), LRC_WF_VARIANT(128, 8), LRC_WF_VARIANT(256, 4), LRC_WF_VARIANT(64, 12),
 };
+#undef LRC_WF_VARIANT
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
 }  // namespace
 
@@ -407,7 +411,8 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     const int shade_grid = std::max(shade_per_sm, 1) * num_sms;
     WfState w = W;
     pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, body_st>>>(d_jobs, njobs, w);
-    void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes};
+    int use_cond = 1;
+    void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
     e = cudaLaunchKernel(V.isect, dim3(grid), dim3(V.block), iargs, 0, body_st);
     if (!e) {
         pt::wf_shade_kernel<<<shade_grid, pt::SHADE_BLOCK, 0, body_st>>>(d_jobs, w, d_status, max_passes);
@@ -420,6 +425,35 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     if (e) return e;
     if (e2) return e2;
     return cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
+                           uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st) {
+    if (variant < 0 || variant >= wf_variants() || W.M == 0 || W.M % pt::ADV_BLOCK) return cudaErrorInvalidValue;
+    const WfVariant &V = kWfVariants[variant];
+    int per_sm = 0, shade_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.isect, V.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, pt::wf_shade_kernel, pt::SHADE_BLOCK, 0);
+    const int grid = std::max(per_sm, 1) * num_sms, shade_grid = std::max(shade_per_sm, 1) * num_sms;
+    WfState w = W;
+    cudaGraphConditionalHandle cond = 0;
+    int use_cond = 0;
+    pt::wf_clear_kernel<<<(W.M + 255) / 256, 256, 0, st>>>(w, ntasks);
+    cudaError_t e = cudaGetLastError();
+    for (uint32_t pass = 0; !e && pass <= max_passes; pass++) {
+        pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, st>>>(d_jobs, njobs, w);
+        void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
+        e = cudaLaunchKernel(V.isect, dim3(grid), dim3(V.block), iargs, 0, st);
+        if (e) break;
+        pt::wf_shade_kernel<<<shade_grid, pt::SHADE_BLOCK, 0, st>>>(d_jobs, w, d_status, max_passes);
+        void *sargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};
+        e = cudaLaunchKernel(V.shadow, dim3(grid), dim3(V.block), sargs, 0, st);
+        uint32_t queued = 0;
+        if (!e) e = cudaMemcpyAsync(&queued, &W.ctl[5], 4, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaStreamSynchronize(st);
+        if (!e && queued == 0) break;
+    }
+    return e;
 }
 
 }  // namespace lrc

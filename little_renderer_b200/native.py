@@ -13,13 +13,13 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
 LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
 LRC_DEVICE = 1
-LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO = 4, 8, 16
+LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED = 4, 8, 16, 32
 
 
 def nvcc():
@@ -113,6 +113,21 @@ def lib():
     L.lrc_batch_set_shape.argtypes = [vp, C.c_int32, C.c_int32]
     L.lrc_batch_tune.argtypes = [vp, u64, vp, vp, vp]
     L.lrc_batch_info.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.lrc_scene_move_instances.argtypes = [vp, vp, u32, C.c_int, C.c_uint]
+    L.lrc_scene_tlas_cost.argtypes = [vp, vp]
+    L.lrc_refit.argtypes = [vp, vp, vp, u32, u32, vp, C.c_uint]
+    L.lrc_server_create.argtypes = [vp, u64, u64, C.POINTER(vp)]
+    L.lrc_server_destroy.argtypes = [vp]
+    L.lrc_server_submit.argtypes = [vp, vp, vp, u32, vp, u32, C.c_int, C.POINTER(u64)]
+    L.lrc_server_step.argtypes = [vp, C.POINTER(C.c_int32)]
+    L.lrc_server_result.argtypes = [vp, u64, C.POINTER(vp), C.POINTER(u64), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.lrc_server_release.argtypes = [vp, u64]
+    L.lrc_server_read.argtypes = [vp, u64, vp]
+    L.lrc_server_state.argtypes = [vp, vp, vp, vp, vp]
+    L.lrc_server_clock.restype = C.c_double
+    L.lrc_server_batch.argtypes = [vp]
+    L.lrc_server_batch.restype = vp
     L.lrc_batch_set_engine.argtypes = [vp, C.c_int32]
     L.lrc_batch_set_wavefront.argtypes = [vp, u32, C.c_int32]
     L.lrc_batch_wavefront_shape.argtypes = [C.c_int32, vp, vp, vp]
@@ -232,6 +247,15 @@ class Context:
         self.check(self.L.lrc_build(self.h, C.byref(params), C.c_void_p(d_boxes), C.c_void_p(d_nodes),
                                     C.c_void_p(d_aux), LRC_DEVICE))
 
+    def refit(self, nodes, aux, boxes, ref_add=0):
+        """lrc_refit with host arrays: the tree's boxes made again for new item boxes (a copy)."""
+        nodes = np.array(nodes, np.uint32, copy=True).reshape(-1, 8)
+        aux = np.ascontiguousarray(aux, np.uint32)
+        boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 8)
+        n = boxes.shape[0]
+        self.check(self.L.lrc_refit(self.h, _ptr(nodes), _ptr(aux), n, ref_add, _ptr(boxes), 0))
+        return nodes
+
     def triangle_boxes(self, tris12):
         tris12 = np.ascontiguousarray(tris12, np.uint32).reshape(-1, 12)
         n = tris12.shape[0]
@@ -328,6 +352,16 @@ class Scene:
 
     def build_instances(self, mesh_builder=1, key_bits=30):
         self.ctx.check(self.ctx.L.lrc_scene_build_instances(self.h, mesh_builder, key_bits))
+
+    def move_instances(self, records, mode=0):
+        """lrc_scene_move_instances: 0 refit, 1 rebuild, 2 auto (the reference's refit policy)."""
+        records = np.ascontiguousarray(records, np.float32).reshape(-1, 32)
+        self.ctx.check(self.ctx.L.lrc_scene_move_instances(self.h, _ptr(records), records.shape[0], mode, 0))
+
+    def tlas_cost(self):
+        c = C.c_double()
+        self.ctx.check(self.ctx.L.lrc_scene_tlas_cost(self.h, C.byref(c)))
+        return c.value
 
     def set_sky(self, rgb, scale=1.0, marg=None, cond=None, prob=None):
         if rgb is None:
@@ -443,8 +477,9 @@ class Batch:
         self.ctx.check(self.ctx.L.lrc_batch_clear(self.h))
         self.keep = []
 
-    def run(self, build=False, graph=False, zero=False):
+    def run(self, build=False, graph=False, zero=False, stepped=False):
         flags = (LRC_BATCH_BUILD if build else 0) | (LRC_BATCH_GRAPH if graph else 0) | (LRC_BATCH_ZERO if zero else 0)
+        flags |= LRC_BATCH_STEPPED if stepped else 0
         self.ctx.check(self.ctx.L.lrc_batch_run(self.h, flags))
 
     def rays(self):
@@ -504,3 +539,77 @@ def batch_shapes():
         L.lrc_batch_shape(v, C.byref(b), C.byref(m), C.byref(r))
         out.append((b.value, m.value, r.value))
     return out
+
+
+class Server:
+    """A render server (lrc_server_*): submit jobs as they arrive, step waves, collect results."""
+
+    def __init__(self, ctx, budget_bytes, wave_paths=1 << 22):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(ctx.L.lrc_server_create(ctx.h, budget_bytes, wave_paths, C.byref(h)))
+        self.h = h
+        self.keep = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.lrc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, scene, params, spp, records=None, tlas_mode=0):
+        jid = C.c_uint64()
+        if records is None:
+            rc = self.ctx.L.lrc_server_submit(self.h, scene.h, C.byref(params), spp, None, 0, 0, C.byref(jid))
+        else:
+            records = np.ascontiguousarray(records, np.float32).reshape(-1, 32)
+            rc = self.ctx.L.lrc_server_submit(self.h, scene.h, C.byref(params), spp, _ptr(records), records.shape[0],
+                                              tlas_mode, C.byref(jid))
+        self.ctx.check(rc)
+        self.keep[jid.value] = (scene, params)
+        return jid.value
+
+    def step(self):
+        n = C.c_int32()
+        self.ctx.check(self.ctx.L.lrc_server_step(self.h, C.byref(n)))
+        return n.value
+
+    def result(self, jid):
+        """(device image pointer, rays, t_submit, t_admit, t_done) of a finished job, or None."""
+        img, rays = C.c_void_p(), C.c_uint64()
+        t0, t1, t2 = C.c_double(), C.c_double(), C.c_double()
+        rc = self.ctx.L.lrc_server_result(self.h, jid, C.byref(img), C.byref(rays), C.byref(t0), C.byref(t1),
+                                          C.byref(t2))
+        if rc == LRC_RETRY:
+            return None
+        self.ctx.check(rc)
+        return img.value, rays.value, t0.value, t1.value, t2.value
+
+    def image(self, jid):
+        """A finished job's image as a host array (h, w, 4): the sum of its samples and their count."""
+        scene, p = self.keep[jid]
+        out = np.zeros((p.height, p.width, 4), np.float32)
+        self.ctx.check(self.ctx.L.lrc_server_read(self.h, jid, _ptr(out)))
+        return out
+
+    def release(self, jid):
+        self.ctx.check(self.ctx.L.lrc_server_release(self.h, jid))
+        self.keep.pop(jid, None)
+
+    def state(self):
+        q, a, f, b = C.c_int32(), C.c_int32(), C.c_int32(), C.c_uint64()
+        self.ctx.check(self.ctx.L.lrc_server_state(self.h, C.byref(q), C.byref(a), C.byref(f), C.byref(b)))
+        return {"queued": q.value, "active": a.value, "finished": f.value, "bytes": b.value}
+
+    def batch_handle(self):
+        return self.ctx.L.lrc_server_batch(self.h)
+
+
+def clock_ms():
+    return lib().lrc_server_clock()
+

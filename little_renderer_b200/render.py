@@ -52,3 +52,15 @@ def instanced_scene(ctx, sc, mesh_builder=1, key_bits=30, blue_noise=None, bsdf_
     if sky:
         s.set_sky(sc["sky"])
     return s
+
+
+def instanced_box_scene(ctx, sc, mesh_builder=1, key_bits=30, blue_noise=None, bsdf_tables=None):
+    """lrc_scene of an instanced box: the walls (world triangles) and the lamp (primitive 0,
+    Scene.light), the meshes and their trees, the instances and their top level."""
+    s = world_scene(ctx, sc, 1, key_bits, blue_noise, bsdf_tables)
+    s.set_meshes([native.pack_tris(W.corners_to_quv(t), np.full(t.shape[0], m, np.int32))
+                  for t, m in zip(sc["meshes"], sc["mesh_mats"])])
+    s.set_instances(W.instance_records(sc))
+    s.build_instances(mesh_builder, key_bits)
+    return s
+

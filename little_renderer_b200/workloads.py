@@ -432,3 +432,58 @@ def instance_records(sc):
     rec[:, 28:31] = hi
     rec[:, 31] = np.full(n, -1, np.int32).view(np.float32)
     return rec
+
+
+def rigid_motion(n, seed, speed=(0.5, 2.0), spin=(0.2, 1.5)):
+    """Per-instance rigid motion: a linear velocity (uniform direction, speed uniform in `speed`
+    units per frame) and an angular one (uniform axis, rate uniform in `spin` radians per frame)."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3))
+    v *= (rng.uniform(*speed, n) / np.linalg.norm(v, axis=1))[:, None]
+    axis = rng.normal(size=(n, 3))
+    axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+    return {"v": v, "axis": axis, "rate": rng.uniform(*spin, n)}
+
+
+def moved_xf(xf0, motion, t):
+    """The transforms at frame t: each instance turned about its axis by rate * t (after its own
+    rotation and scale) and carried by v * t, float32."""
+    xf0 = np.asarray(xf0, np.float64)
+    a, th = motion["axis"], motion["rate"] * t
+    c, s_ = np.cos(th), np.sin(th)
+    x, y, z = a.T
+    rot = np.stack([np.stack([c + x * x * (1 - c), x * y * (1 - c) - z * s_, x * z * (1 - c) + y * s_], -1),
+                    np.stack([y * x * (1 - c) + z * s_, c + y * y * (1 - c), y * z * (1 - c) - x * s_], -1),
+                    np.stack([z * x * (1 - c) - y * s_, z * y * (1 - c) + x * s_, c + z * z * (1 - c)], -1)], 1)
+    out = np.empty_like(xf0)
+    out[:, :, :3] = rot @ xf0[:, :, :3]
+    out[:, :, 3] = xf0[:, :, 3] + motion["v"] * t
+    return out.astype(np.float32)
+
+
+def instanced_box(seed, n_instances=2000, n_meshes=4, width=256, height=256, spp=16, max_depth=8):
+    """The plain render's box and lamp with n_instances instances of n_meshes meshes inside
+    (icospheres of subdivision 2 and bevelled boxes of about 320 triangles), each instance turned
+    at random, scaled to a radius uniform in [4, 12] and placed uniformly in the box; one material
+    (Lambert, GGX metal or dielectric) per mesh."""
+    rng = np.random.default_rng(seed)
+    base = cornell_spheres(seed=seed, n_spheres=0, width=width, height=height)
+    mats = base["materials"]
+    meshes, mesh_mats = [], []
+    for m in range(n_meshes):
+        k = m % 3
+        mats.append(diffuse(rng.uniform(0.2, 0.9, 3)) if k == 0 else
+                    pbr(rng.uniform(0.5, 0.95, 3), 1.0, rng.uniform(0.05, 0.5), 1.5, 0.0) if k == 1 else
+                    glass((1.0, 1.0, 1.0), 1.5))
+        meshes.append((icosphere(2) if m % 2 == 0 else rounded_box(320, rng)).astype(np.float32))
+        mesh_mats.append(len(mats) - 1)
+    rot = random_rotations(n_instances, rng)
+    scale = rng.uniform(4.0, 12.0, n_instances)
+    xf = np.zeros((n_instances, 3, 4), np.float32)
+    xf[:, :, :3] = rot * scale[:, None, None]
+    xf[:, :, 3] = rng.uniform(20.0, 535.0, (n_instances, 3))
+    base.update({"meshes": meshes, "mesh_mats": mesh_mats, "xf": xf,
+                 "mesh_of": rng.integers(0, n_meshes, n_instances).astype(np.int32),
+                 "spp": spp, "max_depth": max_depth})
+    return base
+

@@ -52,4 +52,7 @@ int or_check_tree(const OrNode *nodes, int n, uint32_t node0, double *cost, int 
 void or_trace_tree(const OrNode *nodes, const uint32_t *aux, uint32_t node0, const float *tris,
                    const float *orig, const float *dir, long long nrays, float tmin, float tmax,
                    int *prim, float *t, long long *counts);
+// bvh_refit_boxes on a GPU-layout tree (tree_oracle.c)
+int or_refit(OrNode *w, int nn, const uint32_t *aux, uint32_t ref_add, const float *boxes, int nitems);
+
 #endif

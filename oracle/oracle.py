@@ -54,6 +54,7 @@ def oracle_lib():
         lib.or_check_tree.argtypes = [_u32p, C.c_int, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         lib.or_trace_tree.argtypes = [_u32p, _u32p, C.c_uint32, _f32p, _f32p, _f32p, C.c_longlong, C.c_float,
                                       C.c_float, _i32p, _f32p, _i64p]
+        lib.or_refit.argtypes = [_u32p, C.c_int, _u32p, C.c_uint32, _f32p, C.c_int]
         lib._typed = True
     return lib
 
@@ -115,6 +116,31 @@ def ploc(boxes, lo, ext, bits=30, node0=0, ref0=0, ref_add=0, small=1024):
     return nodes, aux
 
 
+def refit(nodes, aux, boxes, ref_add=0):
+    """bvh_refit_boxes (bvh.c:471-485) restated for a GPU-layout tree (root at node 0): a copy of
+    nodes with every box made again for the items' new boxes (n x 8 floats)."""
+    out = np.array(nodes, np.uint32, copy=True).reshape(-1, 8)
+    boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 8)
+    ok = oracle_lib().or_refit(out.reshape(-1), out.shape[0], np.ascontiguousarray(aux, np.uint32), ref_add,
+                               boxes.reshape(-1), boxes.shape[0])
+    if not ok:
+        raise ValueError("or_refit: not a tree over these items")
+    return out
+
+
+def ref_bvh_refit(boxes, moved):
+    """The reference's own refit: bvh_build_boxes (SAH, leaves of up to 4) over boxes, then
+    bvh_refit_boxes for moved. Returns (nodes in the GPU layout, refs, cost)."""
+    boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 8)
+    moved = np.ascontiguousarray(moved, np.float32).reshape(-1, 8)
+    n = boxes.shape[0]
+    nodes = np.zeros((2 * n - 1, 8), np.uint32)
+    refs = np.zeros(n, np.uint32)
+    cost = C.c_float()
+    nn = ref_lib().rb_bvh_refit(boxes.reshape(-1), moved.reshape(-1), n, nodes.reshape(-1), refs, C.byref(cost))
+    return nodes[:nn], refs, cost.value
+
+
 def check_tree(nodes, n, node0=0):
     cost = C.c_double()
     depth = C.c_int()
@@ -153,6 +179,8 @@ def ref_lib(double=False):
         lib.rb_add_mesh.argtypes = [vp, _f32p, _i32p, C.c_int]
         lib.rb_add_instance.argtypes = [vp, C.c_int, _f32p, C.c_int]
         lib.rb_move_instance.argtypes = [vp, C.c_int, _f32p]
+        lib.rb_update_instances.argtypes = [vp]
+        lib.rb_bvh_refit.argtypes = [_f32p, _f32p, C.c_int, _u32p, _u32p, C.POINTER(C.c_float)]
         lib.rb_instance_data.argtypes = [vp, C.c_int, _f32p, _f32p]
         lib.rb_mesh_box.argtypes = [vp, C.c_int, _f32p]
         lib.rb_set_env.argtypes = [vp, _f32p, C.c_int, C.c_int]
@@ -280,6 +308,13 @@ class RefScene:
 
     def set_accel(self):
         self.lib.rb_set_accel(self.s)
+
+    def move_instance(self, i, xf12):
+        """scene_move_instance (scene.c:743); update_instances then makes the top level again."""
+        self.lib.rb_move_instance(self.s, i, np.ascontiguousarray(xf12, np.float32).reshape(-1))
+
+    def update_instances(self):
+        self.lib.rb_update_instances(self.s)
 
     def prim_data(self):
         n = self.lib.rb_num_prims(self.s)

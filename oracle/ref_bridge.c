@@ -15,6 +15,7 @@
 #include "scene/scene.h"
 #include "scene/env.h"
 #include "rt/accel.h"
+#include "rt/bvh.h"
 #include "rt/tracer.h"
 #include "base/sampler.h"
 #include "scene/brdf_tables.h"
@@ -148,6 +149,8 @@ int rb_set_env(void *sp, const float *rgb, int w, int h){
     return s->env != NULL;
 }
 void rb_set_accel(void *sp){ scene_set_accel(sp, ACCEL_BVH, NULL); }
+// after instances moved: the top level made again (scene_update_instances, accel.c:197)
+void rb_update_instances(void *sp){ scene_update_instances(sp, NULL); }
 
 // the world's triangles as stored (q, u, v: 9 floats each) and their materials
 void rb_tri_data(const void *sp, float *quv, int *mats){
@@ -166,6 +169,37 @@ int rb_num_prims(const void *sp){ return ((const Scene *)sp)->nprims; }
 
 // triangle_bounds (scene.c:65) of n triangles given as q, u, v (9 floats each): 8 floats per box
 // (lo.xyz, 0, hi.xyz, 0), the GPU builder's input layout
+// bvh_build_boxes (binned SAH, leaves of up to 4, 16 bins) over n boxes (8 floats each: lo, -, hi,
+// -), then bvh_refit_boxes (bvh.c:471) for the moved boxes; out: the refit tree in the GPU node
+// layout (8 words: lo, a, hi, b; inner: a / b the children; leaf: a its first ref, b 0x80000000 |
+// count), its refs, and the cost the refit returns. Returns the node count (nodes8: 2n - 1 room).
+int rb_bvh_refit(const float *boxes, const float *moved, int n, uint32_t *nodes8, uint32_t *refs, float *cost){
+    Aabb *a = malloc((size_t)n * sizeof(Aabb)), *m = malloc((size_t)n * sizeof(Aabb));
+    for (int i = 0; i < n; i++){
+        const float *p = boxes + 8 * (size_t)i, *q = moved + 8 * (size_t)i;
+        a[i].lo = v3f(p); a[i].hi = v3f(p + 4);
+        m[i].lo = v3f(q); m[i].hi = v3f(q + 4);
+    }
+    Bvh b;
+    memset(&b, 0, sizeof(b));
+    bvh_build_boxes(&b, a, n, 4, 16, BVH_SPLIT_SAH);
+    *cost = (float)bvh_refit_boxes(&b, m);
+    for (int i = 0; i < b.nnodes; i++){
+        const BvhNode *d = &b.nodes[i];
+        float *f = (float *)(nodes8 + 8 * (size_t)i);
+        f[0] = (float)d->box.lo.x; f[1] = (float)d->box.lo.y; f[2] = (float)d->box.lo.z;
+        f[4] = (float)d->box.hi.x; f[5] = (float)d->box.hi.y; f[6] = (float)d->box.hi.z;
+        nodes8[8 * (size_t)i + 3] = d->count > 0 ? (uint32_t)d->start : (uint32_t)d->left;
+        nodes8[8 * (size_t)i + 7] = d->count > 0 ? 0x80000000u | (uint32_t)d->count : (uint32_t)d->right;
+    }
+    for (int i = 0; i < b.nrefs; i++) refs[i] = (uint32_t)b.refs[i];
+    int nn = b.nnodes;
+    bvh_free(&b);
+    free(a);
+    free(m);
+    return nn;
+}
+
 void rb_triangle_bounds(const float *quv, int n, float *boxes){
     for (int i = 0; i < n; i++){
         const float *p = quv + 9 * (size_t)i;

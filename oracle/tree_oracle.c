@@ -131,3 +131,43 @@ void or_trace_tree(const OrNode *nodes, const uint32_t *aux, uint32_t node0, con
     counts[0] = boxes;
     counts[1] = tests;
 }
+
+// bvh_refit_boxes (engine/rt/bvh.c:471-485) on a tree in the GPU layout (root at node 0, nn
+// nodes): every leaf's box the union of its items' boxes (aux = item + ref_add; boxes 8 floats
+// each), every inner node's its left child's box with the right's added (box_add_box, bvh.c:20,
+// mn / mx: a < b ? a : b), children before parents (an explicit postorder walk).
+static inline float or_mn(float a, float b){ return a < b ? a : b; }
+static inline float or_mx(float a, float b){ return a > b ? a : b; }
+int or_refit(OrNode *w, int nn, const uint32_t *aux, uint32_t ref_add, const float *boxes, int nitems){
+    uint32_t *stack = malloc((size_t)nn * 2 * sizeof(uint32_t));
+    if (!stack) return 0;
+    int top = 0, ok = 1;
+    stack[top++] = 0; stack[top++] = 0;             // (node, children done)
+    while (top > 0 && ok){
+        uint32_t done = stack[--top], i = stack[--top];
+        OrNode *f = &w[i];
+        if (f->b & 0x80000000u){
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t cnt = f->b & 0x7fffffffu;
+            for (uint32_t k = 0; k < cnt; k++){
+                uint32_t item = aux[f->a + k] - ref_add;
+                if ((int)item >= nitems){ ok = 0; break; }
+                const float *b = boxes + 8 * (size_t)item;
+                for (int x = 0; x < 3; x++){ lo[x] = or_mn(lo[x], b[x]); hi[x] = or_mx(hi[x], b[4 + x]); }
+            }
+            for (int x = 0; x < 3; x++){ f->lo[x] = lo[x]; f->hi[x] = hi[x]; }
+            continue;
+        }
+        if ((int)f->a >= nn || (int)f->b >= nn){ ok = 0; break; }
+        if (!done){
+            stack[top++] = i; stack[top++] = 1;
+            stack[top++] = f->b; stack[top++] = 0;
+            stack[top++] = f->a; stack[top++] = 0;
+            continue;
+        }
+        const OrNode *l = &w[f->a], *r = &w[f->b];
+        for (int x = 0; x < 3; x++){ f->lo[x] = or_mn(l->lo[x], r->lo[x]); f->hi[x] = or_mx(l->hi[x], r->hi[x]); }
+    }
+    free(stack);
+    return ok;
+}

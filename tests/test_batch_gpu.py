@@ -150,6 +150,9 @@ def test_wavefront_tuner_and_sizes_change_no_image(ctx, scenes, built):
     b.run()
     for (acc, _), g in zip(want, host(ctx, imgs)):
         assert np.array_equal(g, acc)
+    b.run(zero=True, stepped=True)                       # the host-looped passes (for profilers)
+    for (acc, _), g in zip(want, host(ctx, imgs)):
+        assert np.array_equal(g, acc)
     # tiny pools (paths regenerate in every pass) and every launch shape
     for slots, v in [(256, 0), (4096, 1), (65536, 2)] + [(1 << 16, k) for k in range(len(shapes))]:
         b.set_wavefront(slots, v)

@@ -120,3 +120,20 @@ def test_tree_walk_matches_scene_intersect(oracle, builder):
     assert (pr >= 0).sum() > 2000
     assert np.array_equal(p2, pr)
     assert np.array_equal(t2[pr >= 0], tr[pr >= 0])
+
+
+def test_refit_restatement_is_bvh_refit_boxes(oracle):
+    """or_refit on the reference's own SAH tree (bvh_build_boxes) gives bvh_refit_boxes' boxes."""
+    rng = np.random.default_rng(1)
+    n = 3000
+    lo = rng.uniform(0, 100, (n, 3)).astype(np.float32)
+    boxes = np.zeros((n, 8), np.float32)
+    boxes[:, :3] = lo
+    boxes[:, 4:7] = lo + rng.uniform(0.1, 5, (n, 3)).astype(np.float32)
+    moved = boxes.copy()
+    shift = rng.normal(0, 3, (n, 3)).astype(np.float32)
+    moved[:, :3] += shift
+    moved[:, 4:7] += shift
+    nodes, refs, _ = oracle.ref_bvh_refit(boxes, moved)
+    assert np.array_equal(oracle.refit(nodes, refs, moved), nodes)
+
