@@ -145,11 +145,18 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) { return *(co
 __device__ __forceinline__ void st_volatile(uint32_t *p, uint32_t v) { *(volatile uint32_t *)p = v; }
 
 // One radix pass over bits [shift, shift + 8). first: the values are the items' indices.
+// A tile's keys are ranked warp by warp (the keys of one digit in a warp: __match_any_sync, the
+// group's leader takes the group's places from the warp's counter with one shared atomic - the
+// warp's items in order, so the ranks are stable - results read after all 16 are issued), staged in
+// digit order in shared memory (registers freed before the look-back), and written out at their
+// digit's global offset: the tiles before it (decoupled look-back over posted counts / prefixes)
+// plus the digits before it (the pass's histogram).
 template <typename K, bool FIRST>
-__global__ void __launch_bounds__(OS_THREADS) onesweep_kernel(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-                                                              K *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
-                                                              uint32_t n, int shift, const uint32_t *__restrict__ hist,
-                                                              uint32_t *status, uint32_t *tile_counter, uint32_t *err) {
+__global__ void __launch_bounds__(OS_THREADS, 4) onesweep_kernel(const K *__restrict__ keys_in,
+                                                                 const uint32_t *__restrict__ vals_in,
+                                                                 K *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+                                                                 uint32_t n, int shift, const uint32_t *__restrict__ hist,
+                                                                 uint32_t *status, uint32_t *tile_counter, uint32_t *err) {
     extern __shared__ __align__(16) unsigned char os_smem[];
     OsShared<K> &S = *reinterpret_cast<OsShared<K> *>(os_smem);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -158,27 +165,40 @@ __global__ void __launch_bounds__(OS_THREADS) onesweep_kernel(const K *__restric
     __syncthreads();
     const uint32_t tile = S.tile;
     const uint32_t tile0 = tile * OS_TILE;
+    const uint32_t in_tile = min((uint32_t)OS_TILE, n - tile0);
 
     K key[OS_ITEMS];
-    uint32_t val[OS_ITEMS], rank[OS_ITEMS];
+    uint32_t val[OS_ITEMS], rank[OS_ITEMS];   // rank: the leader's base | leader << 16 | lanes before << 24, then the rank
     const uint32_t lt_mask = (1u << lane) - 1u;
 #pragma unroll
     for (int k = 0; k < OS_ITEMS; k++) {
-        uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
-        bool ok = idx < n;
+        const uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
+        const bool ok = idx < n;
         key[k] = ok ? keys_in[idx] : K(0);
         val[k] = ok ? (FIRST ? idx : vals_in[idx]) : 0u;
-        uint32_t d = ok ? (uint32_t)((key[k] >> shift) & 255u) : 0x100u;
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
-        uint32_t before = __popc(peers & lt_mask);
-        uint32_t base = d < 256 ? S.warp_hist[w][d] : 0u;
-        rank[k] = base + before;
-        __syncwarp();
-        if (d < 256 && (peers & lt_mask) == 0) S.warp_hist[w][d] = base + __popc(peers);
-        __syncwarp();
     }
+#pragma unroll
+    for (int k = 0; k < OS_ITEMS; k++) {
+        const uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
+        const uint32_t d = idx < n ? (uint32_t)((key[k] >> shift) & 255u) : 0x100u;
+        // the lanes with this lane's digit: one ballot per digit bit (and one for validity)
+        uint32_t peers = 0xffffffffu;
+#pragma unroll
+        for (int bit = 0; bit < 9; bit++) {
+            const bool on = (d >> bit) & 1u;
+            const uint32_t bal = __ballot_sync(0xffffffffu, on);
+            peers &= on ? bal : ~bal;
+        }
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (d < 256 && lane == leader) base = atomicAdd(&S.warp_hist[w][d], (uint32_t)__popc(peers));
+        rank[k] = base | (uint32_t)leader << 16 | (uint32_t)__popc(peers & lt_mask) << 24;
+    }
+#pragma unroll
+    for (int k = 0; k < OS_ITEMS; k++)
+        rank[k] = (__shfl_sync(0xffffffffu, rank[k], (rank[k] >> 16) & 31u) & 0xffffu) + (rank[k] >> 24);
     __syncthreads();
-    // this thread's digit: warps' offsets, the tile's count
+    // this thread's digit: the warps' offsets, the tile's count - posted at once for the tiles after
     const uint32_t d = tid;
     uint32_t count = 0;
 #pragma unroll
@@ -187,47 +207,56 @@ __global__ void __launch_bounds__(OS_THREADS) onesweep_kernel(const K *__restric
         S.warp_hist[ww][d] = count;
         count += c;
     }
-    // decoupled look-back: tile t's prefix of digit d over the tiles before it
-    uint32_t excl;
-    if (tile == 0) {
-        uint32_t tot;
-        excl = block_excl_scan<OS_THREADS>(hist[d], S.scan, tot);   // the digits before d, all keys
-        st_volatile(&status[d], FLAG_PRE | (excl + count));
-    } else {
-        st_volatile(&status[(size_t)tile * 256 + d], FLAG_AGG | count);
-        excl = 0;
-        int64_t t = (int64_t)tile - 1;
-        while (t >= 0) {
-            uint32_t s = ld_volatile(&status[(size_t)t * 256 + d]);
-            uint32_t spins = 0;
-            while ((s & ~VAL_MASK) == 0) {
-                if (++spins > SPIN_LIMIT) { atomicOr(err, ST_TIMEOUT_SORT); break; }
-                __nanosleep(32);
-                s = ld_volatile(&status[(size_t)t * 256 + d]);
-            }
-            excl += s & VAL_MASK;
-            if ((s & ~VAL_MASK) != FLAG_AGG) break;      // a prefix (or a timeout): done
-            t--;
-        }
-        st_volatile(&status[(size_t)tile * 256 + d], FLAG_PRE | (excl + count));
-    }
-    S.global_excl[d] = excl;
+    if (tile) st_volatile(&status[(size_t)tile * 256 + d], FLAG_AGG | count);
     uint32_t tot;
     S.digit_start[d] = block_excl_scan<OS_THREADS>(count, S.scan, tot);
     __syncthreads();
     // stage the tile in digit order (stable: warp, then item, then lane order)
 #pragma unroll
     for (int k = 0; k < OS_ITEMS; k++) {
-        uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
+        const uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
         if (idx < n) {
-            uint32_t dk = (uint32_t)((key[k] >> shift) & 255u);
-            uint32_t pos = S.digit_start[dk] + S.warp_hist[w][dk] + rank[k];
+            const uint32_t dk = (uint32_t)((key[k] >> shift) & 255u);
+            const uint32_t pos = S.digit_start[dk] + S.warp_hist[w][dk] + rank[k];
             S.key_stage[pos] = key[k];
             S.val_stage[pos] = val[k];
         }
     }
+    // decoupled look-back: tile t's prefix of digit d over the tiles before it
+    uint32_t excl;
+    if (tile == 0) {
+        excl = block_excl_scan<OS_THREADS>(hist[d], S.scan, tot);   // the digits before d, all keys
+        st_volatile(&status[d], FLAG_PRE | (excl + count));
+    } else {
+        excl = 0;
+        // the tiles before, nearest first, LB_WIDE statuses read at once (independent loads): their
+        // counts summed up to the first inclusive prefix; a status not yet posted is waited for
+        constexpr int LB_WIDE = 8;
+        int64_t t = (int64_t)tile - 1;
+        bool done = false;
+        while (t >= 0 && !done) {
+            uint32_t s[LB_WIDE];
+#pragma unroll
+            for (int j = 0; j < LB_WIDE; j++) s[j] = t - j >= 0 ? ld_volatile(&status[(size_t)(t - j) * 256 + d]) : 0u;
+#pragma unroll
+            for (int j = 0; j < LB_WIDE; j++) {
+                if (done || t - j < 0) continue;
+                uint32_t v = s[j];
+                uint32_t spins = 0;
+                while ((v & ~VAL_MASK) == 0) {
+                    if (++spins > SPIN_LIMIT) { atomicOr(err, ST_TIMEOUT_SORT); break; }
+                    __nanosleep(32);
+                    v = ld_volatile(&status[(size_t)(t - j) * 256 + d]);
+                }
+                excl += v & VAL_MASK;
+                if ((v & ~VAL_MASK) != FLAG_AGG) done = true;   // a prefix (or a timeout): done
+            }
+            t -= LB_WIDE;
+        }
+        st_volatile(&status[(size_t)tile * 256 + d], FLAG_PRE | (excl + count));
+    }
+    S.global_excl[d] = excl;
     __syncthreads();
-    const uint32_t in_tile = min((uint32_t)OS_TILE, n - tile0);
     for (uint32_t i = tid; i < in_tile; i += OS_THREADS) {
         K kk = S.key_stage[i];
         uint32_t dk = (uint32_t)((kk >> shift) & 255u);
