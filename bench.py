@@ -38,6 +38,7 @@ import numpy as np  # noqa: E402
 METRIC = "Mrays/s (build + closest-hit pass over the builder workload)"
 METRIC_BATCH = "Mrays/s (256-scene batched launch: builds + path tracing, closest-hit + shadow rays)"
 METRIC_SERVE = "Mrays/s and p50/p99 job latency (served request stream, Poisson arrivals)"
+METRIC_RENDER = "Mrays/s (one image: closest-hit + shadow rays)"
 
 
 def parse():
@@ -52,7 +53,7 @@ def parse():
     ap.add_argument("--bits", type=int, default=30, choices=[30, 63])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve"])
+    ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve", "render", "instanced"])
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
@@ -546,6 +547,133 @@ def run_serve(a):
     print(json.dumps(line), flush=True)
 
 
+def ref_field_scene(O, sc):
+    ref = O.RefScene()
+    for m in sc["materials"]:
+        ref.material(m["type"], m["albedo"], m["emission"], m["ior"], m["metallic"], m["roughness"], m["transmission"])
+    g = sc["ground"]
+    ref.quad(g["q"], g["u"], g["v"], g["material"])
+    for tri, mm in zip(sc["meshes"], sc["mesh_mats"]):
+        ref.mesh(tri, np.full(tri.shape[0], mm, np.int32))
+    for i in range(sc["xf"].shape[0]):
+        ref.instance(int(sc["mesh_of"][i]), sc["xf"][i].reshape(-1), -1)
+    ref.env(sc["sky"])
+    return ref
+
+
+def run_render(a):
+    """--workload render (configuration 0: the box, its lamp and 64 icospheres, 256^2, 16 spp,
+    depth 8) or --workload instanced (configuration 2: 5000 instances of 14 meshes of 10k-100k
+    triangles, a 2048 x 1024 sky, 1280 x 720, 64 spp, depth 12). One step = one image. The plain
+    path (one lrc_trace launch) is the line's value; the same image through the batch's wavefront
+    and its persistent megakernel (one job each, tuned) is timed in the same run; the images are
+    compared bit for bit. cpu_baseline: the reference's trace_image (16 cores) on a band of rows."""
+    import torch
+    import little_renderer_b200 as L
+    from little_renderer_b200 import render as R, workloads as W
+    from oracle import oracle as O
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    inst = a.workload == "instanced"
+    dev = torch.device("cuda", 0)
+    sc = W.instanced_field() if inst else W.cornell_spheres()
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    s = R.instanced_scene(ctx, sc, 1) if inst else R.world_scene(ctx, sc, 1)
+    w, h, spp = sc["width"], sc["height"], sc["spp"]
+    p = L.native.trace_params(W.camera(sc["camera"], w / h), w, h, sc["max_depth"], 1, 1, 0, 1)
+    img = torch.zeros(h, w, 4, device=dev)
+    torch.cuda.synchronize()
+    _, rays = s.trace(p, spp)                             # (one image on the host: its ray count)
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.sync()
+        return e0.elapsed_time(e1) / n
+
+    def plain():
+        s.trace_device(p, spp, img.data_ptr())
+
+    for _ in range(a.warmup):
+        plain()
+    clk = Clocks(0)
+    ms = timed(plain, a.steps)
+    clocks = clk.stop()
+    img.zero_()
+    plain()
+    ctx.sync()
+    torch.cuda.synchronize()
+    want = img.cpu()
+    engines = {}
+    for name, eng in (("wavefront", 1), ("megakernel", 0)):
+        b = L.native.Batch(ctx)
+        b.set_engine(eng)
+        b.add(s, p, spp, img.data_ptr())
+        b.run(zero=True)
+        v, g, _ = b.tune()
+        for _ in range(a.warmup):
+            b.run(graph=True, zero=True)
+        bms = timed(lambda: b.run(graph=True, zero=True), a.steps)
+        ctx.sync()
+        torch.cuda.synchronize()
+        engines[name] = {"value": rays / (bms / 1e3) / 1e6, "ms_per_step": bms, "variant": v,
+                         ("paths_in_flight" if eng else "grid"): g, "images_equal_plain": bool(torch.equal(img.cpu(), want))}
+        b.close()
+    # end to end: the host image copied in and out around the launch (lrc_trace with a host array)
+    acc = np.zeros((h, w, 4), np.float32)
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(a.steps, 3))):
+        s.trace(p, spp, accum=acc)
+    e_ms = (time.perf_counter() - t0) * 1e3 / max(1, min(a.steps, 3))
+    # the reference's CPU path tracer on a central band of rows
+    ref = ref_field_scene(O, sc) if inst else None
+    if ref is None:
+        ref = O.RefScene()
+        for m in sc["materials"]:
+            ref.material(m["type"], m["albedo"], m["emission"], m["ior"], m["metallic"], m["roughness"],
+                         m["transmission"])
+        ref.triangles(sc["corners"], sc["tri_mats"])
+        lamp = sc["lamp"]
+        ref.quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"], light=True)
+    t0 = time.perf_counter()
+    ref.set_accel()
+    rows = max(1, min(h, (4 if inst else 64)))
+    c = sc["camera"]
+    fau = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
+    _, (cl, sh) = ref.trace_image(fau, c["vfov"], w, h, spp, 1, sc["max_depth"], y0=h // 2 - rows // 2, rows=rows)
+    t_cpu = time.perf_counter() - t0
+    cores = O.ref_lib().rb_max_threads()
+    ref.close()
+    value = rays / (ms / 1e3) / 1e6
+    line = {"metric": METRIC_RENDER, "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": ("instanced scene: 5000 instances of 14 meshes (10k-100k triangles), 2048x1024 sky, "
+                                    "1280x720, 64 spp, depth 12" if inst else
+                                    "the box, its lamp and 64 icospheres (20.5k triangles), 256x256, 16 spp, depth 8"),
+                       "rays_per_image": int(rays), "paths_per_image": w * h * spp,
+                       "l2": "one image's scene and image held in HBM; successive images reuse L2 (the workload's own)"},
+            "clocks": clocks, "engines": engines,
+            "e2e": {"value": rays / (e_ms / 1e3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": w * h * 16,
+                    "d2h_bytes_per_step": w * h * 16, "ms_per_step": e_ms},
+            "gpu_launches": a.steps,
+            "cpu_baseline": {"value": (cl + sh) / t_cpu / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "reference",
+                             "sample": f"scene_set_accel + trace_image of {rows} central rows at {spp} spp "
+                                       f"({cl + sh} rays in {t_cpu:.1f} s)"}}
+    s.close()
+    ctx.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -555,6 +683,9 @@ def main():
                               "CUDA path timed beside the served one in --workload serve"}), flush=True)
         elif a.workload == "batch":
             run_reference_batch(a)
+        elif a.workload in ("render", "instanced"):
+            print(json.dumps({"impl": "reference", "metric": METRIC_RENDER, "unavailable":
+                              "this workload's CPU baseline is the cpu_baseline leg of the ours line"}), flush=True)
         else:
             run_reference(a)
         return
@@ -563,6 +694,9 @@ def main():
         return
     if a.workload == "serve":
         run_serve(a)
+        return
+    if a.workload in ("render", "instanced"):
+        run_render(a)
         return
     import torch
     import little_renderer_b200 as L

@@ -137,3 +137,11 @@ def test_refit_restatement_is_bvh_refit_boxes(oracle):
     nodes, refs, _ = oracle.ref_bvh_refit(boxes, moved)
     assert np.array_equal(oracle.refit(nodes, refs, moved), nodes)
 
+
+
+def test_fp64_golden_fixture():
+    """The FP64 oracle image (tests/golden/make_fp64_golden.py): its shape and a sane mean."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cornell128_fp64_4096spp.npy"))
+    assert g.shape == (128, 128, 3) and g.dtype == np.float32
+    assert np.isfinite(g).all() and 0.05 < g.mean() < 0.5

@@ -95,3 +95,31 @@ def test_fast_mode_is_deterministic(ctx, cornell128):
     a, _ = R.render(ctx, s, sc, spp=16, exact=0, seed=4)
     b, _ = R.render(ctx, s, sc, spp=16, exact=0, seed=4)
     assert np.array_equal(a, b)
+
+
+GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "cornell128_fp64_4096spp.npy")
+
+
+def test_relrmse_against_the_fp64_oracle(ctx, oracle, cornell128):
+    """The FP64 oracle: the reference's double-precision build at 4096 spp (tests/golden). At the
+    same spp and seed, the GPU's exact-mode image is as far from it as the CPU float build's
+    (within 1 % relative); the fast mode's (other random streams) within 10 %; at 1024 spp the GPU
+    is much closer and its mean within 1 % of the oracle's."""
+    golden = np.load(GOLDEN)
+    sc = cornell128
+    spp, seed = 16, 1
+    ref = ref_scene(oracle, sc)
+    cpu, _ = ref.trace_image(cam9(sc), sc["camera"]["vfov"], 128, 128, spp, seed, sc["max_depth"])
+    s = R.world_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    p = L.native.trace_params(oracle.camera(cam9(sc), sc["camera"]["vfov"], 1.0), 128, 128, sc["max_depth"], 1, 1, 1, seed)
+    acc, _ = s.trace(p, spp)
+    exact = acc[..., :3] * (np.float32(1) / np.float32(spp))
+    fast, _ = R.render(ctx, s, sc, spp=spp, exact=0, seed=seed)
+    hi, _ = R.render(ctx, s, sc, spp=1024, exact=0, seed=seed)
+    e_cpu, e_exact, e_fast, e_hi = (rel_rmse(x, golden) for x in (cpu, exact, fast, hi))
+    print(f"relRMSE to the FP64 4096-spp oracle: CPU float {e_cpu:.4f}, GPU exact {e_exact:.4f}, GPU fast {e_fast:.4f} "
+          f"(16 spp); GPU fast 1024 spp {e_hi:.4f}")
+    assert abs(e_exact - e_cpu) / e_cpu < 0.01
+    assert abs(e_fast - e_cpu) / e_cpu < 0.10
+    assert e_hi < 0.35 * e_cpu
+    assert abs(hi.mean() - golden.mean()) / golden.mean() < 0.01
