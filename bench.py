@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
-    ap.add_argument("--wave-paths", type=int, default=8 << 20, help="serve: paths per wave")
+    ap.add_argument("--wave-paths", type=int, default=32 << 20, help="serve: paths per wave")
+    ap.add_argument("--wave-slots", type=int, default=1 << 22, help="serve: the waves' paths in flight")
     ap.add_argument("--scenes", type=int, default=256, help="batch: scenes (jobs)")
     ap.add_argument("--plain-steps", type=int, default=1, help="batch: timed passes of the plain path")
     ap.add_argument("--cpu-scenes", type=int, default=8, help="batch: scenes the CPU baseline samples")
@@ -473,6 +474,7 @@ def run_serve(a):
         recs = [records(j) if j[5] is not None else None for j in jobs]
         # served: submit each job at its arrival, step waves while any job is held
         sv = L.native.Server(ctx, int(a.budget_gb * 2**30), a.wave_paths)
+        sv.set_wavefront(a.wave_slots)
         lat, rays_s, ids = [], 0, {}
         nxt, done = 0, 0
         t0 = L.native.clock_ms()
@@ -539,7 +541,7 @@ def run_serve(a):
             "config": {"workload": f"served request stream: 64 resident scenes ({tris} triangles; 8 with 2000 moving "
                                    "instances), jobs {256^2, 720p, 1080p} x spp {4, 16, 64}, depth 8, Poisson arrivals",
                        "rates": a.rates, "jobs_per_rate": a.jobs, "budget_gb": a.budget_gb,
-                       "wave_paths": a.wave_paths, "parallelism": "one GPU"},
+                       "wave_paths": a.wave_paths, "wave_slots": a.wave_slots, "parallelism": "one GPU"},
             "clocks": clocks, "rates": results}
     for s in scenes:
         s.close()

@@ -138,6 +138,7 @@ int lrc_server_create(lrc_ctx *c, uint64_t hbm_budget_bytes, uint64_t wave_paths
     sv->wave_paths = wave_paths;
     DeviceGuard g(c->device);
     int rc = lrc_batch_create(c, &sv->batch);
+    if (!rc) rc = lrc_batch_set_wavefront(sv->batch, 1u << 22, 0);   // (4M paths in flight: a wave's tail stays short)
     cudaError_t e = rc ? cudaSuccess : cudaMalloc(&sv->d_small, 256);
     if (rc || e) {
         if (sv->batch) lrc_batch_destroy(sv->batch);

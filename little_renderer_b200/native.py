@@ -609,6 +609,10 @@ class Server:
     def batch_handle(self):
         return self.ctx.L.lrc_server_batch(self.h)
 
+    def set_wavefront(self, slots, variant=0):
+        """The waves' wavefront size (paths in flight) and closest-hit / shadow launch shape."""
+        self.ctx.check(self.ctx.L.lrc_batch_set_wavefront(C.c_void_p(self.batch_handle()), slots, variant))
+
 
 def clock_ms():
     return lib().lrc_server_clock()
