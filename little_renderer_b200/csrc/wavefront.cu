@@ -217,8 +217,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJo
 }
 
 // the rest of every queued path's bounce; its shadow rays into the shadow queue
-__global__ void __launch_bounds__(SHADE_BLOCK) wf_shade_kernel(const BatchJob *__restrict__ jobs, WfState W, uint32_t *err,
-                                                                uint32_t max_passes) {
+template <int SMINB>
+__global__ void __launch_bounds__(SHADE_BLOCK, SMINB) wf_shade_kernel(const BatchJob *__restrict__ jobs, WfState W,
+                                                                       uint32_t *err, uint32_t max_passes) {
     const uint32_t count = W.ctl[4] >= max_passes ? 0u : *reinterpret_cast<volatile uint32_t *>(&W.ctl[0]);
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (SHADE_BLOCK / 32);
@@ -307,12 +308,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_shadow_kernel(const BatchJob *
 
 namespace {
 struct WfVariant {
-    int block, minb;
-    const void *isect, *shadow;
+    int block, minb, shade_minb;
+    const void *isect, *shadow, *shade;
 };
-#define LRC_WF_VARIANT(B, M) {B, M, (const void *)pt::wf_intersect_kernel<B, M>, (const void *)pt::wf_shadow_kernel<B, M>}
+#define LRC_WF_VARIANT(B, M, S)                                                                                 \
+    {B, M, S, (const void *)pt::wf_intersect_kernel<B, M>, (const void *)pt::wf_shadow_kernel<B, M>,            \
+     (const void *)pt::wf_shade_kernel<S>}
 const WfVariant kWfVariants[] = {
-    LRC_WF_VARIANT(128, 4), LRC_WF_VARIANT(128, 6), LRC_WF_VARIANT(128, 8), LRC_WF_VARIANT(256, 4), LRC_WF_VARIANT(64, 12),
+    LRC_WF_VARIANT(128, 4, 1), LRC_WF_VARIANT(128, 6, 1), LRC_WF_VARIANT(128, 8, 1), LRC_WF_VARIANT(256, 4, 1),
+    LRC_WF_VARIANT(64, 12, 1), LRC_WF_VARIANT(128, 6, 5), LRC_WF_VARIANT(128, 8, 5), LRC_WF_VARIANT(128, 8, 6),
 };
 #undef LRC_WF_VARIANT
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
@@ -407,7 +411,7 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.isect, V.block, 0);
     const int grid = std::max(per_sm, 1) * num_sms;
     int shade_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, pt::wf_shade_kernel, pt::SHADE_BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, V.shade, pt::SHADE_BLOCK, 0);
     const int shade_grid = std::max(shade_per_sm, 1) * num_sms;
     WfState w = W;
     pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, body_st>>>(d_jobs, njobs, w);
@@ -415,7 +419,10 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
     e = cudaLaunchKernel(V.isect, dim3(grid), dim3(V.block), iargs, 0, body_st);
     if (!e) {
-        pt::wf_shade_kernel<<<shade_grid, pt::SHADE_BLOCK, 0, body_st>>>(d_jobs, w, d_status, max_passes);
+        void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&max_passes};
+        e = cudaLaunchKernel(V.shade, dim3(shade_grid), dim3(pt::SHADE_BLOCK), hargs, 0, body_st);
+    }
+    if (!e) {
         void *sargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};
         e = cudaLaunchKernel(V.shadow, dim3(grid), dim3(V.block), sargs, 0, body_st);
     }
@@ -433,7 +440,7 @@ cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long
     const WfVariant &V = kWfVariants[variant];
     int per_sm = 0, shade_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.isect, V.block, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, pt::wf_shade_kernel, pt::SHADE_BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, V.shade, pt::SHADE_BLOCK, 0);
     const int grid = std::max(per_sm, 1) * num_sms, shade_grid = std::max(shade_per_sm, 1) * num_sms;
     WfState w = W;
     cudaGraphConditionalHandle cond = 0;
@@ -445,7 +452,9 @@ cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long
         void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
         e = cudaLaunchKernel(V.isect, dim3(grid), dim3(V.block), iargs, 0, st);
         if (e) break;
-        pt::wf_shade_kernel<<<shade_grid, pt::SHADE_BLOCK, 0, st>>>(d_jobs, w, d_status, max_passes);
+        void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&max_passes};
+        e = cudaLaunchKernel(V.shade, dim3(shade_grid), dim3(pt::SHADE_BLOCK), hargs, 0, st);
+        if (e) break;
         void *sargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};
         e = cudaLaunchKernel(V.shadow, dim3(grid), dim3(V.block), sargs, 0, st);
         uint32_t queued = 0;
