@@ -236,6 +236,13 @@ int prepare(lrc_batch *b) {
     return LRC_OK;
 }
 
+// whether some job's scene has instances (the traversal kernels then walk two levels)
+bool any_instances(const lrc_batch *b) {
+    for (const lrc::BatchJob &T : b->table)
+        if (T.S.ninst) return true;
+    return false;
+}
+
 // a bound on the wavefront's passes for the first `limit` tasks: each slot runs at most
 // ceil(limit / slots) tasks one after another, each of at most (samples a task holds) paths of at
 // most max_depth + 1 bounces, plus one pass to start and one to end each task
@@ -275,13 +282,13 @@ int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool 
         e = lrc::batch_trace(b->d_jobs, (uint32_t)nj, limit, b->d_ctr, c->d_status, b->variant, b->grid, st);
     if (!e && b->engine == 1 && !capturing && (flags & LRC_BATCH_STEPPED)) {
         const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
-        e = lrc::wf_run_stepped(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, c->num_sms,
-                                max_passes(b, limit), st);
+        e = lrc::wf_run_stepped(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, any_instances(b),
+                                c->num_sms, max_passes(b, limit), st);
     } else if (!e && b->engine == 1) {
         if (!capturing) return fail(c, LRC_E_INVALID, "the wavefront runs as a captured graph");
         const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
-        e = lrc::wf_capture_loop(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, c->num_sms,
-                                 max_passes(b, limit), st, b->body);
+        e = lrc::wf_capture_loop(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, any_instances(b),
+                                 c->num_sms, max_passes(b, limit), st, b->body);
     }
     if (!e && with_resolve) e = lrc::batch_resolve(b->d_jobs, (uint32_t)nj, b->npix, st);
     if (e) return cuda_status(c, e, "batch run");

@@ -265,16 +265,18 @@ int wf_variants();
 int wf_variant_shape(int variant, int *block, int *minb);
 // Captures the wavefront's loop into the graph stream st is capturing: the slots cleared and the
 // task queue set to the first ntasks tasks, then a while node whose body (captured on body_st)
-// runs the advance, closest-hit, shade and shadow kernels until no slot holds a path.
+// runs the advance, closest-hit, shade and shadow kernels until no slot holds a path. instances:
+// some job's scene has instances (else the traversal kernels without the two-level walk run).
 // The loop stops after max_passes passes whatever is left (ST_LOOP in the status word): a bound well
 // above what the tasks need (a pass per bounce of each slot's tasks).
 cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
-                            uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st,
-                            cudaStream_t body_st);
+                            uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
+                            cudaStream_t st, cudaStream_t body_st);
 // The same loop with each pass's kernels launched from the host (no graph; the host reads the
 // queued count after every pass): for profilers that cannot see into a graph's loop.
 cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
-                           uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st);
+                           uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
+                           cudaStream_t st);
 // the sky's sampling tables as env_prepare makes them (host_tables.cu): marg h + 1, cond h x (w + 1),
 // prob w x h; returns false when no pixel weighs anything (sum 0)
 bool env_tables(const float *rgb, int w, int h, float *marg, float *cond, float *prob);

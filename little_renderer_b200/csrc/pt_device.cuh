@@ -301,10 +301,12 @@ __device__ __forceinline__ bool scene_intersect(const PtScene &S, V3 o, V3 d, fl
     }
     return found;
 }
-// scene_occluded (accel.c:280): any hit in (tmin, tmax), the instances first
+// scene_occluded (accel.c:280): any hit in (tmin, tmax), the instances first. INST = false: a
+// scene known to have no instances (the walk of the two levels not compiled in: fewer registers)
+template <bool INST = true>
 __device__ __forceinline__ bool scene_occluded(const PtScene &S, V3 o, V3 d, float tmin, float tmax, uint32_t *err) {
     float best = tmax;
-    if (S.ninst) {
+    if (INST && S.ninst) {
         int inst, tri;
         if (walk_instances<true>(S, o, d, tmin, best, inst, tri, err)) return true;
     }
@@ -510,7 +512,8 @@ __device__ __forceinline__ void path_begin(int mis, V3 ro, V3 rd, PathState &ps)
 }
 
 // scene_intersect's search alone: the closest t, the world shape (or -1) and the instance and its
-// triangle (or -1); make_hit then gives the Hit scene_intersect gives
+// triangle (or -1); make_hit then gives the Hit scene_intersect gives. INST as scene_occluded's.
+template <bool INST = true>
 __device__ __forceinline__ void scene_find(const PtScene &S, V3 o, V3 d, float tmin, float tmax, float &t, int &id, int &inst,
                                            int &tri, uint32_t *err) {
     float best = tmax;
@@ -518,7 +521,7 @@ __device__ __forceinline__ void scene_find(const PtScene &S, V3 o, V3 d, float t
     inst = -1;
     tri = -1;
     if (S.nnodes) id = walk<false>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err);
-    if (S.ninst) {
+    if (INST && S.ninst) {
         int ii = -1, tt = -1;
         if (walk_instances<false>(S, o, d, tmin, best, ii, tt, err)) {
             inst = ii;

@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
 
 // the closest hit of every queued ray (warps fetch 32 rays at a time); sets the loop's condition
 // (another pass while rays are queued)
-template <int BLOCK, int MINB>
+template <int BLOCK, int MINB, bool INST>
 __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJob *__restrict__ jobs, WfState W, uint32_t *err,
                                                                    cudaGraphConditionalHandle cond, uint32_t max_passes,
                                                                    int use_cond) {
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJo
             const V3 o = v3f(W.ro[s]), d = v3f(W.rd[s]);
             float t;
             int id, inst, tri;
-            scene_find(J.S, o, d, RT_EPS, 1e30f, t, id, inst, tri, err);
+            scene_find<INST>(J.S, o, d, RT_EPS, 1e30f, t, id, inst, tri, err);
             W.hit[s] = make_float4(t, __int_as_float(id), __int_as_float(inst), __int_as_float(tri));
         }
     }
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(SHADE_BLOCK, SMINB) wf_shade_kernel(const Batc
 
 // the any-hit test of every queued shadow ray; clears the ray queue and counts the pass for the
 // next one
-template <int BLOCK, int MINB>
+template <int BLOCK, int MINB, bool INST>
 __global__ void __launch_bounds__(BLOCK, MINB) wf_shadow_kernel(const BatchJob *__restrict__ jobs, WfState W, uint32_t *err) {
     const uint32_t count = *reinterpret_cast<volatile uint32_t *>(&W.ctl[1]);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_shadow_kernel(const BatchJob *
             const float4 o = W.sq_o[k], d = W.sq_d[k];
             const uint32_t e = __float_as_uint(o.w);
             const BatchJob &J = jobs[W.job[e >> 1]];
-            W.vis[e] = scene_occluded(J.S, v3f(o), v3f(d), RT_EPS, d.w, err) ? 0 : 1;
+            W.vis[e] = scene_occluded<INST>(J.S, v3f(o), v3f(d), RT_EPS, d.w, err) ? 0 : 1;
         }
     }
 }
@@ -310,10 +310,12 @@ namespace {
 struct WfVariant {
     int block, minb, shade_minb;
     const void *isect, *shadow, *shade;
+    const void *isect_world, *shadow_world;   // (for batches without instances)
 };
 #define LRC_WF_VARIANT(B, M, S)                                                                                 \
-    {B, M, S, (const void *)pt::wf_intersect_kernel<B, M>, (const void *)pt::wf_shadow_kernel<B, M>,            \
-     (const void *)pt::wf_shade_kernel<S>}
+    {B, M, S, (const void *)pt::wf_intersect_kernel<B, M, true>, (const void *)pt::wf_shadow_kernel<B, M, true>,  \
+     (const void *)pt::wf_shade_kernel<S>, (const void *)pt::wf_intersect_kernel<B, M, false>,                  \
+     (const void *)pt::wf_shadow_kernel<B, M, false>}
 const WfVariant kWfVariants[] = {
     LRC_WF_VARIANT(128, 4, 1), LRC_WF_VARIANT(128, 6, 1), LRC_WF_VARIANT(128, 8, 1), LRC_WF_VARIANT(256, 4, 1),
     LRC_WF_VARIANT(64, 12, 1), LRC_WF_VARIANT(128, 6, 5), LRC_WF_VARIANT(128, 8, 5), LRC_WF_VARIANT(128, 8, 6),
@@ -377,8 +379,8 @@ WfState wf_carve(void *base, uint32_t M) {
 }
 
 cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
-                            uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st,
-                            cudaStream_t body_st) {
+                            uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
+                            cudaStream_t st, cudaStream_t body_st) {
     if (variant < 0 || variant >= wf_variants() || W.M == 0 || W.M % pt::ADV_BLOCK) return cudaErrorInvalidValue;
     cudaStreamCaptureStatus cs;
     cudaGraph_t g = nullptr;
@@ -407,8 +409,9 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     e = cudaStreamBeginCaptureToGraph(body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e) return e;
     const WfVariant &V = kWfVariants[variant];
+    const void *isect = instances ? V.isect : V.isect_world, *shadow = instances ? V.shadow : V.shadow_world;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.isect, V.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, isect, V.block, 0);
     const int grid = std::max(per_sm, 1) * num_sms;
     int shade_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, V.shade, pt::SHADE_BLOCK, 0);
@@ -417,14 +420,14 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, body_st>>>(d_jobs, njobs, w);
     int use_cond = 1;
     void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
-    e = cudaLaunchKernel(V.isect, dim3(grid), dim3(V.block), iargs, 0, body_st);
+    e = cudaLaunchKernel(isect, dim3(grid), dim3(V.block), iargs, 0, body_st);
     if (!e) {
         void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&max_passes};
         e = cudaLaunchKernel(V.shade, dim3(shade_grid), dim3(pt::SHADE_BLOCK), hargs, 0, body_st);
     }
     if (!e) {
         void *sargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};
-        e = cudaLaunchKernel(V.shadow, dim3(grid), dim3(V.block), sargs, 0, body_st);
+        e = cudaLaunchKernel(shadow, dim3(grid), dim3(V.block), sargs, 0, body_st);
     }
     if (!e) e = cudaGetLastError();
     cudaGraph_t out = nullptr;
@@ -435,11 +438,13 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
 }
 
 cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
-                           uint32_t *d_status, int variant, int num_sms, uint32_t max_passes, cudaStream_t st) {
+                           uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
+                           cudaStream_t st) {
     if (variant < 0 || variant >= wf_variants() || W.M == 0 || W.M % pt::ADV_BLOCK) return cudaErrorInvalidValue;
     const WfVariant &V = kWfVariants[variant];
+    const void *isect = instances ? V.isect : V.isect_world, *shadow = instances ? V.shadow : V.shadow_world;
     int per_sm = 0, shade_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, V.isect, V.block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, isect, V.block, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, V.shade, pt::SHADE_BLOCK, 0);
     const int grid = std::max(per_sm, 1) * num_sms, shade_grid = std::max(shade_per_sm, 1) * num_sms;
     WfState w = W;
@@ -450,13 +455,13 @@ cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long
     for (uint32_t pass = 0; !e && pass <= max_passes; pass++) {
         pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, st>>>(d_jobs, njobs, w);
         void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
-        e = cudaLaunchKernel(V.isect, dim3(grid), dim3(V.block), iargs, 0, st);
+        e = cudaLaunchKernel(isect, dim3(grid), dim3(V.block), iargs, 0, st);
         if (e) break;
         void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&max_passes};
         e = cudaLaunchKernel(V.shade, dim3(shade_grid), dim3(pt::SHADE_BLOCK), hargs, 0, st);
         if (e) break;
         void *sargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};
-        e = cudaLaunchKernel(V.shadow, dim3(grid), dim3(V.block), sargs, 0, st);
+        e = cudaLaunchKernel(shadow, dim3(grid), dim3(V.block), sargs, 0, st);
         uint32_t queued = 0;
         if (!e) e = cudaMemcpyAsync(&queued, &W.ctl[5], 4, cudaMemcpyDeviceToHost, st);
         if (!e) e = cudaStreamSynchronize(st);
