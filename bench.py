@@ -77,6 +77,22 @@ def config(a, world):
             "l2": "inputs larger than L2 (triangles 48 B x N + rays 24 B x R > 126 MB)"}
 
 
+def max_over_ranks(ms, dist, device):
+    """The step time of the job: the slowest rank's (all ranks take part; one rank: as is)."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, ms):
+    """Replicas: every rank processed units_per_rank units in the job's ms; the whole job's rate
+    in millions of units per second (weak scaling: the work grows with the ranks)."""
+    return world * units_per_rank / (ms / 1e3) / 1e6
+
+
 class Clocks:
     """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -299,12 +315,7 @@ def run_batch(a):
         e1.record(stream)
         torch.cuda.synchronize()
         ctx.sync()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(e0.elapsed_time(e1), dist, dev)
 
     # the plain path: one pass for its images (and its warm-up), then the timed passes
     for img in imgs:
@@ -764,14 +775,11 @@ def main():
     ctx.sync()
     stages = ctx.timings()
     ctx.set_timing(False)
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_step = ms / a.steps
-    value = world * a.rays * a.steps / (ms / 1e3) / 1e6
+    value = whole_job_rate(a.rays * a.steps, world, ms)
 
     # end to end through the C ABI with host (pinned) buffers: copies in and out inside each step
     pin_tris = torch.from_numpy(tris.view(np.int32)).pin_memory()
@@ -799,12 +807,8 @@ def main():
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e2e = {"value": world * a.rays * a.e2e_steps / (e_ms / 1e3) / 1e6, "unit": "Mrays/s",
+    e_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    e2e = {"value": whole_job_rate(a.rays * a.e2e_steps, world, e_ms), "unit": "Mrays/s",
            "h2d_bytes_per_step": int(tris.nbytes + orig.nbytes + dirs.nbytes),
            "d2h_bytes_per_step": int(a.rays * 8), "ms_per_step": e_ms / a.e2e_steps}
 
