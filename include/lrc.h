@@ -60,6 +60,7 @@ int lrc_num_sms(const lrc_ctx *ctx);
 #define LRC_TS_HIERARCHY 3   /* LBVH hierarchy and boxes, or PLOC */
 #define LRC_TS_TRACE 4       /* ray queries */
 #define LRC_TS_SHADE 5       /* path tracing */
+#define LRC_TS_LIGHT 6       /* light tracing (caustics) */
 #define LRC_NUM_STAGES 8
 int lrc_set_timing(lrc_ctx *ctx, int on);
 /* milliseconds of each stage (ms[LRC_NUM_STAGES]) and launches of each (optional) since the last
@@ -224,6 +225,9 @@ typedef struct {
                               up to transcendental rounding; 0: a stream per sample (faster) */
     uint64_t seed;         /* the image's seed (trace_image's) */
     float clamp;           /* largest sample value, 0: none */
+    int32_t skip_caustics; /* 1: leave out the paths light tracing covers (camera -> diffuse first,
+                              then the lamp right after a mirror / glass vertex; TraceParams.skip_caustics,
+                              engine/rt/tracer.h:16-20): set it when lrc_caustics adds them */
 } lrc_trace_params;
 /* Samples [spp0, spp0 + spp) of every pixel of rows [y0, y0 + rows), added into accum (width x
  * height x 4 floats: the sum of the samples' linear RGB and their count, as gpu_view_trace_read
@@ -231,6 +235,27 @@ typedef struct {
  * first sample). rays (optional, host): the closest-hit and shadow rays traced. */
 int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0, uint32_t spp,
               float *accum, uint64_t *rays, unsigned flags);
+
+/* ---- light-traced caustics: replaces light_trace_caustics (engine/rt/tracer.c:553-665) and the
+ * GPU backend's `ltrace` pass into its 64-bit caustic sums (gpu_trace_light, trace_gpu.c:1946-1954;
+ * trace.wgsl:1415-1511) ------------------------------------------------------------------------
+ * `photons` light paths from the scene's lamp through mirrors / glass onto rough surfaces, each
+ * such vertex joined to the camera of p (width, height, max_depth, exact: the random streams as
+ * lrc_trace's modes; the other fields are not read). Light tracing covers exactly the paths
+ * lrc_trace leaves out with p->skip_caustics = 1, so the two images added are the full image.
+ * Contributions are summed as 32.32 fixed-point integers (value * 2^32 / photons, rounded to the
+ * nearest) with integer atomics: the result does not depend on the order or the launch.
+ * No lamp, or no material with a perfectly smooth (mirror / glass) part: nothing is added.
+ * lrc_caustics: image (width x height x 3 floats, linear RGB) += the caustic image (the sums /
+ *   2^32, light_trace_caustics' `out +=`).
+ * lrc_caustics_sums: sums (width x height x 3 uint64, 32.32) += the fixed-point values, the GPU
+ *   backend's `caus` buffer; after passes of equal photon counts the image is sums / 2^32 / passes.
+ * Arrays are host memory, or device memory with LRC_DEVICE. rays (optional, host): the closest-hit
+ * and shadow rays traced. */
+int lrc_caustics(lrc_scene *s, const lrc_trace_params *p, uint64_t photons, uint64_t seed, float *image,
+                 uint64_t *rays, unsigned flags);
+int lrc_caustics_sums(lrc_scene *s, const lrc_trace_params *p, uint64_t photons, uint64_t seed, uint64_t *sums,
+                      uint64_t *rays, unsigned flags);
 
 /* ---- batches: many jobs over many resident scenes, built and traced together --------------
  * No counterpart in the reference, which traces one scene per dispatch and sizes its submits by

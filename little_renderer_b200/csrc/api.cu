@@ -286,6 +286,7 @@ void lrc_scene_destroy(lrc_scene *s) {
     cudaFree(s->d_tlas_nodes);
     cudaFree(s->d_tlas_aux);
     cudaFree(s->d_env);
+    cudaFree(s->d_caus);
     delete s;
 }
 
@@ -465,6 +466,20 @@ int lrc_scene_set_materials(lrc_scene *s, const float *mats, uint32_t n) {
     if (!e && n) e = cudaMemcpyAsync(s->d_mats, mats, (size_t)n * 64, cudaMemcpyHostToDevice, c->st);
     if (e) return cuda_status(c, e, "materials");
     s->nmats = n;
+    // scene_has_specular (tracer.c:547-551): material_has_delta (brdf.h:407-410) of any material,
+    // the roughness as material_resolved fills it in for the presets
+    s->specular = false;
+    for (uint32_t i = 0; i < n; i++) {
+        const float *m = mats + 16 * (size_t)i;
+        int type;
+        std::memcpy(&type, m + 3, 4);
+        float r = m[10];
+        if (type == 3) continue;                  // MAT_LIGHT
+        if (type == 0) r = 1.0f;                  // MAT_DIFFUSE
+        else if (type == 1 || type == 2) r = 0.0f;   // MAT_MIRROR, MAT_GLASS
+        const float c01 = r < 0.0f ? 0.0f : (r > 1.0f ? 1.0f : r);
+        if (c01 <= 0.02f) s->specular = true;
+    }
     return check_status(c);
 }
 
@@ -772,6 +787,7 @@ int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
     P.group = gsz;
     P.seed = p->seed;
     P.clamp = p->clamp;
+    P.skip_caustics = p->skip_caustics != 0;
     P.origin = {p->origin[0], p->origin[1], p->origin[2]};
     P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
     P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};

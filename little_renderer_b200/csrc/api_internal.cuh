@@ -66,6 +66,10 @@ struct lrc_scene {
     float *d_env = nullptr;       // rgbp (w x h float4), cond, marg
     int env_w = 0, env_h = 0, env_weighted = 0;
     float env_scale = 1;
+    // light tracing: a material with a perfectly smooth part (scene_has_specular), the sums' scratch
+    bool specular = false;
+    void *d_caus = nullptr;
+    size_t caus_cap = 0;
 };
 
 namespace lrcapi {

@@ -88,6 +88,7 @@ lrc::PtParams params_of(const lrc_batch::Job &J) {
     P.group = group_for(*p, J.spp);
     P.seed = p->seed;
     P.clamp = p->clamp;
+    P.skip_caustics = p->skip_caustics != 0;
     P.origin = {p->origin[0], p->origin[1], p->origin[2]};
     P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
     P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
@@ -135,7 +136,7 @@ std::vector<unsigned char> signature(const lrc_batch *b, unsigned flags) {
         put(bufs, sizeof bufs);
         const void *ptrs[2] = {J.s, J.accum};
         put(ptrs, sizeof ptrs);
-        put(&J.p, offsetof(lrc_trace_params, clamp) + sizeof(float));
+        put(&J.p, offsetof(lrc_trace_params, skip_caustics) + sizeof(int32_t));
         const int32_t w[6] = {J.y0, J.rows, (int32_t)J.spp0, (int32_t)J.spp, J.builder, J.key_bits};
         put(w, sizeof w);
     }

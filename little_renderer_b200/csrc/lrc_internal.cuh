@@ -197,12 +197,19 @@ struct PtParams {
     uint64_t seed;
     float clamp;
     pt::V3 origin, upper_left, horizontal, vertical;   // the Camera (camera.h)
+    int skip_caustics;                                 // TraceParams.skip_caustics
 };
 cudaError_t pt_prim_boxes(const float *d_prims, uint32_t n, float *d_boxes, cudaStream_t st);
 cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsigned long long *d_rays, uint32_t *d_status,
                      cudaStream_t st);
 cudaError_t pt_intersect(const PtScene &S, const float *d_orig, const float *d_dir, uint64_t n, float tmin, float tmax,
                          int32_t *d_prim, int32_t *d_inst, float *d_t, uint32_t *d_status, cudaStream_t st);
+// light tracing (caustics.cu): `photons` light paths (P's camera, image size, max_depth and exact
+// mode) whose 32.32 contributions are added into d_sums (W x H x 3); and image += sums / 2^32
+cudaError_t lt_trace(const PtScene &S, const PtParams &P, unsigned long long photons, uint64_t seed,
+                     unsigned long long *d_sums, unsigned long long *d_rays, uint32_t *d_status, int num_sms,
+                     cudaStream_t st);
+cudaError_t lt_resolve(const unsigned long long *d_sums, float *d_image, size_t n, int num_sms, cudaStream_t st);
 cudaError_t pt_inst_boxes(const float *d_rec, uint32_t n, float *d_boxes, cudaStream_t st);
 
 // One job of a batch: a band of one image of one scene. Its tasks are (pixel, lane slot) pairs,
@@ -244,7 +251,7 @@ struct WfState {
     uint2 *xy;                  // the task's pixel
     float4 *sum;                // the task's sum so far (rgb, samples)
     float4 *ro;                 // the path's ray origin, bounce_pdf
-    float4 *rd;                 // its direction, depth | emit << 16 (int bits)
+    float4 *rd;                 // its direction, depth | emit << 16 | caus << 24 (int bits)
     float4 *thr;                // its throughput
     float4 *rad;                // its radiance so far
     ulonglong2 *rng;            // its Rng (state, inc)

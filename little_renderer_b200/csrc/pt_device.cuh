@@ -495,13 +495,18 @@ enum { EMIT_FULL, EMIT_NONE, EMIT_MIS };
 // all a path needs to resume, so a thread can hold one path per lane and start the next sample
 // the moment its path ends (path regeneration), or a path can wait in memory between the
 // kernels of a wavefront.
+// skip_caustics' state (tracer.c:371-375): CAUS_CHAIN the camera saw a rough surface first,
+// CAUS_SPEC a mirror / glass vertex since the last rough one; a path with both that reaches the
+// lamp is light tracing's (lrc_caustics), not counted here. CAUS_SKIP: the job leaves them out.
+enum { CAUS_CHAIN = 1, CAUS_SPEC = 2, CAUS_SKIP = 4 };
+
 struct PathState {
     V3 ro, rd, thr, radiance;
     float bounce_pdf;
-    int depth, emit;
+    int depth, emit, caus;
 };
 
-__device__ __forceinline__ void path_begin(int mis, V3 ro, V3 rd, PathState &ps) {
+__device__ __forceinline__ void path_begin(int mis, V3 ro, V3 rd, PathState &ps, int skip_caustics) {
     ps.ro = ro;
     ps.rd = mis ? vnorm(rd) : rd;
     ps.thr = v3(1, 1, 1);
@@ -509,6 +514,7 @@ __device__ __forceinline__ void path_begin(int mis, V3 ro, V3 rd, PathState &ps)
     ps.bounce_pdf = 0.0f;
     ps.depth = 0;
     ps.emit = EMIT_FULL;
+    ps.caus = skip_caustics ? CAUS_SKIP : 0;
 }
 
 // scene_intersect's search alone: the closest t, the world shape (or -1) and the instance and its
@@ -559,7 +565,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
     }
     const Mat m = load_mat(S.mats, hit_material(S, h) & 63);   // (MAX_MATS 64: the buffer's size)
     if (m.type == MAT_LIGHT) {
-        if (h.front) {
+        if (h.front && (ps.caus & (CAUS_CHAIN | CAUS_SPEC)) != (CAUS_CHAIN | CAUS_SPEC)) {
             if (ps.emit == EMIT_FULL) {
                 ps.radiance = vadd(ps.radiance, vmul(ps.thr, m.emission));
             } else if (ps.emit == EMIT_MIS && h.inst < 0 && h.prim == S.light) {
@@ -630,9 +636,12 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
     ps.thr = vmul(ps.thr, bs.w);
     if (bs.delta) {
         ps.emit = EMIT_FULL;
+        ps.caus |= CAUS_SPEC;
     } else {
         ps.bounce_pdf = bs.pdf;
         ps.emit = mis ? EMIT_MIS : EMIT_NONE;
+        if (depth == 0 && (ps.caus & CAUS_SKIP)) ps.caus |= CAUS_CHAIN;
+        ps.caus &= ~CAUS_SPEC;
     }
     if (depth >= RR_START) {                         // russian_roulette_u
         float p = rmin(vmax3(ps.thr), 0.95f);
@@ -659,7 +668,7 @@ __device__ __forceinline__ bool path_bounce(const PtScene &S, int max_depth, int
 // trace_path_sampled (tracer.c:364-545): the bounces of one path
 __device__ inline V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err, uint32_t &rays) {
     PathState ps;
-    path_begin(P.mis, ro, rd, ps);
+    path_begin(P.mis, ro, rd, ps, P.skip_caustics);
     while (path_bounce(S, P.max_depth, P.mis, ps, sm, err, rays)) {
     }
     return ps.radiance;

@@ -157,9 +157,9 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
         V3 o, d;
         camera_ray(J.P, u, v, o, d);
         PathState ps;
-        path_begin(J.P.mis, o, d, ps);
+        path_begin(J.P.mis, o, d, ps, J.P.skip_caustics);
         W.ro[i] = make_float4(ps.ro.x, ps.ro.y, ps.ro.z, ps.bounce_pdf);
-        W.rd[i] = make_float4(ps.rd.x, ps.rd.y, ps.rd.z, __int_as_float(ps.depth | (ps.emit << 16)));
+        W.rd[i] = make_float4(ps.rd.x, ps.rd.y, ps.rd.z, __int_as_float(ps.depth | (ps.emit << 16) | (ps.caus << 24)));
         W.thr[i] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z, 0.0f);
         W.rad[i] = make_float4(0, 0, 0, 0);
         W.rng[i] = make_ulonglong2(rng.state, rng.inc);
@@ -239,7 +239,8 @@ __global__ void __launch_bounds__(SHADE_BLOCK, SMINB) wf_shade_kernel(const Batc
             ps.rd = v3f(rd);
             const int de = __float_as_int(rd.w);
             ps.depth = de & 0xffff;
-            ps.emit = de >> 16;
+            ps.emit = (de >> 16) & 0xff;
+            ps.caus = de >> 24;
             ps.thr = v3f(th);
             ps.radiance = v3f(ra);
             const ulonglong2 r = W.rng[s];
@@ -255,7 +256,7 @@ __global__ void __launch_bounds__(SHADE_BLOCK, SMINB) wf_shade_kernel(const Batc
             uint32_t rays = 0;
             const bool cont = path_shade<true>(J.S, J.P.max_depth, J.P.mis, ps, found, h, sm, err, rays, nee);
             W.ro[s] = make_float4(ps.ro.x, ps.ro.y, ps.ro.z, ps.bounce_pdf);
-            W.rd[s] = make_float4(ps.rd.x, ps.rd.y, ps.rd.z, __int_as_float(ps.depth | (ps.emit << 16)));
+            W.rd[s] = make_float4(ps.rd.x, ps.rd.y, ps.rd.z, __int_as_float(ps.depth | (ps.emit << 16) | (ps.caus << 24)));
             W.thr[s] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z, 0.0f);
             W.rad[s] = make_float4(ps.radiance.x, ps.radiance.y, ps.radiance.z, 0.0f);
             W.rng[s] = make_ulonglong2(rng.state, rng.inc);

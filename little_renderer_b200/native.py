@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -94,6 +94,8 @@ def lib():
     L.lrc_default_blue_noise.argtypes = [vp]
     L.lrc_default_bsdf_tables.argtypes = [vp]
     L.lrc_trace.argtypes = [vp, vp, C.c_int32, C.c_int32, u32, u32, vp, vp, C.c_uint]
+    L.lrc_caustics.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
+    L.lrc_caustics_sums.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
     L.lrc_scene_set_meshes.argtypes = [vp, vp, vp, u32, C.c_uint]
     L.lrc_scene_set_instances.argtypes = [vp, vp, u32, C.c_uint]
     L.lrc_scene_build_instances.argtypes = [vp, C.c_int, C.c_int]
@@ -147,16 +149,16 @@ class TraceParams(C.Structure):
     _fields_ = [("origin", C.c_float * 3), ("upper_left", C.c_float * 3), ("horizontal", C.c_float * 3),
                 ("vertical", C.c_float * 3), ("width", C.c_int32), ("height", C.c_int32), ("max_depth", C.c_int32),
                 ("mis", C.c_int32), ("sampler", C.c_int32), ("exact", C.c_int32), ("seed", C.c_uint64),
-                ("clamp", C.c_float)]
+                ("clamp", C.c_float), ("skip_caustics", C.c_int32)]
 
 
-def trace_params(cam12, width, height, max_depth=8, mis=1, sampler=1, exact=0, seed=0, clamp=0.0):
+def trace_params(cam12, width, height, max_depth=8, mis=1, sampler=1, exact=0, seed=0, clamp=0.0, skip_caustics=0):
     p = TraceParams()
     cam12 = np.asarray(cam12, np.float32).reshape(4, 3)
     for i, name in enumerate(("origin", "upper_left", "horizontal", "vertical")):
         getattr(p, name)[:] = cam12[i].tolist()
-    p.width, p.height, p.max_depth, p.mis, p.sampler, p.exact, p.seed, p.clamp = (
-        width, height, max_depth, mis, sampler, exact, seed, clamp)
+    p.width, p.height, p.max_depth, p.mis, p.sampler, p.exact, p.seed, p.clamp, p.skip_caustics = (
+        width, height, max_depth, mis, sampler, exact, seed, clamp, skip_caustics)
     return p
 
 
@@ -399,6 +401,28 @@ class Scene:
         rows = params.height if rows is None else rows
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), y0, rows, spp0, spp, C.c_void_p(d_accum), None,
                                             LRC_DEVICE))
+
+    def caustics(self, params, photons, seed, image=None):
+        """lrc_caustics with a host image: returns (image (h, w, 3) += the caustic image of `photons`
+        light paths, rays traced)."""
+        if image is None:
+            image = np.zeros((params.height, params.width, 3), np.float32)
+        rays = C.c_uint64()
+        self.ctx.check(self.ctx.L.lrc_caustics(self.h, C.byref(params), photons, seed, _ptr(image), C.byref(rays), 0))
+        return image, rays.value
+
+    def caustics_device(self, params, photons, seed, d_image):
+        self.ctx.check(self.ctx.L.lrc_caustics(self.h, C.byref(params), photons, seed, C.c_void_p(d_image), None,
+                                               LRC_DEVICE))
+
+    def caustics_sums(self, params, photons, seed, sums=None):
+        """lrc_caustics_sums with host sums: returns (sums (h, w, 3) uint64 += the 32.32 values, rays)."""
+        if sums is None:
+            sums = np.zeros((params.height, params.width, 3), np.uint64)
+        rays = C.c_uint64()
+        self.ctx.check(self.ctx.L.lrc_caustics_sums(self.h, C.byref(params), photons, seed, _ptr(sums), C.byref(rays),
+                                                    0))
+        return sums, rays.value
 
     def trace_stats(self, orig, dirs=None, tmin=0.0, tmax=1e30):
         """(box tests, triangle tests) of the closest-hit walk over these rays: host arrays

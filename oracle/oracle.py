@@ -192,7 +192,9 @@ def ref_lib(double=False):
         lib.rb_intersect.argtypes = [vp, _f32p, _f32p, C.c_longlong, C.c_float, C.c_float, _i32p, _i32p, _f32p]
         lib.rb_occluded.argtypes = [vp, _f32p, _f32p, C.c_longlong, C.c_float, C.c_float, _i32p]
         lib.rb_trace_image.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                       C.c_ulonglong, C.c_int, C.c_int, C.c_int, _f32p]
+                                       C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        lib.rb_light_trace_caustics.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_longlong, C.c_int,
+                                                C.c_ulonglong, _f32p]
         lib.rb_rays.argtypes = [_i64p]
         lib.rb_blue_noise.argtypes = [_u16p]
         lib.rb_sampler_owen.argtypes = [C.c_uint32, C.c_uint32]
@@ -345,13 +347,24 @@ class RefScene:
                              np.ascontiguousarray(dirs, np.float32).reshape(-1), n, tmin, tmax, out)
         return out
 
-    def trace_image(self, cam, vfov, w, h, spp, seed, max_depth, mis=1, sampler=1, y0=0, rows=None):
+    def trace_image(self, cam, vfov, w, h, spp, seed, max_depth, mis=1, sampler=1, y0=0, rows=None, skip_caustics=0):
         """trace_image: (rows, w, 3) mean radiance; returns (image, (closest rays, shadow rays))."""
         rows = h if rows is None else rows
         out = np.zeros((rows, w, 3), np.float32)
         self.lib.rb_rays_reset()
         self.lib.rb_trace_image(self.s, np.ascontiguousarray(cam, np.float32).reshape(-1), vfov, w, h, y0, rows,
-                                spp, seed, max_depth, mis, sampler, out.reshape(-1))
+                                spp, seed, max_depth, mis, sampler, skip_caustics, out.reshape(-1))
+        cnt = np.zeros(2, np.int64)
+        self.lib.rb_rays(cnt)
+        return out, (int(cnt[0]), int(cnt[1]))
+
+    def light_trace_caustics(self, cam, vfov, w, h, photons, max_depth, seed):
+        """light_trace_caustics (tracer.c:553-665): the (h, w, 3) caustic image of `photons` light
+        paths; returns (image, (closest rays, shadow rays))."""
+        out = np.zeros((h, w, 3), np.float32)
+        self.lib.rb_rays_reset()
+        self.lib.rb_light_trace_caustics(self.s, np.ascontiguousarray(cam, np.float32).reshape(-1), vfov, w, h,
+                                         photons, max_depth, seed, out.reshape(-1))
         cnt = np.zeros(2, np.int64)
         self.lib.rb_rays(cnt)
         return out, (int(cnt[0]), int(cnt[1]))

@@ -5,6 +5,7 @@
 //   closest hit  scene_intersect   (engine/rt/accel.c:252)
 //   any hit      scene_occluded    (engine/rt/accel.c:280)
 //   image        trace_image       (engine/rt/tracer.c:329)
+//   caustics     light_trace_caustics (engine/rt/tracer.c:553)
 //   boxes        triangle_bounds   (engine/scene/scene.c:65)
 // and counts the tracer's rays through link-time --wrap of scene_intersect/scene_occluded
 // (no edit of the reference). Nothing of the product path calls this file.
@@ -239,13 +240,14 @@ void rb_occluded(const void *sp, const float *orig, const float *dir, long long 
 // trace_image over rows [y0, y0 + rows) of a w x h image (rows = h: all of it); rgb: rows * w * 3
 // floats (the mean of each pixel's spp samples). cam: from, at, up (9 floats), vfov in degrees.
 void rb_trace_image(const void *sp, const float *cam, float vfov, int w, int h, int y0, int rows, int spp,
-                    unsigned long long seed, int max_depth, int mis, int sampler, float *rgb){
+                    unsigned long long seed, int max_depth, int mis, int sampler, int skip_caustics, float *rgb){
     const Scene *s = sp;
     Camera c = camera_make(v3f(cam), v3f(cam + 3), v3f(cam + 6), vfov, (real)w / (real)h);
     TraceParams tp = trace_default_params();
     tp.max_depth = max_depth;
     tp.mis = mis;
     tp.sampler = sampler;
+    tp.skip_caustics = skip_caustics;
     Vec3 *px = malloc(sizeof(Vec3) * (size_t)w * h);
     if (!px) return;
     if (rows == h && y0 == 0) trace_image(s, &c, &tp, w, h, spp, seed, 0, px, NULL, NULL);
@@ -275,6 +277,23 @@ void rb_trace_image(const void *sp, const float *cam, float vfov, int w, int h, 
             float *o = rgb + 3 * ((size_t)(y - y0) * w + x);
             o[0] = (float)p->x; o[1] = (float)p->y; o[2] = (float)p->z;
         }
+    free(px);
+}
+
+// light_trace_caustics of `photons` light paths over a w x h image, added into rgb (w * h * 3
+// floats). cam: from, at, up (9 floats), vfov in degrees.
+void rb_light_trace_caustics(const void *sp, const float *cam, float vfov, int w, int h, long long photons,
+                             int max_depth, unsigned long long seed, float *rgb){
+    const Scene *s = sp;
+    Camera c = camera_make(v3f(cam), v3f(cam + 3), v3f(cam + 6), vfov, (real)w / (real)h);
+    TraceParams tp = trace_default_params();
+    tp.max_depth = max_depth;
+    Vec3 *px = calloc((size_t)w * h, sizeof(Vec3));
+    if (!px) return;
+    light_trace_caustics(s, &c, w, h, photons, &tp, seed, px);
+    for (size_t i = 0; i < (size_t)w * h; i++){
+        rgb[3 * i] += (float)px[i].x; rgb[3 * i + 1] += (float)px[i].y; rgb[3 * i + 2] += (float)px[i].z;
+    }
     free(px);
 }
 
