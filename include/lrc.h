@@ -256,6 +256,10 @@ int lrc_caustics(lrc_scene *s, const lrc_trace_params *p, uint64_t photons, uint
                  uint64_t *rays, unsigned flags);
 int lrc_caustics_sums(lrc_scene *s, const lrc_trace_params *p, uint64_t photons, uint64_t seed, uint64_t *sums,
                       uint64_t *rays, unsigned flags);
+/* the light tracer's launch variant for later calls on ctx (its register cap as blocks of 128
+ * threads per SM: 4, 5, 6, 7, 8, 10; -1 the default, 8): returns how many there are. Results do
+ * not depend on it. */
+int lrc_caustics_variant(lrc_ctx *ctx, int variant);
 
 /* ---- batches: many jobs over many resident scenes, built and traced together --------------
  * No counterpart in the reference, which traces one scene per dispatch and sizes its submits by

@@ -18,6 +18,7 @@ struct lrc_ctx {
     size_t stage_cap = 0;
     lrc::StageTimer timer;
     std::string msg;
+    int lt_variant = -1;          // the light tracer's launch variant (-1: the default)
 };
 
 struct lrc_scene {

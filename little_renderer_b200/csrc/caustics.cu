@@ -23,6 +23,9 @@
 
 #include "pt_device.cuh"
 #include <algorithm>
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 namespace lrc {
 namespace pt {
@@ -66,13 +69,13 @@ __device__ __forceinline__ bool camera_project(const LtView &c, V3 p, float &s, 
 
 // one contribution into the 32.32 sums: per channel value * scale rounded to an integer, left out
 // when it is NaN, not positive or absurd (above 1.8e19, the float build's constant)
-__device__ __forceinline__ void splat(unsigned long long *__restrict__ sums, size_t pix, V3 c, double scale) {
+__device__ __forceinline__ void splat(unsigned long long *__restrict__ sums, uint32_t pix, V3 c, double scale) {
     const float ch[3] = {c.x, c.y, c.z};
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const double cc = __dmul_rn((double)ch[k], scale);
         if (!(cc > 0.0) || cc > (double)1.8e19f) continue;
-        atomicAdd(&sums[pix * 3 + k], (unsigned long long)__dadd_rn(cc, 0.5));
+        atomicAdd(&sums[(size_t)pix * 3 + k], (unsigned long long)__dadd_rn(cc, 0.5));
     }
 }
 
@@ -82,17 +85,27 @@ __device__ __forceinline__ void lt_stream(Rng &rng, uint64_t seed, unsigned long
     else rng_seed(rng, mix64(seed ^ (b * 0x9E3779B97F4A7C15ull)), b);
 }
 
-// One thread per run of streams: streams [first, streams) with step `stride`; stream b holds
-// light paths [b * per, min((b + 1) * per, photons)).
-__global__ void __launch_bounds__(128) caustics_kernel(PtScene S, PtParams P, unsigned long long photons,
-                                                       unsigned long long per, uint64_t seed, double scale,
-                                                       unsigned long long *__restrict__ sums,
-                                                       unsigned long long *ray_count, uint32_t *err) {
+// the next stream for each lane of the warp that asks: one atomic add per warp
+__device__ __forceinline__ unsigned long long fetch_stream(unsigned long long *next) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(next, (unsigned long long)g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
+// Persistent threads (one wave of blocks): each takes streams from the counter `next` (zeroed
+// before the launch) as its light paths end; stream b holds light paths [b * per, min((b + 1) *
+// per, photons)). INST = false: the world alone (no two-level walk compiled in). MINB: the
+// register cap's blocks per SM.
+template <bool INST, int MINB>
+__global__ void __launch_bounds__(128, MINB) caustics_kernel(PtScene S, PtParams P, unsigned long long photons,
+                                                             unsigned long long per, uint64_t seed, double scale,
+                                                             unsigned long long *__restrict__ sums,
+                                                             unsigned long long *next, unsigned long long *ray_count,
+                                                             uint32_t *err) {
     const LtView cam = lt_view(P);
     const Lamp L = load_lamp(S);
     const unsigned long long streams = (photons + per - 1) / per;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    unsigned long long b = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long k = 0, end = 0;   // the stream's next light path and its end
     Rng rng;
     V3 ro = v3(0, 0, 0), rd = v3(0, 0, 0), beta = v3(0, 0, 0), thr = v3(0, 0, 0);
@@ -100,15 +113,10 @@ __global__ void __launch_bounds__(128) caustics_kernel(PtScene S, PtParams P, un
     bool alive = false;
     uint32_t rays = 0;
     const bool exact = per > 1;
-    if (b < streams) {
-        lt_stream(rng, seed, b, exact);
-        k = b * per;
-        end = min(k + per, photons);
-    }
     for (;;) {
         if (!alive) {
             if (k == end) {                          // the stream is done: the thread's next one
-                b += stride;
+                const unsigned long long b = fetch_stream(next);
                 if (b >= streams) break;
                 lt_stream(rng, seed, b, exact);
                 k = b * per;
@@ -132,7 +140,10 @@ __global__ void __launch_bounds__(128) caustics_kernel(PtScene S, PtParams P, un
         }
         Hit h;
         rays++;
-        if (!scene_intersect(S, ro, rd, RT_EPS, 1e30f, h, err)) {
+        float t;
+        int id, inst, tri;
+        scene_find<INST>(S, ro, rd, RT_EPS, 1e30f, t, id, inst, tri, err);
+        if (!make_hit(S, ro, rd, t, id, inst, tri, h)) {
             alive = false;
             continue;
         }
@@ -161,10 +172,10 @@ __global__ void __launch_bounds__(128) caustics_kernel(PtScene S, PtParams P, un
                 const int px = (int)mul(sx, (float)cam.W), py = (int)mul(sy, (float)cam.H);
                 if (px < cam.W && py < cam.H) {
                     rays++;
-                    if (!scene_occluded(S, h.p, wo, RT_EPS, mul(dist, sub(1.0f, 1e-4f)), err)) {
+                    if (!scene_occluded<INST>(S, h.p, wo, RT_EPS, mul(dist, sub(1.0f, 1e-4f)), err)) {
                         const float wgt = dvd(mul(corr, fabsf(cos_o)),
                                               mul(mul(mul(mul(dist2, cam.pix_area), cos_c), cos_c), cos_c));
-                        splat(sums, (size_t)py * cam.W + px, vscale(vmul(beta, f), wgt), scale);
+                        splat(sums, (uint32_t)py * (uint32_t)cam.W + (uint32_t)px, vscale(vmul(beta, f), wgt), scale);
                     }
                 }
             }
@@ -222,17 +233,46 @@ __global__ void caustics_resolve_kernel(const unsigned long long *__restrict__ s
 
 }  // namespace pt
 
+namespace {
+
+using LtKernel = void (*)(PtScene, PtParams, unsigned long long, unsigned long long, uint64_t, double,
+                          unsigned long long *, unsigned long long *, unsigned long long *, uint32_t *);
+struct LtVariant {
+    int minb;
+    LtKernel world, inst;
+};
+const LtVariant kLtVariants[] = {
+    {4, pt::caustics_kernel<false, 4>, pt::caustics_kernel<true, 4>},
+    {5, pt::caustics_kernel<false, 5>, pt::caustics_kernel<true, 5>},
+    {6, pt::caustics_kernel<false, 6>, pt::caustics_kernel<true, 6>},
+    {7, pt::caustics_kernel<false, 7>, pt::caustics_kernel<true, 7>},
+    {8, pt::caustics_kernel<false, 8>, pt::caustics_kernel<true, 8>},
+    {10, pt::caustics_kernel<false, 10>, pt::caustics_kernel<true, 10>},
+};
+constexpr int kLtDefault = 4;   // the fastest on the plain render's caustics (1M light paths)
+
+}  // namespace
+
+int lt_variants() { return (int)(sizeof kLtVariants / sizeof kLtVariants[0]); }
+
 cudaError_t lt_trace(const PtScene &S, const PtParams &P, unsigned long long photons, uint64_t seed,
-                     unsigned long long *d_sums, unsigned long long *d_rays, uint32_t *d_status, int num_sms,
-                     cudaStream_t st) {
+                     unsigned long long *d_sums, unsigned long long *d_next, unsigned long long *d_rays,
+                     uint32_t *d_status, int num_sms, int variant, cudaStream_t st) {
     if (!photons) return cudaSuccess;
+    const LtVariant &V = kLtVariants[variant >= 0 && variant < lt_variants() ? variant : kLtDefault];
+    const LtKernel kern = S.ninst ? V.inst : V.world;
     const unsigned long long per = P.exact ? pt::LT_BATCH : 1ull;
     const unsigned long long streams = (photons + per - 1) / per;
-    // enough warps per SM to hide the traversal's latency; every thread a run of streams
-    const unsigned long long cap = (unsigned long long)std::max(num_sms, 1) * 8;
-    const unsigned blocks = (unsigned)std::min<unsigned long long>((streams + 127) / 128, cap);
+    // one wave of persistent blocks (as many as fit at once), fewer when there are few streams
+    int fit = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kern, 128, 0);
+    if (e) return e;
+    const unsigned long long wave = (unsigned long long)std::max(num_sms, 1) * std::max(fit, 1);
+    const unsigned blocks = (unsigned)std::min<unsigned long long>((streams + 127) / 128, wave);
     const double scale = 4294967296.0 / (double)photons;
-    pt::caustics_kernel<<<blocks, 128, 0, st>>>(S, P, photons, per, seed, scale, d_sums, d_rays, d_status);
+    e = cudaMemsetAsync(d_next, 0, 8, st);
+    if (e) return e;
+    kern<<<blocks, 128, 0, st>>>(S, P, photons, per, seed, scale, d_sums, d_next, d_rays, d_status);
     return cudaGetLastError();
 }
 
@@ -284,8 +324,8 @@ int lt_run(lrc_scene *s, const lrc_trace_params *p, uint64_t photons, uint64_t s
     if (!e) e = cudaMemsetAsync(s->d_rays, 0, 8, c->st);
     if (e) return cuda_status(c, e, "ray counter");
     c->timer.begin(LRC_TS_LIGHT, c->st);
-    e = lrc::lt_trace(pt_scene(s), lt_params(p), photons, seed, d_sums, rays ? s->d_rays : nullptr, c->d_status,
-                      c->num_sms, c->st);
+    e = lrc::lt_trace(pt_scene(s), lt_params(p), photons, seed, d_sums, s->d_rays + 1, rays ? s->d_rays : nullptr,
+                      c->d_status, c->num_sms, c->lt_variant, c->st);
     c->timer.end(c->st);
     return cuda_status(c, e, "light tracing");
 }
@@ -297,6 +337,12 @@ bool lt_valid(const lrc_scene *s, const lrc_trace_params *p, const void *out) {
 }  // namespace
 
 extern "C" {
+
+int lrc_caustics_variant(lrc_ctx *c, int variant) {
+    if (!c || variant >= lrc::lt_variants()) return LRC_E_INVALID;
+    c->lt_variant = variant < 0 ? -1 : variant;
+    return lrc::lt_variants();
+}
 
 int lrc_caustics(lrc_scene *s, const lrc_trace_params *p, uint64_t photons, uint64_t seed, float *image,
                  uint64_t *rays, unsigned flags) {

@@ -206,9 +206,12 @@ cudaError_t pt_intersect(const PtScene &S, const float *d_orig, const float *d_d
                          int32_t *d_prim, int32_t *d_inst, float *d_t, uint32_t *d_status, cudaStream_t st);
 // light tracing (caustics.cu): `photons` light paths (P's camera, image size, max_depth and exact
 // mode) whose 32.32 contributions are added into d_sums (W x H x 3); and image += sums / 2^32
+// (d_next: 8 bytes of scratch for the stream counter; variant: the launch's register cap, -1 the
+// default, lt_variants() of them)
 cudaError_t lt_trace(const PtScene &S, const PtParams &P, unsigned long long photons, uint64_t seed,
-                     unsigned long long *d_sums, unsigned long long *d_rays, uint32_t *d_status, int num_sms,
-                     cudaStream_t st);
+                     unsigned long long *d_sums, unsigned long long *d_next, unsigned long long *d_rays,
+                     uint32_t *d_status, int num_sms, int variant, cudaStream_t st);
+int lt_variants();
 cudaError_t lt_resolve(const unsigned long long *d_sums, float *d_image, size_t n, int num_sms, cudaStream_t st);
 cudaError_t pt_inst_boxes(const float *d_rec, uint32_t n, float *d_boxes, cudaStream_t st);
 

@@ -96,6 +96,7 @@ def lib():
     L.lrc_trace.argtypes = [vp, vp, C.c_int32, C.c_int32, u32, u32, vp, vp, C.c_uint]
     L.lrc_caustics.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
     L.lrc_caustics_sums.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
+    L.lrc_caustics_variant.argtypes = [vp, C.c_int]
     L.lrc_scene_set_meshes.argtypes = [vp, vp, vp, u32, C.c_uint]
     L.lrc_scene_set_instances.argtypes = [vp, vp, u32, C.c_uint]
     L.lrc_scene_build_instances.argtypes = [vp, C.c_int, C.c_int]
@@ -209,6 +210,13 @@ class Context:
 
     def set_stream(self, stream_ptr):
         self.check(self.L.lrc_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def caustics_variant(self, variant=-1):
+        """lrc_caustics_variant: the light tracer's launch variant; returns how many there are."""
+        n = self.L.lrc_caustics_variant(self.h, variant)
+        if n < 0:
+            raise ValueError(f"no light tracer variant {variant}")
+        return n
 
     def num_sms(self):
         return self.L.lrc_num_sms(self.h)
@@ -414,6 +422,10 @@ class Scene:
     def caustics_device(self, params, photons, seed, d_image):
         self.ctx.check(self.ctx.L.lrc_caustics(self.h, C.byref(params), photons, seed, C.c_void_p(d_image), None,
                                                LRC_DEVICE))
+
+    def caustics_sums_device(self, params, photons, seed, d_sums):
+        self.ctx.check(self.ctx.L.lrc_caustics_sums(self.h, C.byref(params), photons, seed, C.c_void_p(d_sums), None,
+                                                    LRC_DEVICE))
 
     def caustics_sums(self, params, photons, seed, sums=None):
         """lrc_caustics_sums with host sums: returns (sums (h, w, 3) uint64 += the 32.32 values, rays)."""
