@@ -21,6 +21,13 @@ x 16 spp = 1M light paths per step, lrc_caustics_sums into device sums, fast mod
 (closest-hit + shadow rays) of the step; the reference's light_trace_caustics on this host's cores
 is the baseline.
 
+--workload denoise: the denoiser (prep + 5 a-trous passes) on a 1920x1080 image of the plain
+render's scene at 4 spp (guide + guided samples made once, outside the timed region). Mpixels/s;
+roofline against HBM with 232 algorithmic bytes per pixel (prep reads the 4 planes, 64 B, and
+writes 16; each pass reads its 8 + 8 B and writes 8; the last reads the albedo, 16, and writes
+the image, 16). The baseline is the numpy restatement of the filter (the reference's own runs only
+as WGSL) on a 480x270 crop.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload builder|batch] ...
   python bench.py --impl reference ...   the reference's own CPU path on this host's cores
 
@@ -45,6 +52,7 @@ METRIC = "Mrays/s (build + closest-hit pass over the builder workload)"
 METRIC_BATCH = "Mrays/s (256-scene batched launch: builds + path tracing, closest-hit + shadow rays)"
 METRIC_SERVE = "Mrays/s and p50/p99 job latency (served request stream, Poisson arrivals)"
 METRIC_RENDER = "Mrays/s (one image: closest-hit + shadow rays)"
+METRIC_DENOISE = "Mpixels/s (denoiser: prep + 5 a-trous passes, 1920x1080)"
 METRIC_CAUSTICS = "Mrays/s (light-traced caustics: closest-hit + shadow rays of the light paths)"
 
 
@@ -61,7 +69,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve", "render", "instanced",
-                                                                     "caustics"])
+                                                                     "caustics", "denoise"])
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
@@ -852,6 +860,92 @@ def run_caustics(a):
                       "gpu_launches": a.steps, "cpu_baseline": cpu}), flush=True)
 
 
+DENOISE_BYTES_PER_PIXEL = 80 + 5 * 24 + 16 + 16
+
+
+def run_denoise(a):
+    """--workload denoise: lrc_denoise (device arrays) on a 1080p image's planes; e2e: lrc_denoise
+    with host planes and image (copied in and out)."""
+    import torch
+    import little_renderer_b200 as L
+    from little_renderer_b200 import render as R, workloads as W
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    w, h, spp = 1920, 1080, 4
+    sc = W.cornell_spheres(width=w, height=h)
+    dev = torch.device("cuda", 0)
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    s = R.world_scene(ctx, sc, 1)
+    p = L.native.trace_params(W.camera(sc["camera"], w / h), w, h, sc["max_depth"], 1, 1, 0, 1)
+    planes = torch.zeros(4, h, w, 4, device=dev)
+    out = torch.zeros(h, w, 4, device=dev)
+    torch.cuda.synchronize()
+    s.guide_device(p, planes.data_ptr())
+    s.trace_guided_device(p, spp, planes.data_ptr())
+    ctx.sync()
+
+    def step():
+        ctx.denoise_device(w, h, planes.data_ptr(), out.data_ptr())
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.sync()
+    clk = Clocks(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    host_planes = planes.cpu().numpy()
+    n_e2e = max(1, min(a.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        img = ctx.denoise(host_planes)
+    e_ms = (time.perf_counter() - t0) * 1e3 / n_e2e
+    assert np.array_equal(img, out.cpu().numpy())
+    cpu = None
+    if not a.no_cpu:
+        from oracle import denoise_oracle as D
+        crop = np.ascontiguousarray(host_planes[:, h // 2 - 135:h // 2 + 135, w // 2 - 240:w // 2 + 240])
+        t0 = time.perf_counter()
+        runs = 0
+        while True:
+            D.denoise(crop)
+            runs += 1
+            if time.perf_counter() - t0 > 10.0:
+                break
+        t = time.perf_counter() - t0
+        cpu = {"value": runs * crop.shape[1] * crop.shape[2] / t / 1e6, "unit": "Mpixels/s", "cores": 1, "kind": "port",
+               "sample": f"{runs} runs of the numpy restatement on a 480x270 crop in {t:.1f} s"}
+    peak_gbs, peak_src = peaks()
+    gbs = DENOISE_BYTES_PER_PIXEL * w * h / (ms / 1e3) / 1e9
+    s.close()
+    ctx.close()
+    print(json.dumps({"metric": METRIC_DENOISE, "value": w * h / (ms / 1e3) / 1e6, "unit": "Mpixels/s", "n_gpus": 1,
+                      "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f16 between passes)", "data": "synthetic",
+                      "config": {"workload": f"denoiser on the plain render's scene at {w}x{h}, {spp} spp (planes "
+                                             "made once), prep + 5 a-trous passes",
+                                 "l2": "the 33 MB of packed passes stay in L2 between passes (the workload's own)"},
+                      "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak_gbs, "unit": "GB/s",
+                                   "frac": gbs / peak_gbs, "traffic": None,
+                                   "algorithmic_bytes_per_pixel": DENOISE_BYTES_PER_PIXEL,
+                                   "peak_source": peak_src},
+                      "clocks": clocks,
+                      "e2e": {"value": w * h / (e_ms / 1e3) / 1e6, "unit": "Mpixels/s", "h2d_bytes_per_step": w * h * 64,
+                              "d2h_bytes_per_step": w * h * 16, "ms_per_step": e_ms},
+                      "gpu_launches": 6 * a.steps, "cpu_baseline": cpu}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -863,6 +957,10 @@ def main():
             run_reference_batch(a)
         elif a.workload == "caustics":
             run_reference_caustics(a)
+        elif a.workload == "denoise":
+            print(json.dumps({"impl": "reference", "metric": METRIC_DENOISE, "unavailable":
+                              "the reference's denoiser exists only as WGSL (denoise.wgsl), which cannot run on this "
+                              "box; its numpy restatement is the cpu_baseline leg of the ours line"}), flush=True)
         elif a.workload in ("render", "instanced"):
             print(json.dumps({"impl": "reference", "metric": METRIC_RENDER, "unavailable":
                               "this workload's CPU baseline is the cpu_baseline leg of the ours line"}), flush=True)
@@ -880,6 +978,9 @@ def main():
         return
     if a.workload == "caustics":
         run_caustics(a)
+        return
+    if a.workload == "denoise":
+        run_denoise(a)
         return
     import torch
     import little_renderer_b200 as L

@@ -61,6 +61,7 @@ int lrc_num_sms(const lrc_ctx *ctx);
 #define LRC_TS_TRACE 4       /* ray queries */
 #define LRC_TS_SHADE 5       /* path tracing */
 #define LRC_TS_LIGHT 6       /* light tracing (caustics) */
+#define LRC_TS_DENOISE 7     /* the denoiser's passes */
 #define LRC_NUM_STAGES 8
 int lrc_set_timing(lrc_ctx *ctx, int on);
 /* milliseconds of each stage (ms[LRC_NUM_STAGES]) and launches of each (optional) since the last
@@ -235,6 +236,24 @@ typedef struct {
  * first sample). rays (optional, host): the closest-hit and shadow rays traced. */
 int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0, uint32_t spp,
               float *accum, uint64_t *rays, unsigned flags);
+#define LRC_TRACE_GUIDED 64u  /* flag: accum is the denoiser's 4 planes (below); each sample's luminance
+                                 over the guide's albedo is added to plane 1's (sum l, sum l^2) */
+
+/* ---- the denoiser: replaces gpu_denoise_create / gpu_denoise_encode (engine/gpu/denoise_gpu.c;
+ * denoise.wgsl `prep`, `atrous`) and the guide pass `gbuf` (trace.wgsl:1045-1104, 1319-1337) ----
+ * Planes: 4 arrays of width x height float4 back to back, as the reference's path tracer keeps
+ * them: 0 the samples' sum and count (lrc_trace's accum), 1 the luminance moments, 2 the guide's
+ * normal and distance, 3 its albedo and kind (0 a rough surface, 1 a lamp / the sky / nothing,
+ * 2 a medium; + 4 (instance + 1)). A new image: planes 0 and 1 zeroed, lrc_guide, then lrc_trace
+ * with LRC_TRACE_GUIDED, then lrc_denoise whenever an image is wanted.
+ * lrc_guide: planes 2 and 3 from the ray through each pixel's centre to its first rough surface,
+ *   through mirrors and glass (the whole image; planes 0 and 1 are not touched).
+ * lrc_denoise: out (width x height float4: rgb, 1) = the edge-avoiding a-trous filter of the
+ *   planes, steered by each pixel's variance (passes 1-5, the hole sizes 1, 2, 4, 8, 16; other
+ *   values: 5). Arrays are host memory, or device memory with LRC_DEVICE. */
+int lrc_guide(lrc_scene *s, const lrc_trace_params *p, float *planes, unsigned flags);
+int lrc_denoise(lrc_ctx *ctx, int32_t width, int32_t height, const float *planes, int32_t passes, float *out,
+                unsigned flags);
 
 /* ---- light-traced caustics: replaces light_trace_caustics (engine/rt/tracer.c:553-665) and the
  * GPU backend's `ltrace` pass into its 64-bit caustic sums (gpu_trace_light, trace_gpu.c:1946-1954;

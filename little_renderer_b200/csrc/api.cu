@@ -125,6 +125,7 @@ void lrc_close(lrc_ctx *c) {
     cudaStreamSynchronize(c->st);
     if (c->scratch) cudaFree(c->scratch);
     if (c->stage) cudaFree(c->stage);
+    if (c->dn) cudaFree(c->dn);
     if (c->d_status) cudaFree(c->d_status);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -792,13 +793,20 @@ int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
     P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
     P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
     P.vertical = {p->vertical[0], p->vertical[1], p->vertical[2]};
-    const size_t bytes = (size_t)p->width * p->height * 16;
+    // LRC_TRACE_GUIDED: accum holds the denoiser's 4 planes; the moments go to plane 1
+    const bool guided = (flags & LRC_TRACE_GUIDED) != 0;
+    const size_t bytes = (size_t)p->width * p->height * (guided ? 64 : 16);
     float *d_acc = accum;
     if (!(flags & LRC_DEVICE)) {
         e = reserve(&c->stage, &c->stage_cap, bytes);
         if (e) return cuda_status(c, e, "image staging");
         d_acc = static_cast<float *>(c->stage);
         e = cudaMemcpyAsync(d_acc, accum, bytes, cudaMemcpyHostToDevice, c->st);
+    }
+    if (guided) {
+        const size_t N = (size_t)p->width * p->height;
+        P.moments = reinterpret_cast<float4 *>(d_acc) + N;
+        P.guide = reinterpret_cast<const float4 *>(d_acc) + 3 * N;
     }
     c->timer.begin(LRC_TS_SHADE, c->st);
     if (!e) e = lrc::pt_trace(pt_scene(s), P, d_acc, s->d_rays, c->d_status, c->st);

@@ -19,6 +19,8 @@ struct lrc_ctx {
     lrc::StageTimer timer;
     std::string msg;
     int lt_variant = -1;          // the light tracer's launch variant (-1: the default)
+    void *dn = nullptr;           // the denoiser's scratch (packed image ping-pong and guide)
+    size_t dn_cap = 0;
 };
 
 struct lrc_scene {

@@ -1,0 +1,391 @@
+// denoise.cu - the path tracer's denoiser on sm_100a: the guide pass (`guide` / `gbuf`,
+// engine/gpu/shaders/trace/trace.wgsl:1045-1104, 1319-1337) and the edge-avoiding a-trous filter
+// steered by each pixel's variance (engine/gpu/denoise_gpu.c; denoise.wgsl `prep`, `atrous`:
+// Dammertz et al. 2010 with SVGF's variance, Schied et al. 2017, without its temporal part).
+//
+// Planes (w x h float4 each, one array): 0 the samples' sum and count (lrc_trace's accum),
+// 1 the moments of each sample's luminance over the guide's albedo (sum l, sum l^2; lrc_trace
+// with LRC_TRACE_GUIDED adds them), 2 the guide's normal and distance, 3 its albedo and kind
+// (0 a rough surface, 1 a lamp / the sky / nothing, 2 a medium; + 4 (instance + 1)).
+//
+// The filter's passes read packed data, as the reference's do: 8 bytes of image per pixel
+// (irradiance and variance as four halves) and 8 of guide (the normal octahedron-encoded in two
+// snorm16, the distance as a float whose sign gives the kind) instead of 48. They are bound by
+// the latency of their 25 scattered taps (L1 / L2 hits at these image sizes); blocks are 32 x 8
+// pixel tiles so that a tile's taps share cache lines.
+
+#include "pt_device.cuh"
+#include <cuda_fp16.h>
+#include <algorithm>
+
+namespace lrc {
+namespace dn {
+
+using pt::V3;
+using pt::v3;
+
+// lowbias32 (util.wgsl hash32)
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+// Rec. 709 luminance (util.wgsl luma)
+__device__ __forceinline__ float luma(float r, float g, float b) { return 0.2126f * r + 0.7152f * g + 0.0722f * b; }
+__device__ __forceinline__ float gkind(float w) { return w - 4.0f * floorf(w * 0.25f); }
+
+// an image value: irradiance (each channel at most 6e4) and variance (< 0: no sample) as halves
+__device__ __forceinline__ uint32_t half2_bits(float a, float b) {
+    return (uint32_t)__half_as_ushort(__float2half_rn(a)) | ((uint32_t)__half_as_ushort(__float2half_rn(b)) << 16);
+}
+__device__ __forceinline__ uint2 put_iv(float r, float g, float b, float v) {
+    return make_uint2(half2_bits(fminf(r, 6e4f), fminf(g, 6e4f)), half2_bits(fminf(b, 6e4f), fminf(fmaxf(v, -1.0f), 6e4f)));
+}
+__device__ __forceinline__ float4 get_iv(uint2 p) {
+    return make_float4(__half2float(__ushort_as_half((unsigned short)(p.x & 0xffff))),
+                       __half2float(__ushort_as_half((unsigned short)(p.x >> 16))),
+                       __half2float(__ushort_as_half((unsigned short)(p.y & 0xffff))),
+                       __half2float(__ushort_as_half((unsigned short)(p.y >> 16))));
+}
+
+// the normal on an octahedron, two snorm16
+__device__ __forceinline__ uint32_t snorm16x2(float a, float b) {
+    int ia = __float2int_rn(fminf(fmaxf(a, -1.0f), 1.0f) * 32767.0f);
+    int ib = __float2int_rn(fminf(fmaxf(b, -1.0f), 1.0f) * 32767.0f);
+    return (uint32_t)(ia & 0xffff) | ((uint32_t)(ib & 0xffff) << 16);
+}
+__device__ __forceinline__ float2 unsnorm16x2(uint32_t p) {
+    float a = (float)(int16_t)(p & 0xffff), b = (float)(int16_t)(p >> 16);
+    return make_float2(fmaxf(a / 32767.0f, -1.0f), fmaxf(b / 32767.0f, -1.0f));
+}
+__device__ __forceinline__ uint32_t oct(float nx, float ny, float nz) {
+    const float s = fmaxf(fabsf(nx) + fabsf(ny) + fabsf(nz), 1e-6f);
+    float px = nx / s, py = ny / s;
+    if (nz < 0.0f) {
+        const float qx = (1.0f - fabsf(py)) * (px >= 0.0f ? 1.0f : -1.0f);
+        const float qy = (1.0f - fabsf(px)) * (py >= 0.0f ? 1.0f : -1.0f);
+        px = qx;
+        py = qy;
+    }
+    return snorm16x2(px, py);
+}
+__device__ __forceinline__ V3 unoct(float2 e) {
+    float x = e.x, y = e.y, z = 1.0f - fabsf(e.x) - fabsf(e.y);
+    const float t = fmaxf(-z, 0.0f);
+    x += x >= 0.0f ? -t : t;
+    y += y >= 0.0f ? -t : t;
+    const float l = sqrtf(x * x + y * y + z * z);
+    return v3(x / l, y / l, z / l);
+}
+struct G {
+    V3 n;
+    float z;
+    int kind;
+};
+__device__ __forceinline__ G get_g(uint2 p) {
+    G g;
+    const float e = __uint_as_float(p.y);
+    g.kind = e >= 0.0f ? 0 : (e < -1e37f ? 1 : 2);
+    g.z = e >= 0.0f ? e : -e - 1.0f;
+    g.n = unoct(unsnorm16x2(p.x));
+    return g;
+}
+
+// the mean of a pixel's samples over its guide's albedo (a surface), or the mean
+__device__ __forceinline__ V3 irradiance(const float4 *__restrict__ px, size_t N, size_t k) {
+    const float4 a = px[k], g = px[3 * N + k];
+    const float c = fmaxf(a.w, 1.0f);
+    V3 m = v3(a.x / c, a.y / c, a.z / c);
+    if (gkind(g.w) == 0.0f) m = v3(m.x / fmaxf(g.x, 1e-3f), m.y / fmaxf(g.y, 1e-3f), m.z / fmaxf(g.z, 1e-3f));
+    return m;
+}
+
+// prep: the packed guide, and each pixel's irradiance with the variance of its mean (its own
+// moments from 4 samples on, else the spread of its 7 x 7 neighbours on the same surface)
+__global__ void __launch_bounds__(256) prep_kernel(const float4 *__restrict__ px, int W, int H, uint2 *__restrict__ dst,
+                                                   uint2 *__restrict__ gd) {
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= W || y >= H) return;
+    const size_t N = (size_t)W * H, k = (size_t)y * W + x;
+    const float4 a = px[k], g = px[3 * N + k], n = px[2 * N + k];
+    const float gk = gkind(g.w);
+    const float e = gk == 0.0f ? n.w : (gk == 1.0f ? -2e38f : -(n.w + 1.0f));
+    gd[k] = make_uint2(oct(n.x, n.y, n.z), __float_as_uint(e));
+    if (a.w == 0.0f) {
+        dst[k] = put_iv(0.0f, 0.0f, 0.0f, -1.0f);
+        return;
+    }
+    const V3 irr = irradiance(px, N, k);
+    if (gk == 1.0f) {
+        dst[k] = put_iv(irr.x, irr.y, irr.z, 0.0f);
+        return;
+    }
+    float v;
+    if (a.w >= 4.0f) {
+        const float4 m = px[N + k];
+        const float el = m.x / a.w;
+        v = fmaxf(m.y / a.w - el * el, 0.0f) / a.w;
+    } else {
+        float s1 = 0.0f, s2 = 0.0f, c = 0.0f;
+        for (int dy = -3; dy <= 3; dy++)
+            for (int dx = -3; dx <= 3; dx++) {
+                const int qx = x + dx, qy = y + dy;
+                if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
+                const size_t q = (size_t)qy * W + qx;
+                if (px[q].w == 0.0f || gkind(px[3 * N + q].w) != gk) continue;
+                if (gk == 0.0f) {
+                    const float4 nq = px[2 * N + q];
+                    if (nq.x * n.x + nq.y * n.y + nq.z * n.z < 0.9f) continue;
+                }
+                const V3 iq = irradiance(px, N, q);
+                const float l = luma(iq.x, iq.y, iq.z);
+                s1 += l;
+                s2 += l * l;
+                c += 1.0f;
+            }
+        const float el = s1 / c;
+        v = fmaxf(s2 / c - el * el, 0.0f);
+    }
+    dst[k] = put_iv(irr.x, irr.y, irr.z, v);
+}
+
+// the B3 spline's weights 1/16, 1/4, 3/8, 1/4, 1/16
+__device__ __forceinline__ float b3(int i) { return i == 2 ? 0.375f : (i == 1 || i == 3 ? 0.25f : 0.0625f); }
+
+// One a-trous pass: a 5 x 5 B3 spline with holes `step` apart, each tap jittered within its hole
+// (but the centre), weighted by luminance (against the noise of the noisier of the two), normal
+// (cos^128) and distance (against how fast it changes here); the variance filtered with the
+// squared weights. The last pass writes the image (times the albedo on surfaces).
+__global__ void __launch_bounds__(256) atrous_kernel(const float4 *__restrict__ px, int W, int H, int step, int last,
+                                                     float sigma_l, float sigma_z, const uint2 *__restrict__ src,
+                                                     uint2 *__restrict__ dst, const uint2 *__restrict__ gd,
+                                                     float4 *__restrict__ outp) {
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= W || y >= H) return;
+    const size_t N = (size_t)W * H, k = (size_t)y * W + x;
+    const float4 c = get_iv(src[k]);
+    const G gp = get_g(gd[k]);
+    if (c.w < 0.0f || gp.kind == 1) {                // no sample yet; a lamp, the sky: as they are
+        if (last) outp[k] = c.w < 0.0f ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : make_float4(c.x, c.y, c.z, 1.0f);
+        else dst[k] = src[k];
+        return;
+    }
+    // the variance blurred 3 x 3
+    float v = 0.0f, vw = 0.0f;
+    for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+            const int qx = min(max(x + dx, 0), W - 1), qy = min(max(y + dy, 0), H - 1);
+            const float4 s = get_iv(src[(size_t)qy * W + qx]);
+            if (s.w < 0.0f) continue;
+            const float w = (dx != 0 ? 0.25f : 0.5f) * (dy != 0 ? 0.25f : 0.5f);
+            v += w * s.w;
+            vw += w;
+        }
+    v /= fmaxf(vw, 1e-6f);
+    const float lp = luma(c.x, c.y, c.z);
+    const bool surface = gp.kind == 0;
+    // how fast the distance changes per pixel here (the smaller side)
+    float gx = 0.0f, gy = 0.0f;
+    if (surface) {
+        const float l = get_g(gd[(size_t)y * W + max(x - 1, 0)]).z, r = get_g(gd[(size_t)y * W + min(x + 1, W - 1)]).z;
+        const float d = get_g(gd[(size_t)max(y - 1, 0) * W + x]).z, u = get_g(gd[(size_t)min(y + 1, H - 1) * W + x]).z;
+        gx = fminf(fabsf(gp.z - l), fabsf(gp.z - r));
+        gy = fminf(fabsf(gp.z - d), fabsf(gp.z - u));
+    }
+    uint32_t seed = hash32(((uint32_t)k * 0x9e3779b9u) ^ ((uint32_t)step * 0x85ebca6bu));
+    const int jit = step / 2;
+    const uint32_t jn = (uint32_t)(2 * jit + 1);
+    float sr = 0.0f, sg = 0.0f, sb = 0.0f, vsum = 0.0f, wsum = 0.0f;
+#pragma unroll 1
+    for (int j = 0; j < 5; j++) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            int ox = (i - 2) * step, oy = (j - 2) * step;
+            if (jit > 0 && (i != 2 || j != 2)) {
+                seed = hash32(seed);
+                ox += (int)(((seed & 0xffffu) * jn) >> 16) - jit;
+                oy += (int)(((seed >> 16) * jn) >> 16) - jit;
+            }
+            const int qx = x + ox, qy = y + oy;
+            if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
+            const size_t q = (size_t)qy * W + qx;
+            const float4 s = get_iv(src[q]);
+            float w = b3(i) * b3(j);
+            if (q != k) {
+                const G gq = get_g(gd[q]);
+                if (s.w < 0.0f || gq.kind != gp.kind) continue;
+                w *= __expf(-fabsf(lp - luma(s.x, s.y, s.z)) / (sigma_l * sqrtf(fmaxf(v, s.w)) + 1e-6f));
+                if (surface) {
+                    float wn = fmaxf(gp.n.x * gq.n.x + gp.n.y * gq.n.y + gp.n.z * gq.n.z, 0.0f);
+#pragma unroll
+                    for (int e = 0; e < 7; e++) wn *= wn;   // cos^128
+                    w *= wn;
+                    const float expect = gx * fabsf((float)ox) + gy * fabsf((float)oy);
+                    w *= __expf(-fabsf(gp.z - gq.z) / (sigma_z * expect + 1e-3f * gp.z + 1e-6f));
+                }
+            }
+            sr += w * s.x;
+            sg += w * s.y;
+            sb += w * s.z;
+            vsum += w * w * s.w;
+            wsum += w;
+        }
+    }
+    const float o0 = sr / wsum, o1 = sg / wsum, o2 = sb / wsum;
+    if (last) {
+        const float4 al = px[3 * N + k];
+        outp[k] = surface ? make_float4(o0 * al.x, o1 * al.y, o2 * al.z, 1.0f) : make_float4(o0, o1, o2, 1.0f);
+    } else {
+        dst[k] = put_iv(o0, o1, o2, vsum / (wsum * wsum));
+    }
+}
+
+// ---- the guide: the ray through the pixel's centre to the first rough surface, through mirrors
+// and glass (refracting unless the glass reflects all), with the albedo of the whole way ------
+__global__ void __launch_bounds__(128) guide_kernel(PtScene S, PtParams P, float4 *__restrict__ planes,
+                                                    uint32_t *err) {
+    using namespace pt;
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t N = (size_t)P.W * P.H;
+    if (idx >= N) return;
+    const uint32_t x = idx % P.W, y = idx / P.W;
+    const V3 pc = vsub(vadd(P.upper_left, vscale(P.horizontal, (x + 0.5f) / (float)P.W)),
+                       vscale(P.vertical, (y + 0.5f) / (float)P.H));
+    V3 ro = P.origin, rd = vnorm(vsub(pc, P.origin));
+    V3 gn = v3(0, 0, 0), ga = v3(1, 1, 1), a = v3(1, 1, 1);
+    float gz = 1e30f, dist = 0.0f, kind = 1.0f;
+    int ginst = -1;
+    for (int i = 0; i < 6; i++) {
+        Hit h;
+        if (!scene_intersect(S, ro, rd, RT_EPS, 1e30f, h, err)) break;
+        const Mat m = load_mat(S.mats, hit_material(S, h) & 63);
+        // a lamp, or a surface glowing at least as bright as white paper under a light of 1
+        if (m.type == MAT_LIGHT || fmaxf(m.emission.x, fmaxf(m.emission.y, m.emission.z)) >= 1.0f) {
+            gn = h.n;
+            gz = dist + h.t;
+            ginst = h.inst;
+            break;
+        }
+        Bsdf b = bsdf_make(m, h.front, S.tab);
+        if (bsdf_rough_part(b)) {                    // a surface the light scatters on
+            gn = h.n;
+            gz = dist + h.t;
+            ga = v3(a.x * m.albedo.x, a.y * m.albedo.y, a.z * m.albedo.z);
+            kind = 0.0f;
+            ginst = h.inst;
+            break;
+        }
+        a = v3(a.x * m.albedo.x, a.y * m.albedo.y, a.z * m.albedo.z);
+        dist += h.t;
+        V3 nxt = vreflect(rd, h.n);
+        if (b.transmission > 0.5f && b.metallic < 0.5f) {
+            const float cos_i = fminf(-vdot(rd, h.n), 1.0f);
+            if (b.eta * b.eta * (1.0f - cos_i * cos_i) <= 1.0f) nxt = vrefract(rd, h.n, b.eta);
+        }
+        ro = h.p;
+        rd = vnorm(nxt);
+    }
+    const float w = kind + 4.0f * (float)(ginst >= 0 ? ((uint32_t)ginst & 0x3fffffu) + 1u : 0u);
+    planes[2 * N + idx] = make_float4(gn.x, gn.y, gn.z, gz);
+    planes[3 * N + idx] = make_float4(ga.x, ga.y, ga.z, w);
+}
+
+}  // namespace dn
+
+cudaError_t dn_guide(const PtScene &S, const PtParams &P, float4 *d_planes, uint32_t *d_status, cudaStream_t st) {
+    const size_t N = (size_t)P.W * P.H;
+    if (!N) return cudaSuccess;
+    dn::guide_kernel<<<(unsigned)((N + 127) / 128), 128, 0, st>>>(S, P, d_planes, d_status);
+    return cudaGetLastError();
+}
+
+size_t dn_scratch_bytes(int W, int H) { return 3 * (size_t)W * H * 8 + 512; }
+
+cudaError_t dn_denoise(const float4 *d_planes, int W, int H, int passes, float4 *d_out, void *scratch,
+                       cudaStream_t st) {
+    const size_t N = (size_t)W * H;
+    if (!N) return cudaSuccess;
+    uint2 *a = static_cast<uint2 *>(scratch), *b = a + N, *gd = b + N;
+    const dim3 grid((unsigned)((W + 31) / 32), (unsigned)((H + 7) / 8));
+    dn::prep_kernel<<<grid, 256, 0, st>>>(d_planes, W, H, a, gd);
+    // a -> b, b -> a, ...; the last pass into out
+    for (int i = 1; i <= passes; i++) {
+        const uint2 *in = i % 2 ? a : b;
+        uint2 *to = i % 2 ? b : a;
+        dn::atrous_kernel<<<grid, 256, 0, st>>>(d_planes, W, H, 1 << (i - 1), i == passes, 4.0f, 1.0f, in, to, gd, d_out);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace lrc
+
+// ---- the C ABI ------------------------------------------------------------------------------
+#include "api_internal.cuh"
+
+using namespace lrcapi;
+
+extern "C" {
+
+int lrc_guide(lrc_scene *s, const lrc_trace_params *p, float *planes, unsigned flags) {
+    if (!s || !p || !planes || p->width <= 0 || p->height <= 0) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    if (!s->built_n && !s->tlas_n) return fail(c, LRC_E_INVALID, "the scene has nothing built (lrc_scene_build)");
+    if (s->ninst && s->tlas_n != s->ninst) return fail(c, LRC_E_INVALID, "instances changed: lrc_scene_build_instances");
+    if (!s->d_mats || !s->nmats) return fail(c, LRC_E_INVALID, "the scene has no materials (lrc_scene_set_materials)");
+    DeviceGuard g(c->device);
+    if (!s->tables) {
+        int rc = lrc_scene_set_tables(s, nullptr, nullptr);
+        if (rc) return rc;
+    }
+    const size_t N = (size_t)p->width * p->height;
+    lrc::PtParams P{};
+    P.W = p->width; P.H = p->height; P.rows = p->height;
+    P.origin = {p->origin[0], p->origin[1], p->origin[2]};
+    P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
+    P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
+    P.vertical = {p->vertical[0], p->vertical[1], p->vertical[2]};
+    float4 *d_planes = reinterpret_cast<float4 *>(planes);
+    cudaError_t e = cudaSuccess;
+    if (!(flags & LRC_DEVICE)) {                     // (planes 2 and 3 are written: only they travel)
+        e = reserve(&c->stage, &c->stage_cap, N * 64);
+        d_planes = static_cast<float4 *>(c->stage);
+    }
+    c->timer.begin(LRC_TS_SHADE, c->st);
+    if (!e) e = lrc::dn_guide(pt_scene(s), P, d_planes, c->d_status, c->st);
+    c->timer.end(c->st);
+    if (!e && !(flags & LRC_DEVICE))
+        e = cudaMemcpyAsync(planes + 8 * N, d_planes + 2 * N, N * 32, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_guide");
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_denoise(lrc_ctx *c, int32_t width, int32_t height, const float *planes, int32_t passes, float *out,
+                unsigned flags) {
+    if (!c || !planes || !out || width <= 0 || height <= 0) return LRC_E_INVALID;
+    if (passes < 1 || passes > 5) passes = 5;
+    DeviceGuard g(c->device);
+    const size_t N = (size_t)width * height;
+    cudaError_t e = reserve(&c->dn, &c->dn_cap, lrc::dn_scratch_bytes(width, height));
+    if (e) return cuda_status(c, e, "denoiser scratch");
+    const float4 *d_planes = reinterpret_cast<const float4 *>(planes);
+    float4 *d_out = reinterpret_cast<float4 *>(out);
+    if (!(flags & LRC_DEVICE)) {
+        e = reserve(&c->stage, &c->stage_cap, N * 80);
+        if (e) return cuda_status(c, e, "image staging");
+        float4 *st = static_cast<float4 *>(c->stage);
+        d_planes = st;
+        d_out = st + 4 * N;
+        e = cudaMemcpyAsync(st, planes, N * 64, cudaMemcpyHostToDevice, c->st);
+    }
+    c->timer.begin(LRC_TS_DENOISE, c->st);
+    if (!e) e = lrc::dn_denoise(d_planes, width, height, passes, d_out, c->dn, c->st);
+    c->timer.end(c->st);
+    if (!e && !(flags & LRC_DEVICE)) e = cudaMemcpyAsync(out, d_out, N * 16, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_denoise");
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+}  // extern "C"

@@ -198,6 +198,10 @@ struct PtParams {
     float clamp;
     pt::V3 origin, upper_left, horizontal, vertical;   // the Camera (camera.h)
     int skip_caustics;                                 // TraceParams.skip_caustics
+    // the denoiser's planes (lrc_trace with LRC_TRACE_GUIDED; null: none): each sample's luminance
+    // over the guide's albedo (plane 3) added to the moments (plane 1) as (l, l^2)
+    float4 *moments;
+    const float4 *guide;
 };
 cudaError_t pt_prim_boxes(const float *d_prims, uint32_t n, float *d_boxes, cudaStream_t st);
 cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsigned long long *d_rays, uint32_t *d_status,
@@ -213,6 +217,12 @@ cudaError_t lt_trace(const PtScene &S, const PtParams &P, unsigned long long pho
                      uint32_t *d_status, int num_sms, int variant, cudaStream_t st);
 int lt_variants();
 cudaError_t lt_resolve(const unsigned long long *d_sums, float *d_image, size_t n, int num_sms, cudaStream_t st);
+// the denoiser (denoise.cu): the guide planes 2 and 3 of an image (W x H: P's whole image), and
+// the denoised image from planes 0-3 (passes a-trous passes; scratch of dn_scratch_bytes)
+cudaError_t dn_guide(const PtScene &S, const PtParams &P, float4 *d_planes, uint32_t *d_status, cudaStream_t st);
+size_t dn_scratch_bytes(int W, int H);
+cudaError_t dn_denoise(const float4 *d_planes, int W, int H, int passes, float4 *d_out, void *scratch,
+                       cudaStream_t st);
 cudaError_t pt_inst_boxes(const float *d_rec, uint32_t n, float *d_boxes, cudaStream_t st);
 
 // One job of a batch: a band of one image of one scene. Its tasks are (pixel, lane slot) pairs,

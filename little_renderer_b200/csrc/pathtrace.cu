@@ -23,6 +23,14 @@
 namespace lrc {
 namespace pt {
 
+// a sample's luminance for the denoiser's moments: over the guide's albedo on a rough surface
+// (kind 0), else as it is (trace.wgsl:1300-1305)
+__device__ __forceinline__ float sample_luma(V3 c, float4 ga) {
+    const float kind = ga.w - 4.0f * floorf(ga.w * 0.25f);
+    if (kind == 0.0f) c = v3(c.x / fmaxf(ga.x, 1e-3f), c.y / fmaxf(ga.y, 1e-3f), c.z / fmaxf(ga.z, 1e-3f));
+    return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
+}
+
 // exact mode: one thread per pixel of rows [y0, y0 + rows), samples [0, spp) in order from the
 // CPU's per-pixel stream (trace_image, tracer.c:337-353)
 __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float4 *accum, unsigned long long *ray_count,
@@ -36,6 +44,8 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
         Rng rng;
         rng_seed(rng, 0x853c49e6748fea9bull ^ (pixel * 0x9E3779B97F4A7C15ull) ^ (P.seed * 0xD1B54A32D192ED03ull), pixel);
         V3 sum = v3(0, 0, 0);
+        float ml = 0.0f, ml2 = 0.0f;
+        const float4 ga = P.moments ? P.guide[pixel] : make_float4(1, 1, 1, 1);
         for (int k = 0; k < P.spp; k++) {
             Sampler sm{&rng, (uint32_t)k, (uint32_t)P.seed * 0x9e3779b9u, (int)x, (int)y, P.sampler_on, S.mask};
             float jx, jy;
@@ -47,9 +57,18 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
             if (!is_number(c)) continue;
             c = clamp_sample(c, P.clamp);
             sum = vadd(sum, c);
+            if (P.moments) {
+                const float l = sample_luma(c, ga);
+                ml += l;
+                ml2 += l * l;
+            }
         }
         float4 a = accum[pixel];
         accum[pixel] = make_float4(a.x + sum.x, a.y + sum.y, a.z + sum.z, a.w + (float)P.spp);
+        if (P.moments) {
+            const float4 m = P.moments[pixel];
+            P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, m.z, m.w);
+        }
     }
     if (ray_count) {
         unsigned long long r = rays;
@@ -70,12 +89,13 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
     const uint64_t npix = (uint64_t)P.W * P.rows;
     uint32_t rays = 0;
     V3 c = v3(0, 0, 0);
-    float cnt = 0.0f;
+    float cnt = 0.0f, ml = 0.0f, ml2 = 0.0f;
     const bool live = pix_local < npix;
     uint64_t pixel = 0;
     if (live) {
         const uint32_t x = (uint32_t)(pix_local % P.W), y = P.y0 + (uint32_t)(pix_local / P.W);
         pixel = (uint64_t)y * P.W + x;
+        const float4 ga = P.moments ? P.guide[pixel] : make_float4(1, 1, 1, 1);
         for (uint32_t k = lane_s; k < (uint32_t)P.spp; k += g) {
             const uint32_t kk = P.spp0 + k;
             Rng rng;
@@ -90,6 +110,11 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
             s = is_number(s) ? clamp_sample(s, P.clamp) : v3(0, 0, 0);
             c = vadd(c, s);
             cnt += 1.0f;
+            if (P.moments) {
+                const float l = sample_luma(s, ga);
+                ml += l;
+                ml2 += l * l;
+            }
         }
     }
     for (uint32_t o = 1; o < g; o <<= 1) {               // fixed-order tree sum over the group
@@ -97,10 +122,18 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
         c.y += __shfl_down_sync(0xffffffffu, c.y, o, g);
         c.z += __shfl_down_sync(0xffffffffu, c.z, o, g);
         cnt += __shfl_down_sync(0xffffffffu, cnt, o, g);
+        if (P.moments) {
+            ml += __shfl_down_sync(0xffffffffu, ml, o, g);
+            ml2 += __shfl_down_sync(0xffffffffu, ml2, o, g);
+        }
     }
     if (live && lane_s == 0) {
         float4 a = accum[pixel];
         accum[pixel] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + cnt);
+        if (P.moments) {
+            const float4 m = P.moments[pixel];
+            P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, m.z, m.w);
+        }
     }
     if (ray_count) {
         unsigned long long r = rays;

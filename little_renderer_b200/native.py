@@ -13,12 +13,13 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
 LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
 LRC_DEVICE = 1
+LRC_TRACE_GUIDED = 64
 LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED = 4, 8, 16, 32
 
 
@@ -97,6 +98,8 @@ def lib():
     L.lrc_caustics.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
     L.lrc_caustics_sums.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
     L.lrc_caustics_variant.argtypes = [vp, C.c_int]
+    L.lrc_guide.argtypes = [vp, vp, vp, C.c_uint]
+    L.lrc_denoise.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp, C.c_uint]
     L.lrc_scene_set_meshes.argtypes = [vp, vp, vp, u32, C.c_uint]
     L.lrc_scene_set_instances.argtypes = [vp, vp, u32, C.c_uint]
     L.lrc_scene_build_instances.argtypes = [vp, C.c_int, C.c_int]
@@ -210,6 +213,18 @@ class Context:
 
     def set_stream(self, stream_ptr):
         self.check(self.L.lrc_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def denoise(self, planes, passes=5):
+        """lrc_denoise with host arrays: planes (4, h, w, 4) -> the denoised image (h, w, 4)."""
+        planes = np.ascontiguousarray(planes, np.float32)
+        h, w = planes.shape[1:3]
+        out = np.zeros((h, w, 4), np.float32)
+        self.check(self.L.lrc_denoise(self.h, w, h, _ptr(planes), passes, _ptr(out), 0))
+        return out
+
+    def denoise_device(self, width, height, d_planes, d_out, passes=5):
+        self.check(self.L.lrc_denoise(self.h, width, height, C.c_void_p(d_planes), passes, C.c_void_p(d_out),
+                                      LRC_DEVICE))
 
     def caustics_variant(self, variant=-1):
         """lrc_caustics_variant: the light tracer's launch variant; returns how many there are."""
@@ -409,6 +424,28 @@ class Scene:
         rows = params.height if rows is None else rows
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), y0, rows, spp0, spp, C.c_void_p(d_accum), None,
                                             LRC_DEVICE))
+
+    def guide(self, params, planes=None):
+        """lrc_guide with host planes (4, h, w, 4): planes 2 and 3 written; returns the planes."""
+        if planes is None:
+            planes = np.zeros((4, params.height, params.width, 4), np.float32)
+        self.ctx.check(self.ctx.L.lrc_guide(self.h, C.byref(params), _ptr(planes), 0))
+        return planes
+
+    def guide_device(self, params, d_planes):
+        self.ctx.check(self.ctx.L.lrc_guide(self.h, C.byref(params), C.c_void_p(d_planes), LRC_DEVICE))
+
+    def trace_guided(self, params, spp, planes, spp0=0):
+        """lrc_trace with LRC_TRACE_GUIDED on host planes (4, h, w, 4): samples into plane 0, the
+        luminance moments into plane 1; returns (planes, rays)."""
+        rays = C.c_uint64()
+        self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), 0, params.height, spp0, spp, _ptr(planes),
+                                            C.byref(rays), LRC_TRACE_GUIDED))
+        return planes, rays.value
+
+    def trace_guided_device(self, params, spp, d_planes, spp0=0):
+        self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), 0, params.height, spp0, spp, C.c_void_p(d_planes),
+                                            None, LRC_TRACE_GUIDED | LRC_DEVICE))
 
     def caustics(self, params, photons, seed, image=None):
         """lrc_caustics with a host image: returns (image (h, w, 3) += the caustic image of `photons`

@@ -193,6 +193,7 @@ def ref_lib(double=False):
         lib.rb_occluded.argtypes = [vp, _f32p, _f32p, C.c_longlong, C.c_float, C.c_float, _i32p]
         lib.rb_trace_image.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        lib.rb_guide.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, _f32p, _f32p]
         lib.rb_light_trace_caustics.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_longlong, C.c_int,
                                                 C.c_ulonglong, _f32p]
         lib.rb_rays.argtypes = [_i64p]
@@ -357,6 +358,14 @@ class RefScene:
         cnt = np.zeros(2, np.int64)
         self.lib.rb_rays(cnt)
         return out, (int(cnt[0]), int(cnt[1]))
+
+    def guide(self, cam, vfov, w, h):
+        """The denoiser's guide planes 2 and 3 ((h, w, 4) each) restated on this scene."""
+        n4 = np.zeros((h, w, 4), np.float32)
+        a4 = np.zeros((h, w, 4), np.float32)
+        self.lib.rb_guide(self.s, np.ascontiguousarray(cam, np.float32).reshape(-1), vfov, w, h, n4.reshape(-1),
+                          a4.reshape(-1))
+        return n4, a4
 
     def light_trace_caustics(self, cam, vfov, w, h, photons, max_depth, seed):
         """light_trace_caustics (tracer.c:553-665): the (h, w, 3) caustic image of `photons` light

@@ -6,6 +6,8 @@
 //   any hit      scene_occluded    (engine/rt/accel.c:280)
 //   image        trace_image       (engine/rt/tracer.c:329)
 //   caustics     light_trace_caustics (engine/rt/tracer.c:553)
+//   guide        the denoiser's guide of the GPU path tracer (trace.wgsl guide(): it has no CPU
+//                counterpart), restated here on the reference's Scene, scene_intersect and BSDF
 //   boxes        triangle_bounds   (engine/scene/scene.c:65)
 // and counts the tracer's rays through link-time --wrap of scene_intersect/scene_occluded
 // (no edit of the reference). Nothing of the product path calls this file.
@@ -18,6 +20,8 @@
 #include "rt/accel.h"
 #include "rt/bvh.h"
 #include "rt/tracer.h"
+#include "rt/intersect.h"
+#include "scene/brdf.h"
 #include "base/sampler.h"
 #include "scene/brdf_tables.h"
 
@@ -295,6 +299,55 @@ void rb_light_trace_caustics(const void *sp, const float *cam, float vfov, int w
         rgb[3 * i] += (float)px[i].x; rgb[3 * i + 1] += (float)px[i].y; rgb[3 * i + 2] += (float)px[i].z;
     }
     free(px);
+}
+
+// The denoiser's guide (trace.wgsl:1045-1104 without media; gbuf's ray through the pixel centre,
+// trace.wgsl:1330-1332): per pixel, through mirrors and glass (refracting unless the glass reflects
+// all), the first rough surface's normal and distance (n4: x y z, distance) and the albedo of the
+// way with the kind (a4: r g b, kind + 4 (instance + 1); kind 0 a rough surface, 1 a lamp, a bright
+// glow or nothing). bsdf_rough_part is tracer.c:258's (static there).
+#ifdef LR_DOUBLE
+#define RB_EPS 1e-4
+#else
+#define RB_EPS 2e-3
+#endif
+void rb_guide(const void *sp, const float *cam, float vfov, int w, int h, float *n4, float *a4){
+    const Scene *s = sp;
+    Camera c = camera_make(v3f(cam), v3f(cam + 3), v3f(cam + 6), vfov, (real)w / (real)h);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int k = 0; k < w * h; k++){
+        const int x = k % w, y = k / w;
+        Vec3 pc = v_sub(v_add(c.upper_left, v_scale(c.horizontal, (x + 0.5f) / (real)w)),
+                        v_scale(c.vertical, (y + 0.5f) / (real)h));
+        Ray ray = {c.origin, v_norm(v_sub(pc, c.origin))};
+        Vec3 gn = vec3(0, 0, 0), ga = vec3(1, 1, 1), a = vec3(1, 1, 1);
+        real gz = 1e30, dist = 0, kind = 1;
+        int ginst = -1;
+        for (int i = 0; i < 6; i++){
+            Hit hit;
+            if (!scene_intersect(s, &ray, RB_EPS, 1e30, &hit)) break;
+            const Material *m = &s->mats[hit_material(s, &hit)];
+            if (m->type == MAT_LIGHT || v_max(m->emission) >= 1){ gn = hit.n; gz = dist + hit.t; ginst = hit.inst; break; }
+            Bsdf b = bsdf_make(m, hit.front_face);
+            if (!b.smooth || (1 - b.metallic) * (1 - b.transmission) > 0){
+                gn = hit.n; gz = dist + hit.t; ga = v_mul(a, m->albedo); kind = 0; ginst = hit.inst;
+                break;
+            }
+            a = v_mul(a, m->albedo);
+            dist += hit.t;
+            Vec3 nxt = v_reflect(ray.d, hit.n);
+            if (b.transmission > 0.5 && b.metallic < 0.5){
+                real cos_i = r_fmin(-v_dot(ray.d, hit.n), 1);
+                if (b.eta * b.eta * (1 - cos_i * cos_i) <= 1) nxt = v_refract(ray.d, hit.n, b.eta);
+            }
+            ray.o = hit.p;
+            ray.d = v_norm(nxt);
+        }
+        float *n = n4 + 4 * (size_t)k, *al = a4 + 4 * (size_t)k;
+        n[0] = (float)gn.x; n[1] = (float)gn.y; n[2] = (float)gn.z; n[3] = (float)gz;
+        al[0] = (float)ga.x; al[1] = (float)ga.y; al[2] = (float)ga.z;
+        al[3] = (float)kind + 4.0f * (float)(ginst >= 0 ? (unsigned)ginst + 1u : 0u);
+    }
 }
 
 // the BSDF's tables (scene/brdf_tables.h) packed as the GPU backend packs them (brdf_gpu.c:20-25)
