@@ -8,11 +8,12 @@
 // with LRC_TRACE_GUIDED adds them), 2 the guide's normal and distance, 3 its albedo and kind
 // (0 a rough surface, 1 a lamp / the sky / nothing, 2 a medium; + 4 (instance + 1)).
 //
-// The filter's passes read packed data, as the reference's do: 8 bytes of image per pixel
-// (irradiance and variance as four halves) and 8 of guide (the normal octahedron-encoded in two
-// snorm16, the distance as a float whose sign gives the kind) instead of 48. They are bound by
-// the latency of their 25 scattered taps (L1 / L2 hits at these image sizes); blocks are 32 x 8
-// pixel tiles so that a tile's taps share cache lines.
+// The filter's passes pass the image packed, as the reference's do: 8 bytes per pixel
+// (irradiance and variance as four halves). The guide's normal goes through the reference's
+// octahedral snorm16 code once, in prep, and the passes read it decoded (16 bytes: the normal and
+// the distance, whose sign gives the kind): the taps are L1 / L2 hits at these image sizes and
+// the passes are bound by instructions, not bytes, so decoding once beats reading half as much.
+// Blocks are 32 x 8 pixel tiles so that a tile's taps share cache lines.
 
 #include "pt_device.cuh"
 #include <cuda_fp16.h>
@@ -85,12 +86,15 @@ struct G {
     float z;
     int kind;
 };
-__device__ __forceinline__ G get_g(uint2 p) {
+// The guide as the passes read it: the normal as its octahedral code decodes (unoct(oct(n)), the
+// values the reference's packed guide gives), decoded once by prep instead of at every tap; w the
+// distance with the kind in its sign (kind 0: z, kind 2: -(z + 1), kind 1: -2e38)
+__device__ __forceinline__ G get_g(float4 p) {
     G g;
-    const float e = __uint_as_float(p.y);
+    const float e = p.w;
     g.kind = e >= 0.0f ? 0 : (e < -1e37f ? 1 : 2);
     g.z = e >= 0.0f ? e : -e - 1.0f;
-    g.n = unoct(unsnorm16x2(p.x));
+    g.n = v3(p.x, p.y, p.z);
     return g;
 }
 
@@ -106,14 +110,15 @@ __device__ __forceinline__ V3 irradiance(const float4 *__restrict__ px, size_t N
 // prep: the packed guide, and each pixel's irradiance with the variance of its mean (its own
 // moments from 4 samples on, else the spread of its 7 x 7 neighbours on the same surface)
 __global__ void __launch_bounds__(256) prep_kernel(const float4 *__restrict__ px, int W, int H, uint2 *__restrict__ dst,
-                                                   uint2 *__restrict__ gd) {
+                                                   float4 *__restrict__ gd) {
     const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
     if (x >= W || y >= H) return;
     const size_t N = (size_t)W * H, k = (size_t)y * W + x;
     const float4 a = px[k], g = px[3 * N + k], n = px[2 * N + k];
     const float gk = gkind(g.w);
     const float e = gk == 0.0f ? n.w : (gk == 1.0f ? -2e38f : -(n.w + 1.0f));
-    gd[k] = make_uint2(oct(n.x, n.y, n.z), __float_as_uint(e));
+    const V3 nd = unoct(unsnorm16x2(oct(n.x, n.y, n.z)));
+    gd[k] = make_float4(nd.x, nd.y, nd.z, e);
     if (a.w == 0.0f) {
         dst[k] = put_iv(0.0f, 0.0f, 0.0f, -1.0f);
         return;
@@ -161,11 +166,11 @@ __device__ __forceinline__ float b3(int i) { return i == 2 ? 0.375f : (i == 1 ||
 // squared weights. The last pass writes the image (times the albedo on surfaces).
 __global__ void __launch_bounds__(256) atrous_kernel(const float4 *__restrict__ px, int W, int H, int step, int last,
                                                      float sigma_l, float sigma_z, const uint2 *__restrict__ src,
-                                                     uint2 *__restrict__ dst, const uint2 *__restrict__ gd,
+                                                     uint2 *__restrict__ dst, const float4 *__restrict__ gd,
                                                      float4 *__restrict__ outp) {
     const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
     if (x >= W || y >= H) return;
-    const size_t N = (size_t)W * H, k = (size_t)y * W + x;
+    const uint32_t N = (uint32_t)W * (uint32_t)H, k = (uint32_t)y * W + x;
     const float4 c = get_iv(src[k]);
     const G gp = get_g(gd[k]);
     if (c.w < 0.0f || gp.kind == 1) {                // no sample yet; a lamp, the sky: as they are
@@ -178,7 +183,7 @@ __global__ void __launch_bounds__(256) atrous_kernel(const float4 *__restrict__ 
     for (int dy = -1; dy <= 1; dy++)
         for (int dx = -1; dx <= 1; dx++) {
             const int qx = min(max(x + dx, 0), W - 1), qy = min(max(y + dy, 0), H - 1);
-            const float4 s = get_iv(src[(size_t)qy * W + qx]);
+            const float4 s = get_iv(src[(uint32_t)qy * W + qx]);
             if (s.w < 0.0f) continue;
             const float w = (dx != 0 ? 0.25f : 0.5f) * (dy != 0 ? 0.25f : 0.5f);
             v += w * s.w;
@@ -190,12 +195,12 @@ __global__ void __launch_bounds__(256) atrous_kernel(const float4 *__restrict__ 
     // how fast the distance changes per pixel here (the smaller side)
     float gx = 0.0f, gy = 0.0f;
     if (surface) {
-        const float l = get_g(gd[(size_t)y * W + max(x - 1, 0)]).z, r = get_g(gd[(size_t)y * W + min(x + 1, W - 1)]).z;
-        const float d = get_g(gd[(size_t)max(y - 1, 0) * W + x]).z, u = get_g(gd[(size_t)min(y + 1, H - 1) * W + x]).z;
+        const float l = get_g(gd[(uint32_t)y * W + max(x - 1, 0)]).z, r = get_g(gd[(uint32_t)y * W + min(x + 1, W - 1)]).z;
+        const float d = get_g(gd[(uint32_t)max(y - 1, 0) * W + x]).z, u = get_g(gd[(uint32_t)min(y + 1, H - 1) * W + x]).z;
         gx = fminf(fabsf(gp.z - l), fabsf(gp.z - r));
         gy = fminf(fabsf(gp.z - d), fabsf(gp.z - u));
     }
-    uint32_t seed = hash32(((uint32_t)k * 0x9e3779b9u) ^ ((uint32_t)step * 0x85ebca6bu));
+    uint32_t seed = hash32((k * 0x9e3779b9u) ^ ((uint32_t)step * 0x85ebca6bu));
     const int jit = step / 2;
     const uint32_t jn = (uint32_t)(2 * jit + 1);
     float sr = 0.0f, sg = 0.0f, sb = 0.0f, vsum = 0.0f, wsum = 0.0f;
@@ -211,20 +216,20 @@ __global__ void __launch_bounds__(256) atrous_kernel(const float4 *__restrict__ 
             }
             const int qx = x + ox, qy = y + oy;
             if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
-            const size_t q = (size_t)qy * W + qx;
+            const uint32_t q = (uint32_t)qy * W + qx;
             const float4 s = get_iv(src[q]);
             float w = b3(i) * b3(j);
             if (q != k) {
                 const G gq = get_g(gd[q]);
                 if (s.w < 0.0f || gq.kind != gp.kind) continue;
-                w *= __expf(-fabsf(lp - luma(s.x, s.y, s.z)) / (sigma_l * sqrtf(fmaxf(v, s.w)) + 1e-6f));
+                w *= __expf(__fdividef(-fabsf(lp - luma(s.x, s.y, s.z)), sigma_l * sqrtf(fmaxf(v, s.w)) + 1e-6f));
                 if (surface) {
                     float wn = fmaxf(gp.n.x * gq.n.x + gp.n.y * gq.n.y + gp.n.z * gq.n.z, 0.0f);
 #pragma unroll
                     for (int e = 0; e < 7; e++) wn *= wn;   // cos^128
                     w *= wn;
                     const float expect = gx * fabsf((float)ox) + gy * fabsf((float)oy);
-                    w *= __expf(-fabsf(gp.z - gq.z) / (sigma_z * expect + 1e-3f * gp.z + 1e-6f));
+                    w *= __expf(__fdividef(-fabsf(gp.z - gq.z), sigma_z * expect + 1e-3f * gp.z + 1e-6f));
                 }
             }
             sr += w * s.x;
@@ -236,7 +241,7 @@ __global__ void __launch_bounds__(256) atrous_kernel(const float4 *__restrict__ 
     }
     const float o0 = sr / wsum, o1 = sg / wsum, o2 = sb / wsum;
     if (last) {
-        const float4 al = px[3 * N + k];
+        const float4 al = px[3 * (size_t)N + k];
         outp[k] = surface ? make_float4(o0 * al.x, o1 * al.y, o2 * al.z, 1.0f) : make_float4(o0, o1, o2, 1.0f);
     } else {
         dst[k] = put_iv(o0, o1, o2, vsum / (wsum * wsum));
@@ -302,13 +307,14 @@ cudaError_t dn_guide(const PtScene &S, const PtParams &P, float4 *d_planes, uint
     return cudaGetLastError();
 }
 
-size_t dn_scratch_bytes(int W, int H) { return 3 * (size_t)W * H * 8 + 512; }
+size_t dn_scratch_bytes(int W, int H) { return 4 * (size_t)W * H * 8 + 512; }
 
 cudaError_t dn_denoise(const float4 *d_planes, int W, int H, int passes, float4 *d_out, void *scratch,
                        cudaStream_t st) {
     const size_t N = (size_t)W * H;
     if (!N) return cudaSuccess;
-    uint2 *a = static_cast<uint2 *>(scratch), *b = a + N, *gd = b + N;
+    uint2 *a = static_cast<uint2 *>(scratch), *b = a + N;
+    float4 *gd = reinterpret_cast<float4 *>(b + N);
     const dim3 grid((unsigned)((W + 31) / 32), (unsigned)((H + 7) / 8));
     dn::prep_kernel<<<grid, 256, 0, st>>>(d_planes, W, H, a, gd);
     // a -> b, b -> a, ...; the last pass into out
@@ -365,6 +371,7 @@ int lrc_guide(lrc_scene *s, const lrc_trace_params *p, float *planes, unsigned f
 int lrc_denoise(lrc_ctx *c, int32_t width, int32_t height, const float *planes, int32_t passes, float *out,
                 unsigned flags) {
     if (!c || !planes || !out || width <= 0 || height <= 0) return LRC_E_INVALID;
+    if ((uint64_t)width * (uint64_t)height >= (1ull << 31)) return fail(c, LRC_E_INVALID, "image too large (2^31 pixels)");
     if (passes < 1 || passes > 5) passes = 5;
     DeviceGuard g(c->device);
     const size_t N = (size_t)width * height;

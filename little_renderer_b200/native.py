@@ -214,11 +214,12 @@ class Context:
     def set_stream(self, stream_ptr):
         self.check(self.L.lrc_set_stream(self.h, C.c_void_p(stream_ptr)))
 
-    def denoise(self, planes, passes=5):
+    def denoise(self, planes, passes=5, out=None):
         """lrc_denoise with host arrays: planes (4, h, w, 4) -> the denoised image (h, w, 4)."""
         planes = np.ascontiguousarray(planes, np.float32)
         h, w = planes.shape[1:3]
-        out = np.zeros((h, w, 4), np.float32)
+        if out is None:
+            out = np.zeros((h, w, 4), np.float32)
         self.check(self.L.lrc_denoise(self.h, w, h, _ptr(planes), passes, _ptr(out), 0))
         return out
 
