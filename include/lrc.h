@@ -302,6 +302,11 @@ void lrc_batch_destroy(lrc_batch *b);
  * scenes: -1). A scene in several jobs is built once, by its first job's builder. */
 int lrc_batch_add(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
                   uint32_t spp, float *d_accum, int32_t builder, int32_t key_bits);
+/* The same with the denoiser's 4 planes (device; the guide made by lrc_guide): lrc_trace with
+ * LRC_TRACE_GUIDED as part of the batch (the moments added as the plain call adds them, to the
+ * bit; LRC_BATCH_ZERO clears the band's planes 0 and 1). */
+int lrc_batch_add_guided(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
+                         uint32_t spp0, uint32_t spp, float *d_planes, int32_t builder, int32_t key_bits);
 int lrc_batch_clear(lrc_batch *b);
 int lrc_batch_jobs(const lrc_batch *b);
 /* Enqueues the run on the context's stream (lrc_sync or lrc_batch_rays wait for it). */
@@ -348,7 +353,11 @@ void lrc_server_destroy(lrc_server *sv);
  * x 32 floats as lrc_scene_set_instances's; n = the scene's instance count) moves its instances for
  * this job only: the job gets its own copy of the instance layer, its top level refit
  * (LRC_TLAS_REFIT) or built again (LRC_TLAS_REBUILD) on the device when admitted; NULL: the scene
- * as it is. A job larger than the whole budget: LRC_E_TOO_BIG. */
+ * as it is. tlas_mode | LRC_SERVE_DENOISE: the job is traced with the denoiser's planes (lrc_guide
+ * at admission, the moments with its samples) and its result is lrc_denoise's image (rgb, 1); it
+ * holds 80 bytes a pixel while traced, 16 once done. A job larger than the whole budget:
+ * LRC_E_TOO_BIG. */
+#define LRC_SERVE_DENOISE 16
 int lrc_server_submit(lrc_server *sv, lrc_scene *s, const lrc_trace_params *p, uint32_t spp, const float *records,
                       uint32_t n, int tlas_mode, uint64_t *id);
 /* One wave: admission, the next band of every admitted job traced in one batch run, waited for;

@@ -219,7 +219,7 @@ struct InstView {
 };
 // lrc_batch_add (no build) with the job's own instances (a server's moving-instance job)
 int batch_add_view(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
-                   uint32_t spp, float *d_accum, const InstView &view);
+                   uint32_t spp, float *d_accum, const InstView &view, bool guided);
 cudaError_t build_tlas_on(lrc_ctx *c, const float *d_inst, uint32_t n, Node *d_nodes, uint32_t *d_aux, float *d_boxes,
                           uint32_t *d_small, void *scratch, size_t scratch_cap, cudaStream_t st, lrc::StageTimer *timer);
 

@@ -36,6 +36,7 @@ struct lrc_batch {
         float *accum;
         int32_t builder, key_bits;
         InstView view;                    // the job's own instances (moved), or none: the scene's
+        bool guided = false;              // accum holds the denoiser's 4 planes (moments added)
     };
     lrc_ctx *ctx = nullptr;
     std::vector<Job> jobs;
@@ -89,6 +90,11 @@ lrc::PtParams params_of(const lrc_batch::Job &J) {
     P.seed = p->seed;
     P.clamp = p->clamp;
     P.skip_caustics = p->skip_caustics != 0;
+    if (J.guided) {
+        const size_t N = (size_t)p->width * p->height;
+        P.moments = reinterpret_cast<float4 *>(J.accum) + N;
+        P.guide = reinterpret_cast<const float4 *>(J.accum) + 3 * N;
+    }
     P.origin = {p->origin[0], p->origin[1], p->origin[2]};
     P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
     P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
@@ -137,6 +143,7 @@ std::vector<unsigned char> signature(const lrc_batch *b, unsigned flags) {
         const void *ptrs[2] = {J.s, J.accum};
         put(ptrs, sizeof ptrs);
         put(&J.p, offsetof(lrc_trace_params, skip_caustics) + sizeof(int32_t));
+        put(&J.guided, sizeof J.guided);
         const int32_t w[6] = {J.y0, J.rows, (int32_t)J.spp0, (int32_t)J.spp, J.builder, J.key_bits};
         put(w, sizeof w);
     }
@@ -210,7 +217,7 @@ int prepare(lrc_batch *b) {
     }
     b->ntasks = task;
     b->npix = pix;
-    cudaError_t e = reserve(&b->d_part, &b->part_cap, al(task * 16) + al(task * 4) + 256);
+    cudaError_t e = reserve(&b->d_part, &b->part_cap, al(task * 16) + al(task * 4) + al(task * 8) + 256);
     if (!e) e = reserve(reinterpret_cast<void **>(&b->d_ctr), &b->ctr_cap, (nj + 1) * 8 + 256);
     if (!e) e = reserve(reinterpret_cast<void **>(&b->d_jobs), &b->jobs_cap, nj * sizeof(lrc::BatchJob) + 256);
     if (!e && b->engine == 1) e = reserve(&b->d_wf, &b->wf_cap, lrc::wf_bytes(b->wf_slots));
@@ -219,10 +226,12 @@ int prepare(lrc_batch *b) {
     char *part = static_cast<char *>(b->d_part);
     float4 *partial = reinterpret_cast<float4 *>(part);
     uint32_t *prays = reinterpret_cast<uint32_t *>(part + al(task * 16));
+    float2 *pmom = reinterpret_cast<float2 *>(part + al(task * 16) + al(task * 4));
     for (size_t q = 0; q < nj; q++) {
         lrc::BatchJob &T = b->table[q];
         T.partial = partial + T.task0;
         T.prays = prays + T.task0;
+        T.pmom = T.P.moments ? pmom + T.task0 : nullptr;
         T.rays = b->d_ctr + 1 + b->order[q];
     }
     e = cudaMemcpyAsync(b->d_jobs, b->table.data(), nj * sizeof(lrc::BatchJob), cudaMemcpyHostToDevice, c->st);
@@ -277,6 +286,9 @@ int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool 
         for (size_t i = 0; i < nj && !e; i++) {
             const lrc_batch::Job &J = b->jobs[i];
             e = cudaMemsetAsync(J.accum + (size_t)J.y0 * J.p.width * 4, 0, (size_t)J.rows * J.p.width * 16, st);
+            if (!e && J.guided)                      // the band's moments (plane 1) too
+                e = cudaMemsetAsync(J.accum + ((size_t)J.p.width * J.p.height + (size_t)J.y0 * J.p.width) * 4, 0,
+                                    (size_t)J.rows * J.p.width * 16, st);
         }
     }
     if (!e && b->engine == 0)
@@ -410,11 +422,15 @@ void note_built(lrc_batch *b) {   // (what captured builds' host side records)
 
 namespace lrcapi {
 int batch_add_view(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
-                   uint32_t spp, float *d_accum, const InstView &view) {
+                   uint32_t spp, float *d_accum, const InstView &view, bool guided) {
     int rc = lrc_batch_add(b, s, p, y0, rows, spp0, spp, d_accum, -1, 30);
     if (rc) return rc;
-    if (view.inst && !s->tlas_n) return fail(b->ctx, LRC_E_INVALID, "own instances for a scene without instances");
+    if (view.inst && !s->tlas_n) {
+        b->jobs.pop_back();
+        return fail(b->ctx, LRC_E_INVALID, "own instances for a scene without instances");
+    }
     b->jobs.back().view = view;
+    b->jobs.back().guided = guided;
     return LRC_OK;
 }
 }  // namespace lrcapi
@@ -459,6 +475,14 @@ int lrc_batch_add(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t
     if (s->ninst && builder >= 0) return fail(c, LRC_E_INVALID, "instanced scenes are built by lrc_scene_build_instances");
     b->jobs.push_back({s, *p, y0, rows, spp0, spp, d_accum, builder, key_bits, InstView{}});
     b->prepared = false;
+    return LRC_OK;
+}
+
+int lrc_batch_add_guided(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
+                         uint32_t spp0, uint32_t spp, float *d_planes, int32_t builder, int32_t key_bits) {
+    int rc = lrc_batch_add(b, s, p, y0, rows, spp0, spp, d_planes, builder, key_bits);
+    if (rc) return rc;
+    b->jobs.back().guided = true;
     return LRC_OK;
 }
 

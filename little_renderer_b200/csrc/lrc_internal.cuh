@@ -238,6 +238,7 @@ struct BatchJob {
     unsigned long long pix0;            // its first pixel among all the batch's bands (resolve pass)
     float4 *partial;                    // ntasks (sum rgb, samples)
     uint32_t *prays;                    // ntasks ray counts
+    float2 *pmom;                       // ntasks luminance moments (a guided job: P.moments), or null
     float4 *accum;                      // the image (W x H)
     unsigned long long *rays;           // the job's ray count (added to)
 };
@@ -263,6 +264,7 @@ struct WfState {
     uint32_t *flags;            // F_PATH, F_ENDED and the Nee flags of the bounce just shaded
     uint2 *xy;                  // the task's pixel
     float4 *sum;                // the task's sum so far (rgb, samples)
+    float2 *mom;                // its luminance moments so far (guided jobs)
     float4 *ro;                 // the path's ray origin, bounce_pdf
     float4 *rd;                 // its direction, depth | emit << 16 | caus << 24 (int bits)
     float4 *thr;                // its throughput

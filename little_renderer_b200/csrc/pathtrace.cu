@@ -23,14 +23,6 @@
 namespace lrc {
 namespace pt {
 
-// a sample's luminance for the denoiser's moments: over the guide's albedo on a rough surface
-// (kind 0), else as it is (trace.wgsl:1300-1305)
-__device__ __forceinline__ float sample_luma(V3 c, float4 ga) {
-    const float kind = ga.w - 4.0f * floorf(ga.w * 0.25f);
-    if (kind == 0.0f) c = v3(c.x / fmaxf(ga.x, 1e-3f), c.y / fmaxf(ga.y, 1e-3f), c.z / fmaxf(ga.z, 1e-3f));
-    return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
-}
-
 // exact mode: one thread per pixel of rows [y0, y0 + rows), samples [0, spp) in order from the
 // CPU's per-pixel stream (trace_image, tracer.c:337-353)
 __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float4 *accum, unsigned long long *ray_count,
@@ -160,7 +152,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
     uint64_t pixel = 0;               // the pixel's index in its image
     uint32_t x = 0, y = 0, slot = 0, kk = 0, kend = 0, g = 1, rays = 0;
     V3 c = v3(0, 0, 0);
-    float cnt = 0.0f;
+    float cnt = 0.0f, ml = 0.0f, ml2 = 0.0f;   // the task's sum, samples, luminance moments
     bool active = false, done = false;
     PathState ps;
     Rng rng;
@@ -172,6 +164,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
             const unsigned long long l = task - J.task0;
             J.partial[l] = make_float4(c.x, c.y, c.z, cnt);
             J.prays[l] = rays;
+            if (J.pmom) J.pmom[l] = make_float2(ml, ml2);
             j = -1;
         }
         const bool need = !done && j < 0;
@@ -199,6 +192,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
                     kend = (uint32_t)(J.P.spp0 + J.P.spp);
                     c = v3(0, 0, 0);
                     cnt = 0.0f;
+                    ml = ml2 = 0.0f;
                     rays = 0;
                     if (J.P.exact)                    // trace_image's per-pixel stream, all samples in order
                         rng_seed(rng, 0x853c49e6748fea9bull ^ (pixel * 0x9E3779B97F4A7C15ull) ^ (J.P.seed * 0xD1B54A32D192ED03ull),
@@ -225,6 +219,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
             V3 s = is_number(ps.radiance) ? clamp_sample(ps.radiance, J.P.clamp) : v3(0, 0, 0);
             c = vadd(c, s);
             cnt += 1.0f;
+            if (J.P.moments) {
+                const float l = sample_luma(s, J.P.guide[pixel]);
+                ml += l;
+                ml2 += l * l;
+            }
             active = false;
             kk += g;
         }
@@ -265,9 +264,23 @@ __global__ void __launch_bounds__(128) batch_resolve_kernel(const BatchJob *__re
                     v[s].w += v[s + o].w;
                 }
         const uint32_t x = (uint32_t)(pl % (uint32_t)J.P.W), y = (uint32_t)J.P.y0 + (uint32_t)(pl / (uint32_t)J.P.W);
-        float4 *a = J.accum + (uint64_t)y * (uint32_t)J.P.W + x;
+        const uint64_t pixel = (uint64_t)y * (uint32_t)J.P.W + x;
+        float4 *a = J.accum + pixel;
         float4 av = *a;
         *a = make_float4(av.x + v[0].x, av.y + v[0].y, av.z + v[0].z, av.w + v[0].w);
+        if (J.pmom) {                                // the moments, in the same order
+            float2 mv[16];
+            for (uint32_t s = 0; s < 16; s++)
+                if (s < g) mv[s] = J.pmom[pl * g + s];
+            for (uint32_t o = 1; o < 16; o <<= 1)
+                for (uint32_t s = 0; s + o < 16; s += 2 * o)
+                    if (s + o < g) {
+                        mv[s].x += mv[s + o].x;
+                        mv[s].y += mv[s + o].y;
+                    }
+            const float4 m = J.P.moments[pixel];
+            J.P.moments[pixel] = make_float4(m.x + mv[0].x, m.y + mv[0].y, m.z, m.w);
+        }
     }
     // the rays of the warp's pixels, one atomic per job present
     const uint32_t peers = __match_any_sync(0xffffffffu, jj);

@@ -681,6 +681,14 @@ __device__ __forceinline__ void camera_ray(const PtParams &P, float s, float t, 
     d = vnorm(vsub(target, P.origin));
 }
 
+// a sample's luminance for the denoiser's moments: over the guide's albedo on a rough surface
+// (kind 0), else as it is (trace.wgsl:1300-1305)
+__device__ __forceinline__ float sample_luma(V3 c, float4 ga) {
+    const float kind = ga.w - 4.0f * floorf(ga.w * 0.25f);
+    if (kind == 0.0f) c = v3(c.x / fmaxf(ga.x, 1e-3f), c.y / fmaxf(ga.y, 1e-3f), c.z / fmaxf(ga.z, 1e-3f));
+    return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
+}
+
 __device__ __forceinline__ bool is_number(V3 c) { return c.x == c.x && c.y == c.y && c.z == c.z; }
 
 __device__ __forceinline__ V3 clamp_sample(V3 c, float clamp) {

@@ -14,7 +14,10 @@
 // against the budget, in arrival order; a job larger than the whole budget is refused at submit.
 // A moved-instance job gets its own copy of the scene's instance layer (records and top level, the
 // meshes' trees shared), its top level refit (bvh_refit_boxes's bottom-up refit) or built again on
-// the device when admitted, so jobs of the same scene at different frames run side by side.
+// the device when admitted, so jobs of the same scene at different frames run side by side. A
+// denoised job (the step after the path tracer for low-spp jobs) holds the denoiser's 4 planes
+// while it is traced: the guide made at admission, the moments added by its waves, the a-trous
+// passes run when its last band is done and the planes freed.
 #include "api_internal.cuh"
 #include <algorithm>
 #include <chrono>
@@ -33,7 +36,9 @@ struct lrc_server {
         uint32_t spp = 0;
         std::vector<float> records;     // moved instances (32 floats each), or none
         int tlas_mode = 0;
-        float *d_img = nullptr;         // W x H float4 (sum, count)
+        bool denoise = false;           // traced with the denoiser's planes, denoised when done
+        float *d_img = nullptr;         // W x H float4 (sum, count); denoised: (rgb, 1)
+        float *d_planes = nullptr;      // a denoised job's 4 planes while it is traced
         float *d_inst = nullptr;        // the job's instance records
         Node *d_tlas = nullptr;         // and their top level
         uint32_t *d_tlas_aux = nullptr;
@@ -57,6 +62,8 @@ struct lrc_server {
     float *d_boxes = nullptr;
     size_t boxes_cap = 0;
     uint32_t *d_small = nullptr;
+    void *dn = nullptr;                 // the denoiser's scratch
+    size_t dn_cap = 0;
 };
 
 namespace {
@@ -67,7 +74,7 @@ double now_ms() {
 }
 
 size_t job_bytes(const lrc_server::Job &J) {
-    size_t b = (size_t)J.p.width * J.p.height * 16;
+    size_t b = (size_t)J.p.width * J.p.height * (J.denoise ? 80 : 16);   // (denoised: planes + image)
     const size_t n = J.records.size() / 32;
     if (n) b += n * 128 + (2 * n - 1) * 32 + n * 4;
     return b;
@@ -76,13 +83,26 @@ size_t job_bytes(const lrc_server::Job &J) {
 void free_job(lrc_server *sv, lrc_server::Job *J) {
     lrc_ctx *c = sv->ctx;
     if (J->d_img) cudaFreeAsync(J->d_img, c->st);
+    if (J->d_planes) cudaFreeAsync(J->d_planes, c->st);
     if (J->d_inst) cudaFreeAsync(J->d_inst, c->st);
     if (J->d_tlas) cudaFreeAsync(J->d_tlas, c->st);
     if (J->d_tlas_aux) cudaFreeAsync(J->d_tlas_aux, c->st);
     J->d_img = nullptr;
+    J->d_planes = nullptr;
     J->d_inst = nullptr;
     J->d_tlas = nullptr;
     J->d_tlas_aux = nullptr;
+}
+
+// the path tracer's view of a job's scene: its own instance layer, if it has one
+lrc::PtScene job_view(const lrc_server::Job *J) {
+    lrc::PtScene S = pt_scene(J->s);
+    if (J->d_inst) {
+        S.inst = reinterpret_cast<const float4 *>(J->d_inst);
+        S.tlas_nodes = reinterpret_cast<const float4 *>(J->d_tlas);
+        S.tlas_aux = J->d_tlas_aux;
+    }
+    return S;
 }
 
 // the job's device memory: its image (cleared) and, for moved instances, its records and top level
@@ -90,7 +110,7 @@ int admit(lrc_server *sv, lrc_server::Job *J) {
     lrc_ctx *c = sv->ctx;
     const size_t img = (size_t)J->p.width * J->p.height * 16;
     cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&J->d_img), img, c->st);
-    if (!e) e = cudaMemsetAsync(J->d_img, 0, img, c->st);
+    if (!e && !J->denoise) e = cudaMemsetAsync(J->d_img, 0, img, c->st);
     const uint32_t n = (uint32_t)(J->records.size() / 32);
     if (!e && n) {
         lrc_scene *s = J->s;
@@ -110,6 +130,20 @@ int admit(lrc_server *sv, lrc_server::Job *J) {
             if (!e) e = reserve(&sv->scratch, &sv->scratch_cap, lrc::refit_scratch_bytes(n));
             if (!e) e = lrc::refit_device(J->d_tlas, J->d_tlas_aux, n, 0, J->d_inst, 8, 6, sv->scratch, sv->scratch_cap,
                                           c->d_status, c->st);
+        }
+    }
+    if (!e && J->denoise) {                          // the planes: samples and moments cleared, the guide
+        const size_t N = (size_t)J->p.width * J->p.height;
+        e = cudaMallocAsync(reinterpret_cast<void **>(&J->d_planes), N * 64, c->st);
+        if (!e) e = cudaMemsetAsync(J->d_planes, 0, N * 32, c->st);
+        if (!e) {
+            lrc::PtParams P{};
+            P.W = J->p.width; P.H = J->p.height; P.rows = J->p.height;
+            P.origin = {J->p.origin[0], J->p.origin[1], J->p.origin[2]};
+            P.upper_left = {J->p.upper_left[0], J->p.upper_left[1], J->p.upper_left[2]};
+            P.horizontal = {J->p.horizontal[0], J->p.horizontal[1], J->p.horizontal[2]};
+            P.vertical = {J->p.vertical[0], J->p.vertical[1], J->p.vertical[2]};
+            e = lrc::dn_guide(job_view(J), P, reinterpret_cast<float4 *>(J->d_planes), c->d_status, c->st);
         }
     }
     if (e) {
@@ -161,6 +195,7 @@ void lrc_server_destroy(lrc_server *sv) {
     cudaFree(sv->scratch);
     cudaFree(sv->d_boxes);
     cudaFree(sv->d_small);
+    cudaFree(sv->dn);
     delete sv;
 }
 
@@ -171,6 +206,9 @@ int lrc_server_submit(lrc_server *sv, lrc_scene *s, const lrc_trace_params *p, u
     if (p->width <= 0 || p->height <= 0 || spp == 0 || spp >= (1u << 31))
         return fail(c, LRC_E_INVALID, "a job is a whole image with spp >= 1");
     if (p->exact) return fail(c, LRC_E_INVALID, "served jobs trace in fast mode");
+    const bool denoise = (tlas_mode & LRC_SERVE_DENOISE) != 0;
+    tlas_mode &= ~LRC_SERVE_DENOISE;
+    if (denoise && (uint64_t)p->width * p->height >= (1ull << 31)) return fail(c, LRC_E_INVALID, "image too large to denoise");
     if (n && (n != s->ninst || !s->tlas_n)) return fail(c, LRC_E_INVALID, "moved instances: the scene's instances, built");
     if (n && (tlas_mode < LRC_TLAS_REFIT || tlas_mode > LRC_TLAS_REBUILD))
         return fail(c, LRC_E_INVALID, "a job's top level is refit or rebuilt");
@@ -182,6 +220,7 @@ int lrc_server_submit(lrc_server *sv, lrc_scene *s, const lrc_trace_params *p, u
     J->spp = spp;
     if (n) J->records.assign(records, records + (size_t)n * 32);
     J->tlas_mode = tlas_mode;
+    J->denoise = denoise;
     J->bytes = job_bytes(*J);
     if (J->bytes > sv->budget) {
         delete J;
@@ -217,7 +256,8 @@ int lrc_server_step(lrc_server *sv, int32_t *finished) {
         rows = std::min(rows, J->p.height - J->next_row);
         J->band = rows;
         InstView v{J->d_inst, J->d_tlas, J->d_tlas_aux};
-        if (!rc) rc = batch_add_view(sv->batch, J->s, &J->p, J->next_row, rows, 0, J->spp, J->d_img, v);
+        if (!rc) rc = batch_add_view(sv->batch, J->s, &J->p, J->next_row, rows, 0, J->spp,
+                                     J->denoise ? J->d_planes : J->d_img, v, J->denoise);
     }
     if (!rc) rc = lrc_batch_run(sv->batch, 0);
     std::vector<uint64_t> rays(sv->active.size());
@@ -230,6 +270,16 @@ int lrc_server_step(lrc_server *sv, int32_t *finished) {
         J->rays += rays[i];
         J->next_row += J->band;
         if (J->next_row >= J->p.height) {
+            if (J->denoise) {                           // the image denoised, the planes freed
+                cudaError_t e = reserve(&sv->dn, &sv->dn_cap, lrc::dn_scratch_bytes(J->p.width, J->p.height));
+                if (!e) e = lrc::dn_denoise(reinterpret_cast<const float4 *>(J->d_planes), J->p.width, J->p.height, 5,
+                                            reinterpret_cast<float4 *>(J->d_img), sv->dn, c->st);
+                if (!e) e = cudaFreeAsync(J->d_planes, c->st);
+                if (e) return cuda_status(c, e, "server denoiser");
+                J->d_planes = nullptr;
+                sv->in_use -= (size_t)J->p.width * J->p.height * 64;
+                J->bytes -= (size_t)J->p.width * J->p.height * 64;
+            }
             J->state = 2;
             J->t_done = t;
             sv->finished++;

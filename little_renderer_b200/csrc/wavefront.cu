@@ -66,11 +66,13 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
     int j = task != NO_TASK ? (int)W.job[i] : -1;
     uint32_t kk = 0, trays = 0;
     float4 sum = make_float4(0, 0, 0, 0);
+    float2 mom = make_float2(0, 0);
     bool path = (f0 & F_PATH) != 0, new_task = false, wrote_sum = false;
     if (j >= 0) {
         kk = W.kk[i];
         trays = W.trays[i];
         sum = W.sum[i];
+        if (jobs[j].pmom) mom = W.mom[i];
     }
     if (path) {
         const BatchJob &J = jobs[j];
@@ -85,6 +87,11 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
             const V3 s = is_number(rad) ? clamp_sample(rad, J.P.clamp) : v3(0, 0, 0);
             const V3 c = vadd(v3(sum.x, sum.y, sum.z), s);
             sum = make_float4(c.x, c.y, c.z, sum.w + 1.0f);
+            if (J.pmom) {                            // the denoiser's moments
+                const uint2 xy = W.xy[i];
+                const float l = sample_luma(s, J.P.guide[(uint64_t)xy.y * (uint32_t)J.P.W + xy.x]);
+                mom = make_float2(mom.x + l, mom.y + l * l);
+            }
             wrote_sum = true;
             kk += (uint32_t)J.P.group;
             path = false;
@@ -98,6 +105,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
             const unsigned long long l = task - J.task0;
             J.partial[l] = sum;
             J.prays[l] = trays;
+            if (J.pmom) J.pmom[l] = mom;
             j = -1;
             task = NO_TASK;
             wrote_sum = false;
@@ -125,6 +133,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
                 W.xy[i] = make_uint2(x, y);
                 kk = (uint32_t)J.P.spp0 + slot;
                 sum = make_float4(0, 0, 0, 0);
+                mom = make_float2(0, 0);
                 trays = 0;
                 new_task = true;
                 wrote_sum = true;
@@ -176,7 +185,10 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
     if (j >= 0) {
         W.kk[i] = kk;
         W.trays[i] = trays;
-        if (wrote_sum) W.sum[i] = sum;
+        if (wrote_sum) {
+            W.sum[i] = sum;
+            if (jobs[j].pmom) W.mom[i] = mom;
+        }
     }
 }
 
@@ -369,7 +381,7 @@ WfState wf_carve(void *base, uint32_t M) {
     W.nvl = reinterpret_cast<float4 *>(take(m * 16));
     W.nve = reinterpret_cast<float4 *>(take(m * 16));
     W.rng = reinterpret_cast<ulonglong2 *>(take(m * 16));
-    take(m * 16);   // (spare)
+    W.mom = reinterpret_cast<float2 *>(take(m * 16));   // (8 of 16 bytes a slot used)
     W.vis = reinterpret_cast<uint8_t *>(take(m * 2));
     take(m * 4);    // (spare)
     W.sq_o = reinterpret_cast<float4 *>(take(m * 2 * 16));

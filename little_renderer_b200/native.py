@@ -20,6 +20,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
 LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
 LRC_DEVICE = 1
 LRC_TRACE_GUIDED = 64
+LRC_SERVE_DENOISE = 16
 LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED = 4, 8, 16, 32
 
 
@@ -111,6 +112,7 @@ def lib():
     L.lrc_batch_create.argtypes = [vp, C.POINTER(vp)]
     L.lrc_batch_destroy.argtypes = [vp]
     L.lrc_batch_add.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, u32, u32, vp, C.c_int32, C.c_int32]
+    L.lrc_batch_add_guided.argtypes = [vp, vp, vp, C.c_int32, C.c_int32, u32, u32, vp, C.c_int32, C.c_int32]
     L.lrc_batch_clear.argtypes = [vp]
     L.lrc_batch_jobs.argtypes = [vp]
     L.lrc_batch_run.argtypes = [vp, C.c_uint]
@@ -540,10 +542,11 @@ class Batch:
         except Exception:
             pass
 
-    def add(self, scene, params, spp, d_accum, y0=0, rows=None, spp0=0, builder=-1, key_bits=30):
+    def add(self, scene, params, spp, d_accum, y0=0, rows=None, spp0=0, builder=-1, key_bits=30, guided=False):
+        """lrc_batch_add (guided: lrc_batch_add_guided, d_accum the 4 planes)."""
         rows = params.height if rows is None else rows
-        self.ctx.check(self.ctx.L.lrc_batch_add(self.h, scene.h, C.byref(params), y0, rows, spp0, spp,
-                                                C.c_void_p(d_accum), builder, key_bits))
+        fn = self.ctx.L.lrc_batch_add_guided if guided else self.ctx.L.lrc_batch_add
+        self.ctx.check(fn(self.h, scene.h, C.byref(params), y0, rows, spp0, spp, C.c_void_p(d_accum), builder, key_bits))
         self.keep.append((scene, params))
         return len(self.keep) - 1
 
@@ -636,14 +639,15 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, scene, params, spp, records=None, tlas_mode=0):
+    def submit(self, scene, params, spp, records=None, tlas_mode=0, denoise=False):
         jid = C.c_uint64()
+        mode = tlas_mode | (LRC_SERVE_DENOISE if denoise else 0)
         if records is None:
-            rc = self.ctx.L.lrc_server_submit(self.h, scene.h, C.byref(params), spp, None, 0, 0, C.byref(jid))
+            rc = self.ctx.L.lrc_server_submit(self.h, scene.h, C.byref(params), spp, None, 0, mode, C.byref(jid))
         else:
             records = np.ascontiguousarray(records, np.float32).reshape(-1, 32)
             rc = self.ctx.L.lrc_server_submit(self.h, scene.h, C.byref(params), spp, _ptr(records), records.shape[0],
-                                              tlas_mode, C.byref(jid))
+                                              mode, C.byref(jid))
         self.ctx.check(rc)
         self.keep[jid.value] = (scene, params)
         return jid.value

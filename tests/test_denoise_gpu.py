@@ -141,3 +141,55 @@ def test_denoise_device_arrays(ctx, oracle, cornell128):
     assert np.array_equal(d_out.cpu().numpy(), first)
     host = ctx.denoise(d_planes.cpu().numpy())
     assert np.array_equal(host, first)
+
+
+@pytest.mark.parametrize("engine", [1, 0])
+def test_batched_guided_equals_plain(ctx, oracle, cornell128, engine):
+    """A guided batch job (lrc_batch_add_guided) beside an unguided one: its samples and moments
+    equal lrc_trace's with LRC_TRACE_GUIDED to the bit (the moments summed in the same tree order),
+    in both engines."""
+    import torch
+    sc = cornell128
+    s = R.world_scene(ctx, sc, 1)
+    p = params(oracle, sc, seed=11)
+    want = guided(ctx, s, p, 8)
+    d_planes = torch.zeros(4, 128, 128, 4, device="cuda")
+    img = torch.zeros(128, 128, 4, device="cuda")
+    torch.cuda.synchronize()
+    s.guide_device(p, d_planes.data_ptr())
+    b = L.native.Batch(ctx)
+    b.set_engine(engine)
+    b.add(s, p, 8, d_planes.data_ptr(), guided=True)
+    b.add(s, params(oracle, sc, seed=12), 4, img.data_ptr())
+    b.run(zero=True)
+    ctx.sync()
+    got = d_planes.cpu().numpy()
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    assert np.array_equal(got[2:], want[2:])
+    plain, _ = s.trace(params(oracle, sc, seed=12), 4)
+    assert np.array_equal(img.cpu().numpy(), plain)
+    b.close()
+
+
+def test_served_denoised_job_is_the_plain_denoise(ctx, oracle, cornell128):
+    """A denoised server job among plain ones: its image is lrc_denoise of the plain guided planes,
+    to the bit (admission's guide, the waves' moments, the passes at its end); the plain jobs keep
+    their lrc_trace images."""
+    sc = cornell128
+    s = R.world_scene(ctx, sc, 1)
+    sv = L.native.Server(ctx, 1 << 30, 200_000)
+    jobs = [(params(oracle, sc, seed=21), 8, True), (params(oracle, sc, seed=22), 4, False),
+            (params(oracle, sc, seed=23), 16, True)]
+    ids = [sv.submit(s, p, spp, denoise=d) for p, spp, d in jobs]
+    while sv.state()["finished"] < len(jobs):
+        sv.step()
+    for jid, (p, spp, d) in zip(ids, jobs):
+        got = sv.image(jid)
+        if d:
+            want = ctx.denoise(guided(ctx, s, p, spp))
+        else:
+            want, _ = s.trace(p, spp)
+        assert np.array_equal(got, want), (jid, d)
+        sv.release(jid)
+    assert sv.state()["bytes"] == 0
+    sv.close()
