@@ -191,6 +191,23 @@ int lrc_scene_tlas_cost(lrc_scene *s, double *cost);
  * the bit bvh_refit_boxes' on that topology. Host arrays, or device ones with LRC_DEVICE. */
 int lrc_refit(lrc_ctx *ctx, uint32_t *nodes, const uint32_t *aux, uint32_t n, uint32_t ref_add, const float *boxes,
               unsigned flags);
+/* Participating media (engine/scene/volume.h: Volume; scene_add_volume, scene.c:575-583): up to 8
+ * voxel grids of density (trilinear between voxel centres, 0 outside), each with its extinction
+ * at density 1, single-scattering albedo and Henyey-Greenstein g. Replaces the scene's media (n = 0:
+ * none); the majorants (largest density, active box, 8^3-voxel brick maxima) are made here as
+ * volume_update makes them. lrc_trace (both modes) and the batch's engine 0 trace them with delta
+ * and ratio tracking (engine/rt/medium.c); lrc_caustics stops light paths that scatter in them and
+ * dims camera connections through them; the wavefront engine and the server refuse such scenes.
+ * Host arrays. */
+typedef struct {
+    int32_t nx, ny, nz;          /* voxels per axis */
+    float lo[3], hi[3];          /* the world box the grid fills */
+    float sigma_t;               /* extinction at density 1, per scene unit */
+    float albedo[3];             /* single-scattering albedo (sigma_s / sigma_t) */
+    float g;                     /* Henyey-Greenstein anisotropy, in (-1, 1) */
+    const float *density;        /* nx * ny * nz values >= 0, x fastest: index (z * ny + y) * nx + x */
+} lrc_volume;
+int lrc_scene_set_volumes(lrc_scene *s, const lrc_volume *v, uint32_t n);
 /* The sky (Env, env.h:29-53; upload_sky, trace_gpu.c:1522-1569): w x h linear RGB, rows top to
  * bottom, times scale; its sampling tables (marg: h + 1 floats, cond: h x (w + 1), prob: w x h =
  * env_pixel_prob) or NULL: made here as env_prepare makes them (env.c:116-167, 341-363). Host.

@@ -288,6 +288,7 @@ void lrc_scene_destroy(lrc_scene *s) {
     cudaFree(s->d_tlas_aux);
     cudaFree(s->d_env);
     cudaFree(s->d_caus);
+    cudaFree(s->d_vols);
     delete s;
 }
 

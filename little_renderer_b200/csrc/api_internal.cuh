@@ -73,6 +73,9 @@ struct lrc_scene {
     bool specular = false;
     void *d_caus = nullptr;
     size_t caus_cap = 0;
+    // participating media: the VolDev table, then each volume's density and brick majorants
+    void *d_vols = nullptr;
+    uint32_t nvol = 0;
 };
 
 namespace lrcapi {
@@ -135,6 +138,7 @@ inline int check_status(lrc_ctx *c) {
         if (s & lrc::ST_STACK_OVERFLOW) return fail(c, LRC_E_STACK, "a traversal stack would have overflowed (tree too deep)");
         if (s & lrc::ST_BAD_TREE) return fail(c, LRC_E_INVALID, "a tree index out of range was met (not followed)");
         if (s & lrc::ST_LOOP) return fail(c, LRC_E_TIMEOUT, "the wavefront loop ran past its bound (stopped)");
+        if (s & lrc::ST_MEDIUM) return fail(c, LRC_E_TIMEOUT, "a medium's tracking ran past its step bound (stopped)");
         return fail(c, LRC_E_TIMEOUT, "a bounded device wait ran out (sort look-back, PLOC look-back or grid barrier)");
     }
     return LRC_OK;
@@ -179,6 +183,10 @@ inline lrc::PtScene pt_scene(const lrc_scene *s) {
         S.mnaux = s->nmtris;
         S.mesh_info = s->d_mesh_info;
         S.nmeshes = (uint32_t)s->mesh_counts.size();
+    }
+    if (s->nvol) {
+        S.vols = static_cast<const lrc::VolDev *>(s->d_vols);
+        S.nvol = s->nvol;
     }
     if (s->d_env) {
         S.env_rgbp = reinterpret_cast<const float4 *>(s->d_env);

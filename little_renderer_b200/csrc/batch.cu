@@ -503,6 +503,10 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
     for (const lrc_batch::Job &J : b->jobs) {
         int rc = check_job(c, J, (flags & LRC_BATCH_BUILD) != 0);
         if (rc) return rc;
+        // (the wavefront defers shadow rays, which a medium's transmittance cannot wait for: it
+        // draws the path's random numbers only when the ray gets through)
+        if (J.s->nvol && b->engine == 1)
+            return fail(c, LRC_E_INVALID, "a scene with media runs on the batch's engine 0 (lrc_batch_set_engine)");
     }
     DeviceGuard g(c->device);
     for (lrc_batch::Job &J : b->jobs) {

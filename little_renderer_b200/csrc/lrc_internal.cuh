@@ -28,6 +28,7 @@ constexpr uint32_t ST_TIMEOUT_PLOC = 2u;
 constexpr uint32_t ST_STACK_OVERFLOW = 4u;
 constexpr uint32_t ST_TIMEOUT_BARRIER = 8u;
 constexpr uint32_t ST_BAD_TREE = 16u;
+constexpr uint32_t ST_MEDIUM = 64u;        // a medium's tracking took more steps than its bound (stopped)
 constexpr uint32_t ST_LOOP = 32u;          // the wavefront's loop ran past its bound (stopped)
 
 // spins before a bounded wait gives up (each ~ a few hundred ns with the back-off): ~1 s
@@ -156,6 +157,19 @@ cudaError_t count_device(const TraceTables &tt, const float *d_orig, const float
 cudaError_t occluded_device(const TraceTables &tt, const float *d_orig, const float *d_dir, const float *d_tmax,
                             uint64_t nrays, float tmin, uint8_t *d_out, uint32_t *d_status, cudaStream_t st);
 
+// A participating medium as the device reads it: the reference's Volume (engine/scene/volume.h:21-46)
+// with its derived majorants (volume_update)
+struct VolDev {
+    float lo[3], hi[3];          // the box the grid fills
+    float alo[3], ahi[3];        // the smallest box around the voxels with density (+ one voxel)
+    float sigma_t, g, max_density;
+    float albedo[3];
+    int nx, ny, nz, bnx, bny, bnz;
+    const float *density;        // nx * ny * nz, x fastest
+    const float *brick_max;      // bnx * bny * bnz: each brick's largest reachable density
+};
+constexpr int kMaxVolumes = 8;   // MAX_VOLUMES (engine/scene/scene.h:12)
+
 // the path tracer's view of a scene (pathtrace.cu)
 struct PtScene {
     const float4 *nodes;        // the world's BVH (shape ids in aux: primitives, then triangles)
@@ -191,6 +205,9 @@ struct PtScene {
     const float *env_cond, *env_marg;
     int env_w, env_h, has_env, env_weighted;
     float env_scale;
+    // participating media (none: nvol 0)
+    const VolDev *vols;
+    uint32_t nvol;
 };
 struct PtParams {
     int W, H, y0, rows, spp0, spp, max_depth, mis, sampler_on, exact, group;

@@ -4,6 +4,7 @@
 #pragma once
 #include "lrc_internal.cuh"
 #include "bsdf.cuh"
+#include "media.cuh"
 
 namespace lrc {
 namespace pt {
@@ -427,8 +428,14 @@ __device__ __forceinline__ float light_pdf(const Lamp &L, float dist2, float cos
 
 // sample_direct_light (tracer.c:56-84) up to its shadow ray: the contribution V if nothing is in
 // the way, the ray's direction and length. False: no ray is traced and the contribution is 0.
+// (M: the pieces a medium's transmittance goes between: f * Le, the geometry term before the MIS
+// weight, that weight, and the lamp's distance; V = fle * (g0 * w), or fle * g0 without MIS)
+struct NeeParts {
+    V3 fle;
+    float g0, w, dist;
+};
 __device__ __forceinline__ bool direct_light_ray(const Lamp &L, const Hit &h, Bsdf &b, V3 v, int mis, float ua, float ub,
-                                                 V3 &V, V3 &wi, float &tmax) {
+                                                 V3 &V, V3 &wi, float &tmax, NeeParts &M) {
     V3 xl = vadd(L.q, vadd(vscale(L.u, ua), vscale(L.v, ub)));
     V3 to = vsub(xl, h.p);
     float dist2 = vdot(to, to);
@@ -441,16 +448,26 @@ __device__ __forceinline__ bool direct_light_ray(const Lamp &L, const Hit &h, Bs
     V3 f = bsdf_eval(b, h.n, v, wi, pdf);
     if (!(vmax3(f) > 0.0f)) return false;
     float g = dvd(mul(mul(fabsf(cos_surf), cos_light), L.area), dist2);
-    if (mis) g = mul(g, power_heuristic(light_pdf(L, dist2, cos_light), pdf));
-    V = vscale(vmul(f, L.le), g);
+    M.g0 = g;
+    M.w = mis ? power_heuristic(light_pdf(L, dist2, cos_light), pdf) : 1.0f;
+    if (mis) g = mul(g, M.w);
+    M.fle = vmul(f, L.le);
+    M.dist = dist;
+    V = vscale(M.fle, g);
     tmax = sub(dist, RT_SHADOW_MARGIN);
     return true;
+}
+// the contribution with a medium's transmittance tr: g0 * tr, then the MIS weight (tracer.c:77-79)
+__device__ __forceinline__ V3 nee_through(const NeeParts &M, int mis, float tr) {
+    float g = mul(M.g0, tr);
+    if (mis) g = mul(g, M.w);
+    return vscale(M.fle, g);
 }
 
 // sample_direct_env (tracer.c:87-101) up to its shadow ray: a sky direction by its luminance,
 // weighted against the BSDF's own sampling. False: no ray is traced and the contribution is 0.
 __device__ __forceinline__ bool direct_env_ray(const PtScene &S, const Hit &h, Bsdf &b, V3 v, int mis, float ua, float ub,
-                                               V3 &V, V3 &wi) {
+                                               V3 &V, V3 &wi, NeeParts &M) {
     wi = v3(0, 0, 0);
     float pdf;
     V3 le = env_sample(S, ua, ub, wi, pdf);
@@ -459,9 +476,51 @@ __device__ __forceinline__ bool direct_env_ray(const PtScene &S, const Hit &h, B
     V3 f = bsdf_eval(b, h.n, v, wi, bpdf);
     if (!(vmax3(f) > 0.0f)) return false;
     float g = dvd(fabsf(vdot(h.n, wi)), pdf);
-    if (mis) g = mul(g, power_heuristic(pdf, bpdf));
-    V = vscale(vmul(f, le), g);
+    M.g0 = g;
+    M.w = mis ? power_heuristic(pdf, bpdf) : 1.0f;
+    if (mis) g = mul(g, M.w);
+    M.fle = vmul(f, le);
+    M.dist = 1e6f;
+    V = vscale(M.fle, g);
     return true;
+}
+
+// sample_light_in_medium (tracer.c:267-288): the lamp seen from a point p in a medium reached
+// along d, through the media (the phase function in place of the BSDF), its shadow ray traced
+__device__ __forceinline__ V3 light_in_medium(const PtScene &S, const Lamp &L, V3 p, V3 d, float g, int mis, float ua,
+                                              float ub, Rng &rng, uint32_t *err, uint32_t &rays) {
+    V3 xl = vadd(L.q, vadd(vscale(L.u, ua), vscale(L.v, ub)));
+    V3 to = vsub(xl, p);
+    float dist2 = vdot(to, to);
+    float dist = __fsqrt_rn(dist2);
+    V3 wi = vscale(to, dvd(1.0f, dist));
+    float cos_light = -vdot(L.normal, wi);
+    if (cos_light <= 0.0f) return v3(0, 0, 0);
+    rays++;
+    if (scene_occluded(S, p, wi, RT_EPS, sub(dist, RT_SHADOW_MARGIN), err)) return v3(0, 0, 0);
+    float tr = scene_medium_transmittance(S, p, wi, 0.0f, dist, rng, err);
+    if (tr <= 0.0f) return v3(0, 0, 0);
+    float ph = phase_hg(vdot(d, wi), g);
+    float w = dvd(mul(mul(mul(ph, tr), cos_light), L.area), dist2);
+    if (mis) w = mul(w, power_heuristic(light_pdf(L, dist2, cos_light), ph));
+    return vscale(L.le, w);
+}
+
+// sample_env_in_medium (tracer.c:104-118): the sky from a point in a medium
+__device__ __forceinline__ V3 env_in_medium(const PtScene &S, V3 p, V3 d, float g, int mis, float ua, float ub, Rng &rng,
+                                            uint32_t *err, uint32_t &rays) {
+    V3 wi;
+    float pdf;
+    V3 le = env_sample(S, ua, ub, wi, pdf);
+    if (!(pdf > 0.0f) || !(vmax3(le) > 0.0f)) return v3(0, 0, 0);
+    rays++;
+    if (scene_occluded(S, p, wi, RT_EPS, 1e30f, err)) return v3(0, 0, 0);
+    float tr = scene_medium_transmittance(S, p, wi, 0.0f, 1e6f, rng, err);
+    if (tr <= 0.0f) return v3(0, 0, 0);
+    float ph = phase_hg(vdot(d, wi), g);
+    float w = dvd(mul(ph, tr), pdf);
+    if (mis) w = mul(w, power_heuristic(pdf, ph));
+    return vscale(le, w);
 }
 
 // One bounce's next event estimation with its shadow rays not yet traced (the wavefront batch):
@@ -506,9 +565,10 @@ struct PathState {
     int depth, emit, caus;
 };
 
-__device__ __forceinline__ void path_begin(int mis, V3 ro, V3 rd, PathState &ps, int skip_caustics) {
+// (norm: MIS or media, whose distances and pdfs need a unit direction: tracer.c:380)
+__device__ __forceinline__ void path_begin(int norm, V3 ro, V3 rd, PathState &ps, int skip_caustics) {
     ps.ro = ro;
-    ps.rd = mis ? vnorm(rd) : rd;
+    ps.rd = norm ? vnorm(rd) : rd;
     ps.thr = v3(1, 1, 1);
     ps.radiance = v3(0, 0, 0);
     ps.bounce_pdf = 0.0f;
@@ -555,6 +615,49 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
     const int depth = ps.depth;
     const bool have_lamp = S.light >= 0;
     if (DEFER) nee.flags = 0;
+    // In a medium the ray may scatter before the surface (delta tracking, tracer.c:384-420): that
+    // point replaces the hit for this bounce. (Media are traced with their shadow rays in place:
+    // their transmittance draws random numbers only when the shadow ray gets through.)
+    if (!DEFER && S.nvol) {
+        float ts;
+        int which;
+        if (scene_medium_collision(S, ps.ro, ps.rd, 0.0f, found ? h.t : 1e30f, *sm.rng, ts, which, err)) {
+            if (depth >= max_depth) return false;
+            const VolDev &vol = S.vols[which];
+            const V3 p = vadd(ps.ro, vscale(ps.rd, ts));
+            ps.thr = vmul(ps.thr, v3(vol.albedo[0], vol.albedo[1], vol.albedo[2]));
+            float la, lb;
+            if (have_lamp) {
+                const Lamp L = load_lamp(S);
+                sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
+                ps.radiance = vadd(ps.radiance, vmul(ps.thr, light_in_medium(S, L, p, ps.rd, vol.g, mis, lb, la, *sm.rng, err, rays)));
+            }
+            if (S.has_env) {
+                if (!have_lamp) sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
+                else {
+                    la = rng_real(*sm.rng);
+                    lb = rng_real(*sm.rng);
+                }
+                ps.radiance = vadd(ps.radiance, vmul(ps.thr, env_in_medium(S, p, ps.rd, vol.g, mis, la, lb, *sm.rng, err, rays)));
+            }
+            float da, db;
+            sampler_2d(sm, SAMPLE_DIR(depth), da, db);
+            const V3 nd = sample_phase_u(ps.rd, vol.g, da, db);
+            ps.bounce_pdf = phase_hg(vdot(ps.rd, nd), vol.g);
+            ps.ro = p;
+            ps.rd = nd;
+            ps.emit = mis ? EMIT_MIS : EMIT_NONE;
+            ps.caus &= ~CAUS_CHAIN;
+            if (depth >= RR_START) {                 // russian_roulette (tracer.c:302-304)
+                const float u = sampler_1d(sm, SAMPLE_MISC(depth), 0);
+                const float pr = rmin(vmax3(ps.thr), 0.95f);
+                if (u >= pr) return false;
+                ps.thr = vscale(ps.thr, dvd(1.0f, pr));
+            }
+            ps.depth = depth + 1;
+            return true;
+        }
+    }
     if (!found) {                                    // escaped: the sky (black without one)
         if (S.has_env && ps.emit != EMIT_NONE) {
             V3 le = env_eval(S, ps.rd);
@@ -594,7 +697,8 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
             sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
             V3 V = v3(0, 0, 0), wi;
             float tmax = 0.0f;
-            const bool ray = direct_light_ray(L, h, b, v, mis, lb, la, V, wi, tmax);
+            NeeParts M;
+            const bool ray = direct_light_ray(L, h, b, v, mis, lb, la, V, wi, tmax, M);
             if (ray) rays++;
             if (DEFER) {
                 nee.flags |= NEE_L | (ray ? NEE_RL : 0);
@@ -603,6 +707,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                 nee.tl = tmax;
             } else {
                 if (ray && scene_occluded(S, h.p, wi, RT_EPS, tmax, err)) V = v3(0, 0, 0);
+                else if (ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S, h.p, wi, 0.0f, M.dist, *sm.rng, err));
                 ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
         }
@@ -614,7 +719,8 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                 lb = rng_real(*sm.rng);
             }
             V3 V = v3(0, 0, 0), wi;
-            const bool ray = direct_env_ray(S, h, b, v, mis, la, lb, V, wi);
+            NeeParts M;
+            const bool ray = direct_env_ray(S, h, b, v, mis, la, lb, V, wi, M);
             if (ray) rays++;
             if (DEFER) {
                 nee.flags |= NEE_E | (ray ? NEE_RE : 0);
@@ -622,6 +728,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                 nee.we = wi;
             } else {
                 if (ray && scene_occluded(S, h.p, wi, RT_EPS, 1e30f, err)) V = v3(0, 0, 0);
+                else if (ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S, h.p, wi, 0.0f, M.dist, *sm.rng, err));
                 ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
         }
@@ -649,7 +756,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
         ps.thr = vscale(ps.thr, dvd(1.0f, p));
     }
     ps.ro = h.p;
-    ps.rd = mis ? vnorm(bs.l) : bs.l;
+    ps.rd = mis || S.nvol ? vnorm(bs.l) : bs.l;
     ps.depth = depth + 1;
     return true;
 }
@@ -668,7 +775,7 @@ __device__ __forceinline__ bool path_bounce(const PtScene &S, int max_depth, int
 // trace_path_sampled (tracer.c:364-545): the bounces of one path
 __device__ inline V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err, uint32_t &rays) {
     PathState ps;
-    path_begin(P.mis, ro, rd, ps, P.skip_caustics);
+    path_begin(P.mis || S.nvol, ro, rd, ps, P.skip_caustics);
     while (path_bounce(S, P.max_depth, P.mis, ps, sm, err, rays)) {
     }
     return ps.radiance;

@@ -206,6 +206,7 @@ int lrc_server_submit(lrc_server *sv, lrc_scene *s, const lrc_trace_params *p, u
     if (p->width <= 0 || p->height <= 0 || spp == 0 || spp >= (1u << 31))
         return fail(c, LRC_E_INVALID, "a job is a whole image with spp >= 1");
     if (p->exact) return fail(c, LRC_E_INVALID, "served jobs trace in fast mode");
+    if (s->nvol) return fail(c, LRC_E_INVALID, "the server's wavefront does not trace media (lrc_trace does)");
     const bool denoise = (tlas_mode & LRC_SERVE_DENOISE) != 0;
     tlas_mode &= ~LRC_SERVE_DENOISE;
     if (denoise && (uint64_t)p->width * p->height >= (1ull << 31)) return fail(c, LRC_E_INVALID, "image too large to denoise");

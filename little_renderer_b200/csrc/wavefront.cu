@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
         V3 o, d;
         camera_ray(J.P, u, v, o, d);
         PathState ps;
-        path_begin(J.P.mis, o, d, ps, J.P.skip_caustics);
+        path_begin(J.P.mis || J.S.nvol, o, d, ps, J.P.skip_caustics);
         W.ro[i] = make_float4(ps.ro.x, ps.ro.y, ps.ro.z, ps.bounce_pdf);
         W.rd[i] = make_float4(ps.rd.x, ps.rd.y, ps.rd.z, __int_as_float(ps.depth | (ps.emit << 16) | (ps.caus << 24)));
         W.thr[i] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z, 0.0f);

@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu", "media.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -100,6 +100,7 @@ def lib():
     L.lrc_caustics_sums.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
     L.lrc_caustics_variant.argtypes = [vp, C.c_int]
     L.lrc_guide.argtypes = [vp, vp, vp, C.c_uint]
+    L.lrc_scene_set_volumes.argtypes = [vp, vp, u32]
     L.lrc_denoise.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp, C.c_uint]
     L.lrc_scene_set_meshes.argtypes = [vp, vp, vp, u32, C.c_uint]
     L.lrc_scene_set_instances.argtypes = [vp, vp, u32, C.c_uint]
@@ -148,6 +149,12 @@ class BuildParams(C.Structure):
     """lrc_build_params (build_queue's BuildParams, engine/gpu/trace_gpu.c:546)."""
     _fields_ = [("n", C.c_uint32), ("node0", C.c_uint32), ("ref0", C.c_uint32), ("ref_add", C.c_uint32),
                 ("lo", C.c_float * 3), ("ext", C.c_float * 3), ("key_bits", C.c_int32), ("builder", C.c_int32)]
+
+
+class Volume(C.Structure):
+    """lrc_volume (engine/scene/volume.h's Volume: grid, box, optics)."""
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("lo", C.c_float * 3), ("hi", C.c_float * 3),
+                ("sigma_t", C.c_float), ("albedo", C.c_float * 3), ("g", C.c_float), ("density", C.c_void_p)]
 
 
 class TraceParams(C.Structure):
@@ -427,6 +434,22 @@ class Scene:
         rows = params.height if rows is None else rows
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), y0, rows, spp0, spp, C.c_void_p(d_accum), None,
                                             LRC_DEVICE))
+
+    def set_volumes(self, vols):
+        """lrc_scene_set_volumes: vols = [(density (nz, ny, nx) float32, lo, hi, sigma_t, albedo, g), ...]."""
+        arr = (Volume * max(len(vols), 1))()
+        self._vol_keep = []
+        for i, (den, lo, hi, sigma_t, albedo, g) in enumerate(vols):
+            den = np.ascontiguousarray(den, np.float32)
+            self._vol_keep.append(den)
+            v = arr[i]
+            v.nz, v.ny, v.nx = den.shape
+            v.lo[:] = list(map(float, lo))
+            v.hi[:] = list(map(float, hi))
+            v.sigma_t, v.g = float(sigma_t), float(g)
+            v.albedo[:] = list(map(float, albedo))
+            v.density = den.ctypes.data
+        self.ctx.check(self.ctx.L.lrc_scene_set_volumes(self.h, arr, len(vols)))
 
     def guide(self, params, planes=None):
         """lrc_guide with host planes (4, h, w, 4): planes 2 and 3 written; returns the planes."""

@@ -17,6 +17,8 @@ def world_scene(ctx, sc, builder=1, key_bits=30, blue_noise=None, bsdf_tables=No
         s.set_light(0)
     s.set_materials(W.material_records(sc["materials"]))
     s.set_tables(blue_noise, bsdf_tables)
+    if sc.get("volumes"):
+        s.set_volumes(sc["volumes"])
     s.build(builder, key_bits)
     return s
 

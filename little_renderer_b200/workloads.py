@@ -152,6 +152,32 @@ def cornell_spheres(seed=7, n_spheres=64, width=256, height=256):
             "width": width, "height": height, "spp": 16, "max_depth": 8}
 
 
+def cloud_grid(seed=3, res=(40, 32, 40), blobs=6):
+    """A cloud-like density grid (nz, ny, nx): a few soft blobs (1 - r^2 / R^2, clipped at 0) with
+    uniform centres in the grid's middle half and radii in [0.15, 0.3] of its size, summed and
+    clipped to [0, 1.2]; the corners stay empty (an active box smaller than the grid)."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = res
+    z, y, x = np.meshgrid((np.arange(nz) + 0.5) / nz, (np.arange(ny) + 0.5) / ny, (np.arange(nx) + 0.5) / nx,
+                          indexing="ij")
+    d = np.zeros(res, np.float64)
+    for _ in range(blobs):
+        c = rng.uniform(0.3, 0.7, 3)
+        r = rng.uniform(0.15, 0.3)
+        q = ((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / (r * r)
+        d += np.clip(1.0 - q, 0.0, None)
+    return np.clip(d, 0.0, 1.2).astype(np.float32)
+
+
+def foggy_cornell(seed=7, width=128, height=128, sigma_t=0.02, g=0.3):
+    """The plain render's box (16 spheres) with a cloud of participating medium (cloud_grid, 40 x 32 x
+    40 voxels) filling x in [80, 480], y in [60, 380], z in [80, 480]: extinction sigma_t per unit
+    at density 1 (optical depth up to about 7 across), albedo (0.9, 0.85, 0.8), Henyey-Greenstein g."""
+    sc = cornell_spheres(seed=seed, n_spheres=16, width=width, height=height)
+    sc["volumes"] = [(cloud_grid(seed), (80.0, 60.0, 80.0), (480.0, 380.0, 480.0), sigma_t, (0.9, 0.85, 0.8), g)]
+    return sc
+
+
 def box_scene(seed, n_tris, width=256, height=256, spp=16, max_depth=8):
     """A scene of the plain render's kind with about n_tris triangles: the open box and its lamp,
     then icospheres and bevelled boxes (a quarter of the objects) with centres uniform in the box.

@@ -193,6 +193,7 @@ def ref_lib(double=False):
         lib.rb_occluded.argtypes = [vp, _f32p, _f32p, C.c_longlong, C.c_float, C.c_float, _i32p]
         lib.rb_trace_image.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        lib.rb_add_volume.argtypes = [vp, C.c_int, C.c_int, C.c_int, _f32p, C.c_float, _f32p, C.c_float, _f32p]
         lib.rb_guide.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, _f32p, _f32p]
         lib.rb_light_trace_caustics.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_longlong, C.c_int,
                                                 C.c_ulonglong, _f32p]
@@ -358,6 +359,13 @@ class RefScene:
         cnt = np.zeros(2, np.int64)
         self.lib.rb_rays(cnt)
         return out, (int(cnt[0]), int(cnt[1]))
+
+    def volume(self, density, lo, hi, sigma_t, albedo, g):
+        """scene_add_volume of a (nz, ny, nx) density grid filling the box lo..hi."""
+        den = np.ascontiguousarray(density, np.float32)
+        nz, ny, nx = den.shape
+        box = np.array([*lo, *hi], np.float32)
+        return self.lib.rb_add_volume(self.s, nx, ny, nz, box, sigma_t, np.asarray(albedo, np.float32), g, den.reshape(-1))
 
     def guide(self, cam, vfov, w, h):
         """The denoiser's guide planes 2 and 3 ((h, w, 4) each) restated on this scene."""

@@ -22,6 +22,7 @@
 #include "rt/tracer.h"
 #include "rt/intersect.h"
 #include "scene/brdf.h"
+#include "scene/volume.h"
 #include "base/sampler.h"
 #include "scene/brdf_tables.h"
 
@@ -145,6 +146,21 @@ void rb_mesh_box(const void *sp, int mesh, float *box6){
     box6[0] = b->lo.x; box6[1] = b->lo.y; box6[2] = b->lo.z; box6[3] = b->hi.x; box6[4] = b->hi.y; box6[5] = b->hi.z;
 }
 // a sky from w x h linear RGB floats (copied; the scene owns it)
+// a participating medium: volume_create + the density + its optics + volume_update + scene_add_volume
+// (box6: lo, hi; albedo3; density nz * ny * nx, x fastest). Returns its index or -1.
+int rb_add_volume(void *sp, int nx, int ny, int nz, const float *box6, float sigma_t, const float *albedo3, float g,
+                  const float *density){
+    Aabb b = {v3f(box6), v3f(box6 + 3)};
+    Volume *v = volume_create(nx, ny, nz, b);
+    if (!v) return -1;
+    memcpy(v->density, density, sizeof(float) * (size_t)nx * ny * nz);
+    v->sigma_t = sigma_t;
+    v->albedo = v3f(albedo3);
+    v->g = g;
+    volume_update(v);
+    return scene_add_volume(sp, v);
+}
+
 int rb_set_env(void *sp, const float *rgb, int w, int h){
     Scene *s = sp;
     float *c = malloc(sizeof(float) * 3 * (size_t)w * h);
