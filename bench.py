@@ -21,6 +21,11 @@ x 16 spp = 1M light paths per step, lrc_caustics_sums into device sums, fast mod
 (closest-hit + shadow rays) of the step; the reference's light_trace_caustics on this host's cores
 is the baseline.
 
+--workload media: the plain render's box with 16 icospheres and a 40x32x40-voxel cloud of
+participating medium (foggy_cornell), 256x256, 16 spp: the plain path and the megakernel batch
+(the wavefront does not take media); the reference's trace_image with the same Volume as the
+baseline.
+
 --workload denoise: the denoiser (prep + 5 a-trous passes) on a 1920x1080 image of the plain
 render's scene at 4 spp (guide + guided samples made once, outside the timed region). Mpixels/s;
 roofline against HBM with 232 algorithmic bytes per pixel (prep reads the 4 planes, 64 B, and
@@ -69,7 +74,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve", "render", "instanced",
-                                                                     "caustics", "denoise"])
+                                                                     "caustics", "denoise", "media"])
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
@@ -605,8 +610,11 @@ def run_render(a):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     inst = a.workload == "instanced"
+    media = a.workload == "media"
     dev = torch.device("cuda", 0)
-    sc = W.instanced_field() if inst else W.cornell_spheres()
+    sc = W.instanced_field() if inst else (W.foggy_cornell(width=256, height=256) if media else W.cornell_spheres())
+    if media:
+        sc["spp"] = 16
     ctx = L.Context(0)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
@@ -643,7 +651,7 @@ def run_render(a):
     torch.cuda.synchronize()
     want = img.cpu()
     engines = {}
-    for name, eng in (("wavefront", 1), ("megakernel", 0)):
+    for name, eng in ((("megakernel", 0),) if media else (("wavefront", 1), ("megakernel", 0))):
         b = L.native.Batch(ctx)
         b.set_engine(eng)
         b.add(s, p, spp, img.data_ptr())
@@ -673,6 +681,8 @@ def run_render(a):
         ref.triangles(sc["corners"], sc["tri_mats"])
         lamp = sc["lamp"]
         ref.quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"], light=True)
+        for v in sc.get("volumes", []):
+            ref.volume(*v)
     t0 = time.perf_counter()
     ref.set_accel()
     rows = max(1, min(h, (4 if inst else 64)))
@@ -688,6 +698,8 @@ def run_render(a):
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": ("instanced scene: 5000 instances of 14 meshes (10k-100k triangles), 2048x1024 sky, "
                                     "1280x720, 64 spp, depth 12" if inst else
+                                    "the box, its lamp, 16 icospheres and a 40x32x40-voxel cloud (optical depth up to "
+                                    "~7), 256x256, 16 spp, depth 8" if media else
                                     "the box, its lamp and 64 icospheres (20.5k triangles), 256x256, 16 spp, depth 8"),
                        "rays_per_image": int(rays), "paths_per_image": w * h * spp,
                        "l2": "one image's scene and image held in HBM; successive images reuse L2 (the workload's own)"},
@@ -864,7 +876,12 @@ DENOISE_BYTES_PER_PIXEL = 80 + 5 * 24 + 16 + 16
 
 
 def run_denoise(a):
-    """--workload denoise: lrc_denoise (device arrays) on a 1080p image's planes; e2e: lrc_denoise
+    """--workload media: the plain render's box with 16 icospheres and a 40x32x40-voxel cloud of
+participating medium (foggy_cornell), 256x256, 16 spp: the plain path and the megakernel batch
+(the wavefront does not take media); the reference's trace_image with the same Volume as the
+baseline.
+
+--workload denoise: lrc_denoise (device arrays) on a 1080p image's planes; e2e: lrc_denoise
     with host planes and image (copied in and out)."""
     import torch
     import little_renderer_b200 as L
@@ -964,7 +981,7 @@ def main():
             print(json.dumps({"impl": "reference", "metric": METRIC_DENOISE, "unavailable":
                               "the reference's denoiser exists only as WGSL (denoise.wgsl), which cannot run on this "
                               "box; its numpy restatement is the cpu_baseline leg of the ours line"}), flush=True)
-        elif a.workload in ("render", "instanced"):
+        elif a.workload in ("render", "instanced", "media"):
             print(json.dumps({"impl": "reference", "metric": METRIC_RENDER, "unavailable":
                               "this workload's CPU baseline is the cpu_baseline leg of the ours line"}), flush=True)
         else:
@@ -976,7 +993,7 @@ def main():
     if a.workload == "serve":
         run_serve(a)
         return
-    if a.workload in ("render", "instanced"):
+    if a.workload in ("render", "instanced", "media"):
         run_render(a)
         return
     if a.workload == "caustics":

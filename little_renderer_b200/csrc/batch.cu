@@ -246,6 +246,13 @@ int prepare(lrc_batch *b) {
     return LRC_OK;
 }
 
+// whether some job's scene has participating media (the megakernel with their tracking then runs)
+bool any_media(const lrc_batch *b) {
+    for (const lrc::BatchJob &T : b->table)
+        if (T.S.nvol) return true;
+    return false;
+}
+
 // whether some job's scene has instances (the traversal kernels then walk two levels)
 bool any_instances(const lrc_batch *b) {
     for (const lrc::BatchJob &T : b->table)
@@ -292,7 +299,7 @@ int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool 
         }
     }
     if (!e && b->engine == 0)
-        e = lrc::batch_trace(b->d_jobs, (uint32_t)nj, limit, b->d_ctr, c->d_status, b->variant, b->grid, st);
+        e = lrc::batch_trace(b->d_jobs, (uint32_t)nj, limit, b->d_ctr, c->d_status, b->variant, b->grid, any_media(b), st);
     if (!e && b->engine == 1 && !capturing && (flags & LRC_BATCH_STEPPED)) {
         const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
         e = lrc::wf_run_stepped(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, any_instances(b),
@@ -655,7 +662,7 @@ int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_
             e = cudaMemsetAsync(b->d_ctr, 0, 8, c->st);
             if (!e) e = cudaEventRecord(e0, c->st);
             if (!e) e = lrc::batch_trace(b->d_jobs, (uint32_t)b->jobs.size(), rep ? n : std::min<unsigned long long>(n, 4096),
-                                         b->d_ctr, c->d_status, v, grid_v, c->st);
+                                         b->d_ctr, c->d_status, v, grid_v, any_media(b), c->st);
             if (!e) e = cudaEventRecord(e1, c->st);
             if (!e) e = cudaEventSynchronize(e1);
             if (!e) e = cudaEventElapsedTime(&ms, e0, e1);

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(128, MINB) caustics_kernel(PtScene S, PtParams
         if (S.nvol) {                                // a scattering in a medium: the path tracer's
             float ts;
             int which;
-            if (scene_medium_collision(S, ro, rd, 0.0f, id >= 0 || inst >= 0 ? t : 1e30f, rng, ts, which, err)) {
+            if (scene_medium_collision(S.vols, S.nvol, ro, rd, 0.0f, id >= 0 || inst >= 0 ? t : 1e30f, rng, ts, which, err)) {
                 alive = false;
                 continue;
             }
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(128, MINB) caustics_kernel(PtScene S, PtParams
                 if (px < cam.W && py < cam.H) {
                     rays++;
                     if (!scene_occluded<INST>(S, h.p, wo, RT_EPS, mul(dist, sub(1.0f, 1e-4f)), err)) {
-                        const float tr = S.nvol ? scene_medium_transmittance(S, h.p, wo, 0.0f, dist, rng, err) : 1.0f;
+                        const float tr = S.nvol ? scene_medium_transmittance(S.vols, S.nvol, h.p, wo, 0.0f, dist, rng, err) : 1.0f;
                         const float wgt = dvd(mul(mul(corr, fabsf(cos_o)), tr),
                                               mul(mul(mul(mul(dist2, cam.pix_area), cos_c), cos_c), cos_c));
                         splat(sums, (uint32_t)py * (uint32_t)cam.W + (uint32_t)px, vscale(vmul(beta, f), wgt), scale);

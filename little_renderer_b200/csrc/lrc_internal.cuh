@@ -262,7 +262,7 @@ struct BatchJob {
 // the persistent trace kernel over the batch's tasks [0, ntasks) in job order (launch shape
 // `variant`, grid blocks), then the resolve pass over its npix pixels
 cudaError_t batch_trace(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, unsigned long long *d_next,
-                        uint32_t *d_status, int variant, int grid, cudaStream_t st);
+                        uint32_t *d_status, int variant, int grid, bool media, cudaStream_t st);
 cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long long npix, cudaStream_t st);
 // the launch shapes: how many; a shape's threads per block, the blocks per SM its registers are
 // capped for, and the blocks of it that fit on one SM (-1: no such shape)

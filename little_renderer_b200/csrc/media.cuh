@@ -225,14 +225,16 @@ __device__ __forceinline__ float medium_transmittance(const VolDev &v, V3 ro, V3
     return tr;
 }
 
+// The two scene-level calls are compiled once per file (not inlined): the path tracer calls them
+// from five places, and inlined copies of the tracking loops overflowed the instruction cache.
 // every medium tracked up to the best collision so far: the earliest one and its medium
-__device__ __forceinline__ bool scene_medium_collision(const PtScene &S, V3 ro, V3 rd, float tmin, float tmax, Rng &rng,
-                                                       float &t, int &which, uint32_t *err) {
+static __device__ __noinline__ bool scene_medium_collision(const VolDev *vols, uint32_t nvol, V3 ro, V3 rd, float tmin,
+                                                           float tmax, Rng &rng, float &t, int &which, uint32_t *err) {
     int w = -1;
     float best = tmax;
-    for (uint32_t i = 0; i < S.nvol; i++) {
+    for (uint32_t i = 0; i < nvol; i++) {
         float ti;
-        if (medium_sample_distance(S.vols[i], ro, rd, tmin, best, rng, ti, err)) {
+        if (medium_sample_distance(vols[i], ro, rd, tmin, best, rng, ti, err)) {
             best = ti;
             w = (int)i;
         }
@@ -243,11 +245,10 @@ __device__ __forceinline__ bool scene_medium_collision(const PtScene &S, V3 ro, 
     return true;
 }
 
-__device__ __forceinline__ float scene_medium_transmittance(const PtScene &S, V3 ro, V3 rd, float tmin, float tmax, Rng &rng,
-                                                           uint32_t *err) {
+static __device__ __noinline__ float scene_medium_transmittance(const VolDev *vols, uint32_t nvol, V3 ro, V3 rd, float tmin,
+                                                               float tmax, Rng &rng, uint32_t *err) {
     float tr = 1.0f;
-    for (uint32_t i = 0; i < S.nvol && tr > 0.0f; i++)
-        tr = mul(tr, medium_transmittance(S.vols[i], ro, rd, tmin, tmax, rng, err));
+    for (uint32_t i = 0; i < nvol && tr > 0.0f; i++) tr = mul(tr, medium_transmittance(vols[i], ro, rd, tmin, tmax, rng, err));
     return tr;
 }
 

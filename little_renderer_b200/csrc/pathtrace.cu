@@ -25,6 +25,7 @@ namespace pt {
 
 // exact mode: one thread per pixel of rows [y0, y0 + rows), samples [0, spp) in order from the
 // CPU's per-pixel stream (trace_image, tracer.c:337-353)
+template <bool MEDIA, bool GUIDED>
 __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float4 *accum, unsigned long long *ray_count,
                                                     uint32_t *err) {
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -37,7 +38,6 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
         rng_seed(rng, 0x853c49e6748fea9bull ^ (pixel * 0x9E3779B97F4A7C15ull) ^ (P.seed * 0xD1B54A32D192ED03ull), pixel);
         V3 sum = v3(0, 0, 0);
         float ml = 0.0f, ml2 = 0.0f;
-        const float4 ga = P.moments ? P.guide[pixel] : make_float4(1, 1, 1, 1);
         for (int k = 0; k < P.spp; k++) {
             Sampler sm{&rng, (uint32_t)k, (uint32_t)P.seed * 0x9e3779b9u, (int)x, (int)y, P.sampler_on, S.mask};
             float jx, jy;
@@ -45,19 +45,19 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
             float u = dvd(add((float)x, jx), (float)P.W), v = dvd(add((float)y, jy), (float)P.H);
             V3 o, d;
             camera_ray(P, u, v, o, d);
-            V3 c = trace_path(S, P, o, d, sm, err, rays);
+            V3 c = trace_path<MEDIA>(S, P, o, d, sm, err, rays);
             if (!is_number(c)) continue;
             c = clamp_sample(c, P.clamp);
             sum = vadd(sum, c);
-            if (P.moments) {
-                const float l = sample_luma(c, ga);
+            if (GUIDED) {
+                const float l = sample_luma(c, P.guide[pixel]);
                 ml += l;
                 ml2 += l * l;
             }
         }
         float4 a = accum[pixel];
         accum[pixel] = make_float4(a.x + sum.x, a.y + sum.y, a.z + sum.z, a.w + (float)P.spp);
-        if (P.moments) {
+        if (GUIDED) {
             const float4 m = P.moments[pixel];
             P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, m.z, m.w);
         }
@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
 // fast mode: P.group lanes (a power of 2 dividing 32) per pixel, lane s tracing samples s, s + g,
 // s + 2g, ... of [spp0, spp0 + spp), each from its own PCG32 stream; the group's sums are then added
 // in a fixed order (deterministic)
+template <bool MEDIA, bool GUIDED>
 __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4 *accum, unsigned long long *ray_count,
                                                    uint32_t *err) {
     const uint32_t g = P.group;
@@ -87,7 +88,6 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
     if (live) {
         const uint32_t x = (uint32_t)(pix_local % P.W), y = P.y0 + (uint32_t)(pix_local / P.W);
         pixel = (uint64_t)y * P.W + x;
-        const float4 ga = P.moments ? P.guide[pixel] : make_float4(1, 1, 1, 1);
         for (uint32_t k = lane_s; k < (uint32_t)P.spp; k += g) {
             const uint32_t kk = P.spp0 + k;
             Rng rng;
@@ -98,12 +98,12 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
             float u = dvd(add((float)x, jx), (float)P.W), v = dvd(add((float)y, jy), (float)P.H);
             V3 o, d;
             camera_ray(P, u, v, o, d);
-            V3 s = trace_path(S, P, o, d, sm, err, rays);
+            V3 s = trace_path<MEDIA>(S, P, o, d, sm, err, rays);
             s = is_number(s) ? clamp_sample(s, P.clamp) : v3(0, 0, 0);
             c = vadd(c, s);
             cnt += 1.0f;
-            if (P.moments) {
-                const float l = sample_luma(s, ga);
+            if (GUIDED) {
+                const float l = sample_luma(s, P.guide[pixel]);
                 ml += l;
                 ml2 += l * l;
             }
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
         c.y += __shfl_down_sync(0xffffffffu, c.y, o, g);
         c.z += __shfl_down_sync(0xffffffffu, c.z, o, g);
         cnt += __shfl_down_sync(0xffffffffu, cnt, o, g);
-        if (P.moments) {
+        if (GUIDED) {
             ml += __shfl_down_sync(0xffffffffu, ml, o, g);
             ml2 += __shfl_down_sync(0xffffffffu, ml2, o, g);
         }
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
     if (live && lane_s == 0) {
         float4 a = accum[pixel];
         accum[pixel] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + cnt);
-        if (P.moments) {
+        if (GUIDED) {
             const float4 m = P.moments[pixel];
             P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, m.z, m.w);
         }
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
 // task of the queue (one atomic per warp and pass for all such lanes). The lanes thus stay busy
 // however the path lengths and the samples per task differ, within a job and across jobs, and
 // the grid drains the queue with no launch per job and no tail per job.
-template <int BLOCK, int MINB>
+template <int BLOCK, int MINB, bool MEDIA>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__restrict__ jobs, uint32_t njobs,
                                                       unsigned long long ntasks, unsigned long long *next, uint32_t *err) {
     const uint32_t lane = threadIdx.x & 31;
@@ -212,10 +212,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
             float u = dvd(add((float)x, jx), (float)J.P.W), v = dvd(add((float)y, jy), (float)J.P.H);
             V3 o, d;
             camera_ray(J.P, u, v, o, d);
-            path_begin(J.P.mis || J.S.nvol, o, d, ps, J.P.skip_caustics);
+            path_begin(J.P.mis || (MEDIA && J.S.nvol), o, d, ps, J.P.skip_caustics);
             active = true;
         }
-        if (!path_bounce(J.S, J.P.max_depth, J.P.mis, ps, sm, err, rays)) {
+        if (!path_bounce<MEDIA>(J.S, J.P.max_depth, J.P.mis, ps, sm, err, rays)) {
             V3 s = is_number(ps.radiance) ? clamp_sample(ps.radiance, J.P.clamp) : v3(0, 0, 0);
             c = vadd(c, s);
             cnt += 1.0f;
@@ -350,13 +350,16 @@ cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsign
                      cudaStream_t st) {
     if (P.rows <= 0 || P.spp <= 0 || P.W <= 0) return cudaSuccess;
     float4 *acc = reinterpret_cast<float4 *>(d_accum);
-    if (P.exact) {
-        const uint64_t threads = (uint64_t)P.W * P.rows;
-        pt::exact_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(S, P, acc, d_rays, d_status);
-    } else {
-        const uint64_t threads = (uint64_t)P.W * P.rows * P.group;
-        pt::fast_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(S, P, acc, d_rays, d_status);
-    }
+    // (kernels compiled with and without the media's tracking and the denoiser's moments: each
+    // holds registers that a scene or an image without them would pay for)
+    using Fn = void (*)(PtScene, PtParams, float4 *, unsigned long long *, uint32_t *);
+    static const Fn exact_fns[4] = {pt::exact_kernel<false, false>, pt::exact_kernel<false, true>,
+                                    pt::exact_kernel<true, false>, pt::exact_kernel<true, true>};
+    static const Fn fast_fns[4] = {pt::fast_kernel<false, false>, pt::fast_kernel<false, true>,
+                                   pt::fast_kernel<true, false>, pt::fast_kernel<true, true>};
+    const int k = (S.nvol ? 2 : 0) + (P.moments ? 1 : 0);
+    const uint64_t threads = P.exact ? (uint64_t)P.W * P.rows : (uint64_t)P.W * P.rows * P.group;
+    (P.exact ? exact_fns[k] : fast_fns[k])<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(S, P, acc, d_rays, d_status);
     return cudaGetLastError();
 }
 
@@ -366,12 +369,14 @@ namespace {
 using BatchFn = void (*)(const BatchJob *, uint32_t, unsigned long long, unsigned long long *, uint32_t *);
 struct BatchVariant {
     int block, minb;
-    BatchFn fn;
+    BatchFn fn, media;   // (media: the kernel compiled with the media's tracking, for batches that have some)
 };
+#define LRC_BATCH_VARIANT(B, M) {B, M, pt::batch_kernel<B, M, false>, pt::batch_kernel<B, M, true>}
 const BatchVariant kBatchVariants[] = {
-    {128, 4, pt::batch_kernel<128, 4>}, {128, 3, pt::batch_kernel<128, 3>}, {128, 5, pt::batch_kernel<128, 5>},
-    {256, 2, pt::batch_kernel<256, 2>}, {64, 8, pt::batch_kernel<64, 8>},   {256, 3, pt::batch_kernel<256, 3>},
+    LRC_BATCH_VARIANT(128, 4), LRC_BATCH_VARIANT(128, 3), LRC_BATCH_VARIANT(128, 5),
+    LRC_BATCH_VARIANT(256, 2), LRC_BATCH_VARIANT(64, 8),  LRC_BATCH_VARIANT(256, 3),
 };
+#undef LRC_BATCH_VARIANT
 }  // namespace
 
 int batch_variants() { return (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0])); }
@@ -386,12 +391,12 @@ int batch_variant_shape(int v, int *block, int *minb) {
 }
 
 cudaError_t batch_trace(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, unsigned long long *d_next,
-                        uint32_t *d_status, int variant, int grid, cudaStream_t st) {
+                        uint32_t *d_status, int variant, int grid, bool media, cudaStream_t st) {
     if (!njobs || !ntasks) return cudaSuccess;
     if (grid < 1 || variant < 0 || variant >= batch_variants()) return cudaErrorInvalidValue;
     void *args[] = {(void *)&d_jobs, (void *)&njobs, (void *)&ntasks, (void *)&d_next, (void *)&d_status};
-    return cudaLaunchKernel((const void *)kBatchVariants[variant].fn, dim3(grid), dim3(kBatchVariants[variant].block), args,
-                            0, st);
+    const BatchVariant &V = kBatchVariants[variant];
+    return cudaLaunchKernel((const void *)(media ? V.media : V.fn), dim3(grid), dim3(V.block), args, 0, st);
 }
 
 cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long long npix, cudaStream_t st) {

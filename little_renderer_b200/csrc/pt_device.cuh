@@ -498,7 +498,7 @@ __device__ __forceinline__ V3 light_in_medium(const PtScene &S, const Lamp &L, V
     if (cos_light <= 0.0f) return v3(0, 0, 0);
     rays++;
     if (scene_occluded(S, p, wi, RT_EPS, sub(dist, RT_SHADOW_MARGIN), err)) return v3(0, 0, 0);
-    float tr = scene_medium_transmittance(S, p, wi, 0.0f, dist, rng, err);
+    float tr = scene_medium_transmittance(S.vols, S.nvol, p, wi, 0.0f, dist, rng, err);
     if (tr <= 0.0f) return v3(0, 0, 0);
     float ph = phase_hg(vdot(d, wi), g);
     float w = dvd(mul(mul(mul(ph, tr), cos_light), L.area), dist2);
@@ -515,7 +515,7 @@ __device__ __forceinline__ V3 env_in_medium(const PtScene &S, V3 p, V3 d, float 
     if (!(pdf > 0.0f) || !(vmax3(le) > 0.0f)) return v3(0, 0, 0);
     rays++;
     if (scene_occluded(S, p, wi, RT_EPS, 1e30f, err)) return v3(0, 0, 0);
-    float tr = scene_medium_transmittance(S, p, wi, 0.0f, 1e6f, rng, err);
+    float tr = scene_medium_transmittance(S.vols, S.nvol, p, wi, 0.0f, 1e6f, rng, err);
     if (tr <= 0.0f) return v3(0, 0, 0);
     float ph = phase_hg(vdot(d, wi), g);
     float w = dvd(mul(ph, tr), pdf);
@@ -609,7 +609,7 @@ __device__ __forceinline__ bool make_hit(const PtScene &S, V3 o, V3 d, float t, 
 // true leaves them in nee (the caller adds vmul(nee.thr, V or 0) for the lamp, then the sky,
 // before the next bounce, which is what this order of additions gives). Returns false when the
 // path has ended (after nee's contributions, if any).
-template <bool DEFER>
+template <bool DEFER, bool MEDIA = false>
 __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int mis, PathState &ps, bool found, const Hit &h,
                                            Sampler &sm, uint32_t *err, uint32_t &rays, Nee &nee) {
     const int depth = ps.depth;
@@ -618,10 +618,10 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
     // In a medium the ray may scatter before the surface (delta tracking, tracer.c:384-420): that
     // point replaces the hit for this bounce. (Media are traced with their shadow rays in place:
     // their transmittance draws random numbers only when the shadow ray gets through.)
-    if (!DEFER && S.nvol) {
+    if (MEDIA && !DEFER && S.nvol) {
         float ts;
         int which;
-        if (scene_medium_collision(S, ps.ro, ps.rd, 0.0f, found ? h.t : 1e30f, *sm.rng, ts, which, err)) {
+        if (scene_medium_collision(S.vols, S.nvol, ps.ro, ps.rd, 0.0f, found ? h.t : 1e30f, *sm.rng, ts, which, err)) {
             if (depth >= max_depth) return false;
             const VolDev &vol = S.vols[which];
             const V3 p = vadd(ps.ro, vscale(ps.rd, ts));
@@ -707,7 +707,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                 nee.tl = tmax;
             } else {
                 if (ray && scene_occluded(S, h.p, wi, RT_EPS, tmax, err)) V = v3(0, 0, 0);
-                else if (ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S, h.p, wi, 0.0f, M.dist, *sm.rng, err));
+                else if (MEDIA && ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S.vols, S.nvol, h.p, wi, 0.0f, M.dist, *sm.rng, err));
                 ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
         }
@@ -728,7 +728,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                 nee.we = wi;
             } else {
                 if (ray && scene_occluded(S, h.p, wi, RT_EPS, 1e30f, err)) V = v3(0, 0, 0);
-                else if (ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S, h.p, wi, 0.0f, M.dist, *sm.rng, err));
+                else if (MEDIA && ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S.vols, S.nvol, h.p, wi, 0.0f, M.dist, *sm.rng, err));
                 ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
         }
@@ -756,27 +756,31 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
         ps.thr = vscale(ps.thr, dvd(1.0f, p));
     }
     ps.ro = h.p;
-    ps.rd = mis || S.nvol ? vnorm(bs.l) : bs.l;
+    ps.rd = mis || (MEDIA && S.nvol) ? vnorm(bs.l) : bs.l;
     ps.depth = depth + 1;
     return true;
 }
 
 // One pass of trace_path_sampled's bounce loop: the closest hit, then the rest of the bounce with
 // its shadow rays traced in place. Returns false when the path has ended (ps.radiance its value).
+template <bool MEDIA = false>
 __device__ __forceinline__ bool path_bounce(const PtScene &S, int max_depth, int mis, PathState &ps, Sampler &sm,
                                             uint32_t *err, uint32_t &rays) {
     Hit h;
     rays++;
     bool found = scene_intersect(S, ps.ro, ps.rd, RT_EPS, 1e30f, h, err);
     Nee unused;
-    return path_shade<false>(S, max_depth, mis, ps, found, h, sm, err, rays, unused);
+    return path_shade<false, MEDIA>(S, max_depth, mis, ps, found, h, sm, err, rays, unused);
 }
 
 // trace_path_sampled (tracer.c:364-545): the bounces of one path
-__device__ inline V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err, uint32_t &rays) {
+// (MEDIA: the scene's media traced; a kernel compiled without them serves the scenes that have none)
+template <bool MEDIA = false>
+__device__ __forceinline__ V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err,
+                                         uint32_t &rays) {
     PathState ps;
-    path_begin(P.mis || S.nvol, ro, rd, ps, P.skip_caustics);
-    while (path_bounce(S, P.max_depth, P.mis, ps, sm, err, rays)) {
+    path_begin(P.mis || (MEDIA && S.nvol), ro, rd, ps, P.skip_caustics);
+    while (path_bounce<MEDIA>(S, P.max_depth, P.mis, ps, sm, err, rays)) {
     }
     return ps.radiance;
 }
