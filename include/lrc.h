@@ -191,6 +191,27 @@ int lrc_scene_tlas_cost(lrc_scene *s, double *cost);
  * the bit bvh_refit_boxes' on that topology. Host arrays, or device ones with LRC_DEVICE. */
 int lrc_refit(lrc_ctx *ctx, uint32_t *nodes, const uint32_t *aux, uint32_t n, uint32_t ref_add, const float *boxes,
               unsigned flags);
+/* Materials' textures (the reference's PBR5: Scene.texmaps, Material.tex_*; engine/scene/texture.h,
+ * scene.h:42-50): up to 255 RGBA8 images (level 0; the path tracers sample it bilinearly), colour
+ * ones sRGB-decoded when read, wrapping as glTF's samplers (0 repeat, 1 clamp, 2 mirror). A
+ * material names them in its fourth 4 floats as the GPU backend packs them (gpu_tex_pack,
+ * engine/gpu/tex_gpu.c:19-29, as uint32 bits): [12] base | emissive << 8, [13] metal-rough
+ * (roughness in green, metallic in blue) | occlusion << 8 | its strength x 255 << 16, [14] normal
+ * map | normal scale x 4096 << 8, [15] uv scale (float; 0 = 1); each 1 + a texmap's index, 0
+ * none. Replaces the scene's texmaps (n = 0: none). Host arrays. */
+typedef struct {
+    int32_t w, h;                /* level 0's size */
+    int32_t srgb;                /* 1: colour (sRGB-encoded texels) */
+    int32_t wrap_u, wrap_v;      /* 0 repeat, 1 clamp, 2 mirror */
+    const uint32_t *rgba;        /* w x h texels r | g << 8 | b << 16 | a << 24, rows top to bottom */
+} lrc_texmap;
+int lrc_scene_set_texmaps(lrc_scene *s, const lrc_texmap *t, uint32_t n);
+/* The world triangles' texture coordinates (Triangle.t, Scene.uvs / .tangents): tri_uv 3 indices
+ * per triangle into uvs (2 floats each) and tangents (xyz + handedness w), -1 none (the triangle's
+ * barycentrics then, as tri_texcoords' fallback). ntris must be the scene's triangle count when it
+ * is traced (else they are not used). Instances' meshes carry none here. Host arrays. */
+int lrc_scene_set_texcoords(lrc_scene *s, const int32_t *tri_uv, uint32_t ntris, const float *uvs, const float *tangents,
+                            uint32_t nuv);
 /* Participating media (engine/scene/volume.h: Volume; scene_add_volume, scene.c:575-583): up to 8
  * voxel grids of density (trilinear between voxel centres, 0 outside), each with its extinction
  * at density 1, single-scattering albedo and Henyey-Greenstein g. Replaces the scene's media (n = 0:

@@ -289,6 +289,8 @@ void lrc_scene_destroy(lrc_scene *s) {
     cudaFree(s->d_env);
     cudaFree(s->d_caus);
     cudaFree(s->d_vols);
+    cudaFree(s->d_tex);
+    cudaFree(s->d_uv);
     delete s;
 }
 
@@ -481,6 +483,9 @@ int lrc_scene_set_materials(lrc_scene *s, const float *mats, uint32_t n) {
         else if (type == 1 || type == 2) r = 0.0f;   // MAT_MIRROR, MAT_GLASS
         const float c01 = r < 0.0f ? 0.0f : (r > 1.0f ? 1.0f : r);
         if (c01 <= 0.02f) s->specular = true;
+        uint32_t mr;                              // (a roughness texture may make any texel smooth)
+        std::memcpy(&mr, m + 13, 4);
+        if (mr & 0xffu) s->specular = true;
     }
     return check_status(c);
 }

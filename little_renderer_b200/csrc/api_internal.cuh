@@ -76,6 +76,13 @@ struct lrc_scene {
     // participating media: the VolDev table, then each volume's density and brick majorants
     void *d_vols = nullptr;
     uint32_t nvol = 0;
+    // textures: the texmap table, the sRGB table, the texels; the triangles' texture coordinates
+    void *d_tex = nullptr;
+    uint32_t ntex = 0;
+    size_t tex_lut_off = 0, texel_off = 0;
+    void *d_uv = nullptr;
+    uint32_t uv_tris = 0, nuv = 0;
+    size_t uv_off = 0, tangent_off = 0;
 };
 
 namespace lrcapi {
@@ -187,6 +194,20 @@ inline lrc::PtScene pt_scene(const lrc_scene *s) {
     if (s->nvol) {
         S.vols = static_cast<const lrc::VolDev *>(s->d_vols);
         S.nvol = s->nvol;
+    }
+    if (s->ntex) {
+        const char *b = static_cast<const char *>(s->d_tex);
+        S.texs = reinterpret_cast<const uint4 *>(b);
+        S.srgb = reinterpret_cast<const float *>(b + s->tex_lut_off);
+        S.texels = reinterpret_cast<const uint32_t *>(b + s->texel_off);
+        S.ntex = s->ntex;
+    }
+    if (s->d_uv && s->uv_tris == s->ntris) {         // (texture coordinates for other triangles: none)
+        const char *b = static_cast<const char *>(s->d_uv);
+        S.tri_uv = reinterpret_cast<const int32_t *>(b);
+        S.uvs = reinterpret_cast<const float2 *>(b + s->uv_off);
+        S.tangents = reinterpret_cast<const float4 *>(b + s->tangent_off);
+        S.nuv = s->nuv;
     }
     if (s->d_env) {
         S.env_rgbp = reinterpret_cast<const float4 *>(s->d_env);

@@ -16,21 +16,31 @@ constexpr int TAB_N = 32;
 constexpr int TAB_E = 0, TAB_B = 1024, TAB_EAVG = 2048, TAB_BAVG = 2080, TAB_FLOATS = 2112;
 
 // a material on the device (16 floats): albedo.xyz, type | emission.xyz, - | ior, metallic,
-// roughness, transmission | -
+// roughness, transmission | its textures as gpu_tex_pack packs them (engine/gpu/tex_gpu.c:19-29):
+// base | emissive << 8, metal-rough | occlusion << 8 | occlusion strength << 16, normal |
+// normal scale x 4096 << 8 (bits), uv scale (float); texture numbers 1 + the texmap's index, 0 none
 struct Mat {
     V3 albedo, emission;
     int type;
     float ior, metallic, roughness, transmission;
+    uint32_t tex0, tex1, tex2;
+    float uv_scale;
 };
 __device__ __forceinline__ Mat load_mat(const float4 *mats, int i) {
-    float4 a = __ldg(&mats[4 * i]), e = __ldg(&mats[4 * i + 1]), p = __ldg(&mats[4 * i + 2]);
+    float4 a = __ldg(&mats[4 * i]), e = __ldg(&mats[4 * i + 1]), p = __ldg(&mats[4 * i + 2]), t = __ldg(&mats[4 * i + 3]);
     Mat m;
     m.albedo = v3(a.x, a.y, a.z);
     m.type = __float_as_int(a.w);
     m.emission = v3(e.x, e.y, e.z);
     m.ior = p.x; m.metallic = p.y; m.roughness = p.z; m.transmission = p.w;
+    m.tex0 = __float_as_uint(t.x);
+    m.tex1 = __float_as_uint(t.y);
+    m.tex2 = __float_as_uint(t.z);
+    m.uv_scale = t.w;
     return m;
 }
+// material_textured (scene.h:76-78): base, metal-rough, normal, emissive or occlusion
+__device__ __forceinline__ bool textured(const Mat &m) { return ((m.tex0 | m.tex1) & 0xffffu) || (m.tex2 & 0xffu); }
 // material_resolved (scene.h): a preset's parameters filled in
 __device__ __forceinline__ Mat resolved(Mat r) {
     switch (r.type) {

@@ -155,7 +155,8 @@ __global__ void __launch_bounds__(128, MINB) caustics_kernel(PtScene S, PtParams
             alive = false;
             continue;
         }
-        const Mat m = load_mat(S.mats, hit_material(S, h) & 63);
+        Mat m = load_mat(S.mats, hit_material(S, h) & 63);
+        if (textured(m)) m = hit_shading(S, h, ro, rd, vneg(rd), m);
         if (m.type == MAT_LIGHT) {
             alive = false;
             continue;

@@ -266,7 +266,8 @@ __global__ void __launch_bounds__(128) guide_kernel(PtScene S, PtParams P, float
     for (int i = 0; i < 6; i++) {
         Hit h;
         if (!scene_intersect(S, ro, rd, RT_EPS, 1e30f, h, err)) break;
-        const Mat m = load_mat(S.mats, hit_material(S, h) & 63);
+        Mat m = load_mat(S.mats, hit_material(S, h) & 63);
+        if (textured(m)) m = hit_shading(S, h, ro, rd, vneg(rd), m);   // (shade_tex)
         // a lamp, or a surface glowing at least as bright as white paper under a light of 1
         if (m.type == MAT_LIGHT || fmaxf(m.emission.x, fmaxf(m.emission.y, m.emission.z)) >= 1.0f) {
             gn = h.n;

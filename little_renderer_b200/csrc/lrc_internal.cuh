@@ -208,6 +208,18 @@ struct PtScene {
     // participating media (none: nvol 0)
     const VolDev *vols;
     uint32_t nvol;
+    // the materials' textures: each texmap's (w, h, srgb | wrap_u << 1 | wrap_v << 3, its first
+    // texel), the RGBA8 texels (level 0), the sRGB decoding table (256); the world triangles'
+    // texture coordinates: 3 indices each (-1: none), the uvs and their tangents (none: ntex 0,
+    // tri_uv null)
+    const uint4 *texs;
+    const uint32_t *texels;
+    const float *srgb;
+    uint32_t ntex;
+    const int32_t *tri_uv;
+    const float2 *uvs;
+    const float4 *tangents;
+    uint32_t nuv;
 };
 struct PtParams {
     int W, H, y0, rows, spp0, spp, max_depth, mis, sampler_on, exact, group;

@@ -221,6 +221,12 @@ __device__ bool walk_instances(const PtScene &S, V3 o, V3 d, float tmin, float &
     return found;
 }
 
+}  // namespace pt
+}  // namespace lrc
+#include "textures.cuh"
+namespace lrc {
+namespace pt {
+
 // set_hit (intersect.c): point, the normal facing the ray, front_face
 __device__ __forceinline__ void set_hit(Hit &h, V3 o, V3 d, float t, V3 outward) {
     h.t = t;
@@ -610,8 +616,9 @@ __device__ __forceinline__ bool make_hit(const PtScene &S, V3 o, V3 d, float t, 
 // before the next bounce, which is what this order of additions gives). Returns false when the
 // path has ended (after nee's contributions, if any).
 template <bool DEFER, bool MEDIA = false>
-__device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int mis, PathState &ps, bool found, const Hit &h,
+__device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int mis, PathState &ps, bool found, const Hit &hit,
                                            Sampler &sm, uint32_t *err, uint32_t &rays, Nee &nee) {
+    Hit h = hit;                                     // (a normal map bends its shading normal)
     const int depth = ps.depth;
     const bool have_lamp = S.light >= 0;
     if (DEFER) nee.flags = 0;
@@ -666,7 +673,8 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
         }
         return false;
     }
-    const Mat m = load_mat(S.mats, hit_material(S, h) & 63);   // (MAX_MATS 64: the buffer's size)
+    Mat m = load_mat(S.mats, hit_material(S, h) & 63);   // (MAX_MATS 64: the buffer's size)
+    if (textured(m)) m = hit_shading(S, h, ps.ro, ps.rd, vneg(vnorm(ps.rd)), m);
     if (m.type == MAT_LIGHT) {
         if (h.front && (ps.caus & (CAUS_CHAIN | CAUS_SPEC)) != (CAUS_CHAIN | CAUS_SPEC)) {
             if (ps.emit == EMIT_FULL) {

@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu", "media.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu", "media.cu", "textures.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -101,6 +101,8 @@ def lib():
     L.lrc_caustics_variant.argtypes = [vp, C.c_int]
     L.lrc_guide.argtypes = [vp, vp, vp, C.c_uint]
     L.lrc_scene_set_volumes.argtypes = [vp, vp, u32]
+    L.lrc_scene_set_texmaps.argtypes = [vp, vp, u32]
+    L.lrc_scene_set_texcoords.argtypes = [vp, vp, u32, vp, vp, u32]
     L.lrc_denoise.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp, C.c_uint]
     L.lrc_scene_set_meshes.argtypes = [vp, vp, vp, u32, C.c_uint]
     L.lrc_scene_set_instances.argtypes = [vp, vp, u32, C.c_uint]
@@ -155,6 +157,12 @@ class Volume(C.Structure):
     """lrc_volume (engine/scene/volume.h's Volume: grid, box, optics)."""
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("lo", C.c_float * 3), ("hi", C.c_float * 3),
                 ("sigma_t", C.c_float), ("albedo", C.c_float * 3), ("g", C.c_float), ("density", C.c_void_p)]
+
+
+class TexMap(C.Structure):
+    """lrc_texmap (level 0 of the reference's TexMap)."""
+    _fields_ = [("w", C.c_int32), ("h", C.c_int32), ("srgb", C.c_int32), ("wrap_u", C.c_int32), ("wrap_v", C.c_int32),
+                ("rgba", C.c_void_p)]
 
 
 class TraceParams(C.Structure):
@@ -450,6 +458,26 @@ class Scene:
             v.albedo[:] = list(map(float, albedo))
             v.density = den.ctypes.data
         self.ctx.check(self.ctx.L.lrc_scene_set_volumes(self.h, arr, len(vols)))
+
+    def set_texmaps(self, maps):
+        """lrc_scene_set_texmaps: maps = [(rgba (h, w) uint32, srgb, wrap_u, wrap_v), ...]."""
+        arr = (TexMap * max(len(maps), 1))()
+        self._tex_keep = []
+        for i, (px, srgb, wu, wv) in enumerate(maps):
+            px = np.ascontiguousarray(px, np.uint32)
+            self._tex_keep.append(px)
+            arr[i].h, arr[i].w = px.shape
+            arr[i].srgb, arr[i].wrap_u, arr[i].wrap_v = int(srgb), int(wu), int(wv)
+            arr[i].rgba = px.ctypes.data
+        self.ctx.check(self.ctx.L.lrc_scene_set_texmaps(self.h, arr, len(maps)))
+
+    def set_texcoords(self, tri_uv, uvs, tangents):
+        """lrc_scene_set_texcoords: tri_uv (ntris, 3) int32, uvs (n, 2), tangents (n, 4)."""
+        tri_uv = np.ascontiguousarray(tri_uv, np.int32)
+        uvs = np.ascontiguousarray(uvs, np.float32)
+        tangents = np.ascontiguousarray(tangents, np.float32)
+        self.ctx.check(self.ctx.L.lrc_scene_set_texcoords(self.h, _ptr(tri_uv), tri_uv.shape[0], _ptr(uvs), _ptr(tangents),
+                                                          uvs.shape[0]))
 
     def guide(self, params, planes=None):
         """lrc_guide with host planes (4, h, w, 4): planes 2 and 3 written; returns the planes."""

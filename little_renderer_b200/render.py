@@ -15,10 +15,14 @@ def world_scene(ctx, sc, builder=1, key_bits=30, blue_noise=None, bsdf_tables=No
     if lamp is not None:
         s.set_prims(W.make_quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"]))
         s.set_light(0)
-    s.set_materials(W.material_records(sc["materials"]))
+    s.set_materials(W.material_records(sc["materials"], len(sc.get("texmaps", []))))
     s.set_tables(blue_noise, bsdf_tables)
     if sc.get("volumes"):
         s.set_volumes(sc["volumes"])
+    if sc.get("texmaps"):
+        s.set_texmaps(sc["texmaps"])
+    if sc.get("texcoords"):
+        s.set_texcoords(*sc["texcoords"])
     s.build(builder, key_bits)
     return s
 

@@ -178,6 +178,59 @@ def foggy_cornell(seed=7, width=128, height=128, sigma_t=0.02, g=0.3):
     return sc
 
 
+def texture_maps(n=64):
+    """Three procedural RGBA8 maps (uint32 (n, n), r | g << 8 | b << 16 | a << 24): a colour
+    checker with value noise (sRGB), a metal-rough map (roughness in green from 0.15 to 1 in
+    bands, metallic in blue in stripes), and a normal map of round bumps (tangent space)."""
+    rng = np.random.default_rng(17)
+    y, x = np.mgrid[0:n, 0:n]
+    cell = ((x // (n // 8)) + (y // (n // 8))) % 2
+    base = np.where(cell[..., None] == 1, [200, 60, 40], [230, 220, 190]).astype(np.float64)
+    base += rng.uniform(-25, 25, (n, n, 1))
+    base = np.clip(base, 0, 255).astype(np.uint32)
+    checker = base[..., 0] | base[..., 1] << 8 | base[..., 2] << 16 | np.uint32(255) << 24
+    rough = (40 + (215 * ((y // (n // 4)) + 1) // 4)).astype(np.uint32)
+    metal = np.where((x // (n // 8)) % 2 == 0, 255, 0).astype(np.uint32)
+    mr = np.uint32(0) | rough << 8 | metal << 16 | np.uint32(255) << 24
+    cx, cy = (x % (n // 4)) - n / 8 + 0.5, (y % (n // 4)) - n / 8 + 0.5
+    r2 = (cx * cx + cy * cy) / (n / 8) ** 2
+    h = np.where(r2 < 1, np.sqrt(np.clip(1 - r2, 0, 1)), 0.0)
+    nx, ny = np.where(r2 < 1, cx / (n / 8) * 0.6, 0.0), np.where(r2 < 1, -cy / (n / 8) * 0.6, 0.0)
+    nz = np.sqrt(np.clip(1 - nx * nx - ny * ny, 0, 1)) + 0 * h
+    enc = lambda v: np.clip(np.rint((v * 0.5 + 0.5) * 255), 0, 255).astype(np.uint32)   # noqa: E731
+    normal = enc(nx) | enc(ny) << 8 | enc(nz) << 16 | np.uint32(255) << 24
+    return [(checker.astype(np.uint32), 1, 0, 0), (mr.astype(np.uint32), 0, 0, 0), (normal.astype(np.uint32), 0, 2, 2)]
+
+
+def textured_cornell(seed=7, width=128, height=128):
+    """The plain render's box (16 spheres) with textured materials: the floor diffuse white under a
+    colour checker and a bump normal map (4 repeats), the back wall a rough metal with the checker
+    and a metal-rough map (2 repeats), one sphere material with the metal-rough map (its triangles
+    sample it at their barycentrics: no texture coordinates). Floor and back wall triangles carry
+    texture coordinates and tangents along +x."""
+    sc = cornell_spheres(seed=seed, n_spheres=16, width=width, height=height)
+    mats = sc["materials"]
+    mats.append(dict(diffuse((0.8, 0.8, 0.8)), tex={"base": 1, "normal": 3, "uv_scale": 4.0}))
+    mats.append(dict(pbr((0.9, 0.9, 0.9), 1.0, 0.6, 1.5, 0.0), tex={"base": 1, "mr": 2, "uv_scale": 2.0}))
+    floor_m, back_m = len(mats) - 2, len(mats) - 1
+    for i, m in enumerate(mats[4:], 4):
+        if m["type"] == MAT_PBR and m.get("tex") is None:
+            mats[i] = dict(m, tex={"mr": 2})
+            break
+    tm = sc["tri_mats"].copy()
+    tm[0:2] = floor_m
+    tm[4:6] = back_m
+    sc["tri_mats"] = tm
+    tri_uv = np.full((sc["corners"].shape[0], 3), -1, np.int32)
+    tri_uv[0], tri_uv[1] = (0, 1, 2), (0, 2, 3)          # floor a b c, a c d
+    tri_uv[4], tri_uv[5] = (4, 5, 6), (4, 6, 7)          # back wall
+    uvs = np.array([[0, 0], [1, 0], [1, 1], [0, 1], [0, 1], [1, 1], [1, 0], [0, 0]], np.float32)
+    tangents = np.tile(np.array([1, 0, 0, 1], np.float32), (8, 1))
+    sc["texmaps"] = texture_maps()
+    sc["texcoords"] = (tri_uv, uvs, tangents)
+    return sc
+
+
 def box_scene(seed, n_tris, width=256, height=256, spp=16, max_depth=8):
     """A scene of the plain render's kind with about n_tris triangles: the open box and its lamp,
     then icospheres and bevelled boxes (a quarter of the objects) with centres uniform in the box.
@@ -235,15 +288,29 @@ def batch_scenes(n_scenes=256, seed=11, tri_range=(1_000, 200_000), resolutions=
     return out
 
 
-def material_records(mats):
+def material_records(mats, ntex=0):
     """Materials as the device reads them: 16 floats each (albedo.xyz, type as int bits |
-    emission.xyz, 0 | ior, metallic, roughness, transmission | 0)."""
+    emission.xyz, 0 | ior, metallic, roughness, transmission | the textures as gpu_tex_pack packs
+    them: base | emissive << 8, mr | occlusion << 8 | strength << 16, normal | scale x 4096 << 8
+    (uint32 bits), uv scale). A material's "tex" dict names texture numbers (1 + index), 0 none."""
     out = np.zeros((len(mats), 16), np.float32)
+    words = out.view(np.uint32)
     for i, m in enumerate(mats):
         out[i, 0:3] = m["albedo"]
         out[i, 3] = np.array([m["type"]], np.int32).view(np.float32)[0]
         out[i, 4:7] = m["emission"]
         out[i, 8:12] = (m["ior"], m["metallic"], m["roughness"], m["transmission"])
+        t = m.get("tex")
+        if t:
+            tx = lambda k: int(t.get(k, 0)) if 0 < int(t.get(k, 0)) <= ntex else 0   # noqa: E731
+            os_ = t.get("occlusion_strength", 0.0) or 1.0
+            ns = t.get("normal_scale", 0.0) or 1.0
+            osq = int(min(os_, 1.0) * 255 + 0.5)
+            nsq = int(min(ns, 4000.0) * 4096 + 0.5)
+            words[i, 12] = tx("base") | tx("emissive") << 8
+            words[i, 13] = tx("mr") | tx("occlusion") << 8 | ((osq << 16) if tx("occlusion") else 0)
+            words[i, 14] = (tx("normal") | nsq << 8) if tx("normal") else 0
+            out[i, 15] = t.get("uv_scale", 0.0)
     return out
 
 

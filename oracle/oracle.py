@@ -193,6 +193,10 @@ def ref_lib(double=False):
         lib.rb_occluded.argtypes = [vp, _f32p, _f32p, C.c_longlong, C.c_float, C.c_float, _i32p]
         lib.rb_trace_image.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        lib.rb_add_texmap.argtypes = [vp, _u32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        lib.rb_material_textures.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                             C.c_float]
+        lib.rb_set_texcoords.argtypes = [vp, _i32p, C.c_int, _f32p, _f32p, C.c_int]
         lib.rb_add_volume.argtypes = [vp, C.c_int, C.c_int, C.c_int, _f32p, C.c_float, _f32p, C.c_float, _f32p]
         lib.rb_guide.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, _f32p, _f32p]
         lib.rb_light_trace_caustics.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_longlong, C.c_int,
@@ -359,6 +363,19 @@ class RefScene:
         cnt = np.zeros(2, np.int64)
         self.lib.rb_rays(cnt)
         return out, (int(cnt[0]), int(cnt[1]))
+
+    def texmap(self, rgba, srgb, wrap_u=0, wrap_v=0):
+        """texmap_make + scene_add_texmap of (h, w) uint32 RGBA8 texels: the texture's number."""
+        px = np.ascontiguousarray(rgba, np.uint32)
+        return self.lib.rb_add_texmap(self.s, px.reshape(-1), px.shape[1], px.shape[0], srgb, wrap_u, wrap_v)
+
+    def material_textures(self, mat, base=0, mr=0, normal=0, emissive=0, occlusion=0, uv_scale=0.0, normal_scale=0.0):
+        self.lib.rb_material_textures(self.s, mat, base, mr, normal, emissive, occlusion, uv_scale, normal_scale)
+
+    def texcoords(self, tri_uv, uvs, tangents):
+        tri_uv = np.ascontiguousarray(tri_uv, np.int32)
+        self.lib.rb_set_texcoords(self.s, tri_uv.reshape(-1), tri_uv.shape[0], np.ascontiguousarray(uvs, np.float32).reshape(-1),
+                                  np.ascontiguousarray(tangents, np.float32).reshape(-1), len(uvs))
 
     def volume(self, density, lo, hi, sigma_t, albedo, g):
         """scene_add_volume of a (nz, ny, nx) density grid filling the box lo..hi."""

@@ -23,6 +23,7 @@
 #include "rt/intersect.h"
 #include "scene/brdf.h"
 #include "scene/volume.h"
+#include "scene/texture.h"
 #include "base/sampler.h"
 #include "scene/brdf_tables.h"
 
@@ -146,6 +147,39 @@ void rb_mesh_box(const void *sp, int mesh, float *box6){
     box6[0] = b->lo.x; box6[1] = b->lo.y; box6[2] = b->lo.z; box6[3] = b->hi.x; box6[4] = b->hi.y; box6[5] = b->hi.z;
 }
 // a sky from w x h linear RGB floats (copied; the scene owns it)
+// a material's texture map (the reference's TexMap: texmap_make from w x h RGBA8 texels, its wrap
+// modes; scene_add_texmap): returns its number (1 + index) or 0
+int rb_add_texmap(void *sp, const uint32_t *rgba, int w, int h, int srgb, int wrap_u, int wrap_v){
+    TexMap t;
+    memset(&t, 0, sizeof(t));
+    if (texmap_make(&t, (const unsigned char *)rgba, w, h, srgb)) return 0;
+    t.wrap_u = wrap_u;
+    t.wrap_v = wrap_v;
+    return scene_add_texmap(sp, &t);
+}
+// material mat's textures (Material.tex_*, uv_scale, normal_scale)
+void rb_material_textures(void *sp, int mat, int base, int mr, int normal, int emissive, int occlusion, float uv_scale,
+                          float normal_scale){
+    Material *m = &((Scene *)sp)->mats[mat];
+    m->tex_base = base; m->tex_mr = mr; m->tex_normal = normal; m->tex_emissive = emissive; m->tex_occlusion = occlusion;
+    m->uv_scale = uv_scale;
+    m->normal_scale = normal_scale;
+}
+// the world triangles' texture coordinates: Triangle.t (3 per triangle, -1 none), Scene.uvs and
+// .tangents (nuv each)
+void rb_set_texcoords(void *sp, const int *tri_uv, int ntris, const float *uvs, const float *tangents, int nuv){
+    Scene *s = sp;
+    s->uvs = malloc(sizeof(Vec2) * (size_t)(nuv > 0 ? nuv : 1));
+    s->tangents = malloc(sizeof(Vec4) * (size_t)(nuv > 0 ? nuv : 1));
+    for (int i = 0; i < nuv; i++){
+        s->uvs[i] = (Vec2){uvs[2 * i], uvs[2 * i + 1]};
+        s->tangents[i] = (Vec4){tangents[4 * i], tangents[4 * i + 1], tangents[4 * i + 2], tangents[4 * i + 3]};
+    }
+    s->nuvs = s->cap_uvs = nuv;
+    for (int i = 0; i < ntris && i < s->ntris; i++)
+        for (int k = 0; k < 3; k++) s->tris[i].t[k] = tri_uv[3 * i + k];
+}
+
 // a participating medium: volume_create + the density + its optics + volume_update + scene_add_volume
 // (box6: lo, hi; albedo3; density nz * ny * nx, x fastest). Returns its index or -1.
 int rb_add_volume(void *sp, int nx, int ny, int nz, const float *box6, float sigma_t, const float *albedo3, float g,
