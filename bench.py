@@ -26,6 +26,10 @@ participating medium (foggy_cornell), 256x256, 16 spp: the plain path and the me
 (the wavefront does not take media); the reference's trace_image with the same Volume as the
 baseline.
 
+--workload textures: the plain render's box with 16 icospheres and textured materials (a colour
+checker, a metal-rough map and a bump normal map, 64x64 RGBA8; textured_cornell), 256x256, 16 spp;
+the reference's trace_image with the same TexMaps as the baseline.
+
 --workload denoise: the denoiser (prep + 5 a-trous passes) on a 1920x1080 image of the plain
 render's scene at 4 spp (guide + guided samples made once, outside the timed region). Mpixels/s;
 roofline against HBM with 232 algorithmic bytes per pixel (prep reads the 4 planes, 64 B, and
@@ -74,7 +78,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve", "render", "instanced",
-                                                                     "caustics", "denoise", "media"])
+                                                                     "caustics", "denoise", "media", "textures"])
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
@@ -611,9 +615,11 @@ def run_render(a):
         return
     inst = a.workload == "instanced"
     media = a.workload == "media"
+    tex = a.workload == "textures"
     dev = torch.device("cuda", 0)
-    sc = W.instanced_field() if inst else (W.foggy_cornell(width=256, height=256) if media else W.cornell_spheres())
-    if media:
+    sc = (W.instanced_field() if inst else W.foggy_cornell(width=256, height=256) if media else
+          W.textured_cornell(width=256, height=256) if tex else W.cornell_spheres())
+    if media or tex:
         sc["spp"] = 16
     ctx = L.Context(0)
     stream = torch.cuda.Stream(dev)
@@ -683,6 +689,15 @@ def run_render(a):
         ref.quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"], light=True)
         for v in sc.get("volumes", []):
             ref.volume(*v)
+        for px, srgb, wu, wv in sc.get("texmaps", []):
+            ref.texmap(px, srgb, wu, wv)
+        for i, m in enumerate(sc["materials"]):
+            t = m.get("tex")
+            if t:
+                ref.material_textures(i, t.get("base", 0), t.get("mr", 0), t.get("normal", 0), t.get("emissive", 0),
+                                      t.get("occlusion", 0), t.get("uv_scale", 0.0), t.get("normal_scale", 0.0))
+        if sc.get("texcoords"):
+            ref.texcoords(*sc["texcoords"])
     t0 = time.perf_counter()
     ref.set_accel()
     rows = max(1, min(h, (4 if inst else 64)))
@@ -700,6 +715,8 @@ def run_render(a):
                                     "1280x720, 64 spp, depth 12" if inst else
                                     "the box, its lamp, 16 icospheres and a 40x32x40-voxel cloud (optical depth up to "
                                     "~7), 256x256, 16 spp, depth 8" if media else
+                                    "the box, its lamp and 16 icospheres with colour, metal-rough and normal maps "
+                                    "(64x64 RGBA8), 256x256, 16 spp, depth 8" if tex else
                                     "the box, its lamp and 64 icospheres (20.5k triangles), 256x256, 16 spp, depth 8"),
                        "rays_per_image": int(rays), "paths_per_image": w * h * spp,
                        "l2": "one image's scene and image held in HBM; successive images reuse L2 (the workload's own)"},
@@ -981,7 +998,7 @@ def main():
             print(json.dumps({"impl": "reference", "metric": METRIC_DENOISE, "unavailable":
                               "the reference's denoiser exists only as WGSL (denoise.wgsl), which cannot run on this "
                               "box; its numpy restatement is the cpu_baseline leg of the ours line"}), flush=True)
-        elif a.workload in ("render", "instanced", "media"):
+        elif a.workload in ("render", "instanced", "media", "textures"):
             print(json.dumps({"impl": "reference", "metric": METRIC_RENDER, "unavailable":
                               "this workload's CPU baseline is the cpu_baseline leg of the ours line"}), flush=True)
         else:
@@ -993,7 +1010,7 @@ def main():
     if a.workload == "serve":
         run_serve(a)
         return
-    if a.workload in ("render", "instanced", "media"):
+    if a.workload in ("render", "instanced", "media", "textures"):
         run_render(a)
         return
     if a.workload == "caustics":
