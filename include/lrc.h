@@ -290,6 +290,15 @@ int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
  *   planes, steered by each pixel's variance (passes 1-5, the hole sizes 1, 2, 4, 8, 16; other
  *   values: 5). Arrays are host memory, or device memory with LRC_DEVICE. */
 int lrc_guide(lrc_scene *s, const lrc_trace_params *p, float *planes, unsigned flags);
+/* A new image's samples carried over from the previous one (gpu_trace_begin_image with history > 0,
+ * trace_gpu.c:2020-2060; trace_reproject.wgsl `main`), without temporal gradients: each new pixel's
+ * first surface (its guide, planes 2 and 3 of new_planes, made by lrc_guide) is placed in the old
+ * camera's image, and the old pixels around that point that saw the same surface (kind and
+ * object, distance within 2 % plus its local change, normal within ~25 degrees) give it their
+ * samples and moments, bilinearly weighted, at most `history` samples' worth. Writes planes 0 and
+ * 1 of new_planes (cleared where nothing matched). Both images of the same size. */
+int lrc_reproject(lrc_ctx *ctx, const lrc_trace_params *old_cam, const lrc_trace_params *new_cam, const float *old_planes,
+                  float *new_planes, int32_t history, unsigned flags);
 int lrc_denoise(lrc_ctx *ctx, int32_t width, int32_t height, const float *planes, int32_t passes, float *out,
                 unsigned flags);
 

@@ -299,6 +299,92 @@ __global__ void __launch_bounds__(128) guide_kernel(PtScene S, PtParams P, float
     planes[3 * N + idx] = make_float4(ga.x, ga.y, ga.z, w);
 }
 
+// ---- reprojection (trace_reproject.wgsl `main` without temporal gradients): a new image's
+// samples from the previous image's, where each pixel still sees the same surface ---------------
+struct RpCam {
+    float3 o, ul, h, v;
+};
+__device__ __forceinline__ float3 f3(pt::V3 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sc3(float3 a, float k) { return make_float3(a.x * k, a.y * k, a.z * k); }
+
+// where new pixel k's surface was in the old image (pixel centres at integers; z its distance
+// from the old eye, w 1 if in front of it)
+__device__ __forceinline__ float4 old_place(const RpCam &oc, const RpCam &nc, int W, int H, uint32_t k, float4 g2) {
+    const float x = (float)(k % (uint32_t)W), y = (float)(k / (uint32_t)W);
+    float3 d = sub3(sub3(add3(nc.ul, sc3(nc.h, (x + 0.5f) / (float)W)), sc3(nc.v, (y + 0.5f) / (float)H)), nc.o);
+    d = sc3(d, rsqrtf(dot3(d, d)));
+    const bool far = g2.w > 1e29f;
+    const float3 p = add3(nc.o, sc3(d, far ? 1e6f : g2.w));
+    const float3 f = sub3(oc.ul, oc.o);
+    const float3 c = sub3(add3(f, sc3(oc.h, 0.5f)), sc3(oc.v, 0.5f));
+    const float3 q0 = sub3(p, oc.o);
+    const float den = dot3(q0, c);
+    if (den <= 0.0f) return make_float4(0, 0, 0, 0);
+    const float3 q = sub3(sc3(q0, dot3(c, c) / den), f);
+    const float fx = dot3(q, oc.h) / dot3(oc.h, oc.h) * (float)W - 0.5f;
+    const float fy = -dot3(q, oc.v) / dot3(oc.v, oc.v) * (float)H - 0.5f;
+    return make_float4(fx, fy, sqrtf(dot3(q0, q0)), 1.0f);
+}
+
+// old pixel o saw what the new one sees: samples, the same kind and object, the distance within
+// 2 % (25 % in a medium) plus how fast it changes there, the normal within ~25 degrees
+__device__ __forceinline__ bool same_surface(const float4 *__restrict__ old, int W, int H, uint32_t o, float4 g2, float4 g3,
+                                             float dist) {
+    const size_t N = (size_t)W * H;
+    if (old[o].w == 0.0f) return false;
+    const float4 o3 = old[3 * N + o];
+    if (o3.w != g3.w) return false;
+    const float gk = gkind(g3.w);
+    const float4 o2 = old[2 * N + o];
+    if (g2.w <= 1e29f) {
+        const uint32_t ux = o % (uint32_t)W, uy = o / (uint32_t)W;
+        const float zl = old[2 * N + o - (ux > 0 ? 1 : 0)].w, zr = old[2 * N + o + (ux + 1 < (uint32_t)W ? 1 : 0)].w;
+        const float zu = old[2 * N + o - (uy > 0 ? W : 0)].w, zd = old[2 * N + o + (uy + 1 < (uint32_t)H ? W : 0)].w;
+        const float grad = fminf(fabsf(zl - o2.w), fabsf(zr - o2.w)) + fminf(fabsf(zu - o2.w), fabsf(zd - o2.w));
+        if (fabsf(o2.w - dist) > (gk == 2.0f ? 0.25f : 0.02f) * dist + grad) return false;
+    }
+    if (gk == 0.0f && o2.x * g2.x + o2.y * g2.y + o2.z * g2.z < 0.9f) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(256) reproject_kernel(RpCam oc, RpCam nc, int W, int H, float history,
+                                                        const float4 *__restrict__ old, float4 *__restrict__ cur) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t N = (size_t)W * H;
+    if (k >= N) return;
+    const float4 g2 = cur[2 * N + k], g3 = cur[3 * N + k];
+    const float4 at = old_place(oc, nc, W, H, k, g2);
+    float4 a0 = make_float4(0, 0, 0, 0), a1 = make_float4(0, 0, 0, 0);
+    float nsum = 0.0f, wsum = 0.0f;
+    if (at.w > 0.0f) {
+        const float x0 = floorf(at.x), y0 = floorf(at.y);
+        for (int j = 0; j < 4; j++) {
+            const float tx = x0 + (float)(j & 1), ty = y0 + (float)(j >> 1);
+            if (tx < 0.0f || ty < 0.0f || tx >= (float)W || ty >= (float)H) continue;
+            const uint32_t o = (uint32_t)ty * (uint32_t)W + (uint32_t)tx;
+            if (!same_surface(old, W, H, o, g2, g3, at.z)) continue;
+            const float4 s = old[o], m = old[N + o];
+            const float w = (1.0f - fabsf(at.x - tx)) * (1.0f - fabsf(at.y - ty));
+            const float ws = w / s.w;
+            a0 = make_float4(a0.x + ws * s.x, a0.y + ws * s.y, a0.z + ws * s.z, a0.w + ws * s.w);
+            a1 = make_float4(a1.x + ws * m.x, a1.y + ws * m.y, a1.z + ws * m.z, a1.w + ws * m.w);
+            nsum += w * s.w;
+            wsum += w;
+        }
+    }
+    if (wsum < 0.05f || history < 0.5f) {
+        cur[k] = make_float4(0, 0, 0, 0);
+        cur[N + k] = make_float4(0, 0, 0, 0);
+        return;
+    }
+    const float n = fminf(nsum / wsum, history);
+    cur[k] = make_float4(a0.x / wsum * n, a0.y / wsum * n, a0.z / wsum * n, n);
+    cur[N + k] = make_float4(a1.x / wsum * n, a1.y / wsum * n, 0.0f, 0.0f);
+}
+
 }  // namespace dn
 
 cudaError_t dn_guide(const PtScene &S, const PtParams &P, float4 *d_planes, uint32_t *d_status, cudaStream_t st) {
@@ -328,6 +414,17 @@ cudaError_t dn_denoise(const float4 *d_planes, int W, int H, int passes, float4 
 }
 
 }  // namespace lrc
+
+namespace {
+lrc::dn::RpCam rp_cam(const lrc_trace_params *p) {
+    lrc::dn::RpCam c;
+    c.o = make_float3(p->origin[0], p->origin[1], p->origin[2]);
+    c.ul = make_float3(p->upper_left[0], p->upper_left[1], p->upper_left[2]);
+    c.h = make_float3(p->horizontal[0], p->horizontal[1], p->horizontal[2]);
+    c.v = make_float3(p->vertical[0], p->vertical[1], p->vertical[2]);
+    return c;
+}
+}  // namespace
 
 // ---- the C ABI ------------------------------------------------------------------------------
 #include "api_internal.cuh"
@@ -366,6 +463,35 @@ int lrc_guide(lrc_scene *s, const lrc_trace_params *p, float *planes, unsigned f
     if (!e && !(flags & LRC_DEVICE))
         e = cudaMemcpyAsync(planes + 8 * N, d_planes + 2 * N, N * 32, cudaMemcpyDeviceToHost, c->st);
     if (e) return cuda_status(c, e, "lrc_guide");
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_reproject(lrc_ctx *c, const lrc_trace_params *old_cam, const lrc_trace_params *new_cam, const float *old_planes,
+                  float *new_planes, int32_t history, unsigned flags) {
+    if (!c || !old_cam || !new_cam || !old_planes || !new_planes || history < 0) return LRC_E_INVALID;
+    const int W = new_cam->width, H = new_cam->height;
+    if (W <= 0 || H <= 0 || old_cam->width != W || old_cam->height != H)
+        return fail(c, LRC_E_INVALID, "reprojection: both images of the same size");
+    DeviceGuard g(c->device);
+    const size_t N = (size_t)W * H;
+    const float4 *d_old = reinterpret_cast<const float4 *>(old_planes);
+    float4 *d_new = reinterpret_cast<float4 *>(new_planes);
+    cudaError_t e = cudaSuccess;
+    if (!(flags & LRC_DEVICE)) {
+        e = reserve(&c->stage, &c->stage_cap, N * 128);
+        float4 *st = static_cast<float4 *>(c->stage);
+        if (!e) e = cudaMemcpyAsync(st, old_planes, N * 64, cudaMemcpyHostToDevice, c->st);
+        if (!e) e = cudaMemcpyAsync(st + 4 * N, new_planes, N * 64, cudaMemcpyHostToDevice, c->st);
+        d_old = st;
+        d_new = st + 4 * N;
+    }
+    if (!e) {
+        lrc::dn::reproject_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>(rp_cam(old_cam), rp_cam(new_cam), W, H,
+                                                                                  (float)history, d_old, d_new);
+        e = cudaGetLastError();
+    }
+    if (!e && !(flags & LRC_DEVICE)) e = cudaMemcpyAsync(new_planes, d_new, N * 32, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_reproject");
     return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 

@@ -100,6 +100,7 @@ def lib():
     L.lrc_caustics_sums.argtypes = [vp, vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint]
     L.lrc_caustics_variant.argtypes = [vp, C.c_int]
     L.lrc_guide.argtypes = [vp, vp, vp, C.c_uint]
+    L.lrc_reproject.argtypes = [vp, vp, vp, vp, vp, C.c_int32, C.c_uint]
     L.lrc_scene_set_volumes.argtypes = [vp, vp, u32]
     L.lrc_scene_set_texmaps.argtypes = [vp, vp, u32]
     L.lrc_scene_set_texcoords.argtypes = [vp, vp, u32, vp, vp, u32]
@@ -239,6 +240,13 @@ class Context:
             out = np.zeros((h, w, 4), np.float32)
         self.check(self.L.lrc_denoise(self.h, w, h, _ptr(planes), passes, _ptr(out), 0))
         return out
+
+    def reproject(self, old_params, new_params, old_planes, new_planes, history):
+        """lrc_reproject with host planes (4, h, w, 4): new_planes' planes 0 and 1 from old_planes."""
+        old_planes = np.ascontiguousarray(old_planes, np.float32)
+        self.check(self.L.lrc_reproject(self.h, C.byref(old_params), C.byref(new_params), _ptr(old_planes),
+                                        _ptr(new_planes), history, 0))
+        return new_planes
 
     def denoise_device(self, width, height, d_planes, d_out, passes=5):
         self.check(self.L.lrc_denoise(self.h, width, height, C.c_void_p(d_planes), passes, C.c_void_p(d_out),

@@ -57,3 +57,26 @@ def test_noise_is_reduced_and_edges_kept():
     noisy = px[0, ..., :3] / spp
     assert out[:, 2:14, :3].std() < 0.5 * noisy[:, 2:14].std()
     assert out[:, :14, 0].mean() < 0.5 and out[:, 18:, 0].mean() > 0.6     # the halves stay apart
+
+
+def test_reprojection_restatement_keeps_an_unmoved_image():
+    """oracle/reproject_oracle.py: with the camera unmoved every pixel keeps its samples (capped at
+    the history), and a pixel whose surface changed (another kind) keeps none."""
+    from oracle import reproject_oracle as RP
+    h = w = 16
+    old = np.zeros((4, h, w, 4), np.float32)
+    old[0, ..., :3], old[0, ..., 3] = 4.0, 8.0
+    old[1, ..., 0], old[1, ..., 1] = 2.0, 1.0
+    old[2, ..., 2], old[2, ..., 3] = -1.0, 100.0
+    old[3, ..., :3] = 0.5
+    cam = [[0, 0, 0], [-0.5, 0.5, 1], [1, 0, 0], [0, 1, 0]]
+    new = old.copy()
+    new[0] = new[1] = 0
+    new[3, 5, 5, 3] = 1.0                        # a lamp now
+    out = RP.reproject(old, new, cam, cam, 64)
+    keep = np.ones((h, w), bool)
+    keep[5, 5] = False
+    assert np.allclose(out[0][keep], old[0][keep]) and np.allclose(out[1][keep][:, :2], old[1][keep][:, :2])
+    assert np.all(out[0][5, 5] == 0)
+    capped = RP.reproject(old, new, cam, cam, 3)
+    assert np.allclose(capped[0][keep][:, 3], 3.0) and np.allclose(capped[0][keep][:, :3], 4.0 * 3 / 8)
