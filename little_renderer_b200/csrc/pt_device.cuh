@@ -320,6 +320,17 @@ __device__ __forceinline__ bool scene_occluded(const PtScene &S, V3 o, V3 d, flo
     return S.nnodes && walk<true>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err) >= 0;
 }
 
+// The any-hit query compiled once (not inlined) for the kernels that trace media: with the
+// in-medium next event estimation they query from four places, and four inlined walks beside
+// the media's tracking overflowed the instruction cache.
+static __device__ __noinline__ bool scene_occluded_once(const PtScene &S, V3 o, V3 d, float tmin, float tmax, uint32_t *err) {
+    return scene_occluded<true>(S, o, d, tmin, tmax, err);
+}
+template <bool ONCE>
+__device__ __forceinline__ bool occluded(const PtScene &S, V3 o, V3 d, float tmin, float tmax, uint32_t *err) {
+    return ONCE ? scene_occluded_once(S, o, d, tmin, tmax, err) : scene_occluded(S, o, d, tmin, tmax, err);
+}
+
 // ---- the sky (engine/scene/env.c: env_eval, env_sample, env_pdf) --------------------------------
 // rgbp: the map's radiance and each pixel's probability (env_pixel_prob), w x h; cond: each row's
 // cumulative distribution (w + 1 per row); marg: the rows' (h + 1)
@@ -503,7 +514,7 @@ __device__ __forceinline__ V3 light_in_medium(const PtScene &S, const Lamp &L, V
     float cos_light = -vdot(L.normal, wi);
     if (cos_light <= 0.0f) return v3(0, 0, 0);
     rays++;
-    if (scene_occluded(S, p, wi, RT_EPS, sub(dist, RT_SHADOW_MARGIN), err)) return v3(0, 0, 0);
+    if (scene_occluded_once(S, p, wi, RT_EPS, sub(dist, RT_SHADOW_MARGIN), err)) return v3(0, 0, 0);
     float tr = scene_medium_transmittance(S.vols, S.nvol, p, wi, 0.0f, dist, rng, err);
     if (tr <= 0.0f) return v3(0, 0, 0);
     float ph = phase_hg(vdot(d, wi), g);
@@ -520,7 +531,7 @@ __device__ __forceinline__ V3 env_in_medium(const PtScene &S, V3 p, V3 d, float 
     V3 le = env_sample(S, ua, ub, wi, pdf);
     if (!(pdf > 0.0f) || !(vmax3(le) > 0.0f)) return v3(0, 0, 0);
     rays++;
-    if (scene_occluded(S, p, wi, RT_EPS, 1e30f, err)) return v3(0, 0, 0);
+    if (scene_occluded_once(S, p, wi, RT_EPS, 1e30f, err)) return v3(0, 0, 0);
     float tr = scene_medium_transmittance(S.vols, S.nvol, p, wi, 0.0f, 1e6f, rng, err);
     if (tr <= 0.0f) return v3(0, 0, 0);
     float ph = phase_hg(vdot(d, wi), g);
@@ -714,7 +725,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                 nee.wl = wi;
                 nee.tl = tmax;
             } else {
-                if (ray && scene_occluded(S, h.p, wi, RT_EPS, tmax, err)) V = v3(0, 0, 0);
+                if (ray && occluded<MEDIA>(S, h.p, wi, RT_EPS, tmax, err)) V = v3(0, 0, 0);
                 else if (MEDIA && ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S.vols, S.nvol, h.p, wi, 0.0f, M.dist, *sm.rng, err));
                 ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
@@ -735,7 +746,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                 nee.ve = V;
                 nee.we = wi;
             } else {
-                if (ray && scene_occluded(S, h.p, wi, RT_EPS, 1e30f, err)) V = v3(0, 0, 0);
+                if (ray && occluded<MEDIA>(S, h.p, wi, RT_EPS, 1e30f, err)) V = v3(0, 0, 0);
                 else if (MEDIA && ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S.vols, S.nvol, h.p, wi, 0.0f, M.dist, *sm.rng, err));
                 ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
