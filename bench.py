@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
     ap.add_argument("--wave-paths", type=int, default=32 << 20, help="serve: paths per wave")
     ap.add_argument("--wave-slots", type=int, default=1 << 22, help="serve: the waves' paths in flight")
+    ap.add_argument("--denoise-low-spp", action="store_true",
+                    help="serve: jobs of 4 spp are denoised (LRC_SERVE_DENOISE; the plain path: guide, guided "
+                         "trace, lrc_denoise)")
     ap.add_argument("--scenes", type=int, default=256, help="batch: scenes (jobs)")
     ap.add_argument("--plain-steps", type=int, default=1, help="batch: timed passes of the plain path")
     ap.add_argument("--cpu-scenes", type=int, default=8, help="batch: scenes the CPU baseline samples")
@@ -502,6 +505,9 @@ def run_serve(a):
     def pct(x, q):
         return float(np.percentile(np.asarray(x), q))
 
+    def denoised(job):
+        return bool(a.denoise_low_spp and job[4] == 4)
+
     results = {}
     check = {}
     clk = Clocks(0)
@@ -518,7 +524,7 @@ def run_serve(a):
             now = (L.native.clock_ms() - t0) / 1e3
             while nxt < len(jobs) and jobs[nxt][0] <= now:
                 j = jobs[nxt]
-                ids[sv.submit(scenes[j[1]], params(j, nxt), j[4], recs[nxt], 0)] = nxt
+                ids[sv.submit(scenes[j[1]], params(j, nxt), j[4], recs[nxt], 0, denoise=denoised(j))] = nxt
                 nxt += 1
             st = sv.state()
             if st["queued"] + st["active"] == 0:
@@ -551,7 +557,13 @@ def run_serve(a):
             if recs[k] is not None:
                 s.move_instances(recs[k], 0)
             img = torch.zeros(j[3], j[2], 4, device=dev)
-            s.trace_device(params(j, k), j[4], img.data_ptr())
+            if denoised(j):
+                planes = torch.zeros(4, j[3], j[2], 4, device=dev)
+                s.guide_device(params(j, k), planes.data_ptr())
+                s.trace_guided_device(params(j, k), j[4], planes.data_ptr())
+                ctx.denoise_device(j[2], j[3], planes.data_ptr(), img.data_ptr())
+            else:
+                s.trace_device(params(j, k), j[4], img.data_ptr())
             ctx.sync()
             lat_p.append(L.native.clock_ms() - (t0 + j[0] * 1e3))
             if rate == float(a.rates.split(",")[0]) and k < 6:
@@ -566,6 +578,7 @@ def run_serve(a):
             "plain": {"p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99), "mrays_s": rays_p / span_p / 1e6,
                       "span_s": span_p},
             "jobs": len(jobs), "motion_jobs": sum(1 for j in jobs if j[5] is not None),
+            "denoised_jobs": sum(1 for j in jobs if denoised(j)),
             "paths": int(sum(j[2] * j[3] * j[4] for j in jobs)), "rays": int(rays_s)}
         if imgs:
             results[str(int(rate))]["images_equal_plain"] = all(np.array_equal(check[k], imgs[k]) for k in imgs)
@@ -577,7 +590,8 @@ def run_serve(a):
             "config": {"workload": f"served request stream: 64 resident scenes ({tris} triangles; 8 with 2000 moving "
                                    "instances), jobs {256^2, 720p, 1080p} x spp {4, 16, 64}, depth 8, Poisson arrivals",
                        "rates": a.rates, "jobs_per_rate": a.jobs, "budget_gb": a.budget_gb,
-                       "wave_paths": a.wave_paths, "wave_slots": a.wave_slots, "parallelism": "one GPU"},
+                       "wave_paths": a.wave_paths, "wave_slots": a.wave_slots, "parallelism": "one GPU",
+                       "denoise_low_spp": bool(a.denoise_low_spp)},
             "clocks": clocks, "rates": results}
     for s in scenes:
         s.close()
