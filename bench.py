@@ -564,6 +564,8 @@ def run_serve(a):
                 ctx.denoise_device(j[2], j[3], planes.data_ptr(), img.data_ptr())
             else:
                 s.trace_device(params(j, k), j[4], img.data_ptr())
+            if recs[k] is not None:                     # (the scene as it was, for the jobs that follow)
+                s.move_instances(originals[j[1]], 0)
             ctx.sync()
             lat_p.append(L.native.clock_ms() - (t0 + j[0] * 1e3))
             if rate == float(a.rates.split(",")[0]) and k < 6:
