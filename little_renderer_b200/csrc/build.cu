@@ -124,10 +124,11 @@ __device__ __forceinline__ T block_excl_scan(T v, T *s_warp, T &total) {
 }
 
 // ---- onesweep radix sort ---------------------------------------------------------------------
-constexpr int OS_THREADS = 256;
+constexpr int OS_THREADS = 512;                     // (the first 256 threads also own one digit each)
 constexpr int OS_WARPS = OS_THREADS / 32;
 constexpr int OS_ITEMS = 16;
-constexpr int OS_TILE = OS_THREADS * OS_ITEMS;      // 4096 keys per tile
+constexpr int OS_TILE = OS_THREADS * OS_ITEMS;      // 8192 keys per tile
+constexpr int OS_MINB = 2;                          // blocks per SM (64 registers a thread)
 constexpr uint32_t FLAG_AGG = 1u << 30, FLAG_PRE = 2u << 30, VAL_MASK = (1u << 30) - 1;
 
 template <typename K>
@@ -152,7 +153,7 @@ __device__ __forceinline__ void st_volatile(uint32_t *p, uint32_t v) { *(volatil
 // digit's global offset: the tiles before it (decoupled look-back over posted counts / prefixes)
 // plus the digits before it (the pass's histogram).
 template <typename K, bool FIRST>
-__global__ void __launch_bounds__(OS_THREADS, 4) onesweep_kernel(const K *__restrict__ keys_in,
+__global__ void __launch_bounds__(OS_THREADS, OS_MINB) onesweep_kernel(const K *__restrict__ keys_in,
                                                                  const uint32_t *__restrict__ vals_in,
                                                                  K *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                  uint32_t n, int shift, const uint32_t *__restrict__ hist,
@@ -198,18 +199,23 @@ __global__ void __launch_bounds__(OS_THREADS, 4) onesweep_kernel(const K *__rest
     for (int k = 0; k < OS_ITEMS; k++)
         rank[k] = (__shfl_sync(0xffffffffu, rank[k], (rank[k] >> 16) & 31u) & 0xffffu) + (rank[k] >> 24);
     __syncthreads();
-    // this thread's digit: the warps' offsets, the tile's count - posted at once for the tiles after
-    const uint32_t d = tid;
+    // this thread's digit (the first 256 threads): the warps' offsets, the tile's count - posted at
+    // once for the tiles after
+    const bool dig = tid < 256;
+    const uint32_t d = dig ? (uint32_t)tid : 0u;
     uint32_t count = 0;
+    if (dig) {
 #pragma unroll
-    for (int ww = 0; ww < OS_WARPS; ww++) {
-        uint32_t c = S.warp_hist[ww][d];
-        S.warp_hist[ww][d] = count;
-        count += c;
+        for (int ww = 0; ww < OS_WARPS; ww++) {
+            uint32_t c = S.warp_hist[ww][d];
+            S.warp_hist[ww][d] = count;
+            count += c;
+        }
+        if (tile) st_volatile(&status[(size_t)tile * 256 + d], FLAG_AGG | count);
     }
-    if (tile) st_volatile(&status[(size_t)tile * 256 + d], FLAG_AGG | count);
     uint32_t tot;
-    S.digit_start[d] = block_excl_scan<OS_THREADS>(count, S.scan, tot);
+    const uint32_t dstart = block_excl_scan<OS_THREADS>(count, S.scan, tot);
+    if (dig) S.digit_start[d] = dstart;
     __syncthreads();
     // stage the tile in digit order (stable: warp, then item, then lane order)
 #pragma unroll
@@ -223,11 +229,11 @@ __global__ void __launch_bounds__(OS_THREADS, 4) onesweep_kernel(const K *__rest
         }
     }
     // decoupled look-back: tile t's prefix of digit d over the tiles before it
-    uint32_t excl;
+    uint32_t excl = 0;
     if (tile == 0) {
-        excl = block_excl_scan<OS_THREADS>(hist[d], S.scan, tot);   // the digits before d, all keys
-        st_volatile(&status[d], FLAG_PRE | (excl + count));
-    } else {
+        excl = block_excl_scan<OS_THREADS>(dig ? hist[d] : 0u, S.scan, tot);   // the digits before d, all keys
+        if (dig) st_volatile(&status[d], FLAG_PRE | (excl + count));
+    } else if (dig) {
         excl = 0;
         // the tiles before, nearest first, LB_WIDE statuses read at once (independent loads): their
         // counts summed up to the first inclusive prefix; a status not yet posted is waited for
@@ -255,7 +261,7 @@ __global__ void __launch_bounds__(OS_THREADS, 4) onesweep_kernel(const K *__rest
         }
         st_volatile(&status[(size_t)tile * 256 + d], FLAG_PRE | (excl + count));
     }
-    S.global_excl[d] = excl;
+    if (dig) S.global_excl[d] = excl;
     __syncthreads();
     for (uint32_t i = tid; i < in_tile; i += OS_THREADS) {
         K kk = S.key_stage[i];
