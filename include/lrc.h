@@ -206,6 +206,8 @@ typedef struct {
     const uint32_t *rgba;        /* w x h texels r | g << 8 | b << 16 | a << 24, rows top to bottom */
 } lrc_texmap;
 int lrc_scene_set_texmaps(lrc_scene *s, const lrc_texmap *t, uint32_t n);
+/* the sRGB decoding table the texmaps use (texmap_srgb_table, texture.c:64-73), host only */
+void lrc_srgb_table(float *out256);
 /* The world triangles' texture coordinates (Triangle.t, Scene.uvs / .tangents): tri_uv 3 indices
  * per triangle into uvs (2 floats each) and tangents (xyz + handedness w), -1 none (the triangle's
  * barycentrics then, as tri_texcoords' fallback). ntris must be the scene's triangle count when it
@@ -229,6 +231,10 @@ typedef struct {
     const float *density;        /* nx * ny * nz values >= 0, x fastest: index (z * ny + y) * nx + x */
 } lrc_volume;
 int lrc_scene_set_volumes(lrc_scene *s, const lrc_volume *v, uint32_t n);
+/* The majorants lrc_scene_set_volumes derives for a volume, on the host (volume_update,
+ * volume.c:47-108): the largest density, the active box (lo xyz, hi xyz) and the 8^3-voxel bricks'
+ * maxima (ceil(nx/8) x ceil(ny/8) x ceil(nz/8), x fastest; NULL: not wanted). */
+int lrc_volume_majorants(const lrc_volume *v, float *max_density, float *active6, float *brick_max);
 /* The sky (Env, env.h:29-53; upload_sky, trace_gpu.c:1522-1569): w x h linear RGB, rows top to
  * bottom, times scale; its sampling tables (marg: h + 1 floats, cond: h x (w + 1), prob: w x h =
  * env_pixel_prob) or NULL: made here as env_prepare makes them (env.c:116-167, 341-363). Host.

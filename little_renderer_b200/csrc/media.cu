@@ -107,6 +107,20 @@ bool valid(const lrc_volume &v) {
 
 extern "C" {
 
+int lrc_volume_majorants(const lrc_volume *v, float *max_density, float *active6, float *brick_max) {
+    if (!v || !max_density || !active6 || !valid(*v)) return LRC_E_INVALID;
+    lrc::VolDev d{};
+    std::vector<float> bricks;
+    derive(*v, d, bricks);
+    *max_density = d.max_density;
+    for (int a = 0; a < 3; a++) {
+        active6[a] = d.alo[a];
+        active6[3 + a] = d.ahi[a];
+    }
+    if (brick_max) std::memcpy(brick_max, bricks.data(), bricks.size() * 4);
+    return LRC_OK;
+}
+
 int lrc_scene_set_volumes(lrc_scene *s, const lrc_volume *vols, uint32_t n) {
     if (!s || n > (uint32_t)lrc::kMaxVolumes || (n && !vols)) return LRC_E_INVALID;
     lrc_ctx *c = s->ctx;

@@ -10,6 +10,17 @@ using namespace lrcapi;
 
 extern "C" {
 
+void lrc_srgb_table(float *out256) {
+    // the sRGB curve per byte as the float build computes it: its constants are single precision
+    // (-fsingle-precision-constant), i / 255 a float division, the rest in double
+    for (int i = 0; i < 256; i++) {
+        const double v = (double)((float)i / 255.0f);
+        const double lim = (double)0.04045f, slope = (double)12.92f, a = (double)0.055f, b = (double)1.055f,
+                     gamma = (double)2.4f;
+        out256[i] = (float)(v <= lim ? v / slope : std::pow((v + a) / b, gamma));
+    }
+}
+
 int lrc_scene_set_texmaps(lrc_scene *s, const lrc_texmap *t, uint32_t n) {
     if (!s || n > 255 || (n && !t)) return LRC_E_INVALID;
     lrc_ctx *c = s->ctx;
@@ -40,12 +51,7 @@ int lrc_scene_set_texmaps(lrc_scene *s, const lrc_texmap *t, uint32_t n) {
     // the sRGB curve per byte as the float build computes it: its constants are single precision
     // (-fsingle-precision-constant), i / 255 a float division, the rest in double
     float lut[256];
-    for (int i = 0; i < 256; i++) {
-        const double v = (double)((float)i / 255.0f);
-        const double lim = (double)0.04045f, slope = (double)12.92f, a = (double)0.055f, b = (double)1.055f,
-                     gamma = (double)2.4f;
-        lut[i] = (float)(v <= lim ? v / slope : std::pow((v + a) / b, gamma));
-    }
+    lrc_srgb_table(lut);
     const size_t tb = al(table.size() * 4), lb = al(256 * 4);
     e = cudaMalloc(&s->d_tex, tb + lb + texels * 4);
     char *base = static_cast<char *>(s->d_tex);

@@ -102,6 +102,8 @@ def lib():
     L.lrc_guide.argtypes = [vp, vp, vp, C.c_uint]
     L.lrc_reproject.argtypes = [vp, vp, vp, vp, vp, C.c_int32, C.c_uint]
     L.lrc_scene_set_volumes.argtypes = [vp, vp, u32]
+    L.lrc_volume_majorants.argtypes = [vp, vp, vp, vp]
+    L.lrc_srgb_table.argtypes = [vp]
     L.lrc_scene_set_texmaps.argtypes = [vp, vp, u32]
     L.lrc_scene_set_texcoords.argtypes = [vp, vp, u32, vp, vp, u32]
     L.lrc_denoise.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp, C.c_uint]
@@ -182,6 +184,32 @@ def trace_params(cam12, width, height, max_depth=8, mis=1, sampler=1, exact=0, s
     p.width, p.height, p.max_depth, p.mis, p.sampler, p.exact, p.seed, p.clamp, p.skip_caustics = (
         width, height, max_depth, mis, sampler, exact, seed, clamp, skip_caustics)
     return p
+
+
+def volume_majorants(density, lo, hi):
+    """lrc_volume_majorants (host): (largest density, active box (6,), brick maxima (bz, by, bx))."""
+    den = np.ascontiguousarray(density, np.float32)
+    v = Volume()
+    v.nz, v.ny, v.nx = den.shape
+    v.lo[:] = list(map(float, lo))
+    v.hi[:] = list(map(float, hi))
+    v.sigma_t, v.g = 0.1, 0.0
+    v.albedo[:] = [1.0, 1.0, 1.0]
+    v.density = den.ctypes.data
+    mx = np.zeros(1, np.float32)
+    act = np.zeros(6, np.float32)
+    b = [(n + 7) // 8 for n in den.shape]
+    bricks = np.zeros(b, np.float32)
+    rc = lib().lrc_volume_majorants(C.byref(v), _ptr(mx), _ptr(act), _ptr(bricks))
+    if rc:
+        raise LrcError(rc, "lrc_volume_majorants")
+    return float(mx[0]), act, bricks
+
+
+def srgb_table():
+    out = np.zeros(256, np.float32)
+    lib().lrc_srgb_table(_ptr(out))
+    return out
 
 
 def sky_tables(rgb):

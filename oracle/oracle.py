@@ -193,6 +193,8 @@ def ref_lib(double=False):
         lib.rb_occluded.argtypes = [vp, _f32p, _f32p, C.c_longlong, C.c_float, C.c_float, _i32p]
         lib.rb_trace_image.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        lib.rb_volume_majorants.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, _f32p]
+        lib.rb_srgb_table.argtypes = [_f32p]
         lib.rb_add_texmap.argtypes = [vp, _u32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         lib.rb_material_textures.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                              C.c_float]

@@ -180,6 +180,24 @@ void rb_set_texcoords(void *sp, const int *tri_uv, int ntris, const float *uvs, 
         for (int k = 0; k < 3; k++) s->tris[i].t[k] = tri_uv[3 * i + k];
 }
 
+// a volume's majorants as volume_update makes them (volume_create + the density + volume_update):
+// the largest density, the active box (lo, hi) and the bricks' maxima
+void rb_volume_majorants(int nx, int ny, int nz, const float *box6, const float *density, float *max_density,
+                         float *active6, float *brick_max){
+    Aabb b = {v3f(box6), v3f(box6 + 3)};
+    Volume *v = volume_create(nx, ny, nz, b);
+    if (!v) return;
+    memcpy(v->density, density, sizeof(float) * (size_t)nx * ny * nz);
+    volume_update(v);
+    *max_density = (float)v->max_density;
+    active6[0] = (float)v->active.lo.x; active6[1] = (float)v->active.lo.y; active6[2] = (float)v->active.lo.z;
+    active6[3] = (float)v->active.hi.x; active6[4] = (float)v->active.hi.y; active6[5] = (float)v->active.hi.z;
+    memcpy(brick_max, v->brick_max, sizeof(float) * (size_t)v->bnx * v->bny * v->bnz);
+    volume_free(v);
+}
+// the sRGB table texmap_srgb_table makes
+void rb_srgb_table(float *out){ memcpy(out, texmap_srgb_table(), sizeof(float) * 256); }
+
 // a participating medium: volume_create + the density + its optics + volume_update + scene_add_volume
 // (box6: lo, hi; albedo3; density nz * ny * nx, x fastest). Returns its index or -1.
 int rb_add_volume(void *sp, int nx, int ny, int nz, const float *box6, float sigma_t, const float *albedo3, float g,

@@ -58,3 +58,32 @@ def test_instance_transforms_and_boxes(oracle):
         box, inv = ref.instance_data(i)
         assert np.array_equal(inv, rec[i, 12:24])
         assert np.array_equal(box[:3], rec[i, 24:27]) and np.array_equal(box[3:], rec[i, 28:31])
+
+
+def test_volume_majorants_are_volume_update_s(oracle):
+    """The majorants lrc_scene_set_volumes derives on the host (largest density, active box, brick
+    maxima) equal the reference's volume_update to the bit, for the workloads' cloud and for grids
+    whose sides are not multiples of the 8-voxel brick (delta tracking draws its random numbers per
+    majorant segment, so these must be the reference's)."""
+    lib = oracle.ref_lib()
+    rng = np.random.default_rng(4)
+    grids = [(W.cloud_grid(3), (80.0, 60.0, 80.0), (480.0, 380.0, 480.0)),
+             (np.clip(rng.normal(0.2, 0.5, (13, 21, 10)), 0, None).astype(np.float32), (-1.5, 0.25, 2.0), (3.5, 2.0, 7.25)),
+             (np.zeros((9, 9, 9), np.float32), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0))]
+    for den, lo, hi in grids:
+        mx, act, bricks = L.native.volume_majorants(den, lo, hi)
+        nz, ny, nx = den.shape
+        rmx = np.zeros(1, np.float32)
+        ract = np.zeros(6, np.float32)
+        rbr = np.zeros(bricks.size, np.float32)
+        lib.rb_volume_majorants(nx, ny, nz, np.array([*lo, *hi], np.float32), np.ascontiguousarray(den).reshape(-1), rmx,
+                                ract, rbr)
+        assert mx == rmx[0]
+        assert np.array_equal(act, ract)
+        assert np.array_equal(bricks.reshape(-1), rbr)
+
+
+def test_srgb_table_is_texmap_srgb_table_s(oracle):
+    want = np.zeros(256, np.float32)
+    oracle.ref_lib().rb_srgb_table(want)
+    assert np.array_equal(L.native.srgb_table(), want)
