@@ -305,6 +305,33 @@ int lrc_guide(lrc_scene *s, const lrc_trace_params *p, float *planes, unsigned f
  * 1 of new_planes (cleared where nothing matched). Both images of the same size. */
 int lrc_reproject(lrc_ctx *ctx, const lrc_trace_params *old_cam, const lrc_trace_params *new_cam, const float *old_planes,
                   float *new_planes, int32_t history, unsigned flags);
+/* The same with temporal gradients (A-SVGF; gpu_trace_begin_image with history_max > 0,
+ * trace_gpu.c:2081-2114; trace_reproject.wgsl gmatch, gfilter and main with dims.w = 1;
+ * trace.wgsl main's gradient branch, :1231-1293): each pixel keeps a history of its own, from how
+ * much the light changed where it is.
+ *   - per tile of 4 x 4 new pixels one surface pixel k (the first from a point that moves each
+ *     image) whose place in the old image is an old pixel o that saw the same surface, and o's last
+ *     sample (plane 1's z and w of old_planes: lrc_trace with LRC_TRACE_GUIDED in fast mode keeps
+ *     them);
+ *   - that sample traced again in s (the new scene, new_p's camera) from the same random numbers
+ *     (old_p's seed and sampler, o's stream, its sample number from its low 24 bits and spp0's
+ *     high bits) through k moved by o's offset: lambda = |l - old l| / max(l, old l) of the two
+ *     samples' luminance over the albedo;
+ *   - lambda filtered over the tiles (3 a-trous passes, 1, 2 and 4 tiles apart, weighted by the
+ *     tiles' first pixels' distance and normal);
+ *   - each pixel keeps floor((1 - lambda) / lambda + 1/2) samples' worth of its old ones, at most
+ *     history_max (all where nothing changed, none where a shadow moved); `history` where no tile
+ *     near had a lambda. With LRC_REPROJECT_EDIT (the scene was edited: colours may have changed,
+ *     which lambda does not see) lambda counts 4 times, a surface's samples are kept only where
+ *     its albedo is the same, and lamps, the sky and media keep `history`.
+ * new_planes: planes 2 and 3 made by lrc_guide for new_p; planes 0 and 1 are written. spp0: the
+ * new image's first sample number (sample numbers keep counting from image to image). tiles_out
+ * (optional): per tile (row-major) 4 floats (k, o, the sample's lambda, the filtered lambda), -1
+ * for none. old_p in fast mode (exact = 0); history_max > 0. */
+#define LRC_REPROJECT_EDIT 128u
+int lrc_reproject_gradients(lrc_scene *s, const lrc_trace_params *old_p, const lrc_trace_params *new_p, uint32_t spp0,
+                            const float *old_planes, float *new_planes, int32_t history_max, int32_t history,
+                            float *tiles_out, unsigned flags);
 int lrc_denoise(lrc_ctx *ctx, int32_t width, int32_t height, const float *planes, int32_t passes, float *out,
                 unsigned flags);
 

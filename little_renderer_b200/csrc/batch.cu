@@ -217,7 +217,7 @@ int prepare(lrc_batch *b) {
     }
     b->ntasks = task;
     b->npix = pix;
-    cudaError_t e = reserve(&b->d_part, &b->part_cap, al(task * 16) + al(task * 4) + al(task * 8) + 256);
+    cudaError_t e = reserve(&b->d_part, &b->part_cap, al(task * 16) + al(task * 4) + al(task * 16) + 256);
     if (!e) e = reserve(reinterpret_cast<void **>(&b->d_ctr), &b->ctr_cap, (nj + 1) * 8 + 256);
     if (!e) e = reserve(reinterpret_cast<void **>(&b->d_jobs), &b->jobs_cap, nj * sizeof(lrc::BatchJob) + 256);
     if (!e && b->engine == 1) e = reserve(&b->d_wf, &b->wf_cap, lrc::wf_bytes(b->wf_slots));
@@ -226,7 +226,7 @@ int prepare(lrc_batch *b) {
     char *part = static_cast<char *>(b->d_part);
     float4 *partial = reinterpret_cast<float4 *>(part);
     uint32_t *prays = reinterpret_cast<uint32_t *>(part + al(task * 16));
-    float2 *pmom = reinterpret_cast<float2 *>(part + al(task * 16) + al(task * 4));
+    float4 *pmom = reinterpret_cast<float4 *>(part + al(task * 16) + al(task * 4));
     for (size_t q = 0; q < nj; q++) {
         lrc::BatchJob &T = b->table[q];
         T.partial = partial + T.task0;

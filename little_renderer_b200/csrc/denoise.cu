@@ -332,7 +332,7 @@ __device__ __forceinline__ float4 old_place(const RpCam &oc, const RpCam &nc, in
 // old pixel o saw what the new one sees: samples, the same kind and object, the distance within
 // 2 % (25 % in a medium) plus how fast it changes there, the normal within ~25 degrees
 __device__ __forceinline__ bool same_surface(const float4 *__restrict__ old, int W, int H, uint32_t o, float4 g2, float4 g3,
-                                             float dist) {
+                                             float dist, bool edit) {
     const size_t N = (size_t)W * H;
     if (old[o].w == 0.0f) return false;
     const float4 o3 = old[3 * N + o];
@@ -347,15 +347,37 @@ __device__ __forceinline__ bool same_surface(const float4 *__restrict__ old, int
         if (fabsf(o2.w - dist) > (gk == 2.0f ? 0.25f : 0.02f) * dist + grad) return false;
     }
     if (gk == 0.0f && o2.x * g2.x + o2.y * g2.y + o2.z * g2.z < 0.9f) return false;
+    if (edit && gk == 0.0f) {                       // an edit's: the same colour too
+        const float dm = fmaxf(fabsf(o3.x - g3.x), fmaxf(fabsf(o3.y - g3.y), fabsf(o3.z - g3.z)));
+        if (dm > 0.02f + 0.1f * fmaxf(g3.x, fmaxf(g3.y, g3.z))) return false;
+    }
     return true;
 }
 
+// the history a pixel keeps with temporal gradients: its tile's filtered lambda as (1 - lambda) /
+// lambda samples' worth (A-SVGF's blend), at most hmax; `fallback` where no tile near had a lambda,
+// and with an edit's move (lambda then counted 4 times) for what is not a surface
+__device__ __forceinline__ float grad_history(const GradTile *__restrict__ tiles, int W, uint32_t k, float4 g3, float hmax,
+                                              float fallback, bool edit) {
+    const uint32_t tw = ((uint32_t)W + GRAD_TILE - 1) / GRAD_TILE;
+    const uint32_t x = k % (uint32_t)W, y = k / (uint32_t)W;
+    const float lam = tiles[(y / GRAD_TILE) * tw + x / GRAD_TILE].lam[3];
+    if (edit && gkind(g3.w) != 0.0f) return fallback;
+    if (!(lam >= 0.0f)) return fallback;
+    const float l = edit ? lam * 4.0f : lam;
+    return fminf(floorf((1.0f - fminf(l, 1.0f)) / fmaxf(l, 1e-3f) + 0.5f), hmax);
+}
+
+// tiles: null without temporal gradients (history for every pixel), else each pixel's history from
+// its tile's lambda (grad_history, history the most)
 __global__ void __launch_bounds__(256) reproject_kernel(RpCam oc, RpCam nc, int W, int H, float history,
-                                                        const float4 *__restrict__ old, float4 *__restrict__ cur) {
+                                                        const float4 *__restrict__ old, float4 *__restrict__ cur,
+                                                        const GradTile *__restrict__ tiles, float fallback, bool edit) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t N = (size_t)W * H;
     if (k >= N) return;
     const float4 g2 = cur[2 * N + k], g3 = cur[3 * N + k];
+    if (tiles) history = grad_history(tiles, W, k, g3, history, fallback, edit);
     const float4 at = old_place(oc, nc, W, H, k, g2);
     float4 a0 = make_float4(0, 0, 0, 0), a1 = make_float4(0, 0, 0, 0);
     float nsum = 0.0f, wsum = 0.0f;
@@ -365,7 +387,7 @@ __global__ void __launch_bounds__(256) reproject_kernel(RpCam oc, RpCam nc, int 
             const float tx = x0 + (float)(j & 1), ty = y0 + (float)(j >> 1);
             if (tx < 0.0f || ty < 0.0f || tx >= (float)W || ty >= (float)H) continue;
             const uint32_t o = (uint32_t)ty * (uint32_t)W + (uint32_t)tx;
-            if (!same_surface(old, W, H, o, g2, g3, at.z)) continue;
+            if (!same_surface(old, W, H, o, g2, g3, at.z, edit)) continue;
             const float4 s = old[o], m = old[N + o];
             const float w = (1.0f - fabsf(at.x - tx)) * (1.0f - fabsf(at.y - ty));
             const float ws = w / s.w;
@@ -383,6 +405,103 @@ __global__ void __launch_bounds__(256) reproject_kernel(RpCam oc, RpCam nc, int 
     const float n = fminf(nsum / wsum, history);
     cur[k] = make_float4(a0.x / wsum * n, a0.y / wsum * n, a0.z / wsum * n, n);
     cur[N + k] = make_float4(a1.x / wsum * n, a1.y / wsum * n, 0.0f, 0.0f);
+}
+
+// the tiles for the caller: (new pixel, old pixel, the sample's lambda, the filtered lambda)
+__global__ void grad_out_kernel(const GradTile *__restrict__ tiles, uint32_t n, float4 *__restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const GradTile T = tiles[t];
+    out[t] = make_float4((float)T.k, (float)T.o, T.lam[0], T.lam[3]);
+}
+
+__device__ __forceinline__ uint32_t hashr(uint32_t x) {     // lowbias32
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+// gmatch: one thread per tile. Its pixels from a different first one each image (`next`: the new
+// image's first sample number): the first surface pixel whose place in the old image lies in an
+// old pixel that saw the same surface and has a last sample; that sample's number from its low 24
+// bits (plane 1's w) and the high bits of `next`
+__global__ void __launch_bounds__(128) gmatch_kernel(RpCam oc, RpCam nc, int W, int H, uint32_t next, bool edit,
+                                                     const float4 *__restrict__ old, const float4 *__restrict__ cur,
+                                                     GradTile *__restrict__ tiles) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t tw = ((uint32_t)W + GRAD_TILE - 1) / GRAD_TILE, th = ((uint32_t)H + GRAD_TILE - 1) / GRAD_TILE;
+    if (t >= tw * th) return;
+    const size_t N = (size_t)W * H;
+    const uint32_t tx = t % tw, ty = t / tw;
+    constexpr uint32_t TT = GRAD_TILE * GRAD_TILE;
+    const uint32_t first = hashr(t ^ hashr(next)) % TT;
+    GradTile T;
+    T.k = T.o = -1;
+    T.dx = T.dy = T.l = 0.0f;
+    T.kk = 0;
+    for (uint32_t i = 0; i < TT; i++) {
+        const uint32_t c = (first + i) % TT;
+        const uint32_t px = tx * GRAD_TILE + c % GRAD_TILE, py = ty * GRAD_TILE + c / GRAD_TILE;
+        if (px >= (uint32_t)W || py >= (uint32_t)H) continue;
+        const uint32_t k = py * (uint32_t)W + px;
+        const float4 g2 = cur[2 * N + k], g3 = cur[3 * N + k];
+        if (gkind(g3.w) != 0.0f) continue;                       // a surface only
+        const float4 at = old_place(oc, nc, W, H, k, g2);
+        if (at.w <= 0.0f) continue;
+        const float ox = floorf(at.x + 0.5f), oy = floorf(at.y + 0.5f);
+        if (ox < 0.0f || oy < 0.0f || ox >= (float)W || oy >= (float)H) continue;
+        const uint32_t o = (uint32_t)oy * (uint32_t)W + (uint32_t)ox;
+        const float4 last = old[N + o];
+        if (last.w < 0.5f || !same_surface(old, W, H, o, g2, g3, at.z, edit)) continue;
+        const uint32_t lo = (uint32_t)last.w - 1u;
+        uint32_t cnt = (next & 0xff000000u) | lo;
+        if (cnt > next) cnt -= 0x1000000u;
+        T.k = (int32_t)k;
+        T.o = (int32_t)o;
+        T.dx = ox - at.x;
+        T.dy = oy - at.y;
+        T.l = last.z;
+        T.kk = cnt;
+        break;
+    }
+    for (int q = 0; q < 4; q++) T.lam[q] = -1.0f;
+    tiles[t] = T;
+}
+
+// gfilter pass `pass` (0, 1, 2): lam[pass] of the tiles 1, 2, 4 tiles apart (3 x 3, B-spline-like
+// weights) weighted by the anchors' (each tile's first pixel's) distance and normal into
+// lam[pass + 1]; -1 where no tile near had one
+__global__ void __launch_bounds__(128) gfilter_kernel(int W, int H, int pass, const float4 *__restrict__ cur,
+                                                      GradTile *__restrict__ tiles) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tw = (W + GRAD_TILE - 1) / GRAD_TILE, th = (H + GRAD_TILE - 1) / GRAD_TILE;
+    if (t >= (uint32_t)(tw * th)) return;
+    const size_t N = (size_t)W * H;
+    const int tx = (int)(t % (uint32_t)tw), ty = (int)(t / (uint32_t)tw);
+    const int step = 1 << pass;
+    const float4 ga = cur[2 * N + (size_t)ty * GRAD_TILE * W + tx * GRAD_TILE];
+    float sum = 0.0f, wsum = 0.0f;
+    for (int dy = -1; dy <= 1; dy++) {
+        for (int dx = -1; dx <= 1; dx++) {
+            const int bx = tx + dx * step, by = ty + dy * step;
+            if (bx < 0 || by < 0 || bx >= tw || by >= th) continue;
+            const float lam = tiles[by * tw + bx].lam[pass];
+            if (lam < 0.0f) continue;
+            const float4 gb = cur[2 * N + (size_t)by * GRAD_TILE * W + bx * GRAD_TILE];
+            float w = (dx == 0 ? 1.0f : 0.5f) * (dy == 0 ? 1.0f : 0.5f);
+            if (ga.w < 1e29f && gb.w < 1e29f) {
+                float nd = fmaxf(ga.x * gb.x + ga.y * gb.y + ga.z * gb.z, 0.0f);
+                nd *= nd;
+                nd *= nd;
+                nd *= nd;
+                w *= expf(-fabsf(ga.w - gb.w) / (0.05f * ga.w + 1e-3f)) * nd;
+            }
+            sum += w * lam;
+            wsum += w;
+        }
+    }
+    tiles[t].lam[pass + 1] = wsum > 1e-4f ? sum / wsum : -1.0f;
 }
 
 }  // namespace dn
@@ -487,11 +606,92 @@ int lrc_reproject(lrc_ctx *c, const lrc_trace_params *old_cam, const lrc_trace_p
     }
     if (!e) {
         lrc::dn::reproject_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>(rp_cam(old_cam), rp_cam(new_cam), W, H,
-                                                                                  (float)history, d_old, d_new);
+                                                                                  (float)history, d_old, d_new, nullptr,
+                                                                                  0.0f, false);
         e = cudaGetLastError();
     }
     if (!e && !(flags & LRC_DEVICE)) e = cudaMemcpyAsync(new_planes, d_new, N * 32, cudaMemcpyDeviceToHost, c->st);
     if (e) return cuda_status(c, e, "lrc_reproject");
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_reproject_gradients(lrc_scene *s, const lrc_trace_params *old_p, const lrc_trace_params *new_p, uint32_t spp0,
+                            const float *old_planes, float *new_planes, int32_t history_max, int32_t history,
+                            float *tiles_out, unsigned flags) {
+    if (!s || !old_p || !new_p || !old_planes || !new_planes || history_max <= 0 || history < 0) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    const int W = new_p->width, H = new_p->height;
+    if (W <= 0 || H <= 0 || old_p->width != W || old_p->height != H)
+        return fail(c, LRC_E_INVALID, "reprojection: both images of the same size");
+    if ((uint64_t)W * (uint64_t)H >= (1ull << 31)) return fail(c, LRC_E_INVALID, "image too large (2^31 pixels)");
+    if (old_p->exact)
+        return fail(c, LRC_E_INVALID, "temporal gradients trace a sample again: the old image in fast mode (exact = 0)");
+    if (!s->built_n && !s->tlas_n) return fail(c, LRC_E_INVALID, "the scene has nothing built (lrc_scene_build)");
+    if (s->ninst && s->tlas_n != s->ninst) return fail(c, LRC_E_INVALID, "instances changed: lrc_scene_build_instances");
+    if (!s->d_mats || !s->nmats) return fail(c, LRC_E_INVALID, "the scene has no materials (lrc_scene_set_materials)");
+    if (s->light >= (int32_t)s->nprims) return fail(c, LRC_E_INVALID, "the light is not one of the primitives");
+    DeviceGuard g(c->device);
+    if (!s->tables) {
+        int rc = lrc_scene_set_tables(s, nullptr, nullptr);
+        if (rc) return rc;
+    }
+    const size_t N = (size_t)W * H;
+    const uint32_t ntiles = (uint32_t)(((W + lrc::GRAD_TILE - 1) / lrc::GRAD_TILE) *
+                                       (size_t)((H + lrc::GRAD_TILE - 1) / lrc::GRAD_TILE));
+    const float4 *d_old = reinterpret_cast<const float4 *>(old_planes);
+    float4 *d_new = reinterpret_cast<float4 *>(new_planes);
+    float4 *d_tout = reinterpret_cast<float4 *>(tiles_out);
+    const size_t tile_bytes = ((size_t)ntiles * sizeof(lrc::GradTile) + 255) / 256 * 256;
+    cudaError_t e = reserve(&c->dn, &c->dn_cap, tile_bytes + (size_t)ntiles * 16 + 256);
+    if (e) return cuda_status(c, e, "gradient tiles");
+    lrc::GradTile *d_tiles = static_cast<lrc::GradTile *>(c->dn);
+    if (!(flags & LRC_DEVICE)) {
+        e = reserve(&c->stage, &c->stage_cap, N * 128);
+        float4 *st = static_cast<float4 *>(c->stage);
+        if (!e) e = cudaMemcpyAsync(st, old_planes, N * 64, cudaMemcpyHostToDevice, c->st);
+        if (!e) e = cudaMemcpyAsync(st + 4 * N, new_planes, N * 64, cudaMemcpyHostToDevice, c->st);
+        d_old = st;
+        d_new = st + 4 * N;
+        d_tout = reinterpret_cast<float4 *>(static_cast<char *>(c->dn) + tile_bytes);
+    }
+    if (!e && !s->d_rays) e = cudaMalloc(&s->d_rays, 256);
+    if (!e) e = cudaMemsetAsync(s->d_rays, 0, 8, c->st);
+    if (e) return cuda_status(c, e, "lrc_reproject_gradients");
+    // the gradient samples' parameters: the new camera and scene, the old image's random numbers
+    lrc::PtParams P{};
+    P.W = W; P.H = H; P.y0 = 0; P.rows = H; P.spp0 = (int)spp0; P.spp = 1; P.group = 1; P.exact = 0;
+    P.max_depth = new_p->max_depth; P.mis = new_p->mis; P.sampler_on = old_p->sampler;
+    P.seed = old_p->seed;
+    P.clamp = new_p->clamp;
+    P.skip_caustics = new_p->skip_caustics != 0;
+    P.origin = {new_p->origin[0], new_p->origin[1], new_p->origin[2]};
+    P.upper_left = {new_p->upper_left[0], new_p->upper_left[1], new_p->upper_left[2]};
+    P.horizontal = {new_p->horizontal[0], new_p->horizontal[1], new_p->horizontal[2]};
+    P.vertical = {new_p->vertical[0], new_p->vertical[1], new_p->vertical[2]};
+    const bool edit = (flags & LRC_REPROJECT_EDIT) != 0;
+    const lrc::dn::RpCam oc = rp_cam(old_p), nc = rp_cam(new_p);
+    c->timer.begin(LRC_TS_SHADE, c->st);
+    lrc::dn::gmatch_kernel<<<(ntiles + 127) / 128, 128, 0, c->st>>>(oc, nc, W, H, spp0, edit, d_old, d_new, d_tiles);
+    e = cudaGetLastError();
+    if (!e) e = lrc::pt_gradients(pt_scene(s), P, d_tiles, ntiles, d_new + 3 * N, s->d_rays, c->d_status, c->st);
+    for (int pass = 0; pass < 3 && !e; pass++) {
+        lrc::dn::gfilter_kernel<<<(ntiles + 127) / 128, 128, 0, c->st>>>(W, H, pass, d_new, d_tiles);
+        e = cudaGetLastError();
+    }
+    if (!e) {
+        lrc::dn::reproject_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>(oc, nc, W, H, (float)history_max, d_old,
+                                                                                  d_new, d_tiles, (float)history, edit);
+        e = cudaGetLastError();
+    }
+    if (!e && tiles_out) {
+        lrc::dn::grad_out_kernel<<<(ntiles + 127) / 128, 128, 0, c->st>>>(d_tiles, ntiles, d_tout);
+        e = cudaGetLastError();
+    }
+    c->timer.end(c->st);
+    if (!e && !(flags & LRC_DEVICE)) e = cudaMemcpyAsync(new_planes, d_new, N * 32, cudaMemcpyDeviceToHost, c->st);
+    if (!e && tiles_out && !(flags & LRC_DEVICE))
+        e = cudaMemcpyAsync(tiles_out, d_tout, (size_t)ntiles * 16, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_reproject_gradients");
     return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 

@@ -228,10 +228,25 @@ struct PtParams {
     pt::V3 origin, upper_left, horizontal, vertical;   // the Camera (camera.h)
     int skip_caustics;                                 // TraceParams.skip_caustics
     // the denoiser's planes (lrc_trace with LRC_TRACE_GUIDED; null: none): each sample's luminance
-    // over the guide's albedo (plane 3) added to the moments (plane 1) as (l, l^2)
+    // over the guide's albedo (plane 3) added to the moments (plane 1) as (l, l^2), and the last
+    // sample's l and number in its z and w
     float4 *moments;
     const float4 *guide;
 };
+// temporal gradients (trace_reproject.wgsl gmatch / gfilter, trace.wgsl main's gradient branch):
+// one gradient sample per tile of GRAD_TILE x GRAD_TILE new pixels, row-major tiles
+constexpr int GRAD_TILE = 4;
+struct GradTile {
+    int32_t k, o;      // the new pixel the sample is for; the old pixel it was taken in (-1: no sample)
+    float dx, dy;      // the old pixel's offset from where the new pixel's centre was in the old image
+    float l;           // the old sample's luminance over the albedo
+    uint32_t kk;       // its sample number
+    float lam[4];      // lambda = |new - old| / max(new, old): the sample's, then after each of the
+                       // filter's 3 passes (-1: none)
+};
+// each tile's gradient sample traced in the scene of P (P.seed: the old image's), lam[0] set
+cudaError_t pt_gradients(const PtScene &S, const PtParams &P, GradTile *d_tiles, uint32_t ntiles, const float4 *d_guide,
+                         unsigned long long *d_rays, uint32_t *d_status, cudaStream_t st);
 cudaError_t pt_prim_boxes(const float *d_prims, uint32_t n, float *d_boxes, cudaStream_t st);
 cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsigned long long *d_rays, uint32_t *d_status,
                      cudaStream_t st);
@@ -267,7 +282,7 @@ struct BatchJob {
     unsigned long long pix0;            // its first pixel among all the batch's bands (resolve pass)
     float4 *partial;                    // ntasks (sum rgb, samples)
     uint32_t *prays;                    // ntasks ray counts
-    float2 *pmom;                       // ntasks luminance moments (a guided job: P.moments), or null
+    float4 *pmom;                       // ntasks (sum l, sum l^2, the last sample's l, 0) (a guided job), or null
     float4 *accum;                      // the image (W x H)
     unsigned long long *rays;           // the job's ray count (added to)
 };
@@ -293,7 +308,7 @@ struct WfState {
     uint32_t *flags;            // F_PATH, F_ENDED and the Nee flags of the bounce just shaded
     uint2 *xy;                  // the task's pixel
     float4 *sum;                // the task's sum so far (rgb, samples)
-    float2 *mom;                // its luminance moments so far (guided jobs)
+    float4 *mom;                // its luminance moments so far and its last sample's (guided jobs)
     float4 *ro;                 // the path's ray origin, bounce_pdf
     float4 *rd;                 // its direction, depth | emit << 16 | caus << 24 (int bits)
     float4 *thr;                // its throughput

@@ -23,6 +23,12 @@
 namespace lrc {
 namespace pt {
 
+// plane 1's w after a guided call: its last sample's number (low 24 bits) + 1, as trace.wgsl keeps
+// it for the temporal gradients (trace.wgsl:1306-1310)
+__device__ __forceinline__ float last_sample_tag(const PtParams &P) {
+    return (float)((((uint32_t)(P.spp0 + P.spp - 1)) & 0xffffffu) + 1u);
+}
+
 // exact mode: one thread per pixel of rows [y0, y0 + rows), samples [0, spp) in order from the
 // CPU's per-pixel stream (trace_image, tracer.c:337-353)
 template <bool MEDIA, bool GUIDED>
@@ -37,7 +43,7 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
         Rng rng;
         rng_seed(rng, 0x853c49e6748fea9bull ^ (pixel * 0x9E3779B97F4A7C15ull) ^ (P.seed * 0xD1B54A32D192ED03ull), pixel);
         V3 sum = v3(0, 0, 0);
-        float ml = 0.0f, ml2 = 0.0f;
+        float ml = 0.0f, ml2 = 0.0f, l_last = 0.0f;
         for (int k = 0; k < P.spp; k++) {
             Sampler sm{&rng, (uint32_t)k, (uint32_t)P.seed * 0x9e3779b9u, (int)x, (int)y, P.sampler_on, S.mask};
             float jx, jy;
@@ -46,20 +52,24 @@ __global__ void __launch_bounds__(128) exact_kernel(PtScene S, PtParams P, float
             V3 o, d;
             camera_ray(P, u, v, o, d);
             V3 c = trace_path<MEDIA>(S, P, o, d, sm, err, rays);
-            if (!is_number(c)) continue;
+            if (!is_number(c)) {
+                if (GUIDED) l_last = 0.0f;           // (a dropped sample counts as black)
+                continue;
+            }
             c = clamp_sample(c, P.clamp);
             sum = vadd(sum, c);
             if (GUIDED) {
                 const float l = sample_luma(c, P.guide[pixel]);
                 ml += l;
                 ml2 += l * l;
+                l_last = l;
             }
         }
         float4 a = accum[pixel];
         accum[pixel] = make_float4(a.x + sum.x, a.y + sum.y, a.z + sum.z, a.w + (float)P.spp);
-        if (GUIDED) {
+        if (GUIDED) {                                // (z, w: the last sample's luminance and number + 1)
             const float4 m = P.moments[pixel];
-            P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, m.z, m.w);
+            P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, l_last, last_sample_tag(P));
         }
     }
     if (ray_count) {
@@ -82,7 +92,7 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
     const uint64_t npix = (uint64_t)P.W * P.rows;
     uint32_t rays = 0;
     V3 c = v3(0, 0, 0);
-    float cnt = 0.0f, ml = 0.0f, ml2 = 0.0f;
+    float cnt = 0.0f, ml = 0.0f, ml2 = 0.0f, l_last = 0.0f;
     const bool live = pix_local < npix;
     uint64_t pixel = 0;
     if (live) {
@@ -106,9 +116,12 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
                 const float l = sample_luma(s, P.guide[pixel]);
                 ml += l;
                 ml2 += l * l;
+                l_last = l;
             }
         }
     }
+    // (the pixel's last sample, spp0 + spp - 1, is lane (spp - 1) % g's last)
+    if (GUIDED) l_last = __shfl_sync(0xffffffffu, l_last, (uint32_t)(P.spp - 1) % g, g);
     for (uint32_t o = 1; o < g; o <<= 1) {               // fixed-order tree sum over the group
         c.x += __shfl_down_sync(0xffffffffu, c.x, o, g);
         c.y += __shfl_down_sync(0xffffffffu, c.y, o, g);
@@ -122,9 +135,9 @@ __global__ void __launch_bounds__(128) fast_kernel(PtScene S, PtParams P, float4
     if (live && lane_s == 0) {
         float4 a = accum[pixel];
         accum[pixel] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + cnt);
-        if (GUIDED) {
+        if (GUIDED) {                                // (z, w: the last sample's luminance and number + 1)
             const float4 m = P.moments[pixel];
-            P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, m.z, m.w);
+            P.moments[pixel] = make_float4(m.x + ml, m.y + ml2, l_last, last_sample_tag(P));
         }
     }
     if (ray_count) {
@@ -152,7 +165,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
     uint64_t pixel = 0;               // the pixel's index in its image
     uint32_t x = 0, y = 0, slot = 0, kk = 0, kend = 0, g = 1, rays = 0;
     V3 c = v3(0, 0, 0);
-    float cnt = 0.0f, ml = 0.0f, ml2 = 0.0f;   // the task's sum, samples, luminance moments
+    float cnt = 0.0f, ml = 0.0f, ml2 = 0.0f, l_last = 0.0f;   // the task's sum, samples, luminance moments
     bool active = false, done = false;
     PathState ps;
     Rng rng;
@@ -164,7 +177,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
             const unsigned long long l = task - J.task0;
             J.partial[l] = make_float4(c.x, c.y, c.z, cnt);
             J.prays[l] = rays;
-            if (J.pmom) J.pmom[l] = make_float2(ml, ml2);
+            if (J.pmom) J.pmom[l] = make_float4(ml, ml2, l_last, 0.0f);
             j = -1;
         }
         const bool need = !done && j < 0;
@@ -192,7 +205,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
                     kend = (uint32_t)(J.P.spp0 + J.P.spp);
                     c = v3(0, 0, 0);
                     cnt = 0.0f;
-                    ml = ml2 = 0.0f;
+                    ml = ml2 = l_last = 0.0f;
                     rays = 0;
                     if (J.P.exact)                    // trace_image's per-pixel stream, all samples in order
                         rng_seed(rng, 0x853c49e6748fea9bull ^ (pixel * 0x9E3779B97F4A7C15ull) ^ (J.P.seed * 0xD1B54A32D192ED03ull),
@@ -223,6 +236,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
                 const float l = sample_luma(s, J.P.guide[pixel]);
                 ml += l;
                 ml2 += l * l;
+                l_last = l;
             }
             active = false;
             kk += g;
@@ -268,10 +282,13 @@ __global__ void __launch_bounds__(128) batch_resolve_kernel(const BatchJob *__re
         float4 *a = J.accum + pixel;
         float4 av = *a;
         *a = make_float4(av.x + v[0].x, av.y + v[0].y, av.z + v[0].z, av.w + v[0].w);
-        if (J.pmom) {                                // the moments, in the same order
-            float2 mv[16];
+        if (J.pmom) {                                // the moments, in the same order; the last sample's
+            float2 mv[16];                           // (spp0 + spp - 1) from slot (spp - 1) % g
             for (uint32_t s = 0; s < 16; s++)
-                if (s < g) mv[s] = J.pmom[pl * g + s];
+                if (s < g) {
+                    const float4 q = J.pmom[pl * g + s];
+                    mv[s] = make_float2(q.x, q.y);
+                }
             for (uint32_t o = 1; o < 16; o <<= 1)
                 for (uint32_t s = 0; s + o < 16; s += 2 * o)
                     if (s + o < g) {
@@ -279,7 +296,8 @@ __global__ void __launch_bounds__(128) batch_resolve_kernel(const BatchJob *__re
                         mv[s].y += mv[s + o].y;
                     }
             const float4 m = J.P.moments[pixel];
-            J.P.moments[pixel] = make_float4(m.x + mv[0].x, m.y + mv[0].y, m.z, m.w);
+            const float lz = J.pmom[pl * g + (uint32_t)(J.P.spp - 1) % g].z;
+            J.P.moments[pixel] = make_float4(m.x + mv[0].x, m.y + mv[0].y, lz, last_sample_tag(J.P));
         }
     }
     // the rays of the warp's pixels, one atomic per job present
@@ -363,6 +381,52 @@ cudaError_t pt_trace(const PtScene &S, const PtParams &P, float *d_accum, unsign
     return cudaGetLastError();
 }
 
+namespace pt {
+
+// a tile's gradient sample (trace.wgsl main with T.txl.w = 1): old pixel o's sample kk traced again
+// in the new scene from the same random numbers (the fast kernel's stream of (o, kk, seed) and the
+// sampler's dimensions of o), through the new pixel k moved by the old one's offset (dx, dy); lam[0]
+// = |l - old l| / max(l, old l, 1e-3) of the two samples' luminance over their albedo, -1 where
+// there is no sample or the new one is not a number
+template <bool MEDIA>
+__global__ void __launch_bounds__(128) grad_kernel(PtScene S, PtParams P, GradTile *tiles, uint32_t ntiles,
+                                                   const float4 *__restrict__ guide, unsigned long long *ray_count,
+                                                   uint32_t *err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t rays = 0;
+    if (t < ntiles && tiles[t].o >= 0) {
+        const GradTile T = tiles[t];
+        const uint32_t W = (uint32_t)P.W;
+        const uint32_t ox = (uint32_t)T.o % W, oy = (uint32_t)T.o / W;
+        const uint32_t kx = (uint32_t)T.k % W, ky = (uint32_t)T.k / W;
+        const uint64_t opix = (uint64_t)(uint32_t)T.o;
+        Rng rng;
+        rng_seed(rng, mix64(opix * 0x9E3779B97F4A7C15ull ^ ((uint64_t)T.kk << 40) ^ P.seed), opix);
+        Sampler sm{&rng, T.kk, (uint32_t)P.seed * 0x9e3779b9u, (int)ox, (int)oy, P.sampler_on, S.mask};
+        float jx, jy;
+        sampler_2d(sm, 0, jx, jy);
+        const float u = dvd(add(add((float)kx, T.dx), jx), (float)P.W);
+        const float v = dvd(add(add((float)ky, T.dy), jy), (float)P.H);
+        V3 o, d;
+        camera_ray(P, u, v, o, d);
+        V3 c = trace_path<MEDIA>(S, P, o, d, sm, err, rays);
+        float lam = -1.0f;
+        if (is_number(c) && vmax3(c) >= 0.0f) {
+            c = clamp_sample(c, P.clamp);
+            const float l = sample_luma(c, guide[T.k]);
+            lam = fabsf(l - T.l) / fmaxf(fmaxf(l, T.l), 1e-3f);
+        }
+        tiles[t].lam[0] = lam;
+    }
+    if (ray_count) {
+        unsigned long long r = rays;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        if ((threadIdx.x & 31) == 0 && r) atomicAdd(ray_count, r);
+    }
+}
+
+}  // namespace pt
+
 // the batch kernel's launch shapes: threads per block and the blocks per SM its registers are
 // capped for (65536 / (threads x blocks) registers a thread)
 namespace {
@@ -402,6 +466,14 @@ cudaError_t batch_trace(const BatchJob *d_jobs, uint32_t njobs, unsigned long lo
 cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long long npix, cudaStream_t st) {
     if (!njobs || !npix) return cudaSuccess;
     pt::batch_resolve_kernel<<<(unsigned)((npix + 127) / 128), 128, 0, st>>>(d_jobs, njobs, npix);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_gradients(const PtScene &S, const PtParams &P, GradTile *d_tiles, uint32_t ntiles, const float4 *d_guide,
+                         unsigned long long *d_rays, uint32_t *d_status, cudaStream_t st) {
+    if (!ntiles) return cudaSuccess;
+    (S.nvol ? pt::grad_kernel<true> : pt::grad_kernel<false>)<<<(ntiles + 127) / 128, 128, 0, st>>>(
+        S, P, d_tiles, ntiles, d_guide, d_rays, d_status);
     return cudaGetLastError();
 }
 

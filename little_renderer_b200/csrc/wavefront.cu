@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
     int j = task != NO_TASK ? (int)W.job[i] : -1;
     uint32_t kk = 0, trays = 0;
     float4 sum = make_float4(0, 0, 0, 0);
-    float2 mom = make_float2(0, 0);
+    float4 mom = make_float4(0, 0, 0, 0);
     bool path = (f0 & F_PATH) != 0, new_task = false, wrote_sum = false;
     if (j >= 0) {
         kk = W.kk[i];
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
             if (J.pmom) {                            // the denoiser's moments
                 const uint2 xy = W.xy[i];
                 const float l = sample_luma(s, J.P.guide[(uint64_t)xy.y * (uint32_t)J.P.W + xy.x]);
-                mom = make_float2(mom.x + l, mom.y + l * l);
+                mom = make_float4(mom.x + l, mom.y + l * l, l, 0.0f);
             }
             wrote_sum = true;
             kk += (uint32_t)J.P.group;
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
                 W.xy[i] = make_uint2(x, y);
                 kk = (uint32_t)J.P.spp0 + slot;
                 sum = make_float4(0, 0, 0, 0);
-                mom = make_float2(0, 0);
+                mom = make_float4(0, 0, 0, 0);
                 trays = 0;
                 new_task = true;
                 wrote_sum = true;
@@ -381,7 +381,7 @@ WfState wf_carve(void *base, uint32_t M) {
     W.nvl = reinterpret_cast<float4 *>(take(m * 16));
     W.nve = reinterpret_cast<float4 *>(take(m * 16));
     W.rng = reinterpret_cast<ulonglong2 *>(take(m * 16));
-    W.mom = reinterpret_cast<float2 *>(take(m * 16));   // (8 of 16 bytes a slot used)
+    W.mom = reinterpret_cast<float4 *>(take(m * 16));
     W.vis = reinterpret_cast<uint8_t *>(take(m * 2));
     take(m * 4);    // (spare)
     W.sq_o = reinterpret_cast<float4 *>(take(m * 2 * 16));

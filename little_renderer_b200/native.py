@@ -20,6 +20,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
 LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
 LRC_DEVICE = 1
 LRC_TRACE_GUIDED = 64
+LRC_REPROJECT_EDIT = 128
 LRC_SERVE_DENOISE = 16
 LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED = 4, 8, 16, 32
 
@@ -101,6 +102,7 @@ def lib():
     L.lrc_caustics_variant.argtypes = [vp, C.c_int]
     L.lrc_guide.argtypes = [vp, vp, vp, C.c_uint]
     L.lrc_reproject.argtypes = [vp, vp, vp, vp, vp, C.c_int32, C.c_uint]
+    L.lrc_reproject_gradients.argtypes = [vp, vp, vp, u32, vp, vp, C.c_int32, C.c_int32, vp, C.c_uint]
     L.lrc_scene_set_volumes.argtypes = [vp, vp, u32]
     L.lrc_volume_majorants.argtypes = [vp, vp, vp, vp]
     L.lrc_srgb_table.argtypes = [vp]
@@ -532,6 +534,20 @@ class Scene:
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), 0, params.height, spp0, spp, _ptr(planes),
                                             C.byref(rays), LRC_TRACE_GUIDED))
         return planes, rays.value
+
+    def reproject_gradients(self, old_params, new_params, spp0, old_planes, new_planes, history_max, history,
+                            edit=False):
+        """lrc_reproject_gradients with host planes (4, h, w, 4): new_planes' planes 0 and 1 from
+        old_planes, each pixel's history from its tile's temporal gradient; returns the tiles
+        ((h + 3) // 4, (w + 3) // 4, 4): new pixel, old pixel, the sample's lambda, the filtered
+        lambda (-1: none)."""
+        old_planes = np.ascontiguousarray(old_planes, np.float32)
+        h, w = new_planes.shape[1:3]
+        tiles = np.zeros(((h + 3) // 4, (w + 3) // 4, 4), np.float32)
+        self.ctx.check(self.ctx.L.lrc_reproject_gradients(
+            self.h, C.byref(old_params), C.byref(new_params), spp0, _ptr(old_planes), _ptr(new_planes), history_max,
+            history, _ptr(tiles), LRC_REPROJECT_EDIT if edit else 0))
+        return tiles
 
     def trace_guided_device(self, params, spp, d_planes, spp0=0):
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), 0, params.height, spp0, spp, C.c_void_p(d_planes),

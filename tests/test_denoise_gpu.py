@@ -65,6 +65,10 @@ def test_guided_trace_keeps_the_image_and_adds_moments(ctx, oracle, cornell128):
     l = 0.2126 * irr[..., 0] + 0.7152 * irr[..., 1] + 0.0722 * irr[..., 2]
     assert np.allclose(planes[1][..., 0], l, rtol=1e-5, atol=1e-6)
     assert np.allclose(planes[1][..., 1], l * l, rtol=1e-4, atol=1e-6)
+    # z, w: the last sample's l and its number + 1 (trace.wgsl keeps them for the temporal gradients)
+    assert np.array_equal(planes[1][..., 2], planes[1][..., 0]) and np.all(planes[1][..., 3] == 1)
+    s.trace_guided(p, 3, planes, spp0=1)
+    assert np.all(planes[1][..., 3] == 4)
     ex = guided(ctx, s, params(oracle, sc, exact=1), 4)
     acc, _ = s.trace(params(oracle, sc, exact=1), 4)
     assert np.array_equal(ex[0], acc)
