@@ -63,6 +63,7 @@ METRIC_SERVE = "Mrays/s and p50/p99 job latency (served request stream, Poisson 
 METRIC_RENDER = "Mrays/s (one image: closest-hit + shadow rays)"
 METRIC_DENOISE = "Mpixels/s (denoiser: prep + 5 a-trous passes, 1920x1080)"
 METRIC_CAUSTICS = "Mrays/s (light-traced caustics: closest-hit + shadow rays of the light paths)"
+METRIC_REALTIME = "frames/s (moving camera: guide + temporal gradients + reprojection + 1-spp guided trace + denoise)"
 
 
 def parse():
@@ -78,7 +79,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve", "render", "instanced",
-                                                                     "caustics", "denoise", "media", "textures"])
+                                                                     "caustics", "denoise", "media", "textures",
+                                                                     "realtime"])
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
@@ -909,12 +911,7 @@ DENOISE_BYTES_PER_PIXEL = 80 + 5 * 24 + 16 + 16
 
 
 def run_denoise(a):
-    """--workload media: the plain render's box with 16 icospheres and a 40x32x40-voxel cloud of
-participating medium (foggy_cornell), 256x256, 16 spp: the plain path and the megakernel batch
-(the wavefront does not take media); the reference's trace_image with the same Volume as the
-baseline.
-
---workload denoise: lrc_denoise (device arrays) on a 1080p image's planes; e2e: lrc_denoise
+    """--workload denoise: lrc_denoise (device arrays) on a 1080p image's planes; e2e: lrc_denoise
     with host planes and image (copied in and out)."""
     import torch
     import little_renderer_b200 as L
@@ -999,6 +996,147 @@ baseline.
                       "gpu_launches": 6 * a.steps, "cpu_baseline": cpu}), flush=True)
 
 
+REALTIME_LAUNCHES = 14   # guide 1, gmatch 1, gradient samples 1, gfilter 3, reprojection 1, trace 1, denoiser 6
+
+
+def run_realtime(a):
+    """--workload realtime: the viewer's loop with temporal gradients on the plain render's scene
+    at 1280x720, the camera sliding 2 units a frame (back and forth): each step (frame) makes the new guide, the
+    tiles' gradient samples and filtered lambda, the previous frame's samples reprojected with each
+    pixel's history (at most 32, 8 without a lambda), 1 guided sample a pixel, and the denoised
+    image. e2e: the same frames with the denoised image read back to pinned host memory each
+    frame (the scene stays resident, as in a viewer). cpu_baseline: the reference's trace_image at
+    1 spp on a band of rows, scaled to the frame (the reference has no CPU reprojection or
+    denoiser)."""
+    import torch
+    import little_renderer_b200 as L
+    from little_renderer_b200 import render as R, workloads as W
+    from oracle import oracle as O
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    w, h = 1280, 720
+    sc = W.cornell_spheres(width=w, height=h)
+    dev = torch.device("cuda", 0)
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    s = R.world_scene(ctx, sc, 1)
+    c0 = sc["camera"]
+
+    def params(f):                   # (back and forth: 2 units a frame, 80 frames a period)
+        cam = dict(c0)
+        dx = 2.0 * (abs(f % 80 - 40) - 20)
+        cam["from"] = (c0["from"][0] + dx, c0["from"][1], c0["from"][2])
+        cam["at"] = (c0["at"][0] + dx, c0["at"][1], c0["at"][2])
+        return L.native.trace_params(W.camera(cam, w / h), w, h, sc["max_depth"], 1, 1, 0, 7)
+
+    planes = [torch.zeros(4, h, w, 4, device=dev), torch.zeros(4, h, w, 4, device=dev)]
+    out = torch.zeros(h, w, 4, device=dev)
+    host_img = torch.zeros(h, w, 4).pin_memory()
+    state = {"f": 0}
+    stage_ms = np.zeros(4)
+
+    def frame(events=None):
+        f = state["f"]
+        cur, prev = planes[f % 2], planes[(f + 1) % 2]
+        p = params(f)
+        if events:
+            events[0].record(stream)
+        s.guide_device(p, cur.data_ptr())
+        if events:
+            events[1].record(stream)
+        if f > 0:
+            s.reproject_gradients_device(params(f - 1), p, f, prev.data_ptr(), cur.data_ptr(), 32, 8)
+        else:
+            cur[:2].zero_()
+        if events:
+            events[2].record(stream)
+        s.trace_guided_device(p, 1, cur.data_ptr(), spp0=f)
+        if events:
+            events[3].record(stream)
+        ctx.denoise_device(w, h, cur.data_ptr(), out.data_ptr())
+        if events:
+            events[4].record(stream)
+        state["f"] = f + 1
+
+    for _ in range(a.warmup):
+        frame()
+    torch.cuda.synchronize()
+    ctx.sync()
+    clk = Clocks(0)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(a.steps)]
+    for i in range(a.steps):
+        frame(evs[i])
+    torch.cuda.synchronize()
+    ctx.sync()
+    clocks = clk.stop()
+    ms = evs[0][0].elapsed_time(evs[-1][4]) / a.steps
+    for e in evs:
+        for k in range(4):
+            stage_ms[k] += e[k].elapsed_time(e[k + 1]) / a.steps
+    cur = planes[(state["f"] - 1) % 2]
+    hist = cur[0][..., 3].float()
+    history_mean = float(hist.mean())
+    finite = bool(torch.isfinite(out).all())
+    # a frame's rays (closest-hit + shadow) of its 1-spp trace, counted on one host call
+    pr = params(state["f"] - 1)
+    host_planes = cur.cpu().numpy().copy()
+    _, rays = s.trace_guided(pr, 1, host_planes, spp0=state["f"])
+    # end to end: each frame's denoised image read back to pinned host memory
+    n_e2e = max(3, min(a.steps, 20))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        frame()
+        host_img.copy_(out, non_blocking=True)
+        stream.synchronize()
+    e_ms = (time.perf_counter() - t0) * 1e3 / n_e2e
+    # the reference's CPU path tracer: 1 spp on a central band of rows
+    cpu = None
+    if not a.no_cpu:
+        ref = ref_cornell(O, sc)
+        rows = 64
+        c = c0
+        fau = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
+        t0 = time.perf_counter()
+        _, (cl, sh) = ref.trace_image(fau, c["vfov"], w, h, 1, 1, sc["max_depth"], y0=h // 2 - rows // 2, rows=rows)
+        t_cpu = time.perf_counter() - t0
+        cores = O.ref_lib().rb_max_threads()
+        ref.close()
+        cpu = {"value": 1e3 / (t_cpu * 1e3 * h / rows), "unit": "frames/s", "cores": cores, "kind": "reference",
+               "sample": f"scene_set_accel + trace_image of {rows} central rows at 1 spp ({cl + sh} rays in "
+                         f"{t_cpu:.2f} s), scaled to the {h}-row frame; the reference has no CPU reprojection or "
+                         "denoiser"}
+    peak_gbs, peak_src = peaks()
+    dn_gbs = DENOISE_BYTES_PER_PIXEL * w * h / (stage_ms[3] / 1e3) / 1e9
+    s.close()
+    ctx.close()
+    print(json.dumps({"metric": METRIC_REALTIME, "value": 1e3 / ms, "unit": "frames/s", "n_gpus": 1,
+                      "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f16 between denoiser passes)",
+                      "data": "synthetic",
+                      "config": {"workload": f"the box, its lamp and 64 icospheres (20.5k triangles), {w}x{h}, depth "
+                                             f"{sc['max_depth']}, the camera sliding 2 units a frame; history at most "
+                                             "32 samples (8 without a gradient), 1 new sample a pixel a frame",
+                                 "stage_ms": {"guide": stage_ms[0], "gradients+reprojection": stage_ms[1],
+                                              "trace_1spp": stage_ms[2], "denoise": stage_ms[3]},
+                                 "rays_per_frame_trace": int(rays),
+                                 "trace_Mrays_per_s": rays / (stage_ms[2] / 1e3) / 1e6,
+                                 "mean_samples_a_pixel_after_trace": history_mean, "image_finite": finite,
+                                 "l2": "the frame's 59 MB of planes and the scene stay in HBM; L2 not flushed (the "
+                                       "workload's own: a viewer's frames follow one another)"},
+                      "roofline": {"kernel": "denoiser passes (the frame's HBM-bound stage; the trace is "
+                                             "traversal-latency-bound)", "bound": "hbm", "achieved": dn_gbs,
+                                   "peak": peak_gbs, "unit": "GB/s", "frac": dn_gbs / peak_gbs, "traffic": None,
+                                   "algorithmic_bytes_per_pixel": DENOISE_BYTES_PER_PIXEL, "peak_source": peak_src},
+                      "clocks": clocks,
+                      "e2e": {"value": 1e3 / e_ms, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": w * h * 16, "ms_per_step": e_ms},
+                      "gpu_launches": REALTIME_LAUNCHES * a.steps, "cpu_baseline": cpu}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -1010,6 +1148,11 @@ def main():
             run_reference_batch(a)
         elif a.workload == "caustics":
             run_reference_caustics(a)
+        elif a.workload == "realtime":
+            print(json.dumps({"impl": "reference", "metric": METRIC_REALTIME, "unavailable":
+                              "the reference's reprojection, temporal gradients and denoiser exist only as WGSL, "
+                              "which cannot run on this box; its CPU path tracer is the cpu_baseline leg of the ours "
+                              "line"}), flush=True)
         elif a.workload == "denoise":
             print(json.dumps({"impl": "reference", "metric": METRIC_DENOISE, "unavailable":
                               "the reference's denoiser exists only as WGSL (denoise.wgsl), which cannot run on this "
@@ -1034,6 +1177,9 @@ def main():
         return
     if a.workload == "denoise":
         run_denoise(a)
+        return
+    if a.workload == "realtime":
+        run_realtime(a)
         return
     import torch
     import little_renderer_b200 as L

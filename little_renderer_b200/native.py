@@ -549,6 +549,13 @@ class Scene:
             history, _ptr(tiles), LRC_REPROJECT_EDIT if edit else 0))
         return tiles
 
+    def reproject_gradients_device(self, old_params, new_params, spp0, d_old, d_new, history_max, history, d_tiles=0,
+                                   edit=False):
+        """lrc_reproject_gradients with device planes (and tiles, 0: none); returns at once."""
+        self.ctx.check(self.ctx.L.lrc_reproject_gradients(
+            self.h, C.byref(old_params), C.byref(new_params), spp0, C.c_void_p(d_old), C.c_void_p(d_new), history_max,
+            history, C.c_void_p(d_tiles) if d_tiles else None, LRC_DEVICE | (LRC_REPROJECT_EDIT if edit else 0)))
+
     def trace_guided_device(self, params, spp, d_planes, spp0=0):
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), 0, params.height, spp0, spp, C.c_void_p(d_planes),
                                             None, LRC_TRACE_GUIDED | LRC_DEVICE))

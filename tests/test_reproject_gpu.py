@@ -204,3 +204,22 @@ def test_gradient_arguments(ctx, oracle, scene):
     for args in ((ex, p, 2, old, guided(s, p, 0), 32, 8), (p, p, 2, old, guided(s, p, 0), 0, 8)):
         with pytest.raises(L.native.LrcError):
             s.reproject_gradients(*args)
+
+
+def test_gradients_device_arrays(ctx, oracle, scene):
+    """The same through device arrays (LRC_DEVICE): planes and tiles equal the host call's."""
+    import torch
+    sc, s = scene
+    c = sc["camera"]
+    p0 = cam_params(oracle, sc, c["from"], c["at"], 1)
+    p1 = cam_params(oracle, sc, (c["from"][0] + 6.0, c["from"][1], c["from"][2]), c["at"], 2)
+    old = guided(s, p0, 4)
+    new, tiles = gradients(s, p0, p1, old, 16, 4, nxt=4)
+    d_old = torch.from_numpy(old).cuda()
+    d_new = torch.from_numpy(guided(s, p1, 0)).cuda()
+    d_tiles = torch.zeros(tiles.shape, device="cuda")
+    torch.cuda.synchronize()
+    s.reproject_gradients_device(p0, p1, 4, d_old.data_ptr(), d_new.data_ptr(), 16, 4, d_tiles.data_ptr())
+    ctx.sync()
+    assert np.array_equal(d_new.cpu().numpy(), new)
+    assert np.array_equal(d_tiles.cpu().numpy(), tiles)
