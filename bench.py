@@ -997,17 +997,20 @@ def run_denoise(a):
 
 
 REALTIME_LAUNCHES = 14   # guide 1, gmatch 1, gradient samples 1, gfilter 3, reprojection 1, trace 1, denoiser 6
+# (lrc_trace_frame adds a memset of planes 0 and 1, not a kernel of ours)
 
 
 def run_realtime(a):
     """--workload realtime: the viewer's loop with temporal gradients on the plain render's scene
-    at 1280x720, the camera sliding 2 units a frame (back and forth): each step (frame) makes the new guide, the
-    tiles' gradient samples and filtered lambda, the previous frame's samples reprojected with each
-    pixel's history (at most 32, 8 without a lambda), 1 guided sample a pixel, and the denoised
-    image. e2e: the same frames with the denoised image read back to pinned host memory each
-    frame (the scene stays resident, as in a viewer). cpu_baseline: the reference's trace_image at
-    1 spp on a band of rows, scaled to the frame (the reference has no CPU reprojection or
-    denoiser)."""
+    at 1280x720, the camera sliding 2 units a frame (back and forth): each step (frame) makes the
+    new guide, the tiles' gradient samples and filtered lambda, the previous frame's samples
+    reprojected with each pixel's history (at most 32, 8 without a lambda), 1 guided sample a
+    pixel (lrc_trace_frame: all of it in one call), and the denoised image. The same frames as
+    separate calls (lrc_guide, lrc_reproject_gradients, lrc_trace, lrc_denoise) are timed beside
+    it, stage by stage, and give the same planes. e2e: the frames
+    with the denoised image read back to pinned host memory each frame (the scene stays resident,
+    as in a viewer). cpu_baseline: the reference's trace_image at 1 spp on a band of rows, scaled
+    to the frame (the reference has no CPU reprojection or denoiser)."""
     import torch
     import little_renderer_b200 as L
     from little_renderer_b200 import render as R, workloads as W
@@ -1038,7 +1041,17 @@ def run_realtime(a):
     state = {"f": 0}
     stage_ms = np.zeros(4)
 
-    def frame(events=None):
+    def frame_one():                 # lrc_trace_frame + lrc_denoise
+        f = state["f"]
+        cur, prev = planes[f % 2], planes[(f + 1) % 2]
+        if f > 0:
+            s.trace_frame_device(params(f - 1), params(f), f, 1, prev.data_ptr(), cur.data_ptr(), 32, 8)
+        else:
+            s.trace_frame_device(None, params(f), f, 1, 0, cur.data_ptr(), 32, 8)
+        ctx.denoise_device(w, h, cur.data_ptr(), out.data_ptr())
+        state["f"] = f + 1
+
+    def frame(events=None):          # the same as separate calls, timed stage by stage
         f = state["f"]
         cur, prev = planes[f % 2], planes[(f + 1) % 2]
         p = params(f)
@@ -1061,21 +1074,45 @@ def run_realtime(a):
             events[4].record(stream)
         state["f"] = f + 1
 
-    for _ in range(a.warmup):
-        frame()
-    torch.cuda.synchronize()
-    ctx.sync()
-    clk = Clocks(0)
+    def warm(fn):                    # frames 0 .. warmup - 1: both ways time the same frames after
+        state["f"] = 0
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ctx.sync()
+
+    # the separate calls, stage by stage
+    warm(frame)
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(a.steps)]
     for i in range(a.steps):
         frame(evs[i])
     torch.cuda.synchronize()
     ctx.sync()
-    clocks = clk.stop()
-    ms = evs[0][0].elapsed_time(evs[-1][4]) / a.steps
+    sep_ms = evs[0][0].elapsed_time(evs[-1][4]) / a.steps
     for e in evs:
         for k in range(4):
             stage_ms[k] += e[k].elapsed_time(e[k + 1]) / a.steps
+    # the same next frame both ways: equal planes
+    f_chk = state["f"]
+    frame()
+    sep_planes = planes[f_chk % 2].clone()
+    state["f"] = f_chk
+    frame_one()
+    torch.cuda.synchronize()
+    ctx.sync()
+    same_planes = bool(torch.equal(sep_planes, planes[f_chk % 2]))
+    # lrc_trace_frame: the line's value
+    warm(frame_one)
+    clk = Clocks(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        frame_one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / a.steps
     cur = planes[(state["f"] - 1) % 2]
     hist = cur[0][..., 3].float()
     history_mean = float(hist.mean())
@@ -1089,7 +1126,7 @@ def run_realtime(a):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(n_e2e):
-        frame()
+        frame_one()
         host_img.copy_(out, non_blocking=True)
         stream.synchronize()
     e_ms = (time.perf_counter() - t0) * 1e3 / n_e2e
@@ -1120,8 +1157,11 @@ def run_realtime(a):
                       "config": {"workload": f"the box, its lamp and 64 icospheres (20.5k triangles), {w}x{h}, depth "
                                              f"{sc['max_depth']}, the camera sliding 2 units a frame; history at most "
                                              "32 samples (8 without a gradient), 1 new sample a pixel a frame",
-                                 "stage_ms": {"guide": stage_ms[0], "gradients+reprojection": stage_ms[1],
-                                              "trace_1spp": stage_ms[2], "denoise": stage_ms[3]},
+                                 "separate_calls": {"ms_per_frame": sep_ms, "frames_per_s": 1e3 / sep_ms,
+                                                    "stage_ms": {"guide": stage_ms[0],
+                                                                 "gradients+reprojection": stage_ms[1],
+                                                                 "trace_1spp": stage_ms[2], "denoise": stage_ms[3]},
+                                                    "planes_equal_trace_frame": same_planes},
                                  "rays_per_frame_trace": int(rays),
                                  "trace_Mrays_per_s": rays / (stage_ms[2] / 1e3) / 1e6,
                                  "mean_samples_a_pixel_after_trace": history_mean, "image_finite": finite,

@@ -332,6 +332,15 @@ int lrc_reproject(lrc_ctx *ctx, const lrc_trace_params *old_cam, const lrc_trace
 int lrc_reproject_gradients(lrc_scene *s, const lrc_trace_params *old_p, const lrc_trace_params *new_p, uint32_t spp0,
                             const float *old_planes, float *new_planes, int32_t history_max, int32_t history,
                             float *tiles_out, unsigned flags);
+/* A viewer's frame in one call (gpu_trace_begin_image with its reprojection and gradients, then
+ * the frame's samples; trace_gpu.c:2040-2114): new_planes (4 planes) = lrc_guide(new_p), then
+ * lrc_reproject_gradients (history_max > 0) or lrc_reproject (history_max = 0) from old_planes
+ * (null: the first frame, no history), then lrc_trace(new_p, spp0, spp, LRC_TRACE_GUIDED) - the
+ * same planes to the bit, in one stream of launches with host copies (without LRC_DEVICE) of
+ * the old planes in and the new ones out only. Fast mode only (new_p and old_p with exact = 0). */
+int lrc_trace_frame(lrc_scene *s, const lrc_trace_params *old_p, const lrc_trace_params *new_p, uint32_t spp0,
+                    uint32_t spp, const float *old_planes, float *new_planes, int32_t history_max, int32_t history,
+                    unsigned flags);
 int lrc_denoise(lrc_ctx *ctx, int32_t width, int32_t height, const float *planes, int32_t passes, float *out,
                 unsigned flags);
 

@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256) reproject_kernel(RpCam oc, RpCam nc, int 
     }
     const float n = fminf(nsum / wsum, history);
     cur[k] = make_float4(a0.x / wsum * n, a0.y / wsum * n, a0.z / wsum * n, n);
-    cur[N + k] = make_float4(a1.x / wsum * n, a1.y / wsum * n, 0.0f, 0.0f);
+    cur[N + k] = make_float4(a1.x / wsum * n, a1.y / wsum * n, 0.0f, 0.0f);   // (z, w: no sample of this image yet)
 }
 
 // the tiles for the caller: (new pixel, old pixel, the sample's lambda, the filtered lambda)
@@ -550,6 +550,60 @@ lrc::dn::RpCam rp_cam(const lrc_trace_params *p) {
 
 using namespace lrcapi;
 
+namespace {
+// what a scene needs before its paths are traced (lrc_trace's checks)
+int scene_traceable(lrc_scene *s) {
+    lrc_ctx *c = s->ctx;
+    if (!s->built_n && !s->tlas_n) return fail(c, LRC_E_INVALID, "the scene has nothing built (lrc_scene_build)");
+    if (s->ninst && s->tlas_n != s->ninst) return fail(c, LRC_E_INVALID, "instances changed: lrc_scene_build_instances");
+    if (!s->d_mats || !s->nmats) return fail(c, LRC_E_INVALID, "the scene has no materials (lrc_scene_set_materials)");
+    if (s->light >= (int32_t)s->nprims) return fail(c, LRC_E_INVALID, "the light is not one of the primitives");
+    if (!s->tables) return lrc_scene_set_tables(s, nullptr, nullptr);
+    return LRC_OK;
+}
+
+lrc::PtParams trace_params_of(const lrc_trace_params *p) {
+    lrc::PtParams P{};
+    P.W = p->width; P.H = p->height; P.y0 = 0; P.rows = p->height;
+    P.max_depth = p->max_depth; P.mis = p->mis; P.sampler_on = p->sampler; P.exact = p->exact;
+    P.seed = p->seed;
+    P.clamp = p->clamp;
+    P.skip_caustics = p->skip_caustics != 0;
+    P.origin = {p->origin[0], p->origin[1], p->origin[2]};
+    P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
+    P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
+    P.vertical = {p->vertical[0], p->vertical[1], p->vertical[2]};
+    return P;
+}
+
+uint32_t grad_tiles(int W, int H) {
+    return (uint32_t)(((W + lrc::GRAD_TILE - 1) / lrc::GRAD_TILE) * (size_t)((H + lrc::GRAD_TILE - 1) / lrc::GRAD_TILE));
+}
+
+// the temporal gradients up to the tiles' filtered lambda: gmatch, the gradient samples (the new
+// camera and scene, the old image's random numbers: its seed and sampler), the filter's 3 passes
+cudaError_t grad_chain(lrc_scene *s, const lrc_trace_params *old_p, const lrc_trace_params *new_p, uint32_t spp0,
+                       const float4 *d_old, float4 *d_new, lrc::GradTile *d_tiles, bool edit, cudaStream_t st) {
+    lrc_ctx *c = s->ctx;
+    const int W = new_p->width, H = new_p->height;
+    const size_t N = (size_t)W * H;
+    const uint32_t ntiles = grad_tiles(W, H);
+    lrc::PtParams P = trace_params_of(new_p);
+    P.spp0 = (int)spp0; P.spp = 1; P.group = 1; P.exact = 0;
+    P.sampler_on = old_p->sampler;
+    P.seed = old_p->seed;
+    lrc::dn::gmatch_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(rp_cam(old_p), rp_cam(new_p), W, H, spp0, edit, d_old,
+                                                                 d_new, d_tiles);
+    cudaError_t e = cudaGetLastError();
+    if (!e) e = lrc::pt_gradients(pt_scene(s), P, d_tiles, ntiles, d_new + 3 * N, s->d_rays, c->d_status, st);
+    for (int pass = 0; pass < 3 && !e; pass++) {
+        lrc::dn::gfilter_kernel<<<(ntiles + 127) / 128, 128, 0, st>>>(W, H, pass, d_new, d_tiles);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+}  // namespace
+
 extern "C" {
 
 int lrc_guide(lrc_scene *s, const lrc_trace_params *p, float *planes, unsigned flags) {
@@ -626,18 +680,11 @@ int lrc_reproject_gradients(lrc_scene *s, const lrc_trace_params *old_p, const l
     if ((uint64_t)W * (uint64_t)H >= (1ull << 31)) return fail(c, LRC_E_INVALID, "image too large (2^31 pixels)");
     if (old_p->exact)
         return fail(c, LRC_E_INVALID, "temporal gradients trace a sample again: the old image in fast mode (exact = 0)");
-    if (!s->built_n && !s->tlas_n) return fail(c, LRC_E_INVALID, "the scene has nothing built (lrc_scene_build)");
-    if (s->ninst && s->tlas_n != s->ninst) return fail(c, LRC_E_INVALID, "instances changed: lrc_scene_build_instances");
-    if (!s->d_mats || !s->nmats) return fail(c, LRC_E_INVALID, "the scene has no materials (lrc_scene_set_materials)");
-    if (s->light >= (int32_t)s->nprims) return fail(c, LRC_E_INVALID, "the light is not one of the primitives");
     DeviceGuard g(c->device);
-    if (!s->tables) {
-        int rc = lrc_scene_set_tables(s, nullptr, nullptr);
-        if (rc) return rc;
-    }
+    int rc = scene_traceable(s);
+    if (rc) return rc;
     const size_t N = (size_t)W * H;
-    const uint32_t ntiles = (uint32_t)(((W + lrc::GRAD_TILE - 1) / lrc::GRAD_TILE) *
-                                       (size_t)((H + lrc::GRAD_TILE - 1) / lrc::GRAD_TILE));
+    const uint32_t ntiles = grad_tiles(W, H);
     const float4 *d_old = reinterpret_cast<const float4 *>(old_planes);
     float4 *d_new = reinterpret_cast<float4 *>(new_planes);
     float4 *d_tout = reinterpret_cast<float4 *>(tiles_out);
@@ -657,30 +704,13 @@ int lrc_reproject_gradients(lrc_scene *s, const lrc_trace_params *old_p, const l
     if (!e && !s->d_rays) e = cudaMalloc(&s->d_rays, 256);
     if (!e) e = cudaMemsetAsync(s->d_rays, 0, 8, c->st);
     if (e) return cuda_status(c, e, "lrc_reproject_gradients");
-    // the gradient samples' parameters: the new camera and scene, the old image's random numbers
-    lrc::PtParams P{};
-    P.W = W; P.H = H; P.y0 = 0; P.rows = H; P.spp0 = (int)spp0; P.spp = 1; P.group = 1; P.exact = 0;
-    P.max_depth = new_p->max_depth; P.mis = new_p->mis; P.sampler_on = old_p->sampler;
-    P.seed = old_p->seed;
-    P.clamp = new_p->clamp;
-    P.skip_caustics = new_p->skip_caustics != 0;
-    P.origin = {new_p->origin[0], new_p->origin[1], new_p->origin[2]};
-    P.upper_left = {new_p->upper_left[0], new_p->upper_left[1], new_p->upper_left[2]};
-    P.horizontal = {new_p->horizontal[0], new_p->horizontal[1], new_p->horizontal[2]};
-    P.vertical = {new_p->vertical[0], new_p->vertical[1], new_p->vertical[2]};
     const bool edit = (flags & LRC_REPROJECT_EDIT) != 0;
-    const lrc::dn::RpCam oc = rp_cam(old_p), nc = rp_cam(new_p);
     c->timer.begin(LRC_TS_SHADE, c->st);
-    lrc::dn::gmatch_kernel<<<(ntiles + 127) / 128, 128, 0, c->st>>>(oc, nc, W, H, spp0, edit, d_old, d_new, d_tiles);
-    e = cudaGetLastError();
-    if (!e) e = lrc::pt_gradients(pt_scene(s), P, d_tiles, ntiles, d_new + 3 * N, s->d_rays, c->d_status, c->st);
-    for (int pass = 0; pass < 3 && !e; pass++) {
-        lrc::dn::gfilter_kernel<<<(ntiles + 127) / 128, 128, 0, c->st>>>(W, H, pass, d_new, d_tiles);
-        e = cudaGetLastError();
-    }
+    e = grad_chain(s, old_p, new_p, spp0, d_old, d_new, d_tiles, edit, c->st);
     if (!e) {
-        lrc::dn::reproject_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>(oc, nc, W, H, (float)history_max, d_old,
-                                                                                  d_new, d_tiles, (float)history, edit);
+        lrc::dn::reproject_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>(rp_cam(old_p), rp_cam(new_p), W, H,
+                                                                                  (float)history_max, d_old, d_new,
+                                                                                  d_tiles, (float)history, edit);
         e = cudaGetLastError();
     }
     if (!e && tiles_out) {
@@ -692,6 +722,67 @@ int lrc_reproject_gradients(lrc_scene *s, const lrc_trace_params *old_p, const l
     if (!e && tiles_out && !(flags & LRC_DEVICE))
         e = cudaMemcpyAsync(tiles_out, d_tout, (size_t)ntiles * 16, cudaMemcpyDeviceToHost, c->st);
     if (e) return cuda_status(c, e, "lrc_reproject_gradients");
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_trace_frame(lrc_scene *s, const lrc_trace_params *old_p, const lrc_trace_params *new_p, uint32_t spp0,
+                    uint32_t spp, const float *old_planes, float *new_planes, int32_t history_max, int32_t history,
+                    unsigned flags) {
+    if (!s || !new_p || !new_planes || !spp || history_max < 0 || history < 0 || (old_planes && !old_p))
+        return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    const int W = new_p->width, H = new_p->height;
+    if (W <= 0 || H <= 0 || (old_planes && (old_p->width != W || old_p->height != H)))
+        return fail(c, LRC_E_INVALID, "reprojection: both images of the same size");
+    if ((uint64_t)W * (uint64_t)H >= (1ull << 31)) return fail(c, LRC_E_INVALID, "image too large (2^31 pixels)");
+    if (new_p->exact) return fail(c, LRC_E_INVALID, "a frame's samples in fast mode (exact = 0)");
+    const bool grads = old_planes && history_max > 0;
+    if (grads && old_p->exact)
+        return fail(c, LRC_E_INVALID, "temporal gradients trace a sample again: the old image in fast mode (exact = 0)");
+    DeviceGuard g(c->device);
+    int rc = scene_traceable(s);
+    if (rc) return rc;
+    const size_t N = (size_t)W * H;
+    const uint32_t ntiles = grad_tiles(W, H);
+    const float4 *d_old = reinterpret_cast<const float4 *>(old_planes);
+    float4 *d_new = reinterpret_cast<float4 *>(new_planes);
+    cudaError_t e = cudaSuccess;
+    if (grads) e = reserve(&c->dn, &c->dn_cap, ((size_t)ntiles * sizeof(lrc::GradTile) + 255) / 256 * 256 + 256);
+    if (!e && !(flags & LRC_DEVICE)) {
+        e = reserve(&c->stage, &c->stage_cap, N * 128);
+        float4 *st = static_cast<float4 *>(c->stage);
+        if (!e && old_planes) e = cudaMemcpyAsync(st, old_planes, N * 64, cudaMemcpyHostToDevice, c->st);
+        d_old = old_planes ? st : nullptr;
+        d_new = st + 4 * N;
+    }
+    if (!e && !s->d_rays) e = cudaMalloc(&s->d_rays, 256);
+    if (!e) e = cudaMemsetAsync(s->d_rays, 0, 8, c->st);
+    if (e) return cuda_status(c, e, "lrc_trace_frame");
+    lrc::PtParams P = trace_params_of(new_p);
+    P.spp0 = (int)spp0;
+    P.spp = (int)spp;
+    int gsz = 1;
+    while (gsz * 2 <= (int)spp && gsz < 16) gsz *= 2;
+    P.group = gsz;
+    P.moments = d_new + N;
+    P.guide = d_new + 3 * N;
+    lrc::GradTile *d_tiles = static_cast<lrc::GradTile *>(c->dn);
+    const bool edit = (flags & LRC_REPROJECT_EDIT) != 0;
+    c->timer.begin(LRC_TS_SHADE, c->st);
+    e = lrc::dn_guide(pt_scene(s), P, d_new, c->d_status, c->st);
+    if (!e && grads) e = grad_chain(s, old_p, new_p, spp0, d_old, d_new, d_tiles, edit, c->st);
+    if (!e && old_planes) {
+        lrc::dn::reproject_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->st>>>(
+            rp_cam(old_p), rp_cam(new_p), W, H, (float)(grads ? history_max : history), d_old, d_new,
+            grads ? d_tiles : nullptr, (float)history, grads && edit);
+        e = cudaGetLastError();
+    } else if (!e) {
+        e = cudaMemsetAsync(d_new, 0, N * 32, c->st);   // (the first frame: no history)
+    }
+    if (!e) e = lrc::pt_trace(pt_scene(s), P, reinterpret_cast<float *>(d_new), s->d_rays, c->d_status, c->st);
+    c->timer.end(c->st);
+    if (!e && !(flags & LRC_DEVICE)) e = cudaMemcpyAsync(new_planes, d_new, N * 64, cudaMemcpyDeviceToHost, c->st);
+    if (e) return cuda_status(c, e, "lrc_trace_frame");
     return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 

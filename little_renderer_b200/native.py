@@ -103,6 +103,7 @@ def lib():
     L.lrc_guide.argtypes = [vp, vp, vp, C.c_uint]
     L.lrc_reproject.argtypes = [vp, vp, vp, vp, vp, C.c_int32, C.c_uint]
     L.lrc_reproject_gradients.argtypes = [vp, vp, vp, u32, vp, vp, C.c_int32, C.c_int32, vp, C.c_uint]
+    L.lrc_trace_frame.argtypes = [vp, vp, vp, u32, u32, vp, vp, C.c_int32, C.c_int32, C.c_uint]
     L.lrc_scene_set_volumes.argtypes = [vp, vp, u32]
     L.lrc_volume_majorants.argtypes = [vp, vp, vp, vp]
     L.lrc_srgb_table.argtypes = [vp]
@@ -555,6 +556,24 @@ class Scene:
         self.ctx.check(self.ctx.L.lrc_reproject_gradients(
             self.h, C.byref(old_params), C.byref(new_params), spp0, C.c_void_p(d_old), C.c_void_p(d_new), history_max,
             history, C.c_void_p(d_tiles) if d_tiles else None, LRC_DEVICE | (LRC_REPROJECT_EDIT if edit else 0)))
+
+    def trace_frame(self, old_params, new_params, spp0, spp, old_planes, history_max, history, edit=False):
+        """lrc_trace_frame with host planes: the new frame's 4 planes (h, w) from old_planes (4, h, w,
+        4) or None (the first frame)."""
+        new = np.zeros((4, new_params.height, new_params.width, 4), np.float32)
+        old = None if old_planes is None else np.ascontiguousarray(old_planes, np.float32)
+        self.ctx.check(self.ctx.L.lrc_trace_frame(
+            self.h, C.byref(old_params) if old_params is not None else None, C.byref(new_params), spp0, spp,
+            _ptr(old) if old is not None else None, _ptr(new), history_max, history,
+            LRC_REPROJECT_EDIT if edit else 0))
+        return new
+
+    def trace_frame_device(self, old_params, new_params, spp0, spp, d_old, d_new, history_max, history, edit=False):
+        """lrc_trace_frame with device planes (d_old 0: the first frame); returns at once."""
+        self.ctx.check(self.ctx.L.lrc_trace_frame(
+            self.h, C.byref(old_params) if old_params is not None else None, C.byref(new_params), spp0, spp,
+            C.c_void_p(d_old) if d_old else None, C.c_void_p(d_new), history_max, history,
+            LRC_DEVICE | (LRC_REPROJECT_EDIT if edit else 0)))
 
     def trace_guided_device(self, params, spp, d_planes, spp0=0):
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), 0, params.height, spp0, spp, C.c_void_p(d_planes),

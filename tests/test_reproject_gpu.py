@@ -223,3 +223,35 @@ def test_gradients_device_arrays(ctx, oracle, scene):
     ctx.sync()
     assert np.array_equal(d_new.cpu().numpy(), new)
     assert np.array_equal(d_tiles.cpu().numpy(), tiles)
+
+
+@pytest.mark.parametrize("hmax,edit", [(32, False), (32, True), (0, False)])
+def test_frame_is_the_separate_calls(ctx, oracle, scene, hmax, edit):
+    """lrc_trace_frame gives the planes of lrc_guide + lrc_reproject_gradients (or lrc_reproject
+    with history_max 0) + lrc_trace with LRC_TRACE_GUIDED, to the bit, from host or device arrays;
+    the first frame (no old planes) those of lrc_guide + lrc_trace."""
+    import torch
+    sc, s = scene
+    c = sc["camera"]
+    p0 = cam_params(oracle, sc, c["from"], c["at"], 3)
+    p1 = cam_params(oracle, sc, (c["from"][0] + 8.0, c["from"][1] - 4.0, c["from"][2]), (c["at"][0] + 6.0, c["at"][1], c["at"][2]), 3)
+    first = s.trace_frame(None, p0, 0, 4, None, hmax, 8, edit)
+    want0 = guided(s, p0, 0)
+    s.trace_guided(p0, 4, want0)
+    assert np.array_equal(first, want0)
+    got = s.trace_frame(p0, p1, 4, 2, first, hmax, 8, edit)
+    want = guided(s, p1, 0)
+    if hmax:
+        s.reproject_gradients(p0, p1, 4, first, want, hmax, 8, edit)
+    else:
+        ctx.reproject(p0, p1, first, want, 8)
+    s.trace_guided(p1, 2, want, spp0=4)
+    print(f"hmax {hmax} edit {edit}: pixels with history {(want[0][..., 3] > 2).mean():.3f}; "
+          f"planes equal {[bool(np.array_equal(got[i], want[i])) for i in range(4)]}")
+    assert np.array_equal(got, want)
+    d_old = torch.from_numpy(first).cuda()
+    d_new = torch.zeros(4, p1.height, p1.width, 4, device="cuda")
+    torch.cuda.synchronize()
+    s.trace_frame_device(p0, p1, 4, 2, d_old.data_ptr(), d_new.data_ptr(), hmax, 8, edit)
+    ctx.sync()
+    assert np.array_equal(d_new.cpu().numpy(), want)
