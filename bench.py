@@ -997,7 +997,6 @@ def run_denoise(a):
 
 
 REALTIME_LAUNCHES = 14   # guide 1, gmatch 1, gradient samples 1, gfilter 3, reprojection 1, trace 1, denoiser 6
-# (lrc_trace_frame adds a memset of planes 0 and 1, not a kernel of ours)
 
 
 def run_realtime(a):

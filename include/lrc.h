@@ -327,7 +327,7 @@ int lrc_reproject(lrc_ctx *ctx, const lrc_trace_params *old_cam, const lrc_trace
  * new_planes: planes 2 and 3 made by lrc_guide for new_p; planes 0 and 1 are written. spp0: the
  * new image's first sample number (sample numbers keep counting from image to image). tiles_out
  * (optional): per tile (row-major) 4 floats (k, o, the sample's lambda, the filtered lambda), -1
- * for none. old_p in fast mode (exact = 0); history_max > 0. */
+ * for none (k and o exact below 2^24 pixels). old_p in fast mode (exact = 0); history_max > 0. */
 #define LRC_REPROJECT_EDIT 128u
 int lrc_reproject_gradients(lrc_scene *s, const lrc_trace_params *old_p, const lrc_trace_params *new_p, uint32_t spp0,
                             const float *old_planes, float *new_planes, int32_t history_max, int32_t history,
