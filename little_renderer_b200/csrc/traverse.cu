@@ -23,8 +23,8 @@
 namespace lrc {
 
 constexpr int TR_THREADS = 128;
-constexpr int TR_SSTACK = 16;              // entries per thread in shared memory (16 KB per block)
-constexpr int TR_LSTACK = 80;              // then in local memory
+constexpr int TR_SSTACK = 8;               // entries per thread in shared memory (8 KB per block)
+constexpr int TR_LSTACK = 88;              // then in local memory
 constexpr uint64_t SORT_RAYS_FROM = 1u << 18;
 
 struct RayCtx {
