@@ -383,7 +383,7 @@ def run_batch(a):
     torch.cuda.synchronize()
     batch_imgs = [img.cpu() for img in imgs]
     same = all(torch.equal(x, y) for x, y in zip(plain_imgs, batch_imgs))
-    per_job, rays = b.rays()
+    _, rays = b.rays()
     clk = Clocks(local)
     ms = timed(batch_step, a.steps)
     clocks = clk.stop()

@@ -799,7 +799,7 @@ class Server:
 
     def image(self, jid):
         """A finished job's image as a host array (h, w, 4): the sum of its samples and their count."""
-        scene, p = self.keep[jid]
+        _, p = self.keep[jid]
         out = np.zeros((p.height, p.width, 4), np.float32)
         self.ctx.check(self.ctx.L.lrc_server_read(self.h, jid, _ptr(out)))
         return out

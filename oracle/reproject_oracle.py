@@ -41,7 +41,6 @@ def old_place(oc, nc, W, H, g2):
 def same_surface_at(old, g2, g3, ox, oy, dist, edit=False):
     """same_surface (trace_reproject.wgsl:62-86) of old pixels (oy, ox) (int arrays, in the image)
     for new pixels whose guide is g2, g3 and whose point is `dist` from the old eye."""
-    H, W = old.shape[1:3]
     zs = old[2][..., 3]
     zl = np.concatenate([zs[:, :1], zs[:, :-1]], 1)
     zr = np.concatenate([zs[:, 1:], zs[:, -1:]], 1)
