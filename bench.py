@@ -93,6 +93,9 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=1, help="batch: timed passes of the plain path")
     ap.add_argument("--cpu-scenes", type=int, default=8, help="batch: scenes the CPU baseline samples")
     ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"], help="batch: the engine")
+    ap.add_argument("--split-samples", action="store_true",
+                    help="render: one image traced by all ranks, each a share of every pixel's samples, then one "
+                         "sum all-reduce (strong scaling)")
     ap.add_argument("--stepped", action="store_true",
                     help="batch: wavefront passes launched from the host (for ncu, which cannot see into graph loops)")
     a = ap.parse_args()
@@ -750,6 +753,94 @@ def run_render(a):
     print(json.dumps(line), flush=True)
 
 
+def run_render_split(a):
+    """--workload render --split-samples: configuration 0's image (the box, its lamp and 64
+    icospheres, 256x256, 16 spp, depth 8, fast mode) traced by all N ranks together: each rank its
+    share of every pixel's samples, then one sum all-reduce of the 1 MB accumulation buffer over
+    NCCL (render.trace_split). Strong scaling: the image's work is fixed. At N = 1 the plain path.
+    Rank 0 compares the split image with one rank's whole image (the same samples summed in
+    another order). e2e: the same with the image read back to pinned host memory each step."""
+    import datetime
+    import torch
+    import little_renderer_b200 as L
+    from little_renderer_b200 import render as R, workloads as W
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    sc = W.cornell_spheres()
+    w, h, spp = sc["width"], sc["height"], sc["spp"]
+    ctx = L.Context(local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    s = R.world_scene(ctx, sc, 1)
+    p = L.native.trace_params(W.camera(sc["camera"], w / h), w, h, sc["max_depth"], 1, 1, 0, 1)
+    acc = torch.zeros(h, w, 4, device=dev)
+    host = torch.zeros(h, w, 4).pin_memory()
+    torch.cuda.synchronize()
+    whole, rays = s.trace(p, spp)                    # (the image's rays, and one rank's whole image)
+
+    def step():
+        acc.zero_()
+        R.trace_split(s, p, spp, acc, dist)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.sync()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ctx.sync()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, dev) / a.steps
+    split = acc.cpu().numpy()
+    err = float(np.sqrt(((split - whole) ** 2).sum() / (whole ** 2).sum()))
+    counts_equal = bool(np.array_equal(split[..., 3], whole[..., 3]))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(max(3, min(a.steps, 10))):
+        step()
+        host.copy_(acc, non_blocking=True)
+        stream.synchronize()
+    e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, dist, dev) / max(3, min(a.steps, 10))
+    s.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC_RENDER, "value": rays / (ms / 1e3) / 1e6, "unit": "Mrays/s",
+                          "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic",
+                          "config": {"workload": "the box, its lamp and 64 icospheres (20.5k triangles), 256x256, "
+                                                 "16 spp, depth 8, one image split by samples over the ranks",
+                                     "parallelism": f"sample split x{world}", "rays_per_image": int(rays),
+                                     "relRMSE_to_one_rank": err, "sample_counts_equal": counts_equal,
+                                     "l2": "one image's scene and image held in HBM; successive images reuse L2 "
+                                           "(the workload's own)"},
+                          "clocks": clocks,
+                          "e2e": {"value": rays / (e_ms / 1e3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": w * h * 16, "ms_per_step": e_ms},
+                          "gpu_launches": a.steps, "cpu_baseline": None}), flush=True)
+
+
 def caustics_setup():
     from little_renderer_b200 import workloads as W
     sc = W.cornell_spheres()
@@ -1207,6 +1298,9 @@ def main():
         return
     if a.workload == "serve":
         run_serve(a)
+        return
+    if a.workload == "render" and a.split_samples:
+        run_render_split(a)
         return
     if a.workload in ("render", "instanced", "media", "textures"):
         run_render(a)

@@ -70,3 +70,34 @@ def instanced_box_scene(ctx, sc, mesh_builder=1, key_bits=30, blue_noise=None, b
     s.build_instances(mesh_builder, key_bits)
     return s
 
+
+
+def sample_range(rank, world, spp):
+    """Rank's share of an image's spp samples split over `world` ranks: (spp0, n), the samples
+    [spp0, spp0 + n); the first spp % world ranks take one more. The shares cover [0, spp) once
+    each, so the sum of the ranks' accumulation buffers holds every sample of every pixel."""
+    if world < 1 or not 0 <= rank < world or spp < 0:
+        raise ValueError("sample_range: 0 <= rank < world and spp >= 0")
+    base, extra = divmod(spp, world)
+    return rank * base + min(rank, extra), base + (1 if rank < extra else 0)
+
+
+def trace_split(scene, params, spp, d_accum, dist=None, group=None):
+    """One image traced by all ranks of a torch.distributed group (the multi-GPU sample split):
+    each rank traces its sample_range of every pixel into d_accum (a device tensor (h, w, 4),
+    cleared by the caller), then one sum all-reduce of the W x H x 16-B buffers gives every rank
+    the whole image. A fast-mode sample's random numbers depend on its pixel, its number and the
+    seed only, so the image has the samples one rank would trace (summed in another order). The
+    scene's context must launch on torch's current stream (lrc_set_stream), which the all-reduce
+    then follows. Exact mode (one stream per pixel from its first sample) cannot be split.
+    Returns this rank's (spp0, n)."""
+    world = dist.get_world_size(group) if dist is not None else 1
+    rank = dist.get_rank(group) if dist is not None else 0
+    if params.exact and world > 1:
+        raise ValueError("trace_split: exact mode cannot be split over ranks")
+    spp0, n = sample_range(rank, world, spp)
+    if n:
+        scene.trace_device(params, n, d_accum.data_ptr(), spp0=spp0)
+    if world > 1:
+        dist.all_reduce(d_accum, op=dist.ReduceOp.SUM, group=group)
+    return spp0, n
