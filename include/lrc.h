@@ -98,13 +98,18 @@ size_t lrc_build_scratch_bytes(uint32_t n, int key_bits, int builder);
  * against that budget), and a frame loop that rebuilds a top-level tree every frame cannot afford
  * cudaMalloc's implicit device synchronisation. This is lrc_build with LRC_DEVICE (every array a
  * device pointer of the current device), the same trees bit for bit, its scratch memory in one
- * fixed device array of LRC_STATIC_SCRATCH_BYTES that every GPU loading the library holds until
- * the process exits; it calls no allocating routine. n above LRC_STATIC_MAX_ITEMS: LRC_E_TOO_BIG,
- * nothing done. The first call on a device sets it up (finds the array's device address, sets the
- * kernels' attributes): make that first call before any stream capture. Every call shares the
- * array: calls that overlap on the GPU (other streams, other host threads) race and must not be
- * made. The work goes to cuda_stream (a cudaStream_t; NULL: the default stream) and the call
- * waits for it, returning LRC_OK, LRC_E_TIMEOUT (a bounded device wait ran out) or LRC_E_CUDA. */
+ * fixed device array of LRC_STATIC_SCRATCH_BYTES; it calls no cudaMalloc, cudaFree or other
+ * allocating routine itself. n above LRC_STATIC_MAX_ITEMS: LRC_E_TOO_BIG, nothing done.
+ * The first call on a device sets it up: it finds the array's device address, and since CUDA
+ * loads a library's kernels lazily, that is when the driver loads this part of the library and
+ * reserves the array on that device (held from then until the process exits; the load may
+ * synchronise the device). Make that first call at initialisation, outside the frame loop. The
+ * kernels' attributes are set on the first use of each key width and of PLOC. Calls cannot be
+ * captured into a CUDA graph: each one waits for its work and reads the status word back.
+ * Every call shares the array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must not be made. The work goes to cuda_stream (a cudaStream_t; NULL: the default
+ * stream) and the call waits for it, returning LRC_OK, LRC_E_TIMEOUT (a bounded device wait ran
+ * out) or LRC_E_CUDA. */
 #define LRC_E_TOO_BIG (-6)
 #define LRC_STATIC_MAX_ITEMS 65536
 #define LRC_STATIC_SCRATCH_BYTES (6u << 20)

@@ -27,7 +27,11 @@ _u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
 def build():
     """Builds liboracle.so and, where the reference sources are present, _ref/*.so."""
     import subprocess
-    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    make = ["make", "-s", "-C", HERE, "all"]
+    ref = os.environ.get("LR_REFERENCE", "/root/reference")   # the reference's checkout, where present
+    if os.path.isfile(os.path.join(ref, "engine", "rt", "tracer.c")):
+        make.append(f"REF={ref}")
+    subprocess.run(make, check=True)
 
 
 def _load(name):

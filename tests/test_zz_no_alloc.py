@@ -62,6 +62,35 @@ def test_static_build_equals_lrc_build_on_two_calls_in_a_row():
     ctx.close()
 
 
+def test_static_build_tiny_ploc_falls_back_as_lrc_build():
+    """PLOC needs three items; with one or two the builder makes the LBVH tree, as lrc_build does."""
+    ctx = L.Context(0)
+    for n in (1, 2):
+        boxes, lo, hi = _boxes(n, 20 + n)
+        p = ctx.params(n, lo, hi, 30, 1)
+        want_nodes, want_aux = ctx.build(p, boxes)
+        rc, nodes, aux = _static_build(p, boxes)
+        assert rc == L.native.LRC_OK
+        assert np.array_equal(nodes, want_nodes) and np.array_equal(aux, want_aux)
+    ctx.close()
+
+
+def test_static_build_on_a_second_device():
+    """The array's address is looked up once per device; a second GPU gets its own."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one GPU visible")
+    with torch.cuda.device(1):
+        ctx = L.Context(1)
+        boxes, lo, hi = _boxes(30000, 31)
+        p = ctx.params(30000, lo, hi, 30, 1)
+        want_nodes, want_aux = ctx.build(p, boxes)
+        rc, nodes, aux = _static_build(p, boxes)
+        assert rc == L.native.LRC_OK
+        assert np.array_equal(nodes, want_nodes) and np.array_equal(aux, want_aux)
+        ctx.close()
+
+
 def test_static_build_refuses_more_than_its_maximum():
     ctx = L.Context(0)
     n = 65536 + 1
