@@ -15,7 +15,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
 SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu", "media.cu", "textures.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+              "-Xcompiler", "-fPIC"]
+OBJ_DIR = os.path.join(PKG, "_build")
 
 LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
 LRC_DEVICE = 1
@@ -33,17 +34,43 @@ def nvcc():
 
 
 def build(force=False, verbose=False):
-    """Compiles liblrc.so for sm_100a when a source is newer than it (or force)."""
-    srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, "lrc_internal.cuh"), os.path.join(ROOT, "include", "lrc.h")]
-    deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
+    """Compiles liblrc.so for sm_100a: each source to an object of its own (in parallel, again
+    only when it or a header is newer than the object), then one link. Returns the library's path."""
+    from concurrent.futures import ThreadPoolExecutor
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    headers.append(os.path.join(ROOT, "include", "lrc.h"))
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    jobs = []
+    objs = []
+    for src in SOURCES:
+        s_path = os.path.join(CSRC, src)
+        o_path = os.path.join(OBJ_DIR, src[:-3] + ".o")
+        d_path = o_path[:-2] + ".d"
+        objs.append(o_path)
+        deps = _deps(d_path) if os.path.exists(d_path) else headers
+        deps = [d for d in deps if os.path.exists(d)] + [s_path]
+        if force or not os.path.exists(o_path) or os.path.getmtime(o_path) < max(os.path.getmtime(d) for d in deps):
+            jobs.append([nvcc()] + NVCC_FLAGS + ["-MD", "-MF", d_path, "-c", s_path, "-o", o_path])
+    if not jobs and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB] + srcs
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=CSRC)
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True, cwd=CSRC)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        list(ex.map(run, jobs))
+    run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs)
     return LIB
+
+
+def _deps(d_path):
+    """The files an object depends on, from its make-style dependency file (nvcc -MD)."""
+    with open(d_path) as f:
+        text = f.read().replace("\\\n", " ")
+    paths = [os.path.normpath(os.path.join(CSRC, t)) for t in text.split(":", 1)[-1].split()]
+    return [t for t in paths if t.startswith(ROOT + os.sep)]     # the project's own files only
 
 
 _lib = None
