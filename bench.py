@@ -1,6 +1,12 @@
 """Benchmarks of the hot path on B200. Prints one JSON line (rank 0).
 
---workload builder (default): a BVH build (LBVH or PLOC over N triangles) plus one pass of
+--workload serve (default): the served request stream (configuration 4): 64 resident scenes, jobs of
+{256^2, 720p, 1080p} x {4, 16, 64} spp arriving as Poisson streams at 50, 200 and 800 jobs/s, served
+in waves by lrc_server (continuous batching under an HBM budget) and, in the same run, one at a time
+through lrc_trace; Mrays/s of the served streams, p50/p99 latency of both, the offered load, a
+stream below capacity and an end-to-end pass with images read back to the host.
+
+--workload builder: a BVH build (LBVH or PLOC over N triangles) plus one pass of
 closest-hit rays through it. N = 4M triangles with centroids uniform in the unit cube, Gaussian
 edges (sigma = 0.002 N^-1/3), 2 % of them scaled x50; 16M rays from a sphere of radius 2 toward
 uniform points of the cube. One step = triangle boxes, Morton codes, radix sort, hierarchy (PLOC
@@ -37,7 +43,7 @@ writes 16; each pass reads its 8 + 8 B and writes 8; the last reads the albedo, 
 the image, 16). The baseline is the numpy restatement of the filter (the reference's own runs only
 as WGSL) on a 480x270 crop.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload builder|batch] ...
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload serve|builder|batch|...] ...
   python bench.py --impl reference ...   the reference's own CPU path on this host's cores
 
 Multi-GPU: replicas (each rank builds and traces its own copy of the workload; no collective on the
@@ -78,14 +84,16 @@ def parse():
     ap.add_argument("--bits", type=int, default=30, choices=[30, 63])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--workload", default="builder", choices=["builder", "batch", "serve", "render", "instanced",
+    ap.add_argument("--workload", default="serve", choices=["builder", "batch", "serve", "render", "instanced",
                                                                      "caustics", "denoise", "media", "textures",
                                                                      "realtime"])
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
-    ap.add_argument("--jobs", type=int, default=120, help="serve: jobs per rate")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
     ap.add_argument("--wave-paths", type=int, default=32 << 20, help="serve: paths per wave")
     ap.add_argument("--wave-slots", type=int, default=1 << 22, help="serve: the waves' paths in flight")
+    ap.add_argument("--serve-policy", type=int, default=0, choices=[0, 1, 2],
+                    help="serve: how a wave is made (lrc_server_set_policy: 0 even shares, 1 oldest first, "
+                         "2 fewest paths left first)")
     ap.add_argument("--denoise-low-spp", action="store_true",
                     help="serve: jobs of 4 spp are denoised (LRC_SERVE_DENOISE; the plain path: guide, guided "
                          "trace, lrc_denoise)")
@@ -193,14 +201,15 @@ def cpu_baseline(a, cor, orig, dirs, sample_rays):
 
 
 def run_reference(a):
-    """--impl reference: the reference's own CPU implementation of the path (SAH BVH build +
-    scene_intersect) on this host's cores, each step a bounded sample of the workload."""
+    """--impl reference --workload builder: the reference's own CPU implementation of the path (SAH
+    BVH build + scene_intersect of every ray) on this host's cores, each step the whole workload
+    (about 25 s on 16 cores: no sample is scaled up)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from little_renderer_b200 import workloads as W
     cor = W.soup(a.n, 1)
-    sample = 1 << 20
+    sample = a.rays
     o, d = W.rays_at_cube(sample, 2)
     from oracle import oracle as O
     lib = O.ref_lib()
@@ -226,7 +235,7 @@ def run_reference(a):
             "data": "synthetic", "impl": "reference", "config": config(a, 1),
             "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "reference",
                              "sample": f"per step: scene_set_accel (4-wide SAH) over {a.n} triangles + "
-                                       f"scene_intersect of {sample} rays, scaled to {a.rays} rays"},
+                                       f"scene_intersect of all {a.rays} rays"},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -446,7 +455,10 @@ def run_batch(a):
         print(json.dumps(line), flush=True)
 
 
-def serve_jobs(n, rate, seed, scenes, inst_ids):
+SERVE_JOBS_PER_STEP = 5      # a serve step: 5 jobs of each rate's stream
+
+
+def serve_jobs(n, rate, seed, nscenes, inst_ids):
     """n jobs with Poisson arrivals at `rate`/s: (arrival s, scene index, width, height, spp, motion
     frame or None); a tenth of them move the instances of an instanced scene."""
     rng = np.random.default_rng(seed)
@@ -459,16 +471,141 @@ def serve_jobs(n, rate, seed, scenes, inst_ids):
         if rng.random() < 0.1:
             out.append((float(t[i]), int(rng.choice(inst_ids)), w, h, spp, float(rng.uniform(1, 30))))
         else:
-            out.append((float(t[i]), int(rng.integers(0, len(scenes))), w, h, spp, None))
+            out.append((float(t[i]), int(rng.integers(0, nscenes)), w, h, spp, None))
     return out
 
 
+def serve_world_counts():
+    """The triangle counts of the stream's 56 box scenes (log-uniform in [1k, 2M], seeded)."""
+    rng = np.random.default_rng(17)
+    lo, hi = np.log(1_000), np.log(2_000_000)
+    return [int(np.exp(rng.uniform(lo, hi))) for _ in range(56)]
+
+
+class ServeWorlds:
+    """The stream's box scenes made on first use (scene k is box_scene(5000 + k, counts[k]))."""
+
+    def __init__(self):
+        self.counts = serve_world_counts()
+        self.made = {}
+
+    def __getitem__(self, k):
+        from little_renderer_b200 import workloads as W
+        if k not in self.made:
+            self.made[k] = W.box_scene(5000 + k, self.counts[k], 256, 256, 16)
+        return self.made[k]
+
+
+def serve_scene_dicts():
+    """The 64 resident scenes of the served stream: 56 box scenes (triangles log-uniform in [1k, 2M])
+    and 8 instanced boxes of 2000 instances; (dicts, indices of the instanced ones, triangles)."""
+    from little_renderer_b200 import workloads as W
+    worlds = ServeWorlds()
+    dicts = [worlds[k] for k in range(56)]
+    inst_ids = []
+    for i in range(8):
+        dicts.append(W.instanced_box(6000 + i, n_instances=2000))
+        inst_ids.append(len(dicts) - 1)
+    tris = sum(worlds.counts) + sum(len(dicts[k]["corners"]) for k in inst_ids)
+    return dicts, inst_ids, tris
+
+
+def serve_cpu_jobs(nscenes_world, seed, count):
+    """A seeded sample of the stream's jobs the reference's CPU path tracer traces whole: world
+    scenes only (no moved instances), jobs of at most 4M paths (256^2 at any spp, 720p at 4 spp)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    res = [(256, 256), (1280, 720)]
+    while len(out) < count:
+        w, h = res[rng.integers(0, 2)]
+        spp = int(rng.choice([4, 16, 64]))
+        if w * h * spp > 4 << 20:
+            continue
+        out.append((int(rng.integers(0, nscenes_world)), w, h, spp, int(rng.integers(0, 1 << 30))))
+    return out
+
+
+def serve_cpu_sample(dicts, seconds, seed=23):
+    """The reference's trace_image (scene_set_accel, 4-wide SAH, all host cores) on whole sampled
+    jobs of the stream until `seconds` are spent: (Mrays/s, cores, rays, seconds, description)."""
+    from oracle import oracle as O
+    from little_renderer_b200 import workloads as W
+    lib = O.ref_lib()
+    cores = lib.rb_max_threads()
+    rays, t_all, done, built = 0, 0.0, [], {}
+    for k, w, h, spp, jseed in serve_cpu_jobs(56, seed, 64):
+        if t_all > seconds:
+            break
+        sc = dicts[k]
+        if k not in built:
+            ref = ref_box_scene(O, sc)
+            ref.set_accel()                          # (the scene's tree is resident, as the served scenes')
+            built[k] = ref
+        ref = built[k]
+        c = sc["camera"]
+        fau = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
+        t0 = time.perf_counter()
+        _, (closest, shadow) = ref.trace_image(fau, c["vfov"], w, h, spp, jseed, sc["max_depth"])
+        t_all += time.perf_counter() - t0
+        rays += closest + shadow
+        done.append(f"{sc['corners'].shape[0]} tris {w}x{h} x {spp} spp")
+    for ref in built.values():
+        ref.close()
+    text = (f"trace_image of {len(done)} whole jobs of the stream (world scenes, jobs of at most 4M paths; "
+            f"trees built beforehand as the served scenes' are resident): " + "; ".join(done) +
+            f"; {rays} rays in {t_all:.1f} s")
+    return rays / t_all / 1e6, cores, rays, t_all, text
+
+
+def run_reference_serve(a):
+    """--impl reference --workload serve: the reference has no server; its own CPU path tracer
+    (trace_image on this host's cores) on whole sampled jobs of the same stream, each step about
+    3 s of them; Mrays/s."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    dicts = ServeWorlds()                             # (only the sampled scenes are made)
+    tris = None
+    vals, rays_all, secs_all, text = [], 0, 0.0, ""
+    for step in range(a.warmup + a.steps):
+        v, cores, rays, secs, text = serve_cpu_sample(dicts, 3.0, seed=100 + step)
+        if step >= a.warmup:
+            vals.append(v)
+            rays_all += rays
+            secs_all += secs
+    v = rays_all / secs_all / 1e6
+    line = {"metric": METRIC_SERVE, "value": v, "unit": "Mrays/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * secs_all / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": serve_config(a, tris),
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "reference",
+                             "sample": "per step about 3 s of " + text.split(":")[0] + " (seeded, one sample a step)"},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_values": vals}
+    print(json.dumps(line), flush=True)
+
+
+def serve_config(a, tris):
+    tris = f"{tris} triangles: " if tris else ""
+    return {"workload": f"served request stream: 64 resident scenes ({tris}56 box scenes of 1k-2M "
+                        "triangles, 8 instanced boxes of 2000 instances), jobs {256^2, 720p, 1080p} x spp "
+                        "{4, 16, 64}, depth 8, a tenth moving their scene's 2000 instances (top level refit), "
+                        "Poisson arrivals", "rates": a.rates, "jobs_per_step": SERVE_JOBS_PER_STEP,
+            "jobs_per_rate": SERVE_JOBS_PER_STEP * a.steps, "budget_gb": a.budget_gb, "wave_paths": a.wave_paths,
+            "wave_slots": a.wave_slots, "serve_policy": a.serve_policy, "parallelism": "one GPU",
+            "denoise_low_spp": bool(a.denoise_low_spp),
+            "l2": "inputs larger than L2 (resident scenes' triangles and trees, images, wavefront state > 126 MB)"}
+
+
 def run_serve(a):
-    """--workload serve: 64 resident scenes (56 box scenes, triangles log-uniform in [1k, 2M], and 8
-    instanced boxes of 2000 instances), jobs (scene, resolution in {256^2, 720p, 1080p}, spp in {4,
-    16, 64}; a tenth move their scene's 2000 instances: the top level refit first) arriving as a
-    Poisson stream, served in waves by lrc_server under an HBM budget; then the same stream through
-    the plain path, one job at a time (lrc_trace per job). Latency = end - arrival (host clock)."""
+    """--workload serve (the default): the served request stream (configuration 4). 64 resident
+    scenes; jobs (scene, resolution in {256^2, 720p, 1080p}, spp in {4, 16, 64}; a tenth move their
+    scene's 2000 instances: the top level refit first) arriving as a Poisson stream at each rate,
+    served in waves by lrc_server under an HBM budget; then the same stream through the plain path
+    one job at a time (lrc_trace per job, in arrival order). A step is SERVE_JOBS_PER_STEP jobs of
+    every rate's stream: --steps K times K x 5 jobs at each rate, after --warmup W x 5 untimed jobs.
+    Latency = end - arrival (host clock). A stream at 0.8 x the measured served capacity follows
+    (below capacity, where a latency is a latency and not a backlog), then the middle rate's stream
+    served again end to end (each image read back to pinned host memory inside the span)."""
     import torch
     import little_renderer_b200 as L
     from little_renderer_b200 import render as R, workloads as W
@@ -476,28 +613,17 @@ def run_serve(a):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     dev = torch.device("cuda", 0)
-    rng = np.random.default_rng(17)
-    lo, hi = np.log(1_000), np.log(2_000_000)
-    counts = [int(np.exp(rng.uniform(lo, hi))) for _ in range(56)]
     ctx = L.Context(0)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    scenes, dicts = [], []
-    for i, n in enumerate(counts):
-        sc = W.box_scene(5000 + i, n, 256, 256, 16)
-        dicts.append(sc)
-        scenes.append(R.world_scene(ctx, sc, 1))
-    inst_ids = []
-    for i in range(8):
-        sc = W.instanced_box(6000 + i, n_instances=2000)
-        dicts.append(sc)
-        inst_ids.append(len(scenes))
-        scenes.append(R.instanced_box_scene(ctx, sc, 1))
+    dicts, inst_ids, tris = serve_scene_dicts()
+    scenes = [R.instanced_box_scene(ctx, sc, 1) if k in inst_ids else R.world_scene(ctx, sc, 1)
+              for k, sc in enumerate(dicts)]
     motions = {k: W.rigid_motion(2000, 7000 + k) for k in inst_ids}
     originals = {k: W.instance_records(dicts[k]) for k in inst_ids}
     ctx.sync()
-    tris = sum(counts) + sum(len(dicts[k]["corners"]) for k in inst_ids)
+    jps = SERVE_JOBS_PER_STEP
 
     def records(job):
         k, frame = job[1], job[5]
@@ -508,21 +634,19 @@ def run_serve(a):
         return L.native.trace_params(W.camera(sc["camera"], job[2] / job[3]), job[2], job[3], 8, 1, 1, 0, 9000 + idx)
 
     def pct(x, q):
-        return float(np.percentile(np.asarray(x), q))
+        return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
     def denoised(job):
         return bool(a.denoise_low_spp and job[4] == 4)
 
-    results = {}
-    check = {}
-    clk = Clocks(0)
-    for rate in [float(r) for r in a.rates.split(",")]:
-        jobs = serve_jobs(a.jobs, rate, int(rate), scenes, inst_ids)
-        recs = [records(j) if j[5] is not None else None for j in jobs]
-        # served: submit each job at its arrival, step waves while any job is held
+    def served(jobs, recs, keep=0, readback=False):
+        """lrc_server over the stream: submit each job at its arrival, step waves while any is held.
+        keep: images of the first jobs kept (host); readback: every image read to pinned host memory."""
         sv = L.native.Server(ctx, int(a.budget_gb * 2**30), a.wave_paths)
         sv.set_wavefront(a.wave_slots)
-        lat, rays_s, ids = [], 0, {}
+        sv.set_policy(a.serve_policy)
+        pinned = torch.empty(1920 * 1080 * 4, dtype=torch.float32).pin_memory() if readback else None
+        lat, rays, ids, kept, d2h = [], 0, {}, {}, 0
         nxt, done = 0, 0
         t0 = L.native.clock_ms()
         while done < len(jobs):
@@ -541,18 +665,30 @@ def run_serve(a):
                     r = sv.result(jid)
                     if r is None:
                         continue
-                    lat.append(r[4] - (t0 + jobs[k][0] * 1e3))
-                    rays_s += r[1]
-                    if rate == float(a.rates.split(",")[0]) and k < 6:
-                        check[k] = sv.image(jid)
+                    if readback:
+                        nb = jobs[k][2] * jobs[k][3] * 16
+                        ctx.check(ctx.L.lrc_server_read(sv.h, jid, L.native.C.c_void_p(pinned.data_ptr())))
+                        d2h += nb
+                        t_end = L.native.clock_ms()
+                    else:
+                        t_end = r[4]
+                    lat.append(t_end - (t0 + jobs[k][0] * 1e3))
+                    rays += r[1]
+                    if k < keep:
+                        kept[k] = sv.image(jid)
                     sv.release(jid)
                     del ids[jid]
                     done += 1
-        span_s = (L.native.clock_ms() - t0) / 1e3
+        span = (L.native.clock_ms() - t0) / 1e3
+        waves, kernels, gpu_ms = sv.stats()
         sv.close()
-        # plain: one job at a time, in arrival order, each traced alone
-        lat_p, rays_p = [], 0
-        imgs = {}
+        return {"lat": lat, "rays": rays, "span": span, "kept": kept, "d2h": d2h, "waves": waves, "kernels": kernels,
+                "gpu_s": gpu_ms / 1e3}
+
+    def plain(jobs, recs, keep=0):
+        """One job at a time in arrival order, each traced alone through lrc_trace (large ones on the
+        wavefront engine, as lrc_trace runs them); the scene put back after a moved-instance job."""
+        lat, rays, kept = [], 0, {}
         t0 = L.native.clock_ms()
         for k, j in enumerate(jobs):
             now = (L.native.clock_ms() - t0) / 1e3
@@ -562,46 +698,146 @@ def run_serve(a):
             if recs[k] is not None:
                 s.move_instances(recs[k], 0)
             img = torch.zeros(j[3], j[2], 4, device=dev)
+            p = params(j, k)
+            nr = L.native.C.c_uint64()
             if denoised(j):
                 planes = torch.zeros(4, j[3], j[2], 4, device=dev)
-                s.guide_device(params(j, k), planes.data_ptr())
-                s.trace_guided_device(params(j, k), j[4], planes.data_ptr())
+                s.guide_device(p, planes.data_ptr())
+                ctx.check(ctx.L.lrc_trace(s.h, L.native.C.byref(p), 0, j[3], 0, j[4],
+                                          L.native.C.c_void_p(planes.data_ptr()), L.native.C.byref(nr),
+                                          L.native.LRC_TRACE_GUIDED | L.native.LRC_DEVICE))
                 ctx.denoise_device(j[2], j[3], planes.data_ptr(), img.data_ptr())
             else:
-                s.trace_device(params(j, k), j[4], img.data_ptr())
-            if recs[k] is not None:                     # (the scene as it was, for the jobs that follow)
+                ctx.check(ctx.L.lrc_trace(s.h, L.native.C.byref(p), 0, j[3], 0, j[4],
+                                          L.native.C.c_void_p(img.data_ptr()), L.native.C.byref(nr),
+                                          L.native.LRC_DEVICE))
+            if recs[k] is not None:
                 s.move_instances(originals[j[1]], 0)
             ctx.sync()
-            lat_p.append(L.native.clock_ms() - (t0 + j[0] * 1e3))
-            if rate == float(a.rates.split(",")[0]) and k < 6:
-                imgs[k] = img.cpu().numpy()
-        span_p = (L.native.clock_ms() - t0) / 1e3
+            rays += nr.value
+            lat.append(L.native.clock_ms() - (t0 + j[0] * 1e3))
+            if k < keep:
+                kept[k] = img.cpu().numpy()
+        span = (L.native.clock_ms() - t0) / 1e3
         for k in inst_ids:
             scenes[k].move_instances(originals[k], 1)
-        # rays of the plain pass: the served count (the same samples; checked on the first jobs' images)
-        rays_p = rays_s
+        return {"lat": lat, "rays": rays, "span": span, "kept": kept}
+
+    def stream_of(rate, n, seed):
+        jobs = serve_jobs(n, rate, seed, 56, inst_ids)
+        return jobs, [records(j) if j[5] is not None else None for j in jobs]
+
+    rates = [float(r) for r in a.rates.split(",")]
+    # warm-up (untimed): W steps' jobs of the first rate, served and plain
+    wj, wr = stream_of(rates[0], jps * a.warmup, 999)
+    served(wj, wr)
+    plain(wj[: max(2, jps)], wr[: max(2, jps)])
+    clk = Clocks(0)
+    results = {}
+    served_rays, served_span, jobs_done, paths_all, check_all, launches, waves = 0, 0.0, 0, 0, True, 0, 0
+    n_per_rate = jps * a.steps
+    for rate in rates:
+        jobs, recs = stream_of(rate, n_per_rate, int(rate))
+        sv = served(jobs, recs, keep=4)
+        pl = plain(jobs, recs, keep=4)
+        equal = all(np.array_equal(sv["kept"][k], pl["kept"][k]) for k in sv["kept"])
+        check_all = check_all and equal and sv["rays"] == pl["rays"]
+        mean_job_s = sv["span"] / len(jobs)              # (the served stream's time per job at capacity)
         results[str(int(rate))] = {
-            "served": {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mrays_s": rays_s / span_s / 1e6, "span_s": span_s},
-            "plain": {"p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99), "mrays_s": rays_p / span_p / 1e6,
-                      "span_s": span_p},
+            "served": {"p50_ms": pct(sv["lat"], 50), "p99_ms": pct(sv["lat"], 99), "mrays_s": sv["rays"] / sv["span"] / 1e6,
+                       "span_s": sv["span"], "latency_samples": len(sv["lat"]), "waves": sv["waves"],
+                       "device_busy": sv["gpu_s"] / sv["span"]},
+            "plain": {"p50_ms": pct(pl["lat"], 50), "p99_ms": pct(pl["lat"], 99), "mrays_s": pl["rays"] / pl["span"] / 1e6,
+                      "span_s": pl["span"], "latency_samples": len(pl["lat"])},
+            "served_vs_plain": (sv["rays"] / sv["span"]) / (pl["rays"] / pl["span"]),
+            "offered_load_rho": rate * mean_job_s,
             "jobs": len(jobs), "motion_jobs": sum(1 for j in jobs if j[5] is not None),
-            "denoised_jobs": sum(1 for j in jobs if denoised(j)),
-            "paths": int(sum(j[2] * j[3] * j[4] for j in jobs)), "rays": int(rays_s)}
-        if imgs:
-            results[str(int(rate))]["images_equal_plain"] = all(np.array_equal(check[k], imgs[k]) for k in imgs)
+            "paths": int(sum(j[2] * j[3] * j[4] for j in jobs)), "rays": int(sv["rays"]),
+            "images_equal_plain": bool(equal), "rays_equal_plain": bool(sv["rays"] == pl["rays"])}
+        served_rays += sv["rays"]
+        served_span += sv["span"]
+        launches += sv["kernels"]
+        waves += sv["waves"]
+        print(f"serve rate {rate:g}/s: served {sv['span']:.1f} s ({sv['rays'] / sv['span'] / 1e6:.0f} Mrays/s, "
+              f"{sv['waves']} waves, device busy {sv['gpu_s'] / sv['span']:.2f}), plain {pl['span']:.1f} s ({pl['rays'] / pl['span'] / 1e6:.0f} Mrays/s); "
+              f"images equal {equal}", file=sys.stderr, flush=True)
+        jobs_done += len(jobs)
+        paths_all += results[str(int(rate))]["paths"]
     clocks = clk.stop()
-    mid = results[sorted(results, key=float)[len(results) // 2]]
-    line = {"metric": METRIC_SERVE, "value": mid["served"]["mrays_s"], "unit": "Mrays/s", "n_gpus": 1,
-            "steps": len(results), "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"served request stream: 64 resident scenes ({tris} triangles; 8 with 2000 moving "
-                                   "instances), jobs {256^2, 720p, 1080p} x spp {4, 16, 64}, depth 8, Poisson arrivals",
-                       "rates": a.rates, "jobs_per_rate": a.jobs, "budget_gb": a.budget_gb,
-                       "wave_paths": a.wave_paths, "wave_slots": a.wave_slots, "parallelism": "one GPU",
-                       "denoise_low_spp": bool(a.denoise_low_spp)},
-            "clocks": clocks, "rates": results}
-    for s in scenes:
-        s.close()
+    # below capacity: 0.8 x the served jobs/s just measured, the same number of jobs
+    capacity = jobs_done / served_span
+    sub_rate = 0.8 * capacity
+    jobs, recs = stream_of(sub_rate, n_per_rate, 4242)
+    sv = served(jobs, recs)
+    pl = plain(jobs, recs)
+    results["sub_capacity"] = {
+        "rate_jobs_s": sub_rate, "capacity_jobs_s": capacity,
+        "served": {"p50_ms": pct(sv["lat"], 50), "p99_ms": pct(sv["lat"], 99), "mrays_s": sv["rays"] / sv["span"] / 1e6,
+                   "span_s": sv["span"], "latency_samples": len(sv["lat"])},
+        "plain": {"p50_ms": pct(pl["lat"], 50), "p99_ms": pct(pl["lat"], 99), "mrays_s": pl["rays"] / pl["span"] / 1e6,
+                  "span_s": pl["span"], "latency_samples": len(pl["lat"])},
+        "jobs": len(jobs)}
+    # end to end: the middle rate's stream again, every finished image read back to pinned host
+    # memory inside the span; the host sends each job's parameters (and moved instances' records)
+    mid = rates[len(rates) // 2]
+    jobs, recs = stream_of(mid, n_per_rate, int(mid))
+    e = served(jobs, recs, readback=True)
+    h2d = sum(96 + (r.nbytes if r is not None else 0) for r in recs)
+    e2e = {"value": e["rays"] / e["span"] / 1e6, "unit": "Mrays/s", "rate_jobs_s": mid,
+           "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(e["d2h"] / a.steps),
+           "ms_per_step": 1e3 * e["span"] / a.steps, "p50_ms": pct(e["lat"], 50), "p99_ms": pct(e["lat"], 99)}
+    # traversal bytes per ray (closest-hit walks of a sample of the jobs' primary rays: the stream's
+    # rays walk the same trees; the estimate is labelled as such) -> the served stream's roofline
+    peak, peak_kind = peaks()
+    rng = np.random.default_rng(5)
+    bt, tt, nr = 0, 0, 0
+    for k in range(0, 56, 7):
+        sc = dicts[k]
+        cam = W.camera(sc["camera"], 1.0).reshape(4, 3)
+        u, v = rng.random((2, 1 << 16)).astype(np.float32)
+        tgt = cam[1] + u[:, None] * cam[2] - v[:, None] * cam[3]
+        d = tgt - cam[0]
+        d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+        o = np.repeat(cam[0][None], d.shape[0], 0).astype(np.float32)
+        tri_only = L.Scene(ctx)                       # (the counting walk reads triangles: the lamp aside)
+        tri_only.set_triangles(L.pack_tris(W.corners_to_quv(sc["corners"])))
+        tri_only.build(1, 30)
+        b_, t_ = tri_only.trace_stats(o, d, 2e-3, 1e30)
+        tri_only.close()
+        bt, tt, nr = bt + b_, tt + t_, nr + d.shape[0]
+    bytes_per_ray = (bt * 32 + tt * 48) / nr
+    achieved = bytes_per_ray * served_rays / served_span / 1e9
+    roofline = {"kernel": "wavefront engine over the served stream (wf_intersect + wf_shadow walks; advance and "
+                          "shade inside the same span)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "peak_kind": peak_kind, "frac": achieved / peak, "traffic": None,
+                "bytes_per_ray": bytes_per_ray,
+                "bytes_per_ray_from": "closest-hit walks of 65536 primary rays of each of 8 of the box scenes' "
+                                      "triangles, PLOC trees (box tests x 32 + triangle tests x 48): an estimate of "
+                                      "the stream's rays"}
+    value = served_rays / served_span / 1e6
+    cpu_v, cores, _, _, text = serve_cpu_sample(dicts, 15.0)
+    line = {"metric": METRIC_SERVE, "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * served_span / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": serve_config(a, tris), "clocks": clocks, "e2e": e2e, "roofline": roofline,
+            "gpu_launches": int(launches), "waves": int(waves),
+            "gpu_launches_counted": "the served streams' trace kernels: per wave the wavefront's clear and resolve "
+                                    "and 4 kernels a pass (advance, closest hit, shade, shadow), passes read from "
+                                    "the device; admission copies, refits and the denoiser not counted",
+            "cpu_baseline": {"value": cpu_v, "unit": "Mrays/s", "cores": cores, "kind": "reference", "sample": text},
+            "plain_mrays_s": sum(r["plain"]["mrays_s"] * r["plain"]["span_s"] for k, r in results.items()
+                                 if k != "sub_capacity") / sum(r["plain"]["span_s"] for k, r in results.items()
+                                                               if k != "sub_capacity"),
+            "served_vs_plain": None, "equal_rmse": {"images_equal_plain": check_all,
+                                                    "how": "the first 4 jobs of each rate: served image = plain "
+                                                           "image to the bit, and served rays = plain rays"},
+            "rates": results, "jobs_timed": jobs_done, "paths_timed": paths_all}
+    plain_rays = sum(r["rays"] for k, r in results.items() if k != "sub_capacity")
+    plain_span = sum(r["plain"]["span_s"] for k, r in results.items() if k != "sub_capacity")
+    line["plain_mrays_s"] = plain_rays / plain_span / 1e6
+    line["served_vs_plain"] = value / line["plain_mrays_s"]
+    for s_ in scenes:
+        s_.close()
     ctx.close()
     print(json.dumps(line), flush=True)
 
@@ -1271,9 +1507,7 @@ def main():
     a = parse()
     if a.impl == "reference":
         if a.workload == "serve":
-            print(json.dumps({"impl": "reference", "metric": METRIC_SERVE, "unavailable":
-                              "the reference has no request server: its latency baseline is the plain one-job-at-a-time "
-                              "CUDA path timed beside the served one in --workload serve"}), flush=True)
+            run_reference_serve(a)
         elif a.workload == "batch":
             run_reference_batch(a)
         elif a.workload == "caustics":

@@ -52,6 +52,19 @@ int lrc_set_stream(lrc_ctx *ctx, void *cuda_stream);
 uint32_t lrc_status(lrc_ctx *ctx);
 /* the CUDA device's SM count (for callers sizing their own work) */
 int lrc_num_sms(const lrc_ctx *ctx);
+/* 1: all the context's work is done, 0: some is still running (does not wait), < 0: an error */
+int lrc_query(lrc_ctx *ctx);
+/* Device memory for callers without the CUDA runtime (the engine's GPU backend, gpu_cuda.c): an
+ * allocation on the context's device (LRC_RETRY when out of memory), its release (after the
+ * context's work), a copy that waits for the context's work and itself (kind below), and a
+ * zeroing enqueued on the context's stream. */
+#define LRC_COPY_H2D 0
+#define LRC_COPY_D2H 1
+#define LRC_COPY_D2D 2
+int lrc_device_alloc(lrc_ctx *ctx, size_t bytes, void **out);
+void lrc_device_free(lrc_ctx *ctx, void *p);
+int lrc_device_copy(lrc_ctx *ctx, void *dst, const void *src, size_t bytes, int kind);
+int lrc_device_zero(lrc_ctx *ctx, void *p, size_t bytes);
 /* GPU time by stage (gpu_set_timing, gpu.h; the reference's GpuTimer stages, trace_gpu.c:330-333):
  * on = 1 records CUDA events around each stage of later calls */
 #define LRC_TS_BOXES 0       /* triangle boxes and the mesh box */
@@ -135,6 +148,15 @@ int lrc_scene_build(lrc_scene *s, int builder, int key_bits);
 /* the scene's nodes (2n - 1) and aux (n) copied out (host), or their device addresses */
 int lrc_scene_tree(lrc_scene *s, uint32_t *nodes, uint32_t *aux, unsigned flags);
 int lrc_scene_tree_device(lrc_scene *s, const uint32_t **nodes, const uint32_t **aux, uint32_t *n);
+/* The scene's world tree given, not built: nnodes nodes in put_nodes' layout (trace_gpu.c:883-896:
+ * lo.xyz, a, hi.xyz, b; inner: a, b the children; leaf: a its first aux entry, b = 0x80000000 |
+ * count, up to any count) with the root at 0, and naux shape ids (primitives, then triangles) -
+ * the engine's own SAH tree (scene_bvh, engine/rt/accel.h:32; Bvh.nodes and .refs), which the
+ * reference's GPU path tracer traces (upload_world, trace_gpu.c:1103-1112). Host arrays are
+ * checked (children, leaf ranges and shape ids in range). The scene's next lrc_scene_build, or a
+ * change of its shapes, replaces it. lrc_scene_tree then copies out nnodes and naux entries. */
+int lrc_scene_set_tree(lrc_scene *s, const uint32_t *nodes, uint32_t nnodes, const uint32_t *aux, uint32_t naux,
+                       unsigned flags);
 
 /* Closest hits of nrays rays (origins, directions: 3 floats each) in (tmin, tmax) through the
  * scene's BVH: prim = the triangle hit (-1: none), t. The reference's Moller-Trumbore arithmetic
@@ -278,15 +300,23 @@ typedef struct {
     int32_t skip_caustics; /* 1: leave out the paths light tracing covers (camera -> diffuse first,
                               then the lamp right after a mirror / glass vertex; TraceParams.skip_caustics,
                               engine/rt/tracer.h:16-20): set it when lrc_caustics adds them */
+    float indirect_clamp;  /* after a path's first rough bounce, each light it brings is held to this
+                              much (its largest channel); 0: no limit (TraceParams.indirect_clamp,
+                              engine/rt/tracer.h:35; GpuTraceParams.indirect_clamp, view_gpu.h:62) */
 } lrc_trace_params;
 /* Samples [spp0, spp0 + spp) of every pixel of rows [y0, y0 + rows), added into accum (width x
  * height x 4 floats: the sum of the samples' linear RGB and their count, as gpu_view_trace_read
  * gives them, view_gpu.h:118-124). exact = 1 needs spp0 = 0 (the streams start at each pixel's
- * first sample). rays (optional, host): the closest-hit and shadow rays traced. */
+ * first sample). rays (optional, host): the closest-hit and shadow rays traced.
+ * A call of at least LRC_TRACE_WAVEFRONT_PATHS paths (width x rows x spp) on a scene without media
+ * runs as a one-job batch on the wavefront engine (the batch's image is this call's to the bit);
+ * smaller ones, scenes with media and calls with LRC_TRACE_MEGAKERNEL run the one-kernel path. */
 int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0, uint32_t spp,
               float *accum, uint64_t *rays, unsigned flags);
 #define LRC_TRACE_GUIDED 64u  /* flag: accum is the denoiser's 4 planes (below); each sample's luminance
                                  over the guide's albedo is added to plane 1's (sum l, sum l^2) */
+#define LRC_TRACE_MEGAKERNEL 256u  /* flag: the one-kernel path tracer whatever the size */
+#define LRC_TRACE_WAVEFRONT_PATHS (1u << 20)
 
 /* ---- the denoiser: replaces gpu_denoise_create / gpu_denoise_encode (engine/gpu/denoise_gpu.c;
  * denoise.wgsl `prep`, `atrous`) and the guide pass `gbuf` (trace.wgsl:1045-1104, 1319-1337) ----
@@ -407,6 +437,9 @@ int lrc_batch_jobs(const lrc_batch *b);
 int lrc_batch_run(lrc_batch *b, unsigned flags);
 /* After a run (synchronises): rays traced per job (in lrc_batch_add order) and in all; either NULL. */
 int lrc_batch_rays(lrc_batch *b, uint64_t *per_job, uint64_t *total);
+/* After a run (synchronises): the wavefront's passes (bounces of the paths in flight, 0 for the
+ * megakernel engine) and the trace kernels the run launched (optional, either NULL). */
+int lrc_batch_passes(lrc_batch *b, uint32_t *passes, uint64_t *kernels);
 /* The trace kernel's launch shapes: shape `variant`'s threads per block, the blocks per SM its
  * registers are capped for, and the blocks that fit per SM; returns the number of shapes, or -1. */
 int lrc_batch_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm);
@@ -471,6 +504,13 @@ int lrc_server_state(const lrc_server *sv, int32_t *queued, int32_t *active, int
 double lrc_server_clock(void);
 /* The batch a server runs its waves with (to set its engine or wavefront size; do not add jobs). */
 lrc_batch *lrc_server_batch(lrc_server *sv);
+/* waves run so far, the trace kernels they launched and their device time (CUDA events around
+ * each wave's run), each optional */
+int lrc_server_stats(const lrc_server *sv, uint64_t *waves, uint64_t *kernels, double *gpu_ms);
+/* How a wave is made from the admitted jobs: 0 (the default) the next band of every job, the wave's
+ * paths shared evenly; 1 the oldest jobs first, each band as large as the wave's paths left allow
+ * (fewer scenes a wave); 2 as 1 with the jobs that have the fewest paths left first. */
+int lrc_server_set_policy(lrc_server *sv, int32_t policy);
 
 #ifdef __cplusplus
 }

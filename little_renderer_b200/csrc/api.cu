@@ -6,6 +6,7 @@
 // Calls with host arrays stage them through a second growing device arena, run, copy back and
 // synchronise; calls with LRC_DEVICE only enqueue (lrc_sync waits and reports).
 #include "api_internal.cuh"
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -28,6 +29,7 @@ int scene_build_on(lrc_scene *s, int builder, int key_bits, void **scratch, size
     // the shapes: primitives, then triangles (their ids as the reference's, scene.h:101-106)
     const uint32_t n = s->ntris + s->nprims;
     if (!no_alloc) s->built_n = 0;
+    s->tree_nnodes = s->tree_naux = 0;
     if (!n) return LRC_OK;
     const size_t need_scratch = lrc::build_scratch_bytes(n, key_bits, builder);
     if (no_alloc) {
@@ -123,6 +125,7 @@ void lrc_close(lrc_ctx *c) {
     if (!c) return;
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->st);
+    if (c->single) lrc_batch_destroy(c->single);
     if (c->scratch) cudaFree(c->scratch);
     if (c->stage) cudaFree(c->stage);
     if (c->dn) cudaFree(c->dn);
@@ -305,6 +308,7 @@ int lrc_scene_set_triangles(lrc_scene *s, const uint32_t *tris, uint32_t n, unsi
     if (e) return cuda_status(c, e, "triangles");
     s->ntris = n;
     s->built_n = 0;
+    s->tree_nnodes = s->tree_naux = 0;
     if (!(flags & LRC_DEVICE)) return check_status(c);   // (the host array may be freed on return)
     return LRC_OK;
 }
@@ -319,13 +323,105 @@ int lrc_scene_tree(lrc_scene *s, uint32_t *nodes, uint32_t *aux, unsigned flags)
     if (!s || !s->built_n) return LRC_E_INVALID;
     lrc_ctx *c = s->ctx;
     DeviceGuard g(c->device);
-    const uint32_t n = s->built_n;
+    const size_t nn = s->tree_nnodes ? s->tree_nnodes : 2 * (size_t)s->built_n - 1;
+    const size_t na = s->tree_nnodes ? s->tree_naux : s->built_n;
     cudaMemcpyKind k = (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     cudaError_t e = cudaSuccess;
-    if (nodes) e = cudaMemcpyAsync(nodes, s->d_nodes, (2 * (size_t)n - 1) * 32, k, c->st);
-    if (!e && aux) e = cudaMemcpyAsync(aux, s->d_aux, (size_t)n * 4, k, c->st);
+    if (nodes) e = cudaMemcpyAsync(nodes, s->d_nodes, nn * 32, k, c->st);
+    if (!e && aux) e = cudaMemcpyAsync(aux, s->d_aux, na * 4, k, c->st);
     if (e) return cuda_status(c, e, "lrc_scene_tree");
     return check_status(c);
+}
+
+int lrc_scene_set_tree(lrc_scene *s, const uint32_t *nodes, uint32_t nnodes, const uint32_t *aux, uint32_t naux,
+                       unsigned flags) {
+    if (!s || !nodes || !aux || !nnodes || !naux) return LRC_E_INVALID;
+    lrc_ctx *c = s->ctx;
+    const uint64_t shapes = (uint64_t)s->nprims + s->ntris;
+    if (!shapes) return fail(c, LRC_E_INVALID, "the scene has no shapes (primitives or triangles) for a tree");
+    if (!(flags & LRC_DEVICE)) {
+        // a tree the walks can follow: children and leaf ranges inside the arrays, shapes that exist
+        for (uint32_t i = 0; i < nnodes; i++) {
+            const uint32_t a = nodes[8 * (size_t)i + 3], b = nodes[8 * (size_t)i + 7];
+            if (b & lrc::LEAF_BIT) {
+                const uint32_t cnt = b & ~lrc::LEAF_BIT;
+                if (a >= naux || cnt > naux - a) return fail(c, LRC_E_INVALID, "a leaf's entries lie outside aux");
+            } else if (a >= nnodes || b >= nnodes) {
+                return fail(c, LRC_E_INVALID, "a node's child lies outside the nodes");
+            }
+        }
+        for (uint32_t i = 0; i < naux; i++)
+            if (aux[i] >= shapes) return fail(c, LRC_E_INVALID, "an aux entry names no shape of the scene");
+    }
+    DeviceGuard g(c->device);
+    const size_t cap = std::max<size_t>(naux, ((size_t)nnodes + 1) / 2);   // (2 cap - 1 nodes, cap aux)
+    cudaError_t e = cudaSuccess;
+    if (s->tree_cap < cap) {
+        cudaFree(s->d_nodes);
+        cudaFree(s->d_aux);
+        s->d_nodes = nullptr;
+        s->d_aux = nullptr;
+        s->tree_cap = 0;
+        e = cudaMalloc(&s->d_nodes, (2 * cap - 1) * 32);
+        if (!e) e = cudaMalloc(&s->d_aux, cap * 4);
+        if (!e) s->tree_cap = cap;
+    }
+    const cudaMemcpyKind k = (flags & LRC_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (!e) e = cudaMemcpyAsync(s->d_nodes, nodes, (size_t)nnodes * 32, k, c->st);
+    if (!e) e = cudaMemcpyAsync(s->d_aux, aux, (size_t)naux * 4, k, c->st);
+    if (e) return cuda_status(c, e, "lrc_scene_set_tree");
+    s->built_n = naux;
+    s->tree_nnodes = nnodes;
+    s->tree_naux = naux;
+    return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
+}
+
+int lrc_device_alloc(lrc_ctx *c, size_t bytes, void **out) {
+    if (!c || !out) return LRC_E_INVALID;
+    *out = nullptr;
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaMalloc(out, bytes ? bytes : 1);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(c, LRC_RETRY, "out of device memory");
+    }
+    return cuda_status(c, e, "lrc_device_alloc");
+}
+
+void lrc_device_free(lrc_ctx *c, void *p) {
+    if (!c || !p) return;
+    DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->st);
+    cudaFree(p);
+}
+
+int lrc_device_copy(lrc_ctx *c, void *dst, const void *src, size_t bytes, int kind) {
+    if (!c || (bytes && (!dst || !src)) || kind < LRC_COPY_H2D || kind > LRC_COPY_D2D) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    const cudaMemcpyKind k = kind == LRC_COPY_H2D ? cudaMemcpyHostToDevice
+                             : kind == LRC_COPY_D2H ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    cudaError_t e = bytes ? cudaMemcpyAsync(dst, src, bytes, k, c->st) : cudaSuccess;
+    if (e) return cuda_status(c, e, "lrc_device_copy");
+    return check_status(c);
+}
+
+int lrc_device_zero(lrc_ctx *c, void *p, size_t bytes) {
+    if (!c || (bytes && !p)) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    cudaError_t e = bytes ? cudaMemsetAsync(p, 0, bytes, c->st) : cudaSuccess;
+    return cuda_status(c, e, "lrc_device_zero");
+}
+
+int lrc_query(lrc_ctx *c) {
+    if (!c) return LRC_E_INVALID;
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaStreamQuery(c->st);
+    if (e == cudaErrorNotReady) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (e) return cuda_status(c, e, "lrc_query");
+    return 1;
 }
 
 int lrc_scene_tree_device(lrc_scene *s, const uint32_t **nodes, const uint32_t **aux, uint32_t *n) {
@@ -445,6 +541,7 @@ int lrc_scene_set_prims(lrc_scene *s, const float *prims, uint32_t n, unsigned f
     if (e) return cuda_status(c, e, "primitives");
     s->nprims = n;
     s->built_n = 0;
+    s->tree_nnodes = s->tree_naux = 0;
     return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 
@@ -795,6 +892,7 @@ int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
     P.seed = p->seed;
     P.clamp = p->clamp;
     P.skip_caustics = p->skip_caustics != 0;
+    P.indirect_clamp = p->indirect_clamp;
     P.origin = {p->origin[0], p->origin[1], p->origin[2]};
     P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
     P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};
@@ -813,6 +911,32 @@ int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
         const size_t N = (size_t)p->width * p->height;
         P.moments = reinterpret_cast<float4 *>(d_acc) + N;
         P.guide = reinterpret_cast<const float4 *>(d_acc) + 3 * N;
+    }
+    // a large image runs as a one-job batch on the wavefront engine: its kernels keep their own
+    // registers (the one-kernel path sits at its cap with every bounce's code in one loop), and its
+    // image is this call's to the bit (a batch task traces a pixel's samples as the one-kernel
+    // path's lanes do and the resolve pass adds them in that path's order)
+    const uint64_t paths = (uint64_t)p->width * (uint64_t)rows * spp;
+    if (!e && !(flags & LRC_TRACE_MEGAKERNEL) && !s->nvol && rows > 0 && spp > 0 && paths >= LRC_TRACE_WAVEFRONT_PATHS) {
+        int rc = LRC_OK;
+        if (!c->single) {
+            rc = lrc_batch_create(c, &c->single);
+            if (rc) return rc;
+        }
+        rc = lrc_batch_set_wavefront(c->single, paths >= (8u << 20) ? 1u << 22 : 1u << 20, 0);
+        if (!rc) rc = lrc_batch_clear(c->single);
+        if (!rc) rc = guided ? lrc_batch_add_guided(c->single, s, p, y0, rows, spp0, spp, d_acc, -1, 30)
+                             : lrc_batch_add(c->single, s, p, y0, rows, spp0, spp, d_acc, -1, 30);
+        c->timer.begin(LRC_TS_SHADE, c->st);
+        if (!rc) rc = lrc_batch_run(c->single, 0);
+        c->timer.end(c->st);
+        if (rc) return rc;
+        if (!(flags & LRC_DEVICE)) {
+            e = cudaMemcpyAsync(accum, d_acc, bytes, cudaMemcpyDeviceToHost, c->st);
+            if (e) return cuda_status(c, e, "lrc_trace");
+        }
+        if (rays) return lrc_batch_rays(c->single, rays, nullptr);   // (waits)
+        return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
     }
     c->timer.begin(LRC_TS_SHADE, c->st);
     if (!e) e = lrc::pt_trace(pt_scene(s), P, d_acc, s->d_rays, c->d_status, c->st);

@@ -21,6 +21,7 @@ struct lrc_ctx {
     int lt_variant = -1;          // the light tracer's launch variant (-1: the default)
     void *dn = nullptr;           // the denoiser's scratch (packed image ping-pong and guide)
     size_t dn_cap = 0;
+    lrc_batch *single = nullptr;  // lrc_trace's one-job batch on the wavefront engine (large images)
 };
 
 struct lrc_scene {
@@ -32,6 +33,8 @@ struct lrc_scene {
     uint32_t *d_aux = nullptr;
     size_t tree_cap = 0;          // items the tree buffers hold
     uint32_t built_n = 0;         // items of the built tree (0: none)
+    uint32_t tree_nnodes = 0;     // a tree given by lrc_scene_set_tree: its nodes and aux entries
+    uint32_t tree_naux = 0;       // (0: the built tree's 2 n - 1 and n)
     float *d_boxes = nullptr;
     size_t boxes_cap = 0;
     uint32_t *d_small = nullptr;  // 6 bound keys, 6 bounds, 6 lo/ext
@@ -162,8 +165,8 @@ inline lrc::PtScene pt_scene(const lrc_scene *s) {
     S.nodes = reinterpret_cast<const float4 *>(s->d_nodes);
     S.aux = s->d_aux;
     S.root = 0;
-    S.nnodes = s->built_n ? 2 * s->built_n - 1 : 0;
-    S.naux = s->built_n;
+    S.nnodes = s->tree_nnodes ? s->tree_nnodes : (s->built_n ? 2 * s->built_n - 1 : 0);
+    S.naux = s->tree_nnodes ? s->tree_naux : s->built_n;
     S.prims = reinterpret_cast<const float4 *>(s->d_prims);
     S.nprims = s->nprims;
     S.tris = reinterpret_cast<const float4 *>(s->d_tris);
@@ -229,8 +232,8 @@ inline lrc::TraceTables tables(const lrc_scene *s) {
     tt.aux = s->d_aux;
     tt.tris = reinterpret_cast<const float4 *>(s->d_tris);
     tt.root = 0;
-    tt.nnodes = 2 * s->built_n - 1;
-    tt.naux = s->built_n;
+    tt.nnodes = s->tree_nnodes ? s->tree_nnodes : 2 * s->built_n - 1;
+    tt.naux = s->tree_nnodes ? s->tree_naux : s->built_n;
     tt.ntris = s->ntris;
     return tt;
 }

@@ -90,6 +90,7 @@ lrc::PtParams params_of(const lrc_batch::Job &J) {
     P.seed = p->seed;
     P.clamp = p->clamp;
     P.skip_caustics = p->skip_caustics != 0;
+    P.indirect_clamp = p->indirect_clamp;
     if (J.guided) {
         const size_t N = (size_t)p->width * p->height;
         P.moments = reinterpret_cast<float4 *>(J.accum) + N;
@@ -600,6 +601,27 @@ int lrc_batch_rays(lrc_batch *b, uint64_t *per_job, uint64_t *total) {
         t += r[i];
     }
     if (total) *total = t;
+    return LRC_OK;
+}
+
+int lrc_batch_passes(lrc_batch *b, uint32_t *passes, uint64_t *kernels) {
+    if (!b) return LRC_E_INVALID;
+    lrc_ctx *c = b->ctx;
+    uint32_t n = 0;
+    uint64_t k = 0;
+    if (b->prepared && b->engine == 1 && b->d_wf) {
+        DeviceGuard g(c->device);
+        int rc = check_status(c);
+        if (rc) return rc;
+        const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
+        cudaError_t e = cudaMemcpy(&n, W.ctl + 4, 4, cudaMemcpyDeviceToHost);
+        if (e) return cuda_status(c, e, "batch passes");
+        k = 2 + 4 * (uint64_t)n;                         // clear, then advance / closest hit / shade / shadow a pass, resolve
+    } else if (b->prepared) {
+        k = 2;                                           // the persistent trace kernel and the resolve pass
+    }
+    if (passes) *passes = n;
+    if (kernels) *kernels = k;
     return LRC_OK;
 }
 

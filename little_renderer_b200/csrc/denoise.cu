@@ -569,6 +569,7 @@ lrc::PtParams trace_params_of(const lrc_trace_params *p) {
     P.seed = p->seed;
     P.clamp = p->clamp;
     P.skip_caustics = p->skip_caustics != 0;
+    P.indirect_clamp = p->indirect_clamp;
     P.origin = {p->origin[0], p->origin[1], p->origin[2]};
     P.upper_left = {p->upper_left[0], p->upper_left[1], p->upper_left[2]};
     P.horizontal = {p->horizontal[0], p->horizontal[1], p->horizontal[2]};

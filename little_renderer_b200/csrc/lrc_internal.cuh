@@ -227,6 +227,7 @@ struct PtParams {
     float clamp;
     pt::V3 origin, upper_left, horizontal, vertical;   // the Camera (camera.h)
     int skip_caustics;                                 // TraceParams.skip_caustics
+    float indirect_clamp;                              // TraceParams.indirect_clamp (0: off)
     // the denoiser's planes (lrc_trace with LRC_TRACE_GUIDED; null: none): each sample's luminance
     // over the guide's albedo (plane 3) added to the moments (plane 1) as (l, l^2), and the last
     // sample's l and number in its z and w

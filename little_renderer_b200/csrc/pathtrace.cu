@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
             float u = dvd(add((float)x, jx), (float)J.P.W), v = dvd(add((float)y, jy), (float)J.P.H);
             V3 o, d;
             camera_ray(J.P, u, v, o, d);
-            path_begin(J.P.mis || (MEDIA && J.S.nvol), o, d, ps, J.P.skip_caustics);
+            path_begin(J.P.mis || (MEDIA && J.S.nvol), o, d, ps, J.P.skip_caustics, J.P.indirect_clamp);
             active = true;
         }
         if (!path_bounce<MEDIA>(J.S, J.P.max_depth, J.P.mis, ps, sm, err, rays)) {

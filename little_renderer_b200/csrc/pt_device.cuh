@@ -543,7 +543,7 @@ __device__ __forceinline__ V3 env_in_medium(const PtScene &S, V3 p, V3 d, float 
 // One bounce's next event estimation with its shadow rays not yet traced (the wavefront batch):
 // the throughput the contributions are weighted by, the lamp's and the sky's contribution if
 // their ray is unoccluded, the rays (from p) and which of it there is.
-enum { NEE_L = 1, NEE_E = 2, NEE_RL = 4, NEE_RE = 8 };
+enum { NEE_L = 1, NEE_E = 2, NEE_RL = 4, NEE_RE = 8, NEE_ROUGH = 16 };   // ROUGH: their indirect cap is on
 struct Nee {
     V3 thr, vl, ve, p, wl, we;
     float tl;
@@ -574,24 +574,39 @@ enum { EMIT_FULL, EMIT_NONE, EMIT_MIS };
 // skip_caustics' state (tracer.c:371-375): CAUS_CHAIN the camera saw a rough surface first,
 // CAUS_SPEC a mirror / glass vertex since the last rough one; a path with both that reaches the
 // lamp is light tracing's (lrc_caustics), not counted here. CAUS_SKIP: the job leaves them out.
-enum { CAUS_CHAIN = 1, CAUS_SPEC = 2, CAUS_SKIP = 4 };
+// CAUS_ROUGH (the same bits): a rough bounce (or a medium's) so far, so that from then on what the
+// path brings is indirect light, each part held to the job's indirect clamp (tracer.c:376-378).
+enum { CAUS_CHAIN = 1, CAUS_SPEC = 2, CAUS_SKIP = 4, CAUS_ROUGH = 8 };
 
 struct PathState {
     V3 ro, rd, thr, radiance;
     float bounce_pdf;
+    float icap;                                      // TraceParams.indirect_clamp (0: off)
     int depth, emit, caus;
 };
 
 // (norm: MIS or media, whose distances and pdfs need a unit direction: tracer.c:380)
-__device__ __forceinline__ void path_begin(int norm, V3 ro, V3 rd, PathState &ps, int skip_caustics) {
+__device__ __forceinline__ void path_begin(int norm, V3 ro, V3 rd, PathState &ps, int skip_caustics, float icap) {
     ps.ro = ro;
     ps.rd = norm ? vnorm(rd) : rd;
     ps.thr = v3(1, 1, 1);
     ps.radiance = v3(0, 0, 0);
     ps.bounce_pdf = 0.0f;
+    ps.icap = icap;
     ps.depth = 0;
     ps.emit = EMIT_FULL;
     ps.caus = skip_caustics ? CAUS_SKIP : 0;
+}
+
+// indirect_cap (tracer.c:358-362): a contribution c after a rough bounce (on) held to k by its
+// largest channel, c scaled by k / max
+__device__ __forceinline__ V3 indirect_cap(V3 c, bool on, float k) {
+    const float m = vmax3(c);
+    return on && k > 0.0f && m > k ? vscale(c, dvd(k, m)) : c;
+}
+// radiance += indirect_cap(c, the path is past a rough bounce)
+__device__ __forceinline__ void path_add(PathState &ps, V3 c) {
+    ps.radiance = vadd(ps.radiance, indirect_cap(c, (ps.caus & CAUS_ROUGH) != 0, ps.icap));
 }
 
 // scene_intersect's search alone: the closest t, the world shape (or -1) and the instance and its
@@ -648,7 +663,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
             if (have_lamp) {
                 const Lamp L = load_lamp(S);
                 sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
-                ps.radiance = vadd(ps.radiance, vmul(ps.thr, light_in_medium(S, L, p, ps.rd, vol.g, mis, lb, la, *sm.rng, err, rays)));
+                path_add(ps, vmul(ps.thr, light_in_medium(S, L, p, ps.rd, vol.g, mis, lb, la, *sm.rng, err, rays)));
             }
             if (S.has_env) {
                 if (!have_lamp) sampler_2d(sm, SAMPLE_LIGHT(depth), la, lb);
@@ -656,7 +671,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
                     la = rng_real(*sm.rng);
                     lb = rng_real(*sm.rng);
                 }
-                ps.radiance = vadd(ps.radiance, vmul(ps.thr, env_in_medium(S, p, ps.rd, vol.g, mis, la, lb, *sm.rng, err, rays)));
+                path_add(ps, vmul(ps.thr, env_in_medium(S, p, ps.rd, vol.g, mis, la, lb, *sm.rng, err, rays)));
             }
             float da, db;
             sampler_2d(sm, SAMPLE_DIR(depth), da, db);
@@ -665,7 +680,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
             ps.ro = p;
             ps.rd = nd;
             ps.emit = mis ? EMIT_MIS : EMIT_NONE;
-            ps.caus &= ~CAUS_CHAIN;
+            ps.caus = (ps.caus & ~CAUS_CHAIN) | CAUS_ROUGH;
             if (depth >= RR_START) {                 // russian_roulette (tracer.c:302-304)
                 const float u = sampler_1d(sm, SAMPLE_MISC(depth), 0);
                 const float pr = rmin(vmax3(ps.thr), 0.95f);
@@ -680,7 +695,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
         if (S.has_env && ps.emit != EMIT_NONE) {
             V3 le = env_eval(S, ps.rd);
             if (ps.emit == EMIT_MIS) le = vscale(le, power_heuristic(ps.bounce_pdf, env_pdf(S, ps.rd)));
-            ps.radiance = vadd(ps.radiance, vmul(ps.thr, le));
+            path_add(ps, vmul(ps.thr, le));
         }
         return false;
     }
@@ -689,19 +704,19 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
     if (m.type == MAT_LIGHT) {
         if (h.front && (ps.caus & (CAUS_CHAIN | CAUS_SPEC)) != (CAUS_CHAIN | CAUS_SPEC)) {
             if (ps.emit == EMIT_FULL) {
-                ps.radiance = vadd(ps.radiance, vmul(ps.thr, m.emission));
+                path_add(ps, vmul(ps.thr, m.emission));
             } else if (ps.emit == EMIT_MIS && h.inst < 0 && h.prim == S.light) {
                 const Lamp L = load_lamp(S);
                 float cos_light = -vdot(L.normal, ps.rd);
                 if (cos_light > 0.0f) {
                     float w = power_heuristic(ps.bounce_pdf, light_pdf(L, mul(h.t, h.t), cos_light));
-                    ps.radiance = vadd(ps.radiance, vmul(ps.thr, vscale(m.emission, w)));
+                    path_add(ps, vmul(ps.thr, vscale(m.emission, w)));
                 }
             }
         }
         return false;
     }
-    if (glows(m)) ps.radiance = vadd(ps.radiance, vmul(ps.thr, m.emission));   // (no glowing shapes sampled)
+    if (glows(m)) path_add(ps, vmul(ps.thr, m.emission));   // (no glowing shapes sampled)
     if (depth >= max_depth) return false;
     V3 v = vneg(vnorm(ps.rd));
     Bsdf b = bsdf_make(m, h.front, S.tab);
@@ -710,6 +725,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
         if (DEFER) {
             nee.thr = ps.thr;
             nee.p = h.p;
+            if ((ps.caus & CAUS_ROUGH) && ps.icap > 0.0f) nee.flags |= NEE_ROUGH;
         }
         if (have_lamp) {
             const Lamp L = load_lamp(S);
@@ -727,7 +743,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
             } else {
                 if (ray && occluded<MEDIA>(S, h.p, wi, RT_EPS, tmax, err)) V = v3(0, 0, 0);
                 else if (MEDIA && ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S.vols, S.nvol, h.p, wi, 0.0f, M.dist, *sm.rng, err));
-                ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
+                path_add(ps, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
         }
         if (S.has_env) {
@@ -748,7 +764,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
             } else {
                 if (ray && occluded<MEDIA>(S, h.p, wi, RT_EPS, 1e30f, err)) V = v3(0, 0, 0);
                 else if (MEDIA && ray && S.nvol) V = nee_through(M, mis, scene_medium_transmittance(S.vols, S.nvol, h.p, wi, 0.0f, M.dist, *sm.rng, err));
-                ps.radiance = vadd(ps.radiance, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
+                path_add(ps, vmul(ps.thr, ray ? V : v3(0, 0, 0)));
             }
         }
     }
@@ -767,7 +783,7 @@ __device__ __forceinline__ bool path_shade(const PtScene &S, int max_depth, int 
         ps.bounce_pdf = bs.pdf;
         ps.emit = mis ? EMIT_MIS : EMIT_NONE;
         if (depth == 0 && (ps.caus & CAUS_SKIP)) ps.caus |= CAUS_CHAIN;
-        ps.caus &= ~CAUS_SPEC;
+        ps.caus = (ps.caus & ~CAUS_SPEC) | CAUS_ROUGH;
     }
     if (depth >= RR_START) {                         // russian_roulette_u
         float p = rmin(vmax3(ps.thr), 0.95f);
@@ -798,7 +814,7 @@ template <bool MEDIA = false>
 __device__ __forceinline__ V3 trace_path(const PtScene &S, const PtParams &P, V3 ro, V3 rd, Sampler &sm, uint32_t *err,
                                          uint32_t &rays) {
     PathState ps;
-    path_begin(P.mis || (MEDIA && S.nvol), ro, rd, ps, P.skip_caustics);
+    path_begin(P.mis || (MEDIA && S.nvol), ro, rd, ps, P.skip_caustics, P.indirect_clamp);
     while (path_bounce<MEDIA>(S, P.max_depth, P.mis, ps, sm, err, rays)) {
     }
     return ps.radiance;

@@ -64,6 +64,10 @@ struct lrc_server {
     uint32_t *d_small = nullptr;
     void *dn = nullptr;                 // the denoiser's scratch
     size_t dn_cap = 0;
+    uint64_t waves = 0, kernels = 0;    // waves run and the trace kernels they launched
+    double gpu_ms = 0;                  // the waves' device time (CUDA events around each)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int policy = 0;                     // how a wave is made (lrc_server_set_policy)
 };
 
 namespace {
@@ -196,6 +200,8 @@ void lrc_server_destroy(lrc_server *sv) {
     cudaFree(sv->d_boxes);
     cudaFree(sv->d_small);
     cudaFree(sv->dn);
+    if (sv->ev0) cudaEventDestroy(sv->ev0);
+    if (sv->ev1) cudaEventDestroy(sv->ev1);
     delete sv;
 }
 
@@ -248,29 +254,64 @@ int lrc_server_step(lrc_server *sv, int32_t *finished) {
         sv->active.push_back(J);
     }
     if (sv->active.empty()) return LRC_OK;
-    // the wave: the next band of every admitted job, the paths shared evenly
+    // the wave: bands of the admitted jobs. Policy 0: the next band of every job, the wave's paths
+    // shared evenly; 1: the oldest jobs first, each band as large as the wave's paths left allow
+    // (few scenes a wave, each wave's jobs ending sooner); 2: as 1, the jobs with the fewest paths
+    // left first.
+    std::vector<lrc_server::Job *> order(sv->active);
+    if (sv->policy == 2)
+        std::stable_sort(order.begin(), order.end(), [](const lrc_server::Job *a, const lrc_server::Job *b) {
+            return (uint64_t)a->p.width * (a->p.height - a->next_row) * a->spp <
+                   (uint64_t)b->p.width * (b->p.height - b->next_row) * b->spp;
+        });
+    for (lrc_server::Job *J : sv->active) J->band = 0;
     const uint64_t share = sv->wave_paths / sv->active.size() + 1;
+    uint64_t used = 0;
     int rc = lrc_batch_clear(sv->batch);
-    for (lrc_server::Job *J : sv->active) {
+    std::vector<lrc_server::Job *> in_wave;
+    for (lrc_server::Job *J : order) {
         const uint64_t row_paths = (uint64_t)J->p.width * J->spp;
-        int32_t rows = (int32_t)std::max<uint64_t>(1, share / row_paths);
+        int32_t rows;
+        if (sv->policy == 0) {
+            rows = (int32_t)std::max<uint64_t>(1, share / row_paths);
+        } else {
+            if (used >= sv->wave_paths) break;
+            rows = (int32_t)std::max<uint64_t>(1, (sv->wave_paths - used + row_paths - 1) / row_paths);
+        }
         rows = std::min(rows, J->p.height - J->next_row);
         J->band = rows;
+        used += (uint64_t)rows * row_paths;
+        in_wave.push_back(J);
         InstView v{J->d_inst, J->d_tlas, J->d_tlas_aux};
         if (!rc) rc = batch_add_view(sv->batch, J->s, &J->p, J->next_row, rows, 0, J->spp,
                                      J->denoise ? J->d_planes : J->d_img, v, J->denoise);
     }
+    if (!sv->ev0 && !rc) {
+        if (cudaEventCreate(&sv->ev0) || cudaEventCreate(&sv->ev1)) return cuda_status(c, cudaGetLastError(), "server events");
+    }
+    if (!rc) cudaEventRecord(sv->ev0, c->st);
     if (!rc) rc = lrc_batch_run(sv->batch, 0);
-    std::vector<uint64_t> rays(sv->active.size());
-    if (!rc) rc = lrc_batch_rays(sv->batch, rays.data(), nullptr);   // (waits for the wave)
+    if (!rc) cudaEventRecord(sv->ev1, c->st);
+    std::vector<uint64_t> wave_rays(in_wave.size());
+    if (!rc) rc = lrc_batch_rays(sv->batch, wave_rays.data(), nullptr);   // (waits for the wave)
+    uint64_t kernels = 0;
+    if (!rc) rc = lrc_batch_passes(sv->batch, nullptr, &kernels);
     if (rc) return rc;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, sv->ev0, sv->ev1) == cudaSuccess) sv->gpu_ms += ms;
+    sv->waves++;
+    sv->kernels += kernels;
+    std::vector<uint64_t> rays(sv->active.size(), 0);   // (in the wave's order: back to the active list's)
+    for (size_t i = 0; i < sv->active.size(); i++)
+        for (size_t q = 0; q < in_wave.size(); q++)
+            if (in_wave[q] == sv->active[i]) rays[i] = wave_rays[q];
     const double t = now_ms();
     std::vector<lrc_server::Job *> still;
     for (size_t i = 0; i < sv->active.size(); i++) {
         lrc_server::Job *J = sv->active[i];
         J->rays += rays[i];
         J->next_row += J->band;
-        if (J->next_row >= J->p.height) {
+        if (J->band && J->next_row >= J->p.height) {
             if (J->denoise) {                           // the image denoised, the planes freed
                 cudaError_t e = reserve(&sv->dn, &sv->dn_cap, lrc::dn_scratch_bytes(J->p.width, J->p.height));
                 if (!e) e = lrc::dn_denoise(reinterpret_cast<const float4 *>(J->d_planes), J->p.width, J->p.height, 5,
@@ -347,6 +388,20 @@ int lrc_server_release(lrc_server *sv, uint64_t id) {
 }
 
 lrc_batch *lrc_server_batch(lrc_server *sv) { return sv ? sv->batch : nullptr; }
+
+int lrc_server_stats(const lrc_server *sv, uint64_t *waves, uint64_t *kernels, double *gpu_ms) {
+    if (!sv) return LRC_E_INVALID;
+    if (waves) *waves = sv->waves;
+    if (kernels) *kernels = sv->kernels;
+    if (gpu_ms) *gpu_ms = sv->gpu_ms;
+    return LRC_OK;
+}
+
+int lrc_server_set_policy(lrc_server *sv, int32_t policy) {
+    if (!sv || policy < 0 || policy > 2) return LRC_E_INVALID;
+    sv->policy = policy;
+    return LRC_OK;
+}
 
 int lrc_server_state(const lrc_server *sv, int32_t *queued, int32_t *active, int32_t *finished, uint64_t *bytes) {
     if (!sv) return LRC_E_INVALID;

@@ -78,10 +78,14 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
         const BatchJob &J = jobs[j];
         const float4 r = W.rad[i];
         V3 rad = v3f(r);
-        if (f0 & (NEE_L | NEE_E)) {
+        if (f0 & (NEE_L | NEE_E)) {                  // (each held to the indirect cap when it was on)
             const V3 thr = v3f(W.nthr[i]);
-            if (f0 & NEE_L) rad = vadd(rad, vmul(thr, (f0 & NEE_RL) && W.vis[2 * i] ? v3f(W.nvl[i]) : v3(0, 0, 0)));
-            if (f0 & NEE_E) rad = vadd(rad, vmul(thr, (f0 & NEE_RE) && W.vis[2 * i + 1] ? v3f(W.nve[i]) : v3(0, 0, 0)));
+            const bool cap = (f0 & NEE_ROUGH) != 0;
+            const float k = J.P.indirect_clamp;
+            if (f0 & NEE_L)
+                rad = vadd(rad, indirect_cap(vmul(thr, (f0 & NEE_RL) && W.vis[2 * i] ? v3f(W.nvl[i]) : v3(0, 0, 0)), cap, k));
+            if (f0 & NEE_E)
+                rad = vadd(rad, indirect_cap(vmul(thr, (f0 & NEE_RE) && W.vis[2 * i + 1] ? v3f(W.nve[i]) : v3(0, 0, 0)), cap, k));
         }
         if (f0 & F_ENDED) {                          // the sample into its task's sum
             const V3 s = is_number(rad) ? clamp_sample(rad, J.P.clamp) : v3(0, 0, 0);
@@ -166,7 +170,7 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
         V3 o, d;
         camera_ray(J.P, u, v, o, d);
         PathState ps;
-        path_begin(J.P.mis || J.S.nvol, o, d, ps, J.P.skip_caustics);
+        path_begin(J.P.mis || J.S.nvol, o, d, ps, J.P.skip_caustics, J.P.indirect_clamp);
         W.ro[i] = make_float4(ps.ro.x, ps.ro.y, ps.ro.z, ps.bounce_pdf);
         W.rd[i] = make_float4(ps.rd.x, ps.rd.y, ps.rd.z, __int_as_float(ps.depth | (ps.emit << 16) | (ps.caus << 24)));
         W.thr[i] = make_float4(ps.thr.x, ps.thr.y, ps.thr.z, 0.0f);
@@ -255,6 +259,7 @@ __global__ void __launch_bounds__(SHADE_BLOCK, SMINB) wf_shade_kernel(const Batc
             ps.caus = de >> 24;
             ps.thr = v3f(th);
             ps.radiance = v3f(ra);
+            ps.icap = J.P.indirect_clamp;
             const ulonglong2 r = W.rng[s];
             Rng rng;
             rng.state = r.x;

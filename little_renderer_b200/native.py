@@ -21,6 +21,7 @@ OBJ_DIR = os.path.join(PKG, "_build")
 LRC_OK, LRC_RETRY, LRC_E_INVALID, LRC_E_CUDA, LRC_E_TIMEOUT, LRC_E_STACK, LRC_E_NODEVICE = 0, 1, -1, -2, -3, -4, -5
 LRC_DEVICE = 1
 LRC_TRACE_GUIDED = 64
+LRC_TRACE_MEGAKERNEL = 256
 LRC_REPROJECT_EDIT = 128
 LRC_SERVE_DENOISE = 16
 LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED = 4, 8, 16, 32
@@ -203,16 +204,18 @@ class TraceParams(C.Structure):
     _fields_ = [("origin", C.c_float * 3), ("upper_left", C.c_float * 3), ("horizontal", C.c_float * 3),
                 ("vertical", C.c_float * 3), ("width", C.c_int32), ("height", C.c_int32), ("max_depth", C.c_int32),
                 ("mis", C.c_int32), ("sampler", C.c_int32), ("exact", C.c_int32), ("seed", C.c_uint64),
-                ("clamp", C.c_float), ("skip_caustics", C.c_int32)]
+                ("clamp", C.c_float), ("skip_caustics", C.c_int32), ("indirect_clamp", C.c_float)]
 
 
-def trace_params(cam12, width, height, max_depth=8, mis=1, sampler=1, exact=0, seed=0, clamp=0.0, skip_caustics=0):
+def trace_params(cam12, width, height, max_depth=8, mis=1, sampler=1, exact=0, seed=0, clamp=0.0, skip_caustics=0,
+                 indirect_clamp=0.0):
     p = TraceParams()
     cam12 = np.asarray(cam12, np.float32).reshape(4, 3)
     for i, name in enumerate(("origin", "upper_left", "horizontal", "vertical")):
         getattr(p, name)[:] = cam12[i].tolist()
     p.width, p.height, p.max_depth, p.mis, p.sampler, p.exact, p.seed, p.clamp, p.skip_caustics = (
         width, height, max_depth, mis, sampler, exact, seed, clamp, skip_caustics)
+    p.indirect_clamp = indirect_clamp
     return p
 
 
@@ -408,6 +411,12 @@ class Scene:
     def build(self, builder=0, key_bits=30):
         self.ctx.check(self.ctx.L.lrc_scene_build(self.h, builder, key_bits))
 
+    def set_tree(self, nodes, aux):
+        """lrc_scene_set_tree: the world tree given (put_nodes' layout, shape ids in aux), not built."""
+        nodes = np.ascontiguousarray(nodes, np.uint32).reshape(-1, 8)
+        aux = np.ascontiguousarray(aux, np.uint32)
+        self.ctx.check(self.ctx.L.lrc_scene_set_tree(self.h, _ptr(nodes), nodes.shape[0], _ptr(aux), aux.shape[0], 0))
+
     def tree(self):
         nodes = np.zeros((2 * self.n - 1, 8), np.uint32)
         aux = np.zeros(self.n, np.uint32)
@@ -494,20 +503,20 @@ class Scene:
                                                          _ptr(inst), _ptr(t), 0))
         return prim, inst, t
 
-    def trace(self, params, spp, accum=None, y0=0, rows=None, spp0=0):
+    def trace(self, params, spp, accum=None, y0=0, rows=None, spp0=0, flags=0):
         """lrc_trace with a host image: returns (accum (h, w, 4) sum + count, rays traced)."""
         rows = params.height if rows is None else rows
         if accum is None:
             accum = np.zeros((params.height, params.width, 4), np.float32)
         rays = C.c_uint64()
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), y0, rows, spp0, spp, _ptr(accum),
-                                            C.byref(rays), 0))
+                                            C.byref(rays), flags))
         return accum, rays.value
 
-    def trace_device(self, params, spp, d_accum, y0=0, rows=None, spp0=0):
+    def trace_device(self, params, spp, d_accum, y0=0, rows=None, spp0=0, flags=0):
         rows = params.height if rows is None else rows
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), y0, rows, spp0, spp, C.c_void_p(d_accum), None,
-                                            LRC_DEVICE))
+                                            LRC_DEVICE | flags))
 
     def set_volumes(self, vols):
         """lrc_scene_set_volumes: vols = [(density (nz, ny, nx) float32, lo, hi, sigma_t, albedo, g), ...]."""
@@ -555,12 +564,12 @@ class Scene:
     def guide_device(self, params, d_planes):
         self.ctx.check(self.ctx.L.lrc_guide(self.h, C.byref(params), C.c_void_p(d_planes), LRC_DEVICE))
 
-    def trace_guided(self, params, spp, planes, spp0=0):
+    def trace_guided(self, params, spp, planes, spp0=0, flags=0):
         """lrc_trace with LRC_TRACE_GUIDED on host planes (4, h, w, 4): samples into plane 0, the
         luminance moments into plane 1; returns (planes, rays)."""
         rays = C.c_uint64()
         self.ctx.check(self.ctx.L.lrc_trace(self.h, C.byref(params), 0, params.height, spp0, spp, _ptr(planes),
-                                            C.byref(rays), LRC_TRACE_GUIDED))
+                                            C.byref(rays), LRC_TRACE_GUIDED | flags))
         return planes, rays.value
 
     def reproject_gradients(self, old_params, new_params, spp0, old_planes, new_planes, history_max, history,
@@ -842,6 +851,15 @@ class Server:
 
     def batch_handle(self):
         return self.ctx.L.lrc_server_batch(self.h)
+
+    def stats(self):
+        """(waves run, trace kernels launched, the waves' device ms) so far (lrc_server_stats)."""
+        w, k, ms = C.c_uint64(), C.c_uint64(), C.c_double()
+        self.ctx.check(self.ctx.L.lrc_server_stats(self.h, C.byref(w), C.byref(k), C.byref(ms)))
+        return w.value, k.value, ms.value
+
+    def set_policy(self, policy):
+        self.ctx.check(self.ctx.L.lrc_server_set_policy(self.h, policy))
 
     def set_wavefront(self, slots, variant=0):
         """The waves' wavefront size (paths in flight) and closest-hit / shadow launch shape."""

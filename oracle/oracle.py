@@ -168,9 +168,16 @@ def trace_tree(nodes, aux, tris_quv, orig, dirs, tmin=0.0, tmax=1e30, node0=0):
 
 
 # ---- the reference's own CPU engine ---------------------------------------------------------------------
-def ref_lib(double=False):
-    name = os.path.join("_ref", "libref_d.so" if double else "libref_f.so")
+def ref_lib(double=False, gpu=False):
+    """The reference's CPU engine (float, or double); gpu: the float build linked with the engine's
+    gpu_frame.c and the CUDA backend (shim/gpu_cuda.c on liblrc), for the drop-in checks."""
+    name = os.path.join("_ref", "libref_gpu.so" if gpu else ("libref_d.so" if double else "libref_f.so"))
     lib = _load(name)
+    if gpu and not getattr(lib, "_gpu_typed", False):
+        lib.rb_gpu_frame_trace.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_int, _f32p]
+        lib.rb_scene_tree.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib._gpu_typed = True
     if not getattr(lib, "_typed", False):
         vp = C.c_void_p
         lib.rb_scene_new.restype = vp
@@ -197,6 +204,7 @@ def ref_lib(double=False):
         lib.rb_occluded.argtypes = [vp, _f32p, _f32p, C.c_longlong, C.c_float, C.c_float, _i32p]
         lib.rb_trace_image.argtypes = [vp, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_ulonglong, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        lib.rb_set_indirect_clamp.argtypes = [C.c_float]
         lib.rb_volume_majorants.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, _f32p]
         lib.rb_srgb_table.argtypes = [_f32p]
         lib.rb_add_texmap.argtypes = [vp, _u32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
@@ -255,9 +263,27 @@ def triangle_bounds(quv):
 class RefScene:
     """A reference Scene made through its public API (scene_add_triangle, make_quad, ...)."""
 
-    def __init__(self, double=False):
-        self.lib = ref_lib(double)
+    def __init__(self, double=False, gpu=False):
+        self.lib = ref_lib(double, gpu)
         self.s = self.lib.rb_scene_new()
+
+    def gpu_frame_trace(self, from_at_up, vfov, w, h, spp, max_depth, mis=1, sampler=1):
+        """The engine's gpu_frame_trace (engine/app/gpu_frame.c:49) through the CUDA backend (a RefScene
+        made with gpu=True): (status, (h, w, 3) mean image)."""
+        out = np.zeros((h, w, 3), np.float32)
+        rc = self.lib.rb_gpu_frame_trace(self.s, np.ascontiguousarray(from_at_up, np.float32).reshape(-1), vfov, w, h,
+                                         spp, max_depth, mis, sampler, out.reshape(-1))
+        return rc, out
+
+    def tree(self):
+        """The scene's own tree (scene_set_accel made it) in put_nodes' layout: ((n, 8) uint32 nodes, refs)."""
+        nn, nr = C.c_int(), C.c_int()
+        if not self.lib.rb_scene_tree(self.s, None, None, C.byref(nn), C.byref(nr)):
+            return None
+        nodes = np.zeros((nn.value, 8), np.uint32)
+        refs = np.zeros(nr.value, np.uint32)
+        self.lib.rb_scene_tree(self.s, nodes.ctypes.data, refs.ctypes.data, C.byref(nn), C.byref(nr))
+        return nodes, refs
 
     def close(self):
         if self.s:
@@ -359,13 +385,18 @@ class RefScene:
                              np.ascontiguousarray(dirs, np.float32).reshape(-1), n, tmin, tmax, out)
         return out
 
-    def trace_image(self, cam, vfov, w, h, spp, seed, max_depth, mis=1, sampler=1, y0=0, rows=None, skip_caustics=0):
+    def trace_image(self, cam, vfov, w, h, spp, seed, max_depth, mis=1, sampler=1, y0=0, rows=None, skip_caustics=0,
+                    indirect_clamp=0.0):
         """trace_image: (rows, w, 3) mean radiance; returns (image, (closest rays, shadow rays))."""
         rows = h if rows is None else rows
         out = np.zeros((rows, w, 3), np.float32)
         self.lib.rb_rays_reset()
-        self.lib.rb_trace_image(self.s, np.ascontiguousarray(cam, np.float32).reshape(-1), vfov, w, h, y0, rows,
-                                spp, seed, max_depth, mis, sampler, skip_caustics, out.reshape(-1))
+        self.lib.rb_set_indirect_clamp(indirect_clamp)
+        try:
+            self.lib.rb_trace_image(self.s, np.ascontiguousarray(cam, np.float32).reshape(-1), vfov, w, h, y0, rows,
+                                    spp, seed, max_depth, mis, sampler, skip_caustics, out.reshape(-1))
+        finally:
+            self.lib.rb_set_indirect_clamp(0.0)
         cnt = np.zeros(2, np.int64)
         self.lib.rb_rays(cnt)
         return out, (int(cnt[0]), int(cnt[1]))

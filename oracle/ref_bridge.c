@@ -309,6 +309,10 @@ void rb_occluded(const void *sp, const float *orig, const float *dir, long long 
     }
 }
 
+// TraceParams.indirect_clamp of the next rb_trace_image calls (0: off, trace_default_params')
+static float g_indirect_clamp = 0;
+void rb_set_indirect_clamp(float v){ g_indirect_clamp = v; }
+
 // trace_image over rows [y0, y0 + rows) of a w x h image (rows = h: all of it); rgb: rows * w * 3
 // floats (the mean of each pixel's spp samples). cam: from, at, up (9 floats), vfov in degrees.
 void rb_trace_image(const void *sp, const float *cam, float vfov, int w, int h, int y0, int rows, int spp,
@@ -320,6 +324,7 @@ void rb_trace_image(const void *sp, const float *cam, float vfov, int w, int h, 
     tp.mis = mis;
     tp.sampler = sampler;
     tp.skip_caustics = skip_caustics;
+    tp.indirect_clamp = g_indirect_clamp;
     Vec3 *px = malloc(sizeof(Vec3) * (size_t)w * h);
     if (!px) return;
     if (rows == h && y0 == 0) trace_image(s, &c, &tp, w, h, spp, seed, 0, px, NULL, NULL);

@@ -1,10 +1,11 @@
-"""Makes tests/golden/cornell128_fp64_4096spp.npy: the plain render's scene (the open box, its
-lamp and 64 icospheres; workloads.cornell_spheres at 128 x 128) rendered by the reference's own
+"""Makes tests/golden/cornell<size>_fp64_4096spp.npy: the plain render's scene (the open box, its
+lamp and 64 icospheres; workloads.cornell_spheres at size x size) rendered by the reference's own
 double-precision CPU build (trace_image, engine/rt/tracer.c:329, built with -DLR_DOUBLE) at 4096
 samples per pixel, seed 1, depth 8, NEE + MIS, Owen-Sobol sampler: the FP64 oracle images are
-measured against. Stored as float32 mean radiance (128, 128, 3).
+measured against. Stored as float32 mean radiance (size, size, 3). Sizes: 128 (the small tests)
+and 256 (the plain render's own size).
 
-    python tests/golden/make_fp64_golden.py      # needs the reference's sources (oracle/_ref)
+    python tests/golden/make_fp64_golden.py [size]   # needs the reference's sources (oracle/_ref)
 """
 import os
 import sys
@@ -32,7 +33,8 @@ def scene(sc, double):
     return ref
 
 
-def main():
+def main(size=SIZE):
+    SIZE = size
     sc = W.cornell_spheres(width=SIZE, height=SIZE)
     c = sc["camera"]
     cam = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
@@ -45,4 +47,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(int(sys.argv[1]) if len(sys.argv) > 1 else SIZE)

@@ -68,10 +68,11 @@ def test_exact_mode_is_the_cpu_image(ctx, oracle, cornell128):
     exact = np.all(gpu == cpu, axis=2).mean()
     err = rel_rmse(gpu, cpu)
     print(f"pixels equal to the bit: {exact:.4f}; relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}")
-    assert exact > 0.5
-    assert err < 0.05
-    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 0.01
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.02
+    # (measured: 85 % of the pixels equal to the bit, relRMSE 3e-6, rays within a few of 10^6)
+    assert exact >= 0.7
+    assert err <= 1e-4
+    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 1e-4
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-3
 
 
 def test_fast_mode_mean_matches_cpu(ctx, oracle, cornell128):
@@ -123,3 +124,106 @@ def test_relrmse_against_the_fp64_oracle(ctx, oracle, cornell128):
     assert abs(e_fast - e_cpu) / e_cpu < 0.10
     assert e_hi < 0.35 * e_cpu
     assert abs(hi.mean() - golden.mean()) / golden.mean() < 0.01
+
+
+@pytest.fixture(scope="module")
+def cornell256(oracle):
+    return W.cornell_spheres(width=256, height=256)
+
+
+def test_plain_render_at_its_size_is_the_cpu_image(ctx, oracle, cornell256):
+    """The plain render as configured (256 x 256, 16 spp, depth 8, NEE + MIS) in exact mode against
+    the reference's trace_image: 1M paths, so lrc_trace runs it on the wavefront engine."""
+    sc = cornell256
+    spp, seed = 16, 3
+    assert sc["max_depth"] == 8
+    ref = ref_scene(oracle, sc)
+    cpu, (closest, shadow) = ref.trace_image(cam9(sc), sc["camera"]["vfov"], 256, 256, spp, seed, sc["max_depth"])
+    s = R.world_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    p = L.native.trace_params(oracle.camera(cam9(sc), sc["camera"]["vfov"], 1.0), 256, 256, sc["max_depth"], 1, 1, 1, seed)
+    acc, rays = s.trace(p, spp)
+    gpu = acc[..., :3] * (np.float32(1) / np.float32(spp))
+    exact = np.all(gpu == cpu, axis=2).mean()
+    err = rel_rmse(gpu, cpu)
+    print(f"256^2 16 spp: pixels equal to the bit {exact:.4f}; relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}")
+    # (measured: 79 % of the pixels equal to the bit, rays 5556201 vs 5556196, relRMSE 1.9e-3: of the
+    # 1M paths a handful part where CUDA's and the C library's transcendentals round differently,
+    # and one that then reaches the lamp through glass is a bright sample of its pixel)
+    assert exact >= 0.7
+    assert err <= 5e-3
+    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 1e-3
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-5
+
+
+GOLDEN256 = __import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "cornell256_fp64_4096spp.npy")
+
+
+def test_plain_render_against_the_fp64_oracle_at_its_size(ctx, oracle, cornell256):
+    """Equal RMSE at the plain render's own size: against the FP64 oracle (the reference's double
+    build, 4096 spp, tests/golden/cornell256_fp64_4096spp.npy), the GPU's exact-mode image at 16
+    spp is as far from it as the CPU float build's, within 1 % relative; the mean radiance of a
+    1024-spp GPU render within 1 % of the oracle's, and its relRMSE well below the 16-spp one."""
+    golden = np.load(GOLDEN256)
+    sc = cornell256
+    spp, seed = 16, 1
+    ref = ref_scene(oracle, sc)
+    cpu, _ = ref.trace_image(cam9(sc), sc["camera"]["vfov"], 256, 256, spp, seed, sc["max_depth"])
+    s = R.world_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    p = L.native.trace_params(oracle.camera(cam9(sc), sc["camera"]["vfov"], 1.0), 256, 256, sc["max_depth"], 1, 1, 1, seed)
+    acc, _ = s.trace(p, spp)
+    exact = acc[..., :3] * (np.float32(1) / np.float32(spp))
+    hi, _ = R.render(ctx, s, sc, spp=1024, exact=0, seed=seed)
+    e_cpu, e_exact, e_hi = (rel_rmse(x, golden) for x in (cpu, exact, hi))
+    print(f"256^2 relRMSE to the FP64 oracle: CPU float {e_cpu:.4f}, GPU exact {e_exact:.4f} (16 spp); "
+          f"GPU fast 1024 spp {e_hi:.4f}; means GPU {hi.mean():.5f} oracle {golden.mean():.5f}")
+    assert abs(e_exact - e_cpu) / e_cpu < 0.01
+    assert e_hi < 0.35 * e_cpu
+    assert abs(hi.mean() - golden.mean()) / golden.mean() < 0.01
+
+
+@pytest.mark.parametrize("exact", [0, 1])
+def test_large_images_on_the_wavefront_are_the_one_kernel_images(ctx, oracle, cornell256, exact):
+    """lrc_trace of at least 2^20 paths runs on the wavefront engine: its image, ray count and the
+    denoiser's moments equal the one-kernel path's (LRC_TRACE_MEGAKERNEL) to the bit."""
+    sc = cornell256
+    s = R.world_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    p = L.native.trace_params(oracle.camera(cam9(sc), sc["camera"]["vfov"], 1.0), 256, 256, sc["max_depth"], 1, 1, exact, 7)
+    a, ra = s.trace(p, 16)
+    b, rb = s.trace(p, 16, flags=L.native.LRC_TRACE_MEGAKERNEL)
+    assert np.array_equal(a, b) and ra == rb
+    # a band of rows with a sample offset (fast mode) and the guided planes
+    if not exact:
+        a, ra = s.trace(p, 32, y0=64, rows=128, spp0=16)
+        b, rb = s.trace(p, 32, y0=64, rows=128, spp0=16, flags=L.native.LRC_TRACE_MEGAKERNEL)
+        assert np.array_equal(a, b) and ra == rb
+        pa = s.guide(p)
+        pb = pa.copy()
+        s.trace_guided(p, 16, pa)
+        s.trace_guided(p, 16, pb, flags=L.native.LRC_TRACE_MEGAKERNEL)
+        assert np.array_equal(pa, pb)
+
+
+@pytest.mark.parametrize("megakernel", [False, True])
+def test_indirect_clamp_is_the_cpu_image(ctx, oracle, cornell128, megakernel):
+    """TraceParams.indirect_clamp (tracer.c:358-361, GpuTraceParams.indirect_clamp): each light a path
+    brings after its first rough bounce held to the clamp. Exact mode against trace_image with the
+    same clamp, on the one-kernel path and (256 x 256: 2^20 paths) on the wavefront."""
+    sc = cornell128 if megakernel else W.cornell_spheres(width=256, height=256)
+    w = sc["width"]
+    spp, seed, clamp = 16, 5, 0.25
+    ref = ref_scene(oracle, sc)
+    cpu, (closest, shadow) = ref.trace_image(cam9(sc), sc["camera"]["vfov"], w, w, spp, seed, sc["max_depth"],
+                                             indirect_clamp=clamp)
+    free, _ = ref.trace_image(cam9(sc), sc["camera"]["vfov"], w, w, spp, seed, sc["max_depth"])
+    assert rel_rmse(cpu, free) > 0.01                 # (the clamp matters in this scene)
+    s = R.world_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    p = L.native.trace_params(oracle.camera(cam9(sc), sc["camera"]["vfov"], 1.0), w, w, sc["max_depth"], 1, 1, 1, seed,
+                              indirect_clamp=clamp)
+    acc, rays = s.trace(p, spp, flags=L.native.LRC_TRACE_MEGAKERNEL if megakernel else 0)
+    gpu = acc[..., :3] * (np.float32(1) / np.float32(spp))
+    exact = np.all(gpu == cpu, axis=2).mean()
+    err = rel_rmse(gpu, cpu)
+    print(f"indirect clamp {clamp}: pixels equal to the bit {exact:.4f}; relRMSE {err:.2e}")
+    assert exact >= 0.7
+    assert err <= 1e-4
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-3
