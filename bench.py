@@ -90,8 +90,8 @@ def parse():
     ap.add_argument("--rates", default="50,200,800", help="serve: Poisson arrival rates (jobs/s)")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
     ap.add_argument("--wave-paths", type=int, default=32 << 20, help="serve: paths per wave")
-    ap.add_argument("--wave-slots", type=int, default=1 << 22, help="serve: the waves' paths in flight")
-    ap.add_argument("--serve-policy", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--wave-slots", type=int, default=1 << 23, help="serve: the waves' paths in flight")
+    ap.add_argument("--serve-policy", type=int, default=2, choices=[0, 1, 2],
                     help="serve: how a wave is made (lrc_server_set_policy: 0 even shares, 1 oldest first, "
                          "2 fewest paths left first)")
     ap.add_argument("--denoise-low-spp", action="store_true",
@@ -685,9 +685,10 @@ def run_serve(a):
         return {"lat": lat, "rays": rays, "span": span, "kept": kept, "d2h": d2h, "waves": waves, "kernels": kernels,
                 "gpu_s": gpu_ms / 1e3}
 
-    def plain(jobs, recs, keep=0):
+    def plain(jobs, recs, keep=0, flags=0):
         """One job at a time in arrival order, each traced alone through lrc_trace (large ones on the
-        wavefront engine, as lrc_trace runs them); the scene put back after a moved-instance job."""
+        wavefront engine, as lrc_trace runs them; flags LRC_TRACE_MEGAKERNEL: all on the one-kernel
+        path); the scene put back after a moved-instance job."""
         lat, rays, kept = [], 0, {}
         t0 = L.native.clock_ms()
         for k, j in enumerate(jobs):
@@ -705,12 +706,12 @@ def run_serve(a):
                 s.guide_device(p, planes.data_ptr())
                 ctx.check(ctx.L.lrc_trace(s.h, L.native.C.byref(p), 0, j[3], 0, j[4],
                                           L.native.C.c_void_p(planes.data_ptr()), L.native.C.byref(nr),
-                                          L.native.LRC_TRACE_GUIDED | L.native.LRC_DEVICE))
+                                          L.native.LRC_TRACE_GUIDED | L.native.LRC_DEVICE | flags))
                 ctx.denoise_device(j[2], j[3], planes.data_ptr(), img.data_ptr())
             else:
                 ctx.check(ctx.L.lrc_trace(s.h, L.native.C.byref(p), 0, j[3], 0, j[4],
                                           L.native.C.c_void_p(img.data_ptr()), L.native.C.byref(nr),
-                                          L.native.LRC_DEVICE))
+                                          L.native.LRC_DEVICE | flags))
             if recs[k] is not None:
                 s.move_instances(originals[j[1]], 0)
             ctx.sync()
@@ -763,6 +764,18 @@ def run_serve(a):
               f"images equal {equal}", file=sys.stderr, flush=True)
         jobs_done += len(jobs)
         paths_all += results[str(int(rate))]["paths"]
+    # the middle rate's stream once more through the one-kernel path alone (LRC_TRACE_MEGAKERNEL: the
+    # plain path before large images went to the wavefront engine)
+    mid = rates[len(rates) // 2]
+    jobs, recs = stream_of(mid, n_per_rate, int(mid))
+    mk = plain(jobs, recs, keep=4, flags=L.native.LRC_TRACE_MEGAKERNEL)
+    r_mid = results[str(int(mid))]
+    r_mid["plain_megakernel"] = {"p50_ms": pct(mk["lat"], 50), "p99_ms": pct(mk["lat"], 99),
+                                 "mrays_s": mk["rays"] / mk["span"] / 1e6, "span_s": mk["span"],
+                                 "latency_samples": len(mk["lat"])}
+    r_mid["served_vs_plain_megakernel"] = r_mid["served"]["mrays_s"] / r_mid["plain_megakernel"]["mrays_s"]
+    print(f"serve rate {mid:g}/s: plain on the one-kernel path {mk['span']:.1f} s "
+          f"({mk['rays'] / mk['span'] / 1e6:.0f} Mrays/s)", file=sys.stderr, flush=True)
     clocks = clk.stop()
     # below capacity: 0.8 x the served jobs/s just measured, the same number of jobs
     capacity = jobs_done / served_span
@@ -779,41 +792,45 @@ def run_serve(a):
         "jobs": len(jobs)}
     # end to end: the middle rate's stream again, every finished image read back to pinned host
     # memory inside the span; the host sends each job's parameters (and moved instances' records)
-    mid = rates[len(rates) // 2]
     jobs, recs = stream_of(mid, n_per_rate, int(mid))
     e = served(jobs, recs, readback=True)
     h2d = sum(96 + (r.nbytes if r is not None else 0) for r in recs)
     e2e = {"value": e["rays"] / e["span"] / 1e6, "unit": "Mrays/s", "rate_jobs_s": mid,
            "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(e["d2h"] / a.steps),
            "ms_per_step": 1e3 * e["span"] / a.steps, "p50_ms": pct(e["lat"], 50), "p99_ms": pct(e["lat"], 99)}
-    # traversal bytes per ray (closest-hit walks of a sample of the jobs' primary rays: the stream's
-    # rays walk the same trees; the estimate is labelled as such) -> the served stream's roofline
+    # the dominant kernel (the wavefront's closest hit) measured live on a sample of the middle rate's
+    # stream: its first jobs without moved instances (about 1G paths) as one batch, run pass by pass (STEPPED: CUDA
+    # events around every closest-hit launch), first with the counting build of the kernel (the
+    # walks' box and triangle tests: the algorithmic bytes), then with the plain one (its time)
     peak, peak_kind = peaks()
-    rng = np.random.default_rng(5)
-    bt, tt, nr = 0, 0, 0
-    for k in range(0, 56, 7):
-        sc = dicts[k]
-        cam = W.camera(sc["camera"], 1.0).reshape(4, 3)
-        u, v = rng.random((2, 1 << 16)).astype(np.float32)
-        tgt = cam[1] + u[:, None] * cam[2] - v[:, None] * cam[3]
-        d = tgt - cam[0]
-        d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
-        o = np.repeat(cam[0][None], d.shape[0], 0).astype(np.float32)
-        tri_only = L.Scene(ctx)                       # (the counting walk reads triangles: the lamp aside)
-        tri_only.set_triangles(L.pack_tris(W.corners_to_quv(sc["corners"])))
-        tri_only.build(1, 30)
-        b_, t_ = tri_only.trace_stats(o, d, 2e-3, 1e30)
-        tri_only.close()
-        bt, tt, nr = bt + b_, tt + t_, nr + d.shape[0]
-    bytes_per_ray = (bt * 32 + tt * 48) / nr
-    achieved = bytes_per_ray * served_rays / served_span / 1e9
-    roofline = {"kernel": "wavefront engine over the served stream (wf_intersect + wf_shadow walks; advance and "
-                          "shade inside the same span)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "peak_kind": peak_kind, "frac": achieved / peak, "traffic": None,
-                "bytes_per_ray": bytes_per_ray,
-                "bytes_per_ray_from": "closest-hit walks of 65536 primary rays of each of 8 of the box scenes' "
-                                      "triangles, PLOC trees (box tests x 32 + triangle tests x 48): an estimate of "
-                                      "the stream's rays"}
+    sample, sample_paths = [], 0
+    for k, j in enumerate(jobs):                     # (the first jobs without moved instances, ~1G paths)
+        if j[5] is None and sample_paths < 1_000_000_000:
+            sample.append((k, j))
+            sample_paths += j[2] * j[3] * j[4]
+    imgs = [torch.zeros(j[3], j[2], 4, device=dev) for _, j in sample]
+    bb = L.native.Batch(ctx)
+    bb.set_wavefront(a.wave_slots, 0)
+    for (k, j), t in zip(sample, imgs):
+        bb.add(scenes[j[1]], params(j, k), j[4], t.data_ptr())
+    bb.run(zero=True, stepped=True, count=True)
+    counted = bb.step_stats()
+    bb.run(zero=True, stepped=True)
+    timed = bb.step_stats()
+    bb.close()
+    bytes_per_ray = (counted["box_tests"] * 32 + counted["tri_tests"] * 48) / max(counted["intersect_rays"], 1)
+    alg_bytes = bytes_per_ray * timed["intersect_rays"]
+    achieved = alg_bytes / (timed["intersect_ms"] / 1e3) / 1e9
+    roofline = {"kernel": "wf_intersect_kernel (the wavefront's closest hit)", "bound": "hbm", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "frac": achieved / peak, "traffic": None,
+                "bytes_per_ray": bytes_per_ray, "box_tests_per_ray": counted["box_tests"] / max(counted["intersect_rays"], 1),
+                "tri_tests_per_ray": counted["tri_tests"] / max(counted["intersect_rays"], 1),
+                "algorithmic_bytes_per_launch": alg_bytes / max((timed["kernels"] - 1) // 4, 1),
+                "ms_per_launch": timed["intersect_ms"] / max((timed["kernels"] - 1) // 4, 1),
+                "measured_on": f"{len(sample)} jobs of the {mid:g}/s stream as one batch, run pass by pass "
+                               f"({timed['intersect_rays']} closest-hit rays, {timed['intersect_ms']:.1f} ms in the "
+                               "kernel); bytes per ray = box tests x 32 + triangle tests x 48 from the counting "
+                               "build of the kernel on the same run"}
     value = served_rays / served_span / 1e6
     cpu_v, cores, _, _, text = serve_cpu_sample(dicts, 15.0)
     line = {"metric": METRIC_SERVE, "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": a.steps,
@@ -836,6 +853,10 @@ def run_serve(a):
     plain_span = sum(r["plain"]["span_s"] for k, r in results.items() if k != "sub_capacity")
     line["plain_mrays_s"] = plain_rays / plain_span / 1e6
     line["served_vs_plain"] = value / line["plain_mrays_s"]
+    line["served_vs_plain_megakernel"] = r_mid["served_vs_plain_megakernel"]
+    line["denominators"] = ("plain_mrays_s: each job alone through lrc_trace as shipped (jobs of 2^20 paths and "
+                            "more on the wavefront engine); served_vs_plain_megakernel: at the middle rate, each "
+                            "job alone on the one-kernel path (LRC_TRACE_MEGAKERNEL)")
     for s_ in scenes:
         s_.close()
     ctx.close()

@@ -418,6 +418,8 @@ typedef struct lrc_batch lrc_batch;
 #define LRC_BATCH_ZERO 16u    /* clear each job's band of its image first */
 #define LRC_BATCH_STEPPED 32u /* wavefront: launch each pass's kernels from the host, no graph (slower;
                                  for profilers that cannot see into a graph's loop); not with GRAPH */
+#define LRC_BATCH_COUNT 64u   /* with STEPPED: the closest-hit walks count their box and triangle tests
+                                 (lrc_batch_step_stats) */
 int lrc_batch_create(lrc_ctx *c, lrc_batch **out);
 void lrc_batch_destroy(lrc_batch *b);
 /* A job: lrc_trace(s, p, y0, rows, spp0, spp, d_accum, ..., LRC_DEVICE) as part of the batch;
@@ -440,6 +442,14 @@ int lrc_batch_rays(lrc_batch *b, uint64_t *per_job, uint64_t *total);
 /* After a run (synchronises): the wavefront's passes (bounces of the paths in flight, 0 for the
  * megakernel engine) and the trace kernels the run launched (optional, either NULL). */
 int lrc_batch_passes(lrc_batch *b, uint32_t *passes, uint64_t *kernels);
+/* The last LRC_BATCH_STEPPED run of the wavefront (each optional): its closest-hit kernel's device
+ * time (CUDA events around each launch) and the rays it traced; with LRC_BATCH_COUNT its walks' box
+ * tests (32-byte node records read) and triangle tests (48-byte triangles read), counted by a
+ * counting build of that kernel run with the default launch shape (lrc_batch_set_wavefront variant
+ * 0; it tests what the plain one does: the same hits, the images the same to the bit); and the
+ * kernels the run launched. */
+int lrc_batch_step_stats(const lrc_batch *b, double *intersect_ms, uint64_t *intersect_rays, uint64_t *box_tests,
+                         uint64_t *tri_tests, uint64_t *kernels);
 /* The trace kernel's launch shapes: shape `variant`'s threads per block, the blocks per SM its
  * registers are capped for, and the blocks that fit per SM; returns the number of shapes, or -1. */
 int lrc_batch_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm);
@@ -507,9 +517,9 @@ lrc_batch *lrc_server_batch(lrc_server *sv);
 /* waves run so far, the trace kernels they launched and their device time (CUDA events around
  * each wave's run), each optional */
 int lrc_server_stats(const lrc_server *sv, uint64_t *waves, uint64_t *kernels, double *gpu_ms);
-/* How a wave is made from the admitted jobs: 0 (the default) the next band of every job, the wave's
- * paths shared evenly; 1 the oldest jobs first, each band as large as the wave's paths left allow
- * (fewer scenes a wave); 2 as 1 with the jobs that have the fewest paths left first. */
+/* How a wave is made from the admitted jobs: 0 the next band of every job, the wave's paths shared
+ * evenly; 1 the oldest jobs first, each band as large as the wave's paths left allow (fewer scenes a
+ * wave); 2 (the default) as 1 with the jobs that have the fewest paths left first. */
 int lrc_server_set_policy(lrc_server *sv, int32_t policy);
 
 #ifdef __cplusplus

@@ -63,6 +63,7 @@ struct lrc_batch {
     size_t wf_cap = 0;
     cudaStream_t body = nullptr;          // the stream the wavefront loop's body is captured on
     // the graph of the last GRAPH run and what it was captured for
+    lrc::WfStepStats step_stats{};        // the last STEPPED run's measurements
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned graph_flags = 0;
@@ -72,7 +73,7 @@ struct lrc_batch {
 
 namespace {
 
-constexpr unsigned kBatchFlags = LRC_BATCH_BUILD | LRC_BATCH_GRAPH | LRC_BATCH_ZERO | LRC_BATCH_STEPPED;
+constexpr unsigned kBatchFlags = LRC_BATCH_BUILD | LRC_BATCH_GRAPH | LRC_BATCH_ZERO | LRC_BATCH_STEPPED | LRC_BATCH_COUNT;
 
 int group_for(const lrc_trace_params &p, uint32_t spp) {
     if (p.exact) return 1;
@@ -304,7 +305,7 @@ int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool 
     if (!e && b->engine == 1 && !capturing && (flags & LRC_BATCH_STEPPED)) {
         const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
         e = lrc::wf_run_stepped(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, any_instances(b),
-                                c->num_sms, max_passes(b, limit), st);
+                                c->num_sms, max_passes(b, limit), st, &b->step_stats, (flags & LRC_BATCH_COUNT) != 0);
     } else if (!e && b->engine == 1) {
         if (!capturing) return fail(c, LRC_E_INVALID, "the wavefront runs as a captured graph");
         const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
@@ -622,6 +623,18 @@ int lrc_batch_passes(lrc_batch *b, uint32_t *passes, uint64_t *kernels) {
     }
     if (passes) *passes = n;
     if (kernels) *kernels = k;
+    return LRC_OK;
+}
+
+int lrc_batch_step_stats(const lrc_batch *b, double *intersect_ms, uint64_t *intersect_rays, uint64_t *box_tests,
+                         uint64_t *tri_tests, uint64_t *kernels) {
+    if (!b) return LRC_E_INVALID;
+    const lrc::WfStepStats &S = b->step_stats;
+    if (intersect_ms) *intersect_ms = S.isect_ms;
+    if (intersect_rays) *intersect_rays = S.isect_rays;
+    if (box_tests) *box_tests = S.box_tests;
+    if (tri_tests) *tri_tests = S.tri_tests;
+    if (kernels) *kernels = S.launches;
     return LRC_OK;
 }
 

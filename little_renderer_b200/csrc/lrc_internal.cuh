@@ -341,9 +341,16 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
                             cudaStream_t st, cudaStream_t body_st);
 // The same loop with each pass's kernels launched from the host (no graph; the host reads the
 // queued count after every pass): for profilers that cannot see into a graph's loop.
+// a stepped run's measurements (stats given): the closest-hit kernel's time (CUDA events around each
+// launch), the rays it traced, its launches, all kernels launched, and (count, with variant 0's
+// shape, whose counting build it then runs) the box and triangle tests of its walks
+struct WfStepStats {
+    double isect_ms;
+    unsigned long long isect_rays, isect_launches, launches, box_tests, tri_tests;
+};
 cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
                            uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
-                           cudaStream_t st);
+                           cudaStream_t st, WfStepStats *stats = nullptr, bool count = false);
 // the sky's sampling tables as env_prepare makes them (host_tables.cu): marg h + 1, cond h x (w + 1),
 // prob w x h; returns false when no pixel weighs anything (sum 0)
 bool env_tables(const float *rgb, int w, int h, float *marg, float *cond, float *prob);

@@ -111,11 +111,14 @@ __device__ __forceinline__ float slab(const RayBox &r, float4 lo, float4 hi, flo
 // leaf(entry) tests one leaf entry (an aux value), lowering best on a hit, and returns true to
 // end the walk (an any-hit found). Entries of a leaf in order; a hit at the same t as the best is
 // not taken (t >= tmax rejects), as the CPU's walk does. Returns true if a leaf ended it.
-template <typename Leaf>
+// COUNT: cnt[0] += the boxes tested (32-byte node records read), cnt[1] += the leaf entries tested
+// (a kernel compiled with it measures the walk's algorithmic bytes; the others never carry it)
+template <bool COUNT = false, typename Leaf>
 __device__ bool bvh_walk(const float4 *nodes, uint32_t root, uint32_t nnodes, const uint32_t *aux, uint32_t naux, V3 o,
-                         V3 d, float tmin, float &best, uint32_t *err, Leaf &&leaf) {
+                         V3 d, float tmin, float &best, uint32_t *err, Leaf &&leaf, uint32_t *cnt = nullptr) {
     RayBox rb = ray_box(o, d);
     float4 r0 = ld4(&nodes[2 * (size_t)root]), r1 = ld4(&nodes[2 * (size_t)root + 1]);
+    if constexpr (COUNT) cnt[0] += 1;
     if (!(slab(rb, r0, r1, tmin, best) <= best)) return false;
     uint2 stack[PT_STACK];
     int sp = 0;
@@ -124,12 +127,15 @@ __device__ bool bvh_walk(const float4 *nodes, uint32_t root, uint32_t nnodes, co
         if (b & LEAF_BIT) {
             const uint32_t count = b & ~LEAF_BIT;
             if (a >= naux || count > naux - a) { atomicOr(err, ST_BAD_TREE); return false; }
-            for (uint32_t k = 0; k < count; k++)
+            for (uint32_t k = 0; k < count; k++) {
+                if constexpr (COUNT) cnt[1] += 1;
                 if (leaf(__ldg(&aux[a + k]))) return true;
+            }
         } else {
             if (a >= nnodes || b >= nnodes) { atomicOr(err, ST_BAD_TREE); return false; }
             float4 l0 = ld4(&nodes[2 * (size_t)a]), l1 = ld4(&nodes[2 * (size_t)a + 1]);
             float4 h0 = ld4(&nodes[2 * (size_t)b]), h1 = ld4(&nodes[2 * (size_t)b + 1]);
+            if constexpr (COUNT) cnt[0] += 2;
             float t0 = slab(rb, l0, l1, tmin, best), t1 = slab(rb, h0, h1, tmin, best);
             bool c0 = t0 <= best, c1 = t1 <= best;
             if (c0 && c1) {
@@ -153,11 +159,11 @@ __device__ bool bvh_walk(const float4 *nodes, uint32_t root, uint32_t nnodes, co
 }
 
 // the closest (ANY = false) or any world shape (primitives, then triangles) in (tmin, best), or -1
-template <bool ANY>
+template <bool ANY, bool COUNT = false>
 __device__ int32_t walk(const PtScene &S, const float4 *nodes, uint32_t root, uint32_t nnodes, const uint32_t *aux,
-                        uint32_t naux, V3 o, V3 d, float tmin, float &best, uint32_t *err) {
+                        uint32_t naux, V3 o, V3 d, float tmin, float &best, uint32_t *err, uint32_t *cnt = nullptr) {
     int32_t hit = -1;
-    bvh_walk(nodes, root, nnodes, aux, naux, o, d, tmin, best, err, [&](uint32_t id) {
+    bvh_walk<COUNT>(nodes, root, nnodes, aux, naux, o, d, tmin, best, err, [&](uint32_t id) {
         if (id >= S.nprims + S.ntris) { atomicOr(err, ST_BAD_TREE); return true; }
         float t;
         if (shape_test(S, id, o, d, tmin, best, t)) {
@@ -166,7 +172,7 @@ __device__ int32_t walk(const PtScene &S, const float4 *nodes, uint32_t root, ui
             return ANY;
         }
         return false;
-    });
+    }, cnt);
     return hit;
 }
 
@@ -195,17 +201,18 @@ __device__ __forceinline__ V3 xnormal(const float4 *inv, V3 n) {  // xform_norma
 // The closest (ANY = false) or any hit on the instances in (tmin, best): the instance and the
 // triangle's index in its mesh; false if none. The top level's leaves are instances; each is
 // entered with the ray in its own space (o' = inv o, d' = inv d: the same t) and its mesh's BVH walked.
-template <bool ANY>
-__device__ bool walk_instances(const PtScene &S, V3 o, V3 d, float tmin, float &best, int &inst, int &tri, uint32_t *err) {
+template <bool ANY, bool COUNT = false>
+__device__ bool walk_instances(const PtScene &S, V3 o, V3 d, float tmin, float &best, int &inst, int &tri, uint32_t *err,
+                               uint32_t *cnt = nullptr) {
     bool found = false;
-    bvh_walk(S.tlas_nodes, 0, S.tlas_nnodes, S.tlas_aux, S.ninst, o, d, tmin, best, err, [&](uint32_t i) {
+    bvh_walk<COUNT>(S.tlas_nodes, 0, S.tlas_nnodes, S.tlas_aux, S.ninst, o, d, tmin, best, err, [&](uint32_t i) {
         if (i >= S.ninst) { atomicOr(err, ST_BAD_TREE); return true; }
         const float4 *rec = S.inst + 8 * (size_t)i;
         const uint32_t mesh = __float_as_uint(ld4(rec + 6).w);
         if (mesh >= S.nmeshes) return false;                       // (shapes: not in these scenes)
         const uint4 mi = __ldg(&S.mesh_info[mesh]);                // root node, first triangle, triangles
         V3 ro = xpoint(rec + 3, o), rd = xdir(rec + 3, d);
-        return bvh_walk(S.mnodes, mi.x, S.mnnodes, S.maux, S.mnaux, ro, rd, tmin, best, err, [&](uint32_t g) {
+        return bvh_walk<COUNT>(S.mnodes, mi.x, S.mnnodes, S.maux, S.mnaux, ro, rd, tmin, best, err, [&](uint32_t g) {
             if (g >= S.nmtris) { atomicOr(err, ST_BAD_TREE); return true; }
             float t;
             if (hit_tri_t(S.mtris + 3 * (size_t)g, ro, rd, tmin, best, t)) {
@@ -216,8 +223,8 @@ __device__ bool walk_instances(const PtScene &S, V3 o, V3 d, float tmin, float &
                 return ANY;
             }
             return false;
-        });
-    });
+        }, cnt);
+    }, cnt);
     return found;
 }
 
@@ -611,17 +618,17 @@ __device__ __forceinline__ void path_add(PathState &ps, V3 c) {
 
 // scene_intersect's search alone: the closest t, the world shape (or -1) and the instance and its
 // triangle (or -1); make_hit then gives the Hit scene_intersect gives. INST as scene_occluded's.
-template <bool INST = true>
+template <bool INST = true, bool COUNT = false>
 __device__ __forceinline__ void scene_find(const PtScene &S, V3 o, V3 d, float tmin, float tmax, float &t, int &id, int &inst,
-                                           int &tri, uint32_t *err) {
+                                           int &tri, uint32_t *err, uint32_t *cnt = nullptr) {
     float best = tmax;
     id = -1;
     inst = -1;
     tri = -1;
-    if (S.nnodes) id = walk<false>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err);
+    if (S.nnodes) id = walk<false, COUNT>(S, S.nodes, S.root, S.nnodes, S.aux, S.naux, o, d, tmin, best, err, cnt);
     if (INST && S.ninst) {
         int ii = -1, tt = -1;
-        if (walk_instances<false>(S, o, d, tmin, best, ii, tt, err)) {
+        if (walk_instances<false, COUNT>(S, o, d, tmin, best, ii, tt, err, cnt)) {
             inst = ii;
             tri = tt;
         }

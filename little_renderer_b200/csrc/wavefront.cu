@@ -47,6 +47,8 @@ __global__ void wf_clear_kernel(WfState W, unsigned long long limit) {
     if (i == 0) {
         W.next[0] = 0;
         W.next[1] = limit;
+        W.next[2] = 0;                               // (the counting closest-hit kernel's box tests
+        W.next[3] = 0;                               //  and triangle tests)
     }
     if (i >= W.M) return;
     W.task[i] = NO_TASK;
@@ -198,7 +200,9 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
 
 // the closest hit of every queued ray (warps fetch 32 rays at a time); sets the loop's condition
 // (another pass while rays are queued)
-template <int BLOCK, int MINB, bool INST>
+// (COUNT: also the walks' box and triangle tests into W.next[2], W.next[3]; only the stepped runs
+// that measure the engine's algorithmic bytes launch it)
+template <int BLOCK, int MINB, bool INST, bool COUNT = false>
 __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJob *__restrict__ jobs, WfState W, uint32_t *err,
                                                                    cudaGraphConditionalHandle cond, uint32_t max_passes,
                                                                    int use_cond) {
@@ -214,6 +218,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJo
         else W.ctl[5] = count;                       // (the stepped loop's host reads it)
     }
     const uint32_t lane = threadIdx.x & 31;
+    uint32_t cnt[2] = {0, 0};
     for (;;) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&W.ctl[2], 32u);
@@ -226,8 +231,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJo
             const V3 o = v3f(W.ro[s]), d = v3f(W.rd[s]);
             float t;
             int id, inst, tri;
-            scene_find<INST>(J.S, o, d, RT_EPS, 1e30f, t, id, inst, tri, err);
+            scene_find<INST, COUNT>(J.S, o, d, RT_EPS, 1e30f, t, id, inst, tri, err, cnt);
             W.hit[s] = make_float4(t, __int_as_float(id), __int_as_float(inst), __int_as_float(tri));
+        }
+    }
+    if constexpr (COUNT) {
+        unsigned long long a = cnt[0], b = cnt[1];
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0 && (a | b)) {
+            atomicAdd(&W.next[2], a);
+            atomicAdd(&W.next[3], b);
         }
     }
 }
@@ -457,10 +473,18 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
 
 cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
                            uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
-                           cudaStream_t st) {
+                           cudaStream_t st, WfStepStats *stats, bool count) {
     if (variant < 0 || variant >= wf_variants() || W.M == 0 || W.M % pt::ADV_BLOCK) return cudaErrorInvalidValue;
     const WfVariant &V = kWfVariants[variant];
     const void *isect = instances ? V.isect : V.isect_world, *shadow = instances ? V.shadow : V.shadow_world;
+    if (stats && count && V.block == 128 && V.minb == 4)   // (the counting kernels: variant 0's shape)
+        isect = instances ? (const void *)pt::wf_intersect_kernel<128, 4, true, true>
+                          : (const void *)pt::wf_intersect_kernel<128, 4, false, true>;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (stats) {
+        *stats = WfStepStats{};
+        if (cudaEventCreate(&e0) || cudaEventCreate(&e1)) return cudaGetLastError();
+    }
     int per_sm = 0, shade_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, isect, V.block, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, V.shade, pt::SHADE_BLOCK, 0);
@@ -473,7 +497,9 @@ cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long
     for (uint32_t pass = 0; !e && pass <= max_passes; pass++) {
         pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, st>>>(d_jobs, njobs, w);
         void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
+        if (stats) cudaEventRecord(e0, st);
         e = cudaLaunchKernel(isect, dim3(grid), dim3(V.block), iargs, 0, st);
+        if (stats) cudaEventRecord(e1, st);
         if (e) break;
         void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&max_passes};
         e = cudaLaunchKernel(V.shade, dim3(shade_grid), dim3(pt::SHADE_BLOCK), hargs, 0, st);
@@ -483,7 +509,24 @@ cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long
         uint32_t queued = 0;
         if (!e) e = cudaMemcpyAsync(&queued, &W.ctl[5], 4, cudaMemcpyDeviceToHost, st);
         if (!e) e = cudaStreamSynchronize(st);
+        if (!e && stats) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            stats->isect_ms += ms;
+            stats->isect_rays += queued;
+            stats->isect_launches++;
+            stats->launches += 4;
+        }
         if (!e && queued == 0) break;
+    }
+    if (stats) {
+        unsigned long long c[2] = {0, 0};
+        if (!e) e = cudaMemcpy(c, &W.next[2], 16, cudaMemcpyDeviceToHost);
+        stats->box_tests = c[0];
+        stats->tri_tests = c[1];
+        stats->launches += 1;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
     }
     return e;
 }

@@ -24,7 +24,7 @@ LRC_TRACE_GUIDED = 64
 LRC_TRACE_MEGAKERNEL = 256
 LRC_REPROJECT_EDIT = 128
 LRC_SERVE_DENOISE = 16
-LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED = 4, 8, 16, 32
+LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED, LRC_BATCH_COUNT = 4, 8, 16, 32, 64
 
 
 def nvcc():
@@ -719,10 +719,18 @@ class Batch:
         self.ctx.check(self.ctx.L.lrc_batch_clear(self.h))
         self.keep = []
 
-    def run(self, build=False, graph=False, zero=False, stepped=False):
+    def run(self, build=False, graph=False, zero=False, stepped=False, count=False):
         flags = (LRC_BATCH_BUILD if build else 0) | (LRC_BATCH_GRAPH if graph else 0) | (LRC_BATCH_ZERO if zero else 0)
-        flags |= LRC_BATCH_STEPPED if stepped else 0
+        flags |= (LRC_BATCH_STEPPED if stepped else 0) | (LRC_BATCH_COUNT if count else 0)
         self.ctx.check(self.ctx.L.lrc_batch_run(self.h, flags))
+
+    def step_stats(self):
+        """The last stepped run: {intersect_ms, intersect_rays, box_tests, tri_tests, kernels}."""
+        ms, rays, bt, tt, k = C.c_double(), C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.ctx.check(self.ctx.L.lrc_batch_step_stats(self.h, C.byref(ms), C.byref(rays), C.byref(bt), C.byref(tt),
+                                                       C.byref(k)))
+        return {"intersect_ms": ms.value, "intersect_rays": rays.value, "box_tests": bt.value, "tri_tests": tt.value,
+                "kernels": k.value}
 
     def rays(self):
         """(rays per job, total) of the last run (waits for it)."""

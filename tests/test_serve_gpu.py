@@ -52,8 +52,10 @@ def alone_plain(job, original):
     return acc, rays
 
 
-def serve_all(ctx, jobs, budget, wave_paths):
+def serve_all(ctx, jobs, budget, wave_paths, policy=None):
     sv = L.native.Server(ctx, budget, wave_paths)
+    if policy is not None:
+        sv.set_policy(policy)
     ids = [sv.submit(s, p, spp, rec, mode) for (_, s, p, spp, rec, mode) in jobs]
     waves, most_active, most_queued = 0, 0, 0
     while sv.state()["finished"] < len(jobs):
@@ -73,13 +75,16 @@ def serve_all(ctx, jobs, budget, wave_paths):
     return out, waves, most_active, most_queued
 
 
-def test_served_images_are_the_jobs_alone(ctx, world, inst):
+@pytest.mark.parametrize("policy", [0, 1, 2])
+def test_served_images_are_the_jobs_alone(ctx, world, inst, policy):
+    """Whatever the wave policy (even shares, oldest first, fewest paths left first)."""
     sc_i, s_i = inst
     original = W.instance_records(sc_i)
     jobs = jobs_of(world, inst)
     # in the mix: a small wave (bands of a few rows, many waves) and a budget below the jobs' total
     total = sum(p.width * p.height * 16 for (_, _, p, _, _, _) in jobs)
-    served, waves, most_active, most_queued = serve_all(ctx, jobs, budget=total // 2 + (4 << 20), wave_paths=20_000)
+    served, waves, most_active, most_queued = serve_all(ctx, jobs, budget=total // 2 + (4 << 20), wave_paths=20_000,
+                                                        policy=policy)
     assert waves > 10 and most_active > 1 and most_queued > 0
     for job, (img, rays) in zip(jobs, served):
         acc, want_rays = alone_plain(job, original)
