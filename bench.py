@@ -82,6 +82,9 @@ def parse():
     ap.add_argument("--rays", type=int, default=16 * 1024 * 1024)
     ap.add_argument("--builder", default="ploc", choices=["ploc", "lbvh"])
     ap.add_argument("--bits", type=int, default=30, choices=[30, 63])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="builder: the soup and its rays scaled by this (555: the reference's scene units, where the "
+                         "triangles' 1e-3 box padding has its intended relative size)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="serve", choices=["builder", "batch", "serve", "render", "instanced",
@@ -105,17 +108,30 @@ def parse():
                     help="render: one image traced by all ranks, each a share of every pixel's samples, then one "
                          "sum all-reduce (strong scaling)")
     ap.add_argument("--stepped", action="store_true",
-                    help="batch: wavefront passes launched from the host (for ncu, which cannot see into graph loops)")
+                    help="batch, render, instanced: the wavefront engine's passes launched from the host (for ncu, "
+                         "which cannot see into graph loops)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)      # (at least 3 untimed steps before the timed ones)
     return a
 
 
+# DRAM bytes read + written by one launch of the builder line's closest-hit kernel at the default
+# configuration (4M soup triangles, 16M rays, PLOC 30-bit, the walk's tree) and that launch's
+# duration under the profiler: one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum,
+# gpu__time_duration.sum) of the 4th closest_kernel launch in
+# `python bench.py --workload builder --steps 1 --warmup 3 --no-cpu --e2e-steps 1`
+BUILDER_CLOSEST_DRAM = {"bytes_per_launch": 216.0e9, "ms_per_launch": 127.97}
+
+
 def config(a, world):
-    return {"workload": f"builder+closest-hit: {a.n} triangles (soup), {a.rays} rays, {a.builder.upper()} "
-                        f"{a.bits}-bit Morton", "triangles": a.n, "rays": a.rays, "builder": a.builder,
-            "key_bits": a.bits, "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (triangles 48 B x N + rays 24 B x R > 126 MB)"}
+    scaled = f", scaled x{a.scale:g}" if a.scale != 1.0 else ""
+    c = {"workload": f"builder+closest-hit: {a.n} triangles (soup{scaled}), {a.rays} rays, {a.builder.upper()} "
+                     f"{a.bits}-bit Morton", "triangles": a.n, "rays": a.rays, "builder": a.builder,
+         "key_bits": a.bits, "parallelism": f"replicas x{world}",
+         "l2": "inputs larger than L2 (triangles 48 B x N + rays 24 B x R > 126 MB)"}
+    if a.scale != 1.0:
+        c["scale"] = a.scale
+    return c
 
 
 def max_over_ranks(ms, dist, device):
@@ -208,9 +224,9 @@ def run_reference(a):
     if rank != 0:
         return
     from little_renderer_b200 import workloads as W
-    cor = W.soup(a.n, 1)
+    cor = W.soup(a.n, 1) * np.float32(a.scale)
     sample = a.rays
-    o, d = W.rays_at_cube(sample, 2)
+    o, d = W.rays_at_cube(sample, 2, scale=a.scale)
     from oracle import oracle as O
     lib = O.ref_lib()
     cores = lib.rb_max_threads()
@@ -456,6 +472,11 @@ def run_batch(a):
 
 
 SERVE_JOBS_PER_STEP = 5      # a serve step: 5 jobs of each rate's stream
+# DRAM bytes read + written by one launch of the served line's closest-hit kernel, and that
+# launch's duration under the profiler: one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum, gpu__time_duration.sum) of launches 81-83 of wf_intersect_kernel in
+# `python bench.py --steps 2 --warmup 3 --rates 200` (the timed stepped run's full-queue passes)
+SERVE_ISECT_DRAM = {"bytes_per_launch": 474.6e6, "ms_per_launch": 3.77}
 
 
 def serve_jobs(n, rate, seed, nscenes, inst_ids):
@@ -821,8 +842,13 @@ def run_serve(a):
     bytes_per_ray = (counted["box_tests"] * 32 + counted["tri_tests"] * 48) / max(counted["intersect_rays"], 1)
     alg_bytes = bytes_per_ray * timed["intersect_rays"]
     achieved = alg_bytes / (timed["intersect_ms"] / 1e3) / 1e9
+    dram_gbs = SERVE_ISECT_DRAM["bytes_per_launch"] / (SERVE_ISECT_DRAM["ms_per_launch"] / 1e3) / 1e9
     roofline = {"kernel": "wf_intersect_kernel (the wavefront's closest hit)", "bound": "hbm", "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "frac": achieved / peak, "traffic": None,
+                "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "frac": achieved / peak,
+                "traffic": SERVE_ISECT_DRAM["bytes_per_launch"],
+                "traffic_from": "ncu dram__bytes_read.sum + dram__bytes_write.sum, launches 81-83 of the kernel in "
+                                "`python bench.py --steps 2 --warmup 3 --rates 200` (full queues)",
+                "dram_gbs": dram_gbs, "frac_dram": dram_gbs / peak,
                 "bytes_per_ray": bytes_per_ray, "box_tests_per_ray": counted["box_tests"] / max(counted["intersect_rays"], 1),
                 "tri_tests_per_ray": counted["tri_tests"] / max(counted["intersect_rays"], 1),
                 "algorithmic_bytes_per_launch": alg_bytes / max((timed["kernels"] - 1) // 4, 1),
@@ -887,7 +913,6 @@ def run_render(a):
     import torch
     import little_renderer_b200 as L
     from little_renderer_b200 import render as R, workloads as W
-    from oracle import oracle as O
 
     if int(os.environ.get("RANK", "0")) != 0:
         return
@@ -939,11 +964,18 @@ def run_render(a):
         b = L.native.Batch(ctx)
         b.set_engine(eng)
         b.add(s, p, spp, img.data_ptr())
-        b.run(zero=True)
+        b.run(zero=True, stepped=a.stepped and eng == 1)
         v, g, _ = b.tune()
+
+        def run_engine():
+            if a.stepped and eng == 1:
+                b.run(zero=True, stepped=True)
+            else:
+                b.run(graph=True, zero=True)
+
         for _ in range(a.warmup):
-            b.run(graph=True, zero=True)
-        bms = timed(lambda: b.run(graph=True, zero=True), a.steps)
+            run_engine()
+        bms = timed(run_engine, a.steps)
         ctx.sync()
         torch.cuda.synchronize()
         engines[name] = {"value": rays / (bms / 1e3) / 1e6, "ms_per_step": bms, "variant": v,
@@ -956,35 +988,41 @@ def run_render(a):
         s.trace(p, spp, accum=acc)
     e_ms = (time.perf_counter() - t0) * 1e3 / max(1, min(a.steps, 3))
     # the reference's CPU path tracer on a central band of rows
-    ref = ref_field_scene(O, sc) if inst else None
-    if ref is None:
-        ref = O.RefScene()
-        for m in sc["materials"]:
-            ref.material(m["type"], m["albedo"], m["emission"], m["ior"], m["metallic"], m["roughness"],
-                         m["transmission"])
-        ref.triangles(sc["corners"], sc["tri_mats"])
-        lamp = sc["lamp"]
-        ref.quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"], light=True)
-        for v in sc.get("volumes", []):
-            ref.volume(*v)
-        for px, srgb, wu, wv in sc.get("texmaps", []):
-            ref.texmap(px, srgb, wu, wv)
-        for i, m in enumerate(sc["materials"]):
-            t = m.get("tex")
-            if t:
-                ref.material_textures(i, t.get("base", 0), t.get("mr", 0), t.get("normal", 0), t.get("emissive", 0),
-                                      t.get("occlusion", 0), t.get("uv_scale", 0.0), t.get("normal_scale", 0.0))
-        if sc.get("texcoords"):
-            ref.texcoords(*sc["texcoords"])
-    t0 = time.perf_counter()
-    ref.set_accel()
-    rows = max(1, min(h, (4 if inst else 64)))
-    c = sc["camera"]
-    fau = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
-    _, (cl, sh) = ref.trace_image(fau, c["vfov"], w, h, spp, 1, sc["max_depth"], y0=h // 2 - rows // 2, rows=rows)
-    t_cpu = time.perf_counter() - t0
-    cores = O.ref_lib().rb_max_threads()
-    ref.close()
+    cpu = None
+    if not a.no_cpu:
+        from oracle import oracle as O
+        ref = ref_field_scene(O, sc) if inst else None
+        if ref is None:
+            ref = O.RefScene()
+            for m in sc["materials"]:
+                ref.material(m["type"], m["albedo"], m["emission"], m["ior"], m["metallic"], m["roughness"],
+                             m["transmission"])
+            ref.triangles(sc["corners"], sc["tri_mats"])
+            lamp = sc["lamp"]
+            ref.quad(lamp["q"], lamp["u"], lamp["v"], lamp["material"], light=True)
+            for v in sc.get("volumes", []):
+                ref.volume(*v)
+            for px, srgb, wu, wv in sc.get("texmaps", []):
+                ref.texmap(px, srgb, wu, wv)
+            for i, m in enumerate(sc["materials"]):
+                t = m.get("tex")
+                if t:
+                    ref.material_textures(i, t.get("base", 0), t.get("mr", 0), t.get("normal", 0), t.get("emissive", 0),
+                                          t.get("occlusion", 0), t.get("uv_scale", 0.0), t.get("normal_scale", 0.0))
+            if sc.get("texcoords"):
+                ref.texcoords(*sc["texcoords"])
+        t0 = time.perf_counter()
+        ref.set_accel()
+        rows = max(1, min(h, (4 if inst else 64)))
+        c = sc["camera"]
+        fau = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
+        _, (cl, sh) = ref.trace_image(fau, c["vfov"], w, h, spp, 1, sc["max_depth"], y0=h // 2 - rows // 2, rows=rows)
+        t_cpu = time.perf_counter() - t0
+        cores = O.ref_lib().rb_max_threads()
+        ref.close()
+        cpu = {"value": (cl + sh) / t_cpu / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "reference",
+               "sample": f"scene_set_accel + trace_image of {rows} central rows at {spp} spp "
+                         f"({cl + sh} rays in {t_cpu:.1f} s)"}
     value = rays / (ms / 1e3) / 1e6
     line = {"metric": METRIC_RENDER, "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -1001,10 +1039,9 @@ def run_render(a):
             "clocks": clocks, "engines": engines,
             "e2e": {"value": rays / (e_ms / 1e3) / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": w * h * 16,
                     "d2h_bytes_per_step": w * h * 16, "ms_per_step": e_ms},
-            "gpu_launches": a.steps,
-            "cpu_baseline": {"value": (cl + sh) / t_cpu / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "reference",
-                             "sample": f"scene_set_accel + trace_image of {rows} central rows at {spp} spp "
-                                       f"({cl + sh} rays in {t_cpu:.1f} s)"}}
+            "gpu_launches": a.steps}
+    if cpu:
+        line["cpu_baseline"] = cpu
     s.close()
     ctx.close()
     print(json.dumps(line), flush=True)
@@ -1585,10 +1622,10 @@ def main():
     dev = torch.device("cuda", local)
     builder = 1 if a.builder == "ploc" else 0
 
-    cor = W.soup(a.n, 1 + rank)
+    cor = W.soup(a.n, 1 + rank) * np.float32(a.scale)
     quv = W.corners_to_quv(cor)
     tris = L.pack_tris(quv)
-    orig, dirs = W.rays_at_cube(a.rays, 2 + rank)
+    orig, dirs = W.rays_at_cube(a.rays, 2 + rank, scale=a.scale)
 
     ctx = L.Context(local)
     # a stream of our own (the default stream's handle is 0, which lrc_set_stream reads as "the
@@ -1683,6 +1720,12 @@ def main():
                 "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
                 "algorithmic_bytes_per_launch": trace_bytes, "bytes_per_ray": bytes_per_ray,
                 "ms_per_launch": trace_ms}
+    if (a.n, a.rays, a.builder, a.bits, a.scale) == (4 << 20, 16 << 20, "ploc", 30, 1.0):
+        dram_gbs = BUILDER_CLOSEST_DRAM["bytes_per_launch"] / (BUILDER_CLOSEST_DRAM["ms_per_launch"] / 1e3) / 1e9
+        rl_trace.update({"traffic": BUILDER_CLOSEST_DRAM["bytes_per_launch"],
+                         "traffic_from": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4th closest_kernel "
+                                         "launch of `python bench.py --workload builder --steps 1 --warmup 3 --no-cpu "
+                                         "--e2e-steps 1`", "dram_gbs": dram_gbs, "frac_dram": dram_gbs / peak})
     rl_trace["frac"] = rl_trace["achieved"] / peak
     rl_sort = {"kernel": "onesweep (all passes)", "bound": "hbm", "achieved": sort_bytes / (sort_ms / 1e3) / 1e9,
                "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,

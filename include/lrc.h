@@ -157,6 +157,14 @@ int lrc_scene_tree_device(lrc_scene *s, const uint32_t **nodes, const uint32_t *
  * change of its shapes, replaces it. lrc_scene_tree then copies out nnodes and naux entries. */
 int lrc_scene_set_tree(lrc_scene *s, const uint32_t *nodes, uint32_t nnodes, const uint32_t *aux, uint32_t naux,
                        unsigned flags);
+/* The walk's tree of a scene of triangles alone (no primitives). tight = 1 (the default): after
+ * each lrc_scene_build or lrc_scene_set_tree, the ray queries below (closest hit, any hit, walk
+ * statistics) follow a copy of the tree - the same nodes and leaves - whose boxes are the
+ * triangles' own bounds widened by 2^-17 of the root box's largest coordinate (at most the 1e-3
+ * of triangle_bounds, scene.c:65-74), inner boxes their unions: the same hits as the padded tree,
+ * fewer box tests where the padding is large beside the triangles. tight = 0: the tree as built.
+ * lrc_scene_tree always gives the tree as built (the reference's); the path tracer walks that. */
+int lrc_scene_set_walk(lrc_scene *s, int tight);
 
 /* Closest hits of nrays rays (origins, directions: 3 floats each) in (tmin, tmax) through the
  * scene's BVH: prim = the triangle hit (-1: none), t. The reference's Moller-Trumbore arithmetic

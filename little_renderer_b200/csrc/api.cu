@@ -30,6 +30,7 @@ int scene_build_on(lrc_scene *s, int builder, int key_bits, void **scratch, size
     const uint32_t n = s->ntris + s->nprims;
     if (!no_alloc) s->built_n = 0;
     s->tree_nnodes = s->tree_naux = 0;
+    s->walk_ok = false;
     if (!n) return LRC_OK;
     const size_t need_scratch = lrc::build_scratch_bytes(n, key_bits, builder);
     if (no_alloc) {
@@ -86,6 +87,32 @@ cudaError_t build_tlas_on(lrc_ctx *c, const float *d_inst, uint32_t n, Node *d_n
     if (!e) e = lrc::build_device_ext(p, d_boxes, lo_ext, d_nodes, d_aux, scratch, scratch_cap, c->d_status, c->num_sms,
                                       st, nullptr, timer);
     return e;
+}
+
+// the walk's tree of a triangle scene (no primitives): its tree's topology with tight boxes, for
+// the closest- and any-hit queries; the path tracer walks the tree as built
+int make_walk(lrc_scene *s) {
+    s->walk_ok = false;
+    if (!s->walk_tight || s->nprims || !s->built_n || !s->ntris) return LRC_OK;
+    lrc_ctx *c = s->ctx;
+    const size_t nn = s->tree_nnodes ? s->tree_nnodes : 2 * (size_t)s->built_n - 1;
+    const size_t na = s->tree_nnodes ? s->tree_naux : s->built_n;
+    cudaError_t e = cudaSuccess;
+    if (s->wnodes_cap < nn) {
+        cudaFree(s->d_wnodes);
+        s->d_wnodes = nullptr;
+        s->wnodes_cap = 0;
+        e = cudaMalloc(&s->d_wnodes, nn * 32);
+        if (!e) s->wnodes_cap = nn;
+    }
+    if (!e) e = reserve(&c->scratch, &c->scratch_cap, lrc::walk_tree_scratch_bytes((uint32_t)nn));
+    c->timer.begin(LRC_TS_HIERARCHY, c->st);
+    if (!e) e = lrc::walk_tree_device(s->d_nodes, (uint32_t)nn, s->d_aux, (uint32_t)na, reinterpret_cast<const float *>(s->d_tris),
+                                      s->ntris, s->d_wnodes, c->scratch, c->scratch_cap, c->d_status, c->st);
+    c->timer.end(c->st);
+    if (e) return cuda_status(c, e, "the walk's tree");
+    s->walk_ok = true;
+    return LRC_OK;
 }
 
 }  // namespace lrcapi
@@ -274,6 +301,7 @@ void lrc_scene_destroy(lrc_scene *s) {
     cudaStreamSynchronize(s->ctx->st);
     cudaFree(s->d_tris);
     cudaFree(s->d_nodes);
+    cudaFree(s->d_wnodes);
     cudaFree(s->d_aux);
     cudaFree(s->d_boxes);
     cudaFree(s->d_small);
@@ -309,6 +337,7 @@ int lrc_scene_set_triangles(lrc_scene *s, const uint32_t *tris, uint32_t n, unsi
     s->ntris = n;
     s->built_n = 0;
     s->tree_nnodes = s->tree_naux = 0;
+    s->walk_ok = false;
     if (!(flags & LRC_DEVICE)) return check_status(c);   // (the host array may be freed on return)
     return LRC_OK;
 }
@@ -316,7 +345,15 @@ int lrc_scene_set_triangles(lrc_scene *s, const uint32_t *tris, uint32_t n, unsi
 int lrc_scene_build(lrc_scene *s, int builder, int key_bits) {
     if (!s) return LRC_E_INVALID;
     lrc_ctx *c = s->ctx;
-    return scene_build_on(s, builder, key_bits, &c->scratch, &c->scratch_cap, c->st, &c->timer, false);
+    int rc = scene_build_on(s, builder, key_bits, &c->scratch, &c->scratch_cap, c->st, &c->timer, false);
+    return rc ? rc : make_walk(s);
+}
+
+int lrc_scene_set_walk(lrc_scene *s, int tight) {
+    if (!s || tight < 0 || tight > 1) return LRC_E_INVALID;
+    DeviceGuard g(s->ctx->device);
+    s->walk_tight = tight != 0;
+    return make_walk(s);
 }
 
 int lrc_scene_tree(lrc_scene *s, uint32_t *nodes, uint32_t *aux, unsigned flags) {
@@ -354,6 +391,7 @@ int lrc_scene_set_tree(lrc_scene *s, const uint32_t *nodes, uint32_t nnodes, con
             if (aux[i] >= shapes) return fail(c, LRC_E_INVALID, "an aux entry names no shape of the scene");
     }
     DeviceGuard g(c->device);
+    s->walk_ok = false;
     const size_t cap = std::max<size_t>(naux, ((size_t)nnodes + 1) / 2);   // (2 cap - 1 nodes, cap aux)
     cudaError_t e = cudaSuccess;
     if (s->tree_cap < cap) {
@@ -373,6 +411,8 @@ int lrc_scene_set_tree(lrc_scene *s, const uint32_t *nodes, uint32_t nnodes, con
     s->built_n = naux;
     s->tree_nnodes = nnodes;
     s->tree_naux = naux;
+    int rc = make_walk(s);
+    if (rc) return rc;
     return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 
@@ -542,6 +582,7 @@ int lrc_scene_set_prims(lrc_scene *s, const float *prims, uint32_t n, unsigned f
     s->nprims = n;
     s->built_n = 0;
     s->tree_nnodes = s->tree_naux = 0;
+    s->walk_ok = false;
     return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 

@@ -35,6 +35,10 @@ struct lrc_scene {
     uint32_t built_n = 0;         // items of the built tree (0: none)
     uint32_t tree_nnodes = 0;     // a tree given by lrc_scene_set_tree: its nodes and aux entries
     uint32_t tree_naux = 0;       // (0: the built tree's 2 n - 1 and n)
+    Node *d_wnodes = nullptr;     // the walk's copy of a triangle tree with tight boxes (lrc_scene_set_walk)
+    size_t wnodes_cap = 0;        // (nodes)
+    bool walk_ok = false;         // d_wnodes is the current tree's
+    bool walk_tight = true;
     float *d_boxes = nullptr;
     size_t boxes_cap = 0;
     uint32_t *d_small = nullptr;  // 6 bound keys, 6 bounds, 6 lo/ext
@@ -228,7 +232,7 @@ inline lrc::PtScene pt_scene(const lrc_scene *s) {
 // the walk's view of a scene: its tree (root 0), leaves' triangles, and the sizes it checks against
 inline lrc::TraceTables tables(const lrc_scene *s) {
     lrc::TraceTables tt{};
-    tt.nodes = s->d_nodes;
+    tt.nodes = s->walk_ok ? s->d_wnodes : s->d_nodes;
     tt.aux = s->d_aux;
     tt.tris = reinterpret_cast<const float4 *>(s->d_tris);
     tt.root = 0;

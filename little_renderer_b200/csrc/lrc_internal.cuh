@@ -137,6 +137,13 @@ cudaError_t refit_device(Node *d_nodes, const uint32_t *d_aux, uint32_t n, uint3
                          uint32_t stride4, uint32_t lo_at, void *scratch, size_t scratch_bytes, uint32_t *d_status,
                          cudaStream_t st);
 cudaError_t tree_cost_device(const Node *d_nodes, uint32_t n, double *d_out, cudaStream_t st);
+// the walk's tree of a triangle tree (nn nodes, root at 0, leaves' aux = triangle ids): the same
+// nodes with each leaf's box the bounds of its triangles' corners widened by 2^-17 of the largest
+// coordinate of the source root box (at most the 1e-3 the builders pad with), inner boxes the unions
+size_t walk_tree_scratch_bytes(uint32_t nn);
+cudaError_t walk_tree_device(const Node *d_src, uint32_t nn, const uint32_t *d_aux, uint32_t naux, const float *d_tris,
+                             uint32_t ntris, Node *d_dst, void *scratch, size_t scratch_bytes, uint32_t *d_status,
+                             cudaStream_t st);
 
 // traversal internals (traverse.cu)
 struct TraceTables {

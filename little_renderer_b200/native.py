@@ -117,6 +117,7 @@ def lib():
     L.lrc_scene_intersect.argtypes = [vp, vp, vp, u64, f32, f32, vp, vp, C.c_uint]
     L.lrc_scene_occluded.argtypes = [vp, vp, vp, vp, u64, f32, vp, C.c_uint]
     L.lrc_scene_trace_stats.argtypes = [vp, vp, vp, u64, f32, f32, vp, C.c_uint]
+    L.lrc_scene_set_walk.argtypes = [vp, C.c_int]
     L.lrc_scene_set_prims.argtypes = [vp, vp, u32, C.c_uint]
     L.lrc_scene_set_normals.argtypes = [vp, vp, u32, C.c_uint]
     L.lrc_scene_set_materials.argtypes = [vp, vp, u32]
@@ -416,6 +417,11 @@ class Scene:
         nodes = np.ascontiguousarray(nodes, np.uint32).reshape(-1, 8)
         aux = np.ascontiguousarray(aux, np.uint32)
         self.ctx.check(self.ctx.L.lrc_scene_set_tree(self.h, _ptr(nodes), nodes.shape[0], _ptr(aux), aux.shape[0], 0))
+
+    def set_walk(self, tight):
+        """lrc_scene_set_walk: ray queries over a copy of the tree with tight boxes (1, the default)
+        or over the tree as built (0)."""
+        self.ctx.check(self.ctx.L.lrc_scene_set_walk(self.h, int(tight)))
 
     def tree(self):
         nodes = np.zeros((2 * self.n - 1, 8), np.uint32)

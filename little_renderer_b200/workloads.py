@@ -33,14 +33,15 @@ def soup(n, seed=1):
     return corners
 
 
-def rays_at_cube(n, seed=2, radius=2.0, centre=(0.5, 0.5, 0.5)):
+def rays_at_cube(n, seed=2, radius=2.0, centre=(0.5, 0.5, 0.5), scale=1.0):
     """n rays: origins uniform on the sphere of `radius` about `centre`, unit directions toward
-    uniform points of the unit cube. Returns (orig, dir) float32 (n, 3) each."""
+    uniform points of the unit cube; scale: the cube, the sphere and its centre scaled by it (the
+    scaled soup's rays). Returns (orig, dir) float32 (n, 3) each."""
     rng = np.random.default_rng(seed)
     g = rng.normal(size=(n, 3))
     g /= np.linalg.norm(g, axis=1, keepdims=True)
-    o = (np.asarray(centre) + radius * g).astype(np.float32)
-    target = rng.random((n, 3), dtype=np.float64).astype(np.float32)
+    o = (np.asarray(centre) * scale + (radius * scale) * g).astype(np.float32)
+    target = (rng.random((n, 3), dtype=np.float64) * scale).astype(np.float32)
     d = (target - o).astype(np.float32)
     d = (d / np.linalg.norm(d.astype(np.float64), axis=1, keepdims=True)).astype(np.float32)
     return np.ascontiguousarray(o), np.ascontiguousarray(d)

@@ -75,7 +75,7 @@ def test_build_flat_axis_and_outside_bounds(ctx, oracle, builder):
     _check_same(ctx, oracle, boxes, np.array([0, 0.5, 0], np.float32), np.array([1, 0.5, 1], np.float32), 30, builder)
 
 
-@pytest.mark.parametrize("builder,bits", [(0, 30), (1, 30), (0, 63)])
+@pytest.mark.parametrize("builder,bits", [(0, 30), (1, 30), (0, 63), (1, 63)])
 def test_build_full_size_4m(ctx, oracle, builder, bits):
     """The builder workload at its full size (N = 4M), bit for bit against the oracle."""
     _, boxes, blo, bhi = _inputs(oracle, 4 * 1024 * 1024, 77)

@@ -39,11 +39,13 @@ def test_exact_mode_is_the_cpu_light_tracer(ctx, oracle, cornell128):
     err = rel_rmse(gpu, cpu)
     print(f"lit pixels {lit.mean():.3f}, of them equal to the bit {equal:.4f}; relRMSE {err:.2e}; "
           f"rays GPU {rays} CPU {closest + shadow}")
+    # measured: 63 % of the lit pixels equal to the bit, relRMSE 2e-3 (a light path whose sinf / cosf
+    # rounds differently lands a whole splat elsewhere)
     assert lit.mean() > 0.3
-    assert equal > 0.5
-    assert err < 0.05
-    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 0.01
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.01
+    assert equal >= 0.55
+    assert err <= 5e-3
+    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 2e-3
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-3
 
 
 def test_sums_are_the_image_and_order_free(ctx, oracle, cornell128):
@@ -100,8 +102,9 @@ def test_skip_caustics_is_the_cpu_image(ctx, oracle, cornell128):
     exact = np.all(gpu == cpu, axis=2).mean()
     err = rel_rmse(gpu, cpu)
     print(f"pixels equal to the bit: {exact:.4f}; relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}")
-    assert exact > 0.5 and err < 0.05
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.02
+    # measured: 85 % of the pixels equal to the bit, relRMSE 3.1e-6
+    assert exact >= 0.7 and err <= 1e-4
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-3
     assert gpu.sum() < (full[..., :3] / spp).sum()
 
 

@@ -66,6 +66,83 @@ def test_exact_image_with_sky_matches_trace_image(ctx, oracle, field):
     equal = np.all(gpu == cpu, axis=2).mean()
     err = float(np.sqrt(((gpu.astype(np.float64) - cpu) ** 2).sum() / (cpu.astype(np.float64) ** 2).sum()))
     print(f"instanced + sky: pixels equal {equal:.4f}; relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}")
-    assert equal > 0.3
-    assert err < 0.05
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.01
+    # measured: 47 % of the pixels equal to the bit (4 samples of up to 12 bounces each), relRMSE
+    # 1.9e-6, ray counts equal
+    assert equal >= 0.4
+    assert err <= 1e-4
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-4
+
+
+@pytest.fixture(scope="module")
+def full_field():
+    """The instanced scene at its own size: 5000 instances of 14 meshes (10k-100k triangles each),
+    a 2048 x 1024 sky, 1280 x 720, 64 spp, depth 12."""
+    return W.instanced_field()
+
+
+def _field_rays(sc, n, seed):
+    """n rays over the field: half aimed at instance centres from above the ground, half in
+    uniform directions of the upper hemisphere (ground, sky and grazing hits)."""
+    rng = np.random.default_rng(seed)
+    o = np.stack([rng.uniform(-5, 45, n), rng.uniform(0.5, 8, n), rng.uniform(-5, 45, n)], 1).astype(np.float32)
+    tgt = sc["xf"][rng.integers(0, sc["xf"].shape[0], n), :, 3].astype(np.float64)
+    d = tgt - o
+    h = n // 2
+    v = rng.normal(size=(n - h, 3))
+    v[:, 1] = -np.abs(v[:, 1]) * rng.uniform(0.05, 1.0, n - h)
+    d[h:] = v
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    return o, d
+
+
+@pytest.mark.parametrize("mesh_builder", [0, 1])
+def test_full_field_hits_match_scene_intersect(ctx, oracle, full_field, mesh_builder):
+    """Closest hits on the full field (262144 rays) against scene_intersect over the reference's
+    own two-level SAH trees: the same (primitive, instance) and t to the bit, except ties within
+    1e-6 relative t."""
+    sc = full_field
+    ref = ref_field(oracle, sc)
+    s = R.instanced_scene(ctx, sc, mesh_builder, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    o, d = _field_rays(sc, 262144, 21)
+    rp, ri, rt = ref.intersect(o, d, 2e-3, 1e30)
+    p, i, t = s.intersect_ex(o, d, 2e-3, 1e30)
+    hit = (rp >= 0) | (ri >= 0)
+    same = (p == rp) & (i == ri)
+    diff = ~same
+    print(f"full field, mesh builder {mesh_builder}: {hit.mean():.3f} of rays hit, {int((ri >= 0).sum())} instance "
+          f"hits, {int(diff.sum())} differ")
+    assert (ri >= 0).mean() > 0.4 and hit.mean() > 0.7
+    assert diff.sum() <= 30
+    assert np.all(np.abs(t[diff] - rt[diff]) <= 1e-6 * np.abs(rt[diff]))
+    assert np.array_equal(t[same], rt[same])
+    s.close()
+
+
+def test_full_field_exact_band_at_720p(ctx, oracle, full_field):
+    """A band of 16 rows of the 1280 x 720 image at 64 spp, depth 12, with the sky's next event
+    estimation, in exact mode against trace_image's same rows (relRMSE and ray count); the same
+    band on the one-kernel path and through lrc_trace's default route (1.3M paths: the wavefront
+    engine) equal to the bit."""
+    sc = full_field
+    ref = ref_field(oracle, sc)
+    c = sc["camera"]
+    fau = np.array([*c["from"], *c["at"], *c["up"]], np.float32)
+    w, h, spp, seed, y0, rows = sc["width"], sc["height"], sc["spp"], 7, 352, 16
+    cpu, (closest, shadow) = ref.trace_image(fau, c["vfov"], w, h, spp, seed, sc["max_depth"], y0=y0, rows=rows)
+    s = R.instanced_scene(ctx, sc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    p = L.native.trace_params(oracle.camera(fau, c["vfov"], w / h), w, h, sc["max_depth"], 1, 1, 1, seed)
+    acc, rays = s.trace(p, spp, y0=y0, rows=rows)
+    mk, rays_mk = s.trace(p, spp, y0=y0, rows=rows, flags=L.native.LRC_TRACE_MEGAKERNEL)
+    assert np.array_equal(acc, mk) and rays == rays_mk
+    gpu = acc[y0:y0 + rows, :, :3] * (np.float32(1) / np.float32(spp))
+    equal = np.all(gpu == cpu, axis=2).mean()
+    err = float(np.sqrt(((gpu.astype(np.float64) - cpu) ** 2).sum() / (cpu.astype(np.float64) ** 2).sum()))
+    rel_rays = abs(rays - (closest + shadow)) / (closest + shadow)
+    print(f"720p band, rows {y0}-{y0 + rows}: pixels equal {equal:.4f}; relRMSE {err:.2e}; rays GPU {rays} "
+          f"CPU {closest + shadow} ({rel_rays:.2e})")
+    # measured: relRMSE 1.9e-5, 20 of 7.7M rays apart. A pixel here sums 64 paths of up to 12
+    # bounces, and one ulp anywhere in one of them changes the sum: 0.4 % of the pixels are equal
+    # to the bit, so the band is held to its relRMSE and its ray count
+    assert err <= 1e-4
+    assert rel_rays < 1e-5
+    s.close()

@@ -48,10 +48,11 @@ def test_exact_mode_is_the_cpu_image_with_media(ctx, oracle, foggy):
     print(f"media: pixels equal to the bit {exact:.4f}; relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}; "
           f"the medium changes {np.any(acc != clear, axis=2).mean():.3f} of the pixels")
     assert np.any(acc != clear, axis=2).mean() > 0.5
-    assert exact > 0.3
-    assert err < 0.05
-    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 0.01
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.02
+    # measured: 74 % of the pixels equal to the bit, relRMSE 3e-8
+    assert exact >= 0.65
+    assert err <= 1e-5
+    assert abs(gpu.mean() - cpu.mean()) / cpu.mean() < 1e-4
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-3
 
 
 def test_fast_mode_mean_matches_cpu_with_media(ctx, oracle, foggy):
@@ -110,5 +111,5 @@ def test_light_tracing_through_media_is_the_cpu_one(ctx, oracle, foggy):
     gpu, rays = s.caustics(params(oracle, sc, 1, 0), photons, seed)
     err = rel_rmse(gpu, cpu)
     print(f"caustics through media: relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}")
-    assert err < 0.05
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.02
+    assert err <= 1e-2                              # (measured 2.7e-3)
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 2e-3

@@ -51,9 +51,10 @@ def test_exact_mode_is_the_cpu_image_with_textures(ctx, oracle, textured):
     print(f"textures: pixels equal to the bit {exact:.4f}; relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}; "
           f"the textures change {np.any(acc != plain, axis=2).mean():.3f} of the pixels")
     assert np.any(acc != plain, axis=2).mean() > 0.3
-    assert exact > 0.5
-    assert err < 0.05
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.02
+    # measured: 70 % of the pixels equal to the bit, relRMSE 5e-6 (the rest differ in the last bits)
+    assert exact >= 0.6
+    assert err <= 1e-4
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 1e-3
 
 
 def test_light_tracing_with_textures_is_the_cpu_one(ctx, oracle, textured):
@@ -68,8 +69,8 @@ def test_light_tracing_with_textures_is_the_cpu_one(ctx, oracle, textured):
     gpu, rays = s.caustics(params(oracle, sc, 1, 0), photons, seed)
     err = rel_rmse(gpu, cpu)
     print(f"caustics with textures: relRMSE {err:.2e}; rays GPU {rays} CPU {closest + shadow}")
-    assert err < 0.05
-    assert abs(rays - (closest + shadow)) / (closest + shadow) < 0.02
+    assert err <= 2e-3                              # (measured 2.4e-4)
+    assert abs(rays - (closest + shadow)) / (closest + shadow) < 2e-3
 
 
 @pytest.mark.parametrize("engine", [1, 0])
