@@ -146,12 +146,13 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) { return *(co
 __device__ __forceinline__ void st_volatile(uint32_t *p, uint32_t v) { *(volatile uint32_t *)p = v; }
 
 // One radix pass over bits [shift, shift + 8). first: the values are the items' indices.
-// A tile's keys are ranked warp by warp (the keys of one digit in a warp: __match_any_sync, the
+// A tile's keys are ranked warp by warp (the lanes holding one digit: one ballot per digit bit; the
 // group's leader takes the group's places from the warp's counter with one shared atomic - the
 // warp's items in order, so the ranks are stable - results read after all 16 are issued), staged in
-// digit order in shared memory (registers freed before the look-back), and written out at their
-// digit's global offset: the tiles before it (decoupled look-back over posted counts / prefixes)
-// plus the digits before it (the pass's histogram).
+// digit order in shared memory with their values (read only then, so that the ranking keeps its
+// registers), and written out at their digit's global offset: the tiles before it (decoupled
+// look-back over posted counts / prefixes) plus the digits before it (the pass's histogram). A
+// full tile (all but the last) ranks without bounds checks and without the validity ballot.
 template <typename K, bool FIRST>
 __global__ void __launch_bounds__(OS_THREADS, OS_MINB) onesweep_kernel(const K *__restrict__ keys_in,
                                                                  const uint32_t *__restrict__ vals_in,
@@ -167,33 +168,52 @@ __global__ void __launch_bounds__(OS_THREADS, OS_MINB) onesweep_kernel(const K *
     const uint32_t tile = S.tile;
     const uint32_t tile0 = tile * OS_TILE;
     const uint32_t in_tile = min((uint32_t)OS_TILE, n - tile0);
+    const bool full = in_tile == (uint32_t)OS_TILE;
 
     K key[OS_ITEMS];
-    uint32_t val[OS_ITEMS], rank[OS_ITEMS];   // rank: the leader's base | leader << 16 | lanes before << 24, then the rank
+    uint32_t rank[OS_ITEMS];   // rank: the leader's base | leader << 16 | lanes before << 24, then the rank
     const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t idx0 = tile0 + w * (32 * OS_ITEMS) + lane;
 #pragma unroll
     for (int k = 0; k < OS_ITEMS; k++) {
-        const uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
-        const bool ok = idx < n;
-        key[k] = ok ? keys_in[idx] : K(0);
-        val[k] = ok ? (FIRST ? idx : vals_in[idx]) : 0u;
+        const uint32_t idx = idx0 + k * 32;
+        key[k] = (full || idx < n) ? keys_in[idx] : K(0);
     }
+    if (full) {
 #pragma unroll
-    for (int k = 0; k < OS_ITEMS; k++) {
-        const uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
-        const uint32_t d = idx < n ? (uint32_t)((key[k] >> shift) & 255u) : 0x100u;
-        // the lanes with this lane's digit: one ballot per digit bit (and one for validity)
-        uint32_t peers = 0xffffffffu;
+        for (int k = 0; k < OS_ITEMS; k++) {
+            const uint32_t d = (uint32_t)((key[k] >> shift) & 255u);
+            // the lanes with this lane's digit: one ballot per digit bit
+            uint32_t peers = 0xffffffffu;
 #pragma unroll
-        for (int bit = 0; bit < 9; bit++) {
-            const bool on = (d >> bit) & 1u;
-            const uint32_t bal = __ballot_sync(0xffffffffu, on);
-            peers &= on ? bal : ~bal;
+            for (int bit = 0; bit < 8; bit++) {
+                const bool on = (d >> bit) & 1u;
+                const uint32_t bal = __ballot_sync(0xffffffffu, on);
+                peers &= on ? bal : ~bal;
+            }
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&S.warp_hist[w][d], (uint32_t)__popc(peers));
+            rank[k] = base | (uint32_t)leader << 16 | (uint32_t)__popc(peers & lt_mask) << 24;
         }
-        const int leader = __ffs(peers) - 1;
-        uint32_t base = 0;
-        if (d < 256 && lane == leader) base = atomicAdd(&S.warp_hist[w][d], (uint32_t)__popc(peers));
-        rank[k] = base | (uint32_t)leader << 16 | (uint32_t)__popc(peers & lt_mask) << 24;
+    } else {
+#pragma unroll
+        for (int k = 0; k < OS_ITEMS; k++) {
+            const uint32_t idx = idx0 + k * 32;
+            const uint32_t d = idx < n ? (uint32_t)((key[k] >> shift) & 255u) : 0x100u;
+            // (and one ballot for validity)
+            uint32_t peers = 0xffffffffu;
+#pragma unroll
+            for (int bit = 0; bit < 9; bit++) {
+                const bool on = (d >> bit) & 1u;
+                const uint32_t bal = __ballot_sync(0xffffffffu, on);
+                peers &= on ? bal : ~bal;
+            }
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (d < 256 && lane == leader) base = atomicAdd(&S.warp_hist[w][d], (uint32_t)__popc(peers));
+            rank[k] = base | (uint32_t)leader << 16 | (uint32_t)__popc(peers & lt_mask) << 24;
+        }
     }
 #pragma unroll
     for (int k = 0; k < OS_ITEMS; k++)
@@ -217,15 +237,15 @@ __global__ void __launch_bounds__(OS_THREADS, OS_MINB) onesweep_kernel(const K *
     const uint32_t dstart = block_excl_scan<OS_THREADS>(count, S.scan, tot);
     if (dig) S.digit_start[d] = dstart;
     __syncthreads();
-    // stage the tile in digit order (stable: warp, then item, then lane order)
+    // stage the tile in digit order (stable: warp, then item, then lane order), the values read now
 #pragma unroll
     for (int k = 0; k < OS_ITEMS; k++) {
-        const uint32_t idx = tile0 + w * (32 * OS_ITEMS) + k * 32 + lane;
-        if (idx < n) {
+        const uint32_t idx = idx0 + k * 32;
+        if (full || idx < n) {
             const uint32_t dk = (uint32_t)((key[k] >> shift) & 255u);
             const uint32_t pos = S.digit_start[dk] + S.warp_hist[w][dk] + rank[k];
             S.key_stage[pos] = key[k];
-            S.val_stage[pos] = val[k];
+            S.val_stage[pos] = FIRST ? idx : vals_in[idx];
         }
     }
     // decoupled look-back: tile t's prefix of digit d over the tiles before it
