@@ -200,32 +200,128 @@ __device__ __forceinline__ V3 xnormal(const float4 *inv, V3 n) {  // xform_norma
 
 // The closest (ANY = false) or any hit on the instances in (tmin, best): the instance and the
 // triangle's index in its mesh; false if none. The top level's leaves are instances; each is
-// entered with the ray in its own space (o' = inv o, d' = inv d: the same t) and its mesh's BVH walked.
+// entered with the ray in its own space (o' = inv o, d' = inv d: the same t) and its mesh's BVH
+// walked. One loop walks both levels: a top-level node and a mesh's node take the same box-test
+// code (the level picks the node array and the ray), so the lanes of a warp that are in different
+// levels still run together (walking each mesh in a walk of its own, nested in the top level's
+// leaf, left 2 of 32 lanes active per instruction). Entering an instance pushes a mark that
+// brings the walk back to the top level when its mesh is done, and a leaf's further instances
+// wait on the stack in order, so the instances, their nodes and their triangles are visited in the
+// nested walk's order: the same hits and the same ties. COUNT as bvh_walk's.
 template <bool ANY, bool COUNT = false>
 __device__ bool walk_instances(const PtScene &S, V3 o, V3 d, float tmin, float &best, int &inst, int &tri, uint32_t *err,
                                uint32_t *cnt = nullptr) {
-    bool found = false;
-    bvh_walk<COUNT>(S.tlas_nodes, 0, S.tlas_nnodes, S.tlas_aux, S.ninst, o, d, tmin, best, err, [&](uint32_t i) {
-        if (i >= S.ninst) { atomicOr(err, ST_BAD_TREE); return true; }
+    constexpr uint32_t MARK = 0xffffffffu, ENTER = 0xfffffffeu;   // (stack entries' first word; node indices are smaller)
+    const RayBox rw = ray_box(o, d);
+    const float4 *tn = S.tlas_nodes;
+    float4 r0 = ld4(&tn[0]), r1 = ld4(&tn[1]);
+    if constexpr (COUNT) cnt[0] += 1;
+    if (!(slab(rw, r0, r1, tmin, best) <= best)) return false;
+    uint2 stack[PT_STACK];
+    int sp = 0;
+    bool found = false, in_mesh = false;
+    RayBox rb = rw;
+    V3 ro = o, rd = d;
+    uint32_t cur = 0, first = 0;
+    const float4 *nodes = tn;
+    uint32_t nn = S.tlas_nnodes;
+    uint32_t a = __float_as_uint(r0.w), b = __float_as_uint(r1.w);
+    // instance i entered: its mesh's root box against the ray in its space; true with (a, b) its
+    // root's record when the walk goes into the mesh; sp = -1: the walk ends (a bad index, a full stack)
+    auto enter = [&](uint32_t i) -> bool {
+        if (i >= S.ninst) { atomicOr(err, ST_BAD_TREE); sp = -1; return false; }
         const float4 *rec = S.inst + 8 * (size_t)i;
         const uint32_t mesh = __float_as_uint(ld4(rec + 6).w);
-        if (mesh >= S.nmeshes) return false;                       // (shapes: not in these scenes)
-        const uint4 mi = __ldg(&S.mesh_info[mesh]);                // root node, first triangle, triangles
-        V3 ro = xpoint(rec + 3, o), rd = xdir(rec + 3, d);
-        return bvh_walk<COUNT>(S.mnodes, mi.x, S.mnnodes, S.maux, S.mnaux, ro, rd, tmin, best, err, [&](uint32_t g) {
-            if (g >= S.nmtris) { atomicOr(err, ST_BAD_TREE); return true; }
-            float t;
-            if (hit_tri_t(S.mtris + 3 * (size_t)g, ro, rd, tmin, best, t)) {
-                best = t;
-                inst = (int)i;
-                tri = (int)(g - mi.y);
-                found = true;
-                return ANY;
+        if (mesh >= S.nmeshes) return false;                        // (shapes: not in these scenes)
+        const uint4 mi = __ldg(&S.mesh_info[mesh]);                 // root node, first triangle, triangles
+        const V3 io = xpoint(rec + 3, o), id = xdir(rec + 3, d);
+        const RayBox ib = ray_box(io, id);
+        const float4 m0 = ld4(&S.mnodes[2 * (size_t)mi.x]), m1 = ld4(&S.mnodes[2 * (size_t)mi.x + 1]);
+        if constexpr (COUNT) cnt[0] += 1;
+        if (!(slab(ib, m0, m1, tmin, best) <= best)) return false;
+        if (sp >= PT_STACK) { atomicOr(err, ST_STACK_OVERFLOW); sp = -1; return false; }
+        stack[sp++] = make_uint2(MARK, 0u);
+        in_mesh = true;
+        ro = io; rd = id; rb = ib;
+        nodes = S.mnodes;
+        nn = S.mnnodes;
+        cur = i;
+        first = mi.y;
+        a = __float_as_uint(m0.w);
+        b = __float_as_uint(m1.w);
+        return true;
+    };
+    while (true) {
+        if (b & LEAF_BIT) {
+            const uint32_t count = b & ~LEAF_BIT;
+            if (!in_mesh) {
+                if (a >= S.ninst || count > S.ninst - a) { atomicOr(err, ST_BAD_TREE); return found; }
+                if (count) {
+                    for (uint32_t k = count - 1; k >= 1; k--) {             // the leaf's later instances wait
+                        if (sp >= PT_STACK) { atomicOr(err, ST_STACK_OVERFLOW); return found; }
+                        stack[sp++] = make_uint2(ENTER, __ldg(&S.tlas_aux[a + k]));
+                    }
+                    if constexpr (COUNT) cnt[1] += 1;
+                    const bool in = enter(__ldg(&S.tlas_aux[a]));
+                    if (sp < 0) return found;
+                    if (in) continue;
+                }
+            } else {
+                if (a >= S.mnaux || count > S.mnaux - a) { atomicOr(err, ST_BAD_TREE); return found; }
+                for (uint32_t k = 0; k < count; k++) {
+                    if constexpr (COUNT) cnt[1] += 1;
+                    const uint32_t g = __ldg(&S.maux[a + k]);
+                    if (g >= S.nmtris) { atomicOr(err, ST_BAD_TREE); return found; }
+                    float t;
+                    if (hit_tri_t(S.mtris + 3 * (size_t)g, ro, rd, tmin, best, t)) {
+                        best = t;
+                        inst = (int)cur;
+                        tri = (int)(g - first);
+                        found = true;
+                        if (ANY) return true;
+                    }
+                }
             }
-            return false;
-        }, cnt);
-    }, cnt);
-    return found;
+        } else {
+            if (a >= nn || b >= nn) { atomicOr(err, ST_BAD_TREE); return found; }
+            float4 l0 = ld4(&nodes[2 * (size_t)a]), l1 = ld4(&nodes[2 * (size_t)a + 1]);
+            float4 h0 = ld4(&nodes[2 * (size_t)b]), h1 = ld4(&nodes[2 * (size_t)b + 1]);
+            if constexpr (COUNT) cnt[0] += 2;
+            float t0 = slab(rb, l0, l1, tmin, best), t1 = slab(rb, h0, h1, tmin, best);
+            bool c0 = t0 <= best, c1 = t1 <= best;
+            if (c0 && c1) {
+                bool first0 = t0 <= t1;
+                if (sp >= PT_STACK) { atomicOr(err, ST_STACK_OVERFLOW); return found; }
+                stack[sp++] = first0 ? make_uint2(__float_as_uint(h0.w), __float_as_uint(h1.w))
+                                     : make_uint2(__float_as_uint(l0.w), __float_as_uint(l1.w));
+                a = first0 ? __float_as_uint(l0.w) : __float_as_uint(h0.w);
+                b = first0 ? __float_as_uint(l1.w) : __float_as_uint(h1.w);
+                continue;
+            }
+            if (c0) { a = __float_as_uint(l0.w); b = __float_as_uint(l1.w); continue; }
+            if (c1) { a = __float_as_uint(h0.w); b = __float_as_uint(h1.w); continue; }
+        }
+        // the next entry: a node of this level, a mark (back to the top level) or an instance to enter
+        bool next = false;
+        while (!next) {
+            if (sp == 0) return found;
+            const uint2 e = stack[--sp];
+            if (e.x == MARK) {
+                in_mesh = false;
+                ro = o; rd = d; rb = rw;
+                nodes = tn;
+                nn = S.tlas_nnodes;
+            } else if (e.x == ENTER) {
+                if constexpr (COUNT) cnt[1] += 1;
+                next = enter(e.y);
+                if (sp < 0) return found;
+            } else {
+                a = e.x;
+                b = e.y;
+                next = true;
+            }
+        }
+    }
 }
 
 }  // namespace pt
