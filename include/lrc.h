@@ -505,11 +505,14 @@ void lrc_server_destroy(lrc_server *sv);
 #define LRC_SERVE_DENOISE 16
 int lrc_server_submit(lrc_server *sv, lrc_scene *s, const lrc_trace_params *p, uint32_t spp, const float *records,
                       uint32_t n, int tlas_mode, uint64_t *id);
-/* One wave: admission, the next band of every admitted job traced in one batch run, waited for;
- * *finished: the jobs it finished. */
+/* One step: admission, then the next wave (bands of the admitted jobs with rows left, as the
+ * policy below makes them) planned and launched as one batch run, then the wave launched by the
+ * step before waited for and the jobs whose last band it held finished; *finished: those jobs. The
+ * waves alternate between two batches, so the device runs one wave while the host plans the next. */
 int lrc_server_step(lrc_server *sv, int32_t *finished);
-/* A finished job (LRC_RETRY while not): its image (device, W x H x 4 floats: sum and count), its
- * rays, and the server clock's times (ms) of its submit, admission and end. */
+/* A finished job (LRC_RETRY while not): its image (device, W x H x 4 floats: sum and count; complete
+ * on the context's stream, or through lrc_server_read), its rays, and the server clock's times (ms)
+ * of its submit, admission and end. */
 int lrc_server_result(lrc_server *sv, uint64_t id, const float **d_image, uint64_t *rays, double *t_submit,
                       double *t_admit, double *t_done);
 /* A finished job's image copied to host memory (W x H x 4 floats; gpu_view_trace_read's sum and
@@ -520,10 +523,13 @@ int lrc_server_release(lrc_server *sv, uint64_t id);
 int lrc_server_state(const lrc_server *sv, int32_t *queued, int32_t *active, int32_t *finished, uint64_t *bytes);
 /* The server's clock (ms; monotonic). */
 double lrc_server_clock(void);
-/* The batch a server runs its waves with (to set its engine or wavefront size; do not add jobs). */
+/* The first of the two batches a server runs its waves with (do not add jobs). */
 lrc_batch *lrc_server_batch(lrc_server *sv);
-/* waves run so far, the trace kernels they launched and their device time (CUDA events around
- * each wave's run), each optional */
+/* The waves' wavefront size (paths in flight) and closest-hit / shadow launch shape, both batches
+ * (lrc_batch_set_wavefront). */
+int lrc_server_set_wavefront(lrc_server *sv, uint32_t slots, int32_t variant);
+/* waves run so far, the trace kernels they launched and their device time (CUDA events from each
+ * wave's launch to its end), each optional */
 int lrc_server_stats(const lrc_server *sv, uint64_t *waves, uint64_t *kernels, double *gpu_ms);
 /* How a wave is made from the admitted jobs: 0 the next band of every job, the wave's paths shared
  * evenly; 1 the oldest jobs first, each band as large as the wave's paths left allow (fewer scenes a

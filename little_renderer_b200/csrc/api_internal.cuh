@@ -254,6 +254,14 @@ struct InstView {
     const uint32_t *tlas_aux;
 };
 // lrc_batch_add (no build) with the job's own instances (a server's moving-instance job)
+// an event lrc_batch_run records right before it launches the run's trace (null: none)
+void batch_set_launch_event(lrc_batch *b, cudaEvent_t e);
+// the run buffers sized for up to `tasks` tasks of up to `jobs` jobs now, so that runs within
+// those sizes neither allocate nor free device memory (which would wait for the device)
+int batch_reserve(lrc_batch *b, unsigned long long tasks, size_t jobs);
+// the last run's ray counts per job (h_rays, nj entries) and its wavefront passes, copied to pinned
+// host memory on the context's stream, not waited for
+cudaError_t batch_counts_async(lrc_batch *b, unsigned long long *h_rays, uint32_t *h_passes);
 int batch_add_view(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
                    uint32_t spp, float *d_accum, const InstView &view, bool guided);
 cudaError_t build_tlas_on(lrc_ctx *c, const float *d_inst, uint32_t n, Node *d_nodes, uint32_t *d_aux, float *d_boxes,

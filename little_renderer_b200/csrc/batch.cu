@@ -69,6 +69,10 @@ struct lrc_batch {
     unsigned graph_flags = 0;
     std::vector<unsigned char> graph_sig;
     int graph_used = 0;
+    cudaEvent_t ev_launch = nullptr;      // recorded right before a run's trace is launched (the server's wave timing)
+    lrc::BatchJob *h_table = nullptr;     // pinned staging of the job table's upload (and the run block after it)
+    size_t h_table_cap = 0;
+    cudaEvent_t ev_table = nullptr;       // the last upload from it done (it may be written again)
 };
 
 namespace {
@@ -189,6 +193,8 @@ int build_job(lrc_batch *b, const lrc_batch::Job *J, cudaStream_t st, bool captu
     return rc;
 }
 
+uint32_t max_passes(const lrc_batch *b, unsigned long long limit);
+
 // the job table in queue order, the partial buffers and counters sized, the table uploaded
 int prepare(lrc_batch *b) {
     lrc_ctx *c = b->ctx;
@@ -236,8 +242,31 @@ int prepare(lrc_batch *b) {
         T.pmom = T.P.moments ? pmom + T.task0 : nullptr;
         T.rays = b->d_ctr + 1 + b->order[q];
     }
-    e = cudaMemcpyAsync(b->d_jobs, b->table.data(), nj * sizeof(lrc::BatchJob), cudaMemcpyHostToDevice, c->st);
-    if (!e) e = cudaStreamSynchronize(c->st);   // (the table is a host vector the next prepare rewrites)
+    // the table uploaded from pinned staging, without waiting for the stream: work queued before
+    // (another run still on the device) goes on; the staging is written again only once the copy
+    // from it is done
+    if (b->ev_table) e = cudaEventSynchronize(b->ev_table);
+    else e = cudaEventCreateWithFlags(&b->ev_table, cudaEventDisableTiming);
+    if (!e && b->h_table_cap < nj + 1) {                // (+1: the wavefront's run block)
+        if (b->h_table) cudaFreeHost(b->h_table);
+        b->h_table = nullptr;
+        b->h_table_cap = 0;
+        e = cudaMallocHost(reinterpret_cast<void **>(&b->h_table), (nj + nj / 4 + 16) * sizeof(lrc::BatchJob));
+        if (!e) b->h_table_cap = nj + nj / 4 + 16;
+    }
+    if (!e) {
+        std::copy(b->table.begin(), b->table.end(), b->h_table);
+        e = cudaMemcpyAsync(b->d_jobs, b->h_table, nj * sizeof(lrc::BatchJob), cudaMemcpyHostToDevice, c->st);
+    }
+    if (!e && b->engine == 1) {                         // the run block: tasks, jobs, pass bound, pixels
+        unsigned long long *run = reinterpret_cast<unsigned long long *>(b->h_table + nj);
+        run[0] = b->ntasks;
+        run[1] = nj;
+        run[2] = max_passes(b, b->ntasks);
+        run[3] = b->npix;
+        e = lrc::wf_set_run(lrc::wf_carve(b->d_wf, b->wf_slots), run, c->st);
+    }
+    if (!e) e = cudaEventRecord(b->ev_table, c->st);
     if (e) return cuda_status(c, e, "batch table");
     if (b->grid <= 0) {
         int block = 0, minb = 0;
@@ -290,8 +319,11 @@ int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool 
         }
     }
     const size_t nj = b->jobs.size();
-    cudaError_t e = with_resolve ? cudaMemsetAsync(b->d_ctr, 0, (nj + 1) * 8, st) : cudaSuccess;
-    if (!e && with_resolve && (flags & LRC_BATCH_ZERO)) {
+    // (a captured wavefront run depends on the buffers alone: the counters cleared whole, the bands
+    // zeroed before its launch, its counts in the run block)
+    const bool wf_graph = b->engine == 1 && capturing;
+    cudaError_t e = with_resolve ? cudaMemsetAsync(b->d_ctr, 0, wf_graph ? b->ctr_cap : (nj + 1) * 8, st) : cudaSuccess;
+    if (!e && with_resolve && (flags & LRC_BATCH_ZERO) && !wf_graph) {
         for (size_t i = 0; i < nj && !e; i++) {
             const lrc_batch::Job &J = b->jobs[i];
             e = cudaMemsetAsync(J.accum + (size_t)J.y0 * J.p.width * 4, 0, (size_t)J.rows * J.p.width * 16, st);
@@ -309,10 +341,11 @@ int enqueue(lrc_batch *b, unsigned flags, cudaStream_t st, bool capturing, bool 
     } else if (!e && b->engine == 1) {
         if (!capturing) return fail(c, LRC_E_INVALID, "the wavefront runs as a captured graph");
         const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
-        e = lrc::wf_capture_loop(b->d_jobs, (uint32_t)nj, limit, W, c->d_status, b->wf_variant, any_instances(b),
-                                 c->num_sms, max_passes(b, limit), st, b->body);
+        e = lrc::wf_capture_loop(b->d_jobs, W, c->d_status, b->wf_variant, any_instances(b), c->num_sms, st, b->body);
     }
-    if (!e && with_resolve) e = lrc::batch_resolve(b->d_jobs, (uint32_t)nj, b->npix, st);
+    if (!e && with_resolve)
+        e = wf_graph ? lrc::batch_resolve_run(b->d_jobs, lrc::wf_carve(b->d_wf, b->wf_slots).run, c->num_sms, st)
+                     : lrc::batch_resolve(b->d_jobs, (uint32_t)nj, b->npix, st);
     if (e) return cuda_status(c, e, "batch run");
     return LRC_OK;
 }
@@ -344,13 +377,33 @@ int capture_exec(lrc_batch *b, unsigned flags, bool with_builds, bool with_resol
 
 // the run's graph, kept for replays: builds inside when GRAPH (the megakernel engine captures only
 // GRAPH runs; the wavefront's trace is always a graph, its builds plain launches without GRAPH)
-int capture(lrc_batch *b, unsigned flags) {
+int capture(lrc_batch *b, unsigned flags, const std::vector<unsigned char> &key) {
     destroy_graph(b);
     int rc = capture_exec(b, flags, (flags & LRC_BATCH_GRAPH) != 0, true, b->ntasks, &b->graph, &b->exec);
     if (rc) return rc;
     b->graph_flags = flags;
-    b->graph_sig = signature(b, flags);
+    b->graph_sig = key;
     return LRC_OK;
+}
+
+// what a captured wavefront run without builds depends on: its buffers and shape (the jobs, tasks
+// and bounds travel in the table and the run block); with builds, every job (signature)
+std::vector<unsigned char> graph_key(const lrc_batch *b, unsigned flags) {
+    if (b->engine != 1 || ((flags & LRC_BATCH_BUILD) && (flags & LRC_BATCH_GRAPH))) return signature(b, flags);
+    std::vector<unsigned char> k;
+    auto put = [&](const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        k.insert(k.end(), c, c + n);
+    };
+    const unsigned f = flags & ~LRC_BATCH_ZERO;
+    const void *bufs[5] = {b->d_jobs, b->d_ctr, b->d_wf, b->body, b->ctx->d_status};
+    const unsigned long long sizes[2] = {b->ctr_cap, b->wf_slots};
+    const int shape[3] = {b->wf_variant, any_instances(b) ? 1 : 0, b->ctx->num_sms};
+    put(&f, sizeof f);
+    put(bufs, sizeof bufs);
+    put(sizes, sizeof sizes);
+    put(shape, sizeof shape);
+    return k;
 }
 
 // the wavefront's autotuner: the time of the first n tasks at each wavefront size (paths in
@@ -373,6 +426,10 @@ int tune_wavefront(lrc_batch *b, unsigned long long n, int32_t *variant, int32_t
     auto time_one = [&](uint32_t m, int v, float &ms) -> int {
         b->wf_slots = m;
         b->wf_variant = v;
+        // (the run block at this size's place: the first n tasks)
+        const unsigned long long run[4] = {n, b->jobs.size(), max_passes(b, n), b->npix};
+        cudaError_t er = lrc::wf_set_run(lrc::wf_carve(b->d_wf, m), run, c->st);
+        if (er) return cuda_status(c, er, "batch tune");
         cudaGraph_t g;
         cudaGraphExec_t x;
         int rc = capture_exec(b, 0, false, false, n, &g, &x);
@@ -430,6 +487,38 @@ void note_built(lrc_batch *b) {   // (what captured builds' host side records)
 }  // namespace
 
 namespace lrcapi {
+void batch_set_launch_event(lrc_batch *b, cudaEvent_t e) { b->ev_launch = e; }
+
+int batch_reserve(lrc_batch *b, unsigned long long tasks, size_t jobs) {
+    lrc_ctx *c = b->ctx;
+    DeviceGuard g(c->device);
+    cudaError_t e = reserve(&b->d_part, &b->part_cap, al(tasks * 16) + al(tasks * 4) + al(tasks * 16) + 256);
+    if (!e) e = reserve(reinterpret_cast<void **>(&b->d_ctr), &b->ctr_cap, (jobs + 1) * 8 + 256);
+    if (!e) e = reserve(reinterpret_cast<void **>(&b->d_jobs), &b->jobs_cap, jobs * sizeof(lrc::BatchJob) + 256);
+    if (!e && b->engine == 1) e = reserve(&b->d_wf, &b->wf_cap, lrc::wf_bytes(b->wf_slots));
+    if (!e && b->h_table_cap < jobs + 1) {
+        if (b->h_table) cudaFreeHost(b->h_table);
+        b->h_table = nullptr;
+        b->h_table_cap = 0;
+        e = cudaMallocHost(reinterpret_cast<void **>(&b->h_table), (jobs + 16) * sizeof(lrc::BatchJob));
+        if (!e) b->h_table_cap = jobs + 16;
+    }
+    return e ? cuda_status(c, e, "batch reserve") : LRC_OK;
+}
+
+cudaError_t batch_counts_async(lrc_batch *b, unsigned long long *h_rays, uint32_t *h_passes) {
+    lrc_ctx *c = b->ctx;
+    const size_t nj = b->jobs.size();
+    cudaError_t e = cudaSuccess;
+    if (nj && b->prepared) e = cudaMemcpyAsync(h_rays, b->d_ctr + 1, nj * 8, cudaMemcpyDeviceToHost, c->st);
+    *h_passes = 0;
+    if (!e && b->prepared && b->engine == 1 && b->d_wf) {
+        const lrc::WfState W = lrc::wf_carve(b->d_wf, b->wf_slots);
+        e = cudaMemcpyAsync(h_passes, W.ctl + 4, 4, cudaMemcpyDeviceToHost, c->st);
+    }
+    return e;
+}
+
 int batch_add_view(lrc_batch *b, lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows, uint32_t spp0,
                    uint32_t spp, float *d_accum, const InstView &view, bool guided) {
     int rc = lrc_batch_add(b, s, p, y0, rows, spp0, spp, d_accum, -1, 30);
@@ -466,6 +555,8 @@ void lrc_batch_destroy(lrc_batch *b) {
     cudaFree(b->d_ctr);
     cudaFree(b->scratch);
     cudaFree(b->d_wf);
+    if (b->h_table) cudaFreeHost(b->h_table);
+    if (b->ev_table) cudaEventDestroy(b->ev_table);
     if (b->body) cudaStreamDestroy(b->body);
     delete b;
 }
@@ -537,23 +628,41 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
     }
     const bool cached = b->exec && b->prepared && b->graph_flags == flags && signature(b, flags) == b->graph_sig;
     if (b->engine == 1) {
-        if (!cached || ((flags & LRC_BATCH_BUILD) && !(flags & LRC_BATCH_GRAPH))) {
-            // builds as plain launches: a first run sizes the buffers a captured build needs
-            if (flags & LRC_BATCH_BUILD)
-                for (const lrc_batch::Job *J : builds_of(b)) {
-                    int rc = build_job(b, J, c->st, false);
-                    if (rc) return rc;
-                }
+        // The wavefront: the table and the run block uploaded every run (behind the work queued
+        // before, not waiting for it); the graph captured again only when its buffers or shape
+        // changed (or, with builds inside, any job), so that consecutive runs of different jobs
+        // replay one graph and a run can be queued while the one before still runs.
+        const bool graph_builds = (flags & LRC_BATCH_BUILD) && (flags & LRC_BATCH_GRAPH);
+        if ((flags & LRC_BATCH_BUILD) && (!graph_builds || !cached)) {
+            // builds as plain launches (with GRAPH: a first run sizes the buffers a captured build needs)
+            for (const lrc_batch::Job *J : builds_of(b)) {
+                int rc = build_job(b, J, c->st, false);
+                if (rc) return rc;
+            }
         }
-        if (!cached) {
-            int rc = prepare(b);
-            if (!rc) rc = capture(b, flags);
+        int rc = prepare(b);
+        if (rc) return rc;
+        const std::vector<unsigned char> key = graph_key(b, flags);
+        const bool reuse = b->exec && b->graph_flags == flags && key == b->graph_sig;
+        if (!reuse) {
+            rc = capture(b, flags, key);
             if (rc) return rc;
         }
-        cudaError_t e = cudaGraphLaunch(b->exec, c->st);
+        cudaError_t e = cudaSuccess;
+        if (flags & LRC_BATCH_ZERO) {                       // (the bands zeroed outside the graph)
+            for (size_t i = 0; i < b->jobs.size() && !e; i++) {
+                const lrc_batch::Job &J = b->jobs[i];
+                e = cudaMemsetAsync(J.accum + (size_t)J.y0 * J.p.width * 4, 0, (size_t)J.rows * J.p.width * 16, c->st);
+                if (!e && J.guided)                         // the band's moments (plane 1) too
+                    e = cudaMemsetAsync(J.accum + ((size_t)J.p.width * J.p.height + (size_t)J.y0 * J.p.width) * 4, 0,
+                                        (size_t)J.rows * J.p.width * 16, c->st);
+            }
+        }
+        if (!e && b->ev_launch) e = cudaEventRecord(b->ev_launch, c->st);
+        if (!e) e = cudaGraphLaunch(b->exec, c->st);
         if (e) return cuda_status(c, e, "batch graph launch");
-        b->graph_used = cached ? 1 : 0;
-        if ((flags & LRC_BATCH_BUILD) && (flags & LRC_BATCH_GRAPH)) note_built(b);
+        b->graph_used = reuse ? 1 : 0;
+        if (graph_builds) note_built(b);
         return LRC_OK;
     }
     if ((flags & LRC_BATCH_GRAPH) && cached) {
@@ -578,7 +687,7 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
         // the next run replays this one: captured now, with every buffer sized
         cudaError_t e = cudaStreamSynchronize(c->st);
         if (e) return cuda_status(c, e, "batch run");
-        rc = capture(b, flags);
+        rc = capture(b, flags, signature(b, flags));
         if (rc) return rc;
     }
     return LRC_OK;

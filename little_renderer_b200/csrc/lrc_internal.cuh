@@ -299,6 +299,8 @@ struct BatchJob {
 cudaError_t batch_trace(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, unsigned long long *d_next,
                         uint32_t *d_status, int variant, int grid, bool media, cudaStream_t st);
 cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long long npix, cudaStream_t st);
+// the same with the job and pixel counts read from a run block in device memory (run[1], run[3])
+cudaError_t batch_resolve_run(const BatchJob *d_jobs, const unsigned long long *d_run, int num_sms, cudaStream_t st);
 // the launch shapes: how many; a shape's threads per block, the blocks per SM its registers are
 // capped for, and the blocks of it that fit on one SM (-1: no such shape)
 int batch_variants();
@@ -329,6 +331,8 @@ struct WfState {
     float4 *sq_o, *sq_d;        // the shadow queue (2M): origin + (slot << 1 | kind) bits, direction + tmax
     uint32_t *ctl;              // [0] rays queued, [1] shadow rays queued, [2] [3] their fetch counters, [4] passes
     unsigned long long *next;   // the task queue's next task; next[1]: how many tasks this run takes
+    unsigned long long *run;    // the run: [0] its tasks, [1] jobs, [2] largest pass count, [3] pixels
+                                // (written before each run, so that one captured graph serves every run)
 };
 // the device bytes of a wavefront of M slots, and its arrays carved from them (256-byte aligned base)
 size_t wf_bytes(uint32_t M);
@@ -338,14 +342,16 @@ WfState wf_carve(void *base, uint32_t M);
 int wf_variants();
 int wf_variant_shape(int variant, int *block, int *minb);
 // Captures the wavefront's loop into the graph stream st is capturing: the slots cleared and the
-// task queue set to the first ntasks tasks, then a while node whose body (captured on body_st)
-// runs the advance, closest-hit, shade and shadow kernels until no slot holds a path. instances:
-// some job's scene has instances (else the traversal kernels without the two-level walk run).
-// The loop stops after max_passes passes whatever is left (ST_LOOP in the status word): a bound well
-// above what the tasks need (a pass per bounce of each slot's tasks).
-cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
-                            uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
-                            cudaStream_t st, cudaStream_t body_st);
+// task queue set to the run block's tasks (W.run[0]), then a while node whose body (captured on
+// body_st) runs the advance, closest-hit, shade and shadow kernels until no slot holds a path.
+// instances: some job's scene has instances (else the traversal kernels without the two-level
+// walk run). The loop stops after W.run[2] passes whatever is left (ST_LOOP in the status word): a
+// bound well above what the tasks need (a pass per bounce of each slot's tasks). Nothing of the
+// run (its jobs, tasks, bounds) is in the graph: one capture serves every run of the same buffers.
+// The run block's four words (tasks, jobs, largest pass count, pixels) from host memory, on st.
+cudaError_t wf_set_run(const WfState &W, const unsigned long long *h_run4, cudaStream_t st);
+cudaError_t wf_capture_loop(const BatchJob *d_jobs, const WfState &W, uint32_t *d_status, int variant, bool instances,
+                            int num_sms, cudaStream_t st, cudaStream_t body_st);
 // The same loop with each pass's kernels launched from the host (no graph; the host reads the
 // queued count after every pass): for profilers that cannot see into a graph's loop.
 // a stepped run's measurements (stats given): the closest-hit kernel's time (CUDA events around each

@@ -244,11 +244,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(const BatchJob *__re
     }
 }
 
-// one thread per pixel of all the batch's bands: the pixel's slots summed in the fast kernel's
-// shuffle order (pairs, then pairs of pairs, ...) and added to its image, its rays to its job
-__global__ void __launch_bounds__(128) batch_resolve_kernel(const BatchJob *__restrict__ jobs, uint32_t njobs,
-                                                            unsigned long long npix) {
-    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+// pixel i of all the batch's bands (a whole warp calls it together): the pixel's slots summed in
+// the fast kernel's shuffle order (pairs, then pairs of pairs, ...) and added to its image, its rays
+// to its job
+__device__ __forceinline__ void resolve_pixel(const BatchJob *__restrict__ jobs, uint32_t njobs, unsigned long long npix,
+                                              unsigned long long i) {
     uint32_t jj = 0xffffffffu;
     unsigned long long r = 0;
     if (i < npix) {
@@ -305,6 +305,24 @@ __global__ void __launch_bounds__(128) batch_resolve_kernel(const BatchJob *__re
     const uint32_t sum = __reduce_add_sync(peers, (uint32_t)r);
     if (jj != 0xffffffffu && (threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1) && sum)
         atomicAdd(jobs[jj].rays, (unsigned long long)sum);
+}
+
+// one thread per pixel
+__global__ void __launch_bounds__(128) batch_resolve_kernel(const BatchJob *__restrict__ jobs, uint32_t njobs,
+                                                            unsigned long long npix) {
+    resolve_pixel(jobs, njobs, npix, (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// the same over a fixed grid, the job and pixel counts read from the run block (run[1], run[3]):
+// a graph captured once resolves any run
+__global__ void __launch_bounds__(128) batch_resolve_run_kernel(const BatchJob *__restrict__ jobs,
+                                                                const unsigned long long *__restrict__ run) {
+    const uint32_t njobs = (uint32_t)run[1];
+    const unsigned long long npix = run[3];
+    if (!njobs) return;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < npix;
+         base += (unsigned long long)gridDim.x * blockDim.x)
+        resolve_pixel(jobs, njobs, npix, base + threadIdx.x);
 }
 
 // closest hits over shape ids (primitives, then triangles): lrc_scene_intersect for world scenes
@@ -466,6 +484,11 @@ cudaError_t batch_trace(const BatchJob *d_jobs, uint32_t njobs, unsigned long lo
 cudaError_t batch_resolve(const BatchJob *d_jobs, uint32_t njobs, unsigned long long npix, cudaStream_t st) {
     if (!njobs || !npix) return cudaSuccess;
     pt::batch_resolve_kernel<<<(unsigned)((npix + 127) / 128), 128, 0, st>>>(d_jobs, njobs, npix);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_resolve_run(const BatchJob *d_jobs, const unsigned long long *d_run, int num_sms, cudaStream_t st) {
+    pt::batch_resolve_run_kernel<<<16 * num_sms, 128, 0, st>>>(d_jobs, d_run);
     return cudaGetLastError();
 }
 

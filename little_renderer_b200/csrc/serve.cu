@@ -13,6 +13,12 @@
 // admitted jobs, policy 1 serves the oldest first. A band traces all of its pixels' samples, so a
 // job's image is the one lrc_trace makes of it alone, to the bit, whatever else shares its waves.
 //
+// Waves are pipelined on two batches: a step plans the next wave (rows are handed out as waves are
+// planned, so its bands are known before the wave ahead of it ends), captures and launches it, and
+// only then waits for the wave ahead and reads its ray counts (copied to pinned memory behind it on
+// the stream): the device goes from one wave to the next while the host builds the one after. A
+// job admitted in a step is planned into that step's wave.
+//
 // Admission holds a job's bytes - its image, and for moved instances its own records and top level -
 // against the budget, in arrival order; a job larger than the whole budget is refused at submit.
 // A moved-instance job gets its own copy of the scene's instance layer (records and top level, the
@@ -46,13 +52,31 @@ struct lrc_server {
         Node *d_tlas = nullptr;         // and their top level
         uint32_t *d_tlas_aux = nullptr;
         size_t bytes = 0;
-        int32_t next_row = 0, band = 0;
+        int32_t next_row = 0;           // rows handed to waves so far
         uint64_t rays = 0;
         double t_submit = 0, t_admit = 0, t_done = 0;
         int state = 0;                  // 0 queued, 1 admitted, 2 finished
+        cudaEvent_t ev_done = nullptr;  // on the side stream: its image complete (finished jobs)
+    };
+    // a wave on one of the two batches: its jobs (in the batch's job order), whether its band ends
+    // each, the ray counts and passes copied back behind it, its events (launch, end)
+    struct Wave {
+        lrc_batch *batch = nullptr;
+        std::vector<Job *> jobs;
+        std::vector<char> last;
+        unsigned long long *h_rays = nullptr;   // pinned
+        size_t rays_cap = 0;
+        uint32_t *h_passes = nullptr;           // pinned
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        bool pending = false;
     };
     lrc_ctx *ctx = nullptr;
-    lrc_batch *batch = nullptr;
+    lrc_batch *batch = nullptr;         // (wave[0]'s: lrc_server_batch)
+    Wave wave[2];
+    int next = 0;                       // the slot the next wave is planned into
+    unsigned long long reserved_tasks = 0;   // both batches' run buffers hold waves this large
+    size_t reserved_jobs = 0;
+    cudaStream_t side = nullptr;        // finished jobs' denoising and reads, behind their last wave only
     uint64_t budget = 0, wave_paths = 0, in_use = 0;
     uint64_t next_id = 1;
     std::deque<Job *> queued;
@@ -68,8 +92,7 @@ struct lrc_server {
     void *dn = nullptr;                 // the denoiser's scratch
     size_t dn_cap = 0;
     uint64_t waves = 0, kernels = 0;    // waves run and the trace kernels they launched
-    double gpu_ms = 0;                  // the waves' device time (CUDA events around each)
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double gpu_ms = 0;                  // the waves' device time (CUDA events from each launch to its end)
     int policy = 2;                     // how a wave is made (lrc_server_set_policy)
 };
 
@@ -89,6 +112,11 @@ size_t job_bytes(const lrc_server::Job &J) {
 
 void free_job(lrc_server *sv, lrc_server::Job *J) {
     lrc_ctx *c = sv->ctx;
+    if (J->ev_done) {                                   // (its denoising on the side stream done first)
+        cudaStreamWaitEvent(c->st, J->ev_done, 0);
+        cudaEventDestroy(J->ev_done);
+        J->ev_done = nullptr;
+    }
     if (J->d_img) cudaFreeAsync(J->d_img, c->st);
     if (J->d_planes) cudaFreeAsync(J->d_planes, c->st);
     if (J->d_inst) cudaFreeAsync(J->d_inst, c->st);
@@ -163,6 +191,69 @@ int admit(lrc_server *sv, lrc_server::Job *J) {
     return LRC_OK;
 }
 
+// a launched wave waited for: its device time and passes, each job's rays; the jobs whose last
+// band it held finished (a denoised one's planes filtered into its image, on the side stream after
+// the wave, not after the wave launched behind it), their instance layers freed
+int finish_wave(lrc_server *sv, lrc_server::Wave &W, int32_t *finished) {
+    lrc_ctx *c = sv->ctx;
+    cudaError_t e = cudaEventSynchronize(W.ev1);
+    if (e) return cuda_status(c, e, "server wave");
+    W.pending = false;
+    if (W.h_passes[1]) {                                // (an error the wave's kernels reported)
+        int rc = check_status(c);
+        if (rc) return rc;
+    }
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, W.ev0, W.ev1) == cudaSuccess) sv->gpu_ms += ms;
+    sv->waves++;
+    sv->kernels += 2 + 4 * (uint64_t)W.h_passes[0];   // clear, then advance / closest hit / shade / shadow a pass, resolve
+    const double t = now_ms();
+    bool any = false;
+    for (size_t q = 0; q < W.jobs.size(); q++) {
+        lrc_server::Job *J = W.jobs[q];
+        J->rays += W.h_rays[q];
+        if (!W.last[q]) continue;
+        any = true;
+        if (!J->ev_done && (e = cudaEventCreateWithFlags(&J->ev_done, cudaEventDisableTiming)))
+            return cuda_status(c, e, "server job event");
+        e = cudaStreamWaitEvent(sv->side, W.ev1, 0);
+        if (!e && J->denoise) {                         // the image denoised, the planes freed
+            e = reserve(&sv->dn, &sv->dn_cap, lrc::dn_scratch_bytes(J->p.width, J->p.height));
+            if (!e) e = lrc::dn_denoise(reinterpret_cast<const float4 *>(J->d_planes), J->p.width, J->p.height, 5,
+                                        reinterpret_cast<float4 *>(J->d_img), sv->dn, sv->side);
+            if (!e) e = cudaFreeAsync(J->d_planes, sv->side);
+            if (!e) {
+                J->d_planes = nullptr;
+                sv->in_use -= (size_t)J->p.width * J->p.height * 64;
+                J->bytes -= (size_t)J->p.width * J->p.height * 64;
+            }
+        }
+        if (!e) e = cudaEventRecord(J->ev_done, sv->side);
+        if (e) return cuda_status(c, e, "server finish");
+        J->state = 2;
+        J->t_done = t;
+        sv->finished++;
+        if (finished) (*finished)++;
+        if (J->d_inst) {                                // (its instances are done with; its image stays)
+            cudaFreeAsync(J->d_inst, c->st);
+            cudaFreeAsync(J->d_tlas, c->st);
+            cudaFreeAsync(J->d_tlas_aux, c->st);
+            J->d_inst = nullptr;
+            J->d_tlas = nullptr;
+            J->d_tlas_aux = nullptr;
+            sv->in_use -= J->bytes - (size_t)J->p.width * J->p.height * 16;
+            J->bytes = (size_t)J->p.width * J->p.height * 16;
+        }
+    }
+    if (any) {
+        std::vector<lrc_server::Job *> still;
+        for (lrc_server::Job *J : sv->active)
+            if (J->state != 2) still.push_back(J);
+        sv->active.swap(still);
+    }
+    return LRC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -178,12 +269,21 @@ int lrc_server_create(lrc_ctx *c, uint64_t hbm_budget_bytes, uint64_t wave_paths
     sv->budget = hbm_budget_bytes;
     sv->wave_paths = wave_paths;
     DeviceGuard g(c->device);
-    int rc = lrc_batch_create(c, &sv->batch);
-    if (!rc) rc = lrc_batch_set_wavefront(sv->batch, 1u << 22, 0);   // (4M paths in flight: a wave's tail stays short)
-    cudaError_t e = rc ? cudaSuccess : cudaMalloc(&sv->d_small, 256);
+    int rc = LRC_OK;
+    cudaError_t e = cudaSuccess;
+    for (lrc_server::Wave &W : sv->wave) {
+        if (!rc) rc = lrc_batch_create(c, &W.batch);
+        if (!rc) rc = lrc_batch_set_wavefront(W.batch, 1u << 22, 0);   // (4M paths in flight: a wave's tail stays short)
+        if (!rc && !e) e = cudaEventCreate(&W.ev0);
+        if (!rc && !e) e = cudaEventCreate(&W.ev1);
+        if (!rc && !e) e = cudaMallocHost(reinterpret_cast<void **>(&W.h_passes), 16);
+        if (!rc && !e) batch_set_launch_event(W.batch, W.ev0);
+    }
+    sv->batch = sv->wave[0].batch;
+    if (!rc && !e) e = cudaStreamCreateWithFlags(&sv->side, cudaStreamNonBlocking);
+    if (!rc && !e) e = cudaMalloc(&sv->d_small, 256);
     if (rc || e) {
-        if (sv->batch) lrc_batch_destroy(sv->batch);
-        delete sv;
+        lrc_server_destroy(sv);
         return rc ? rc : cuda_status(c, e, "server");
     }
     *out = sv;
@@ -193,18 +293,27 @@ int lrc_server_create(lrc_ctx *c, uint64_t hbm_budget_bytes, uint64_t wave_paths
 void lrc_server_destroy(lrc_server *sv) {
     if (!sv) return;
     DeviceGuard g(sv->ctx->device);
-    lrc_batch_destroy(sv->batch);
+    cudaStreamSynchronize(sv->ctx->st);
+    for (lrc_server::Wave &W : sv->wave) {
+        if (W.batch) lrc_batch_destroy(W.batch);
+        if (W.ev0) cudaEventDestroy(W.ev0);
+        if (W.ev1) cudaEventDestroy(W.ev1);
+        if (W.h_rays) cudaFreeHost(W.h_rays);
+        if (W.h_passes) cudaFreeHost(W.h_passes);
+    }
     for (auto &kv : sv->jobs) {
         free_job(sv, kv.second);
         delete kv.second;
     }
     cudaStreamSynchronize(sv->ctx->st);
+    if (sv->side) {
+        cudaStreamSynchronize(sv->side);
+        cudaStreamDestroy(sv->side);
+    }
     cudaFree(sv->scratch);
     cudaFree(sv->d_boxes);
     cudaFree(sv->d_small);
     cudaFree(sv->dn);
-    if (sv->ev0) cudaEventDestroy(sv->ev0);
-    if (sv->ev1) cudaEventDestroy(sv->ev1);
     delete sv;
 }
 
@@ -256,95 +365,81 @@ int lrc_server_step(lrc_server *sv, int32_t *finished) {
         sv->queued.pop_front();
         sv->active.push_back(J);
     }
-    if (sv->active.empty()) return LRC_OK;
-    // the wave: bands of the admitted jobs. Policy 0: the next band of every job, the wave's paths
-    // shared evenly; 1: the oldest jobs first, each band as large as the wave's paths left allow
-    // (few scenes a wave, each wave's jobs ending sooner); 2: as 1, the jobs with the fewest paths
-    // left first.
-    std::vector<lrc_server::Job *> order(sv->active);
+    // the next wave, into the free slot: bands of the admitted jobs with rows left. Policy 0: the
+    // next band of every job, the wave's paths shared evenly; 1: the oldest jobs first, each band
+    // as large as the wave's paths left allow (few scenes a wave, each wave's jobs ending sooner);
+    // 2: as 1, the jobs with the fewest paths left first. Rows are handed out here, so the wave
+    // after can be planned before this one ends.
+    lrc_server::Wave &N = sv->wave[sv->next];
+    int rc = N.pending ? finish_wave(sv, N, finished) : LRC_OK;   // (never: a slot is freed before it is planned again)
+    if (rc) return rc;
+    std::vector<lrc_server::Job *> order;
+    for (lrc_server::Job *J : sv->active)
+        if (J->next_row < J->p.height) order.push_back(J);
     if (sv->policy == 2)
         std::stable_sort(order.begin(), order.end(), [](const lrc_server::Job *a, const lrc_server::Job *b) {
             return (uint64_t)a->p.width * (a->p.height - a->next_row) * a->spp <
                    (uint64_t)b->p.width * (b->p.height - b->next_row) * b->spp;
         });
-    for (lrc_server::Job *J : sv->active) J->band = 0;
-    const uint64_t share = sv->wave_paths / sv->active.size() + 1;
-    uint64_t used = 0;
-    int rc = lrc_batch_clear(sv->batch);
-    std::vector<lrc_server::Job *> in_wave;
-    for (lrc_server::Job *J : order) {
-        const uint64_t row_paths = (uint64_t)J->p.width * J->spp;
-        int32_t rows;
-        if (sv->policy == 0) {
-            rows = (int32_t)std::max<uint64_t>(1, share / row_paths);
-        } else {
-            if (used >= sv->wave_paths) break;
-            rows = (int32_t)std::max<uint64_t>(1, (sv->wave_paths - used + row_paths - 1) / row_paths);
-        }
-        rows = std::min(rows, J->p.height - J->next_row);
-        J->band = rows;
-        used += (uint64_t)rows * row_paths;
-        in_wave.push_back(J);
-        InstView v{J->d_inst, J->d_tlas, J->d_tlas_aux};
-        if (!rc) rc = batch_add_view(sv->batch, J->s, &J->p, J->next_row, rows, 0, J->spp,
-                                     J->denoise ? J->d_planes : J->d_img, v, J->denoise);
-    }
-    if (!sv->ev0 && !rc) {
-        if (cudaEventCreate(&sv->ev0) || cudaEventCreate(&sv->ev1)) return cuda_status(c, cudaGetLastError(), "server events");
-    }
-    if (!rc) cudaEventRecord(sv->ev0, c->st);
-    if (!rc) rc = lrc_batch_run(sv->batch, 0);
-    if (!rc) cudaEventRecord(sv->ev1, c->st);
-    std::vector<uint64_t> wave_rays(in_wave.size());
-    if (!rc) rc = lrc_batch_rays(sv->batch, wave_rays.data(), nullptr);   // (waits for the wave)
-    uint64_t kernels = 0;
-    if (!rc) rc = lrc_batch_passes(sv->batch, nullptr, &kernels);
-    if (rc) return rc;
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, sv->ev0, sv->ev1) == cudaSuccess) sv->gpu_ms += ms;
-    sv->waves++;
-    sv->kernels += kernels;
-    std::vector<uint64_t> rays(sv->active.size(), 0);   // (in the wave's order: back to the active list's)
-    for (size_t i = 0; i < sv->active.size(); i++)
-        for (size_t q = 0; q < in_wave.size(); q++)
-            if (in_wave[q] == sv->active[i]) rays[i] = wave_rays[q];
-    const double t = now_ms();
-    std::vector<lrc_server::Job *> still;
-    for (size_t i = 0; i < sv->active.size(); i++) {
-        lrc_server::Job *J = sv->active[i];
-        J->rays += rays[i];
-        J->next_row += J->band;
-        if (J->band && J->next_row >= J->p.height) {
-            if (J->denoise) {                           // the image denoised, the planes freed
-                cudaError_t e = reserve(&sv->dn, &sv->dn_cap, lrc::dn_scratch_bytes(J->p.width, J->p.height));
-                if (!e) e = lrc::dn_denoise(reinterpret_cast<const float4 *>(J->d_planes), J->p.width, J->p.height, 5,
-                                            reinterpret_cast<float4 *>(J->d_img), sv->dn, c->st);
-                if (!e) e = cudaFreeAsync(J->d_planes, c->st);
-                if (e) return cuda_status(c, e, "server denoiser");
-                J->d_planes = nullptr;
-                sv->in_use -= (size_t)J->p.width * J->p.height * 64;
-                J->bytes -= (size_t)J->p.width * J->p.height * 64;
+    bool launched = false;
+    if (!order.empty()) {
+        const uint64_t share = sv->wave_paths / order.size() + 1;
+        uint64_t used = 0;
+        rc = lrc_batch_clear(N.batch);
+        N.jobs.clear();
+        N.last.clear();
+        for (lrc_server::Job *J : order) {
+            const uint64_t row_paths = (uint64_t)J->p.width * J->spp;
+            int32_t rows;
+            if (sv->policy == 0) {
+                rows = (int32_t)std::max<uint64_t>(1, share / row_paths);
+            } else {
+                if (used >= sv->wave_paths) break;
+                rows = (int32_t)std::max<uint64_t>(1, (sv->wave_paths - used + row_paths - 1) / row_paths);
             }
-            J->state = 2;
-            J->t_done = t;
-            sv->finished++;
-            if (finished) (*finished)++;
-            if (J->d_inst) {                            // (its instances are done with; its image stays)
-                cudaFreeAsync(J->d_inst, c->st);
-                cudaFreeAsync(J->d_tlas, c->st);
-                cudaFreeAsync(J->d_tlas_aux, c->st);
-                J->d_inst = nullptr;
-                J->d_tlas = nullptr;
-                J->d_tlas_aux = nullptr;
-                sv->in_use -= J->bytes - (size_t)J->p.width * J->p.height * 16;
-                J->bytes = (size_t)J->p.width * J->p.height * 16;
-            }
-        } else {
-            still.push_back(J);
+            rows = std::min(rows, J->p.height - J->next_row);
+            used += (uint64_t)rows * row_paths;
+            InstView v{J->d_inst, J->d_tlas, J->d_tlas_aux};
+            if (!rc) rc = batch_add_view(N.batch, J->s, &J->p, J->next_row, rows, 0, J->spp,
+                                         J->denoise ? J->d_planes : J->d_img, v, J->denoise);
+            if (rc) break;
+            J->next_row += rows;
+            N.jobs.push_back(J);
+            N.last.push_back(J->next_row >= J->p.height);
         }
+        // both batches' buffers sized for a wave (its paths bound its tasks) before any wave runs,
+        // and again should a wave outgrow them: a run that must allocate waits for the device
+        cudaError_t e = cudaSuccess;
+        const unsigned long long want = std::max<unsigned long long>(used, sv->wave_paths + (2ull << 20));
+        const size_t want_jobs = std::max<size_t>(N.jobs.size(), 256);
+        if (!rc && (want > sv->reserved_tasks || want_jobs > sv->reserved_jobs)) {
+            for (lrc_server::Wave &W : sv->wave)
+                if (!rc) rc = batch_reserve(W.batch, want, want_jobs);
+            sv->reserved_tasks = want;
+            sv->reserved_jobs = want_jobs;
+        }
+        if (!rc && N.rays_cap < N.jobs.size()) {
+            if (N.h_rays) cudaFreeHost(N.h_rays);
+            N.h_rays = nullptr;
+            N.rays_cap = 0;
+            e = cudaMallocHost(reinterpret_cast<void **>(&N.h_rays), (N.jobs.size() + 64) * 8);
+            if (!e) N.rays_cap = N.jobs.size() + 64;
+        }
+        if (!rc && !e) rc = lrc_batch_run(N.batch, 0);
+        // behind it on the stream: its counts, the status word, its end
+        if (!rc && !e) e = batch_counts_async(N.batch, N.h_rays, N.h_passes);
+        if (!rc && !e) e = cudaMemcpyAsync(N.h_passes + 1, c->d_status, 4, cudaMemcpyDeviceToHost, c->st);
+        if (!rc && !e) e = cudaEventRecord(N.ev1, c->st);
+        if (e) return cuda_status(c, e, "server wave");
+        if (rc) return rc;
+        N.pending = true;
+        launched = true;
     }
-    sv->active.swap(still);
-    return LRC_OK;
+    // the wave ahead: waited for, its counts read, the jobs it ends finished
+    lrc_server::Wave &P = sv->wave[1 - sv->next];
+    if (P.pending) rc = finish_wave(sv, P, finished);
+    if (launched) sv->next = 1 - sv->next;
+    return rc;
 }
 
 int lrc_server_result(lrc_server *sv, uint64_t id, const float **d_image, uint64_t *rays, double *t_submit,
@@ -369,10 +464,12 @@ int lrc_server_read(lrc_server *sv, uint64_t id, float *out) {
     const lrc_server::Job *J = it->second;
     if (J->state != 2) return LRC_RETRY;
     DeviceGuard g(sv->ctx->device);
-    cudaError_t e = cudaMemcpyAsync(out, J->d_img, (size_t)J->p.width * J->p.height * 16, cudaMemcpyDeviceToHost,
-                                    sv->ctx->st);
+    // on the side stream, behind the job's own completion only (not the wave launched since)
+    cudaError_t e = J->ev_done ? cudaStreamWaitEvent(sv->side, J->ev_done, 0) : cudaSuccess;
+    if (!e) e = cudaMemcpyAsync(out, J->d_img, (size_t)J->p.width * J->p.height * 16, cudaMemcpyDeviceToHost, sv->side);
+    if (!e) e = cudaStreamSynchronize(sv->side);
     if (e) return cuda_status(sv->ctx, e, "server read");
-    return check_status(sv->ctx);
+    return LRC_OK;
 }
 
 int lrc_server_release(lrc_server *sv, uint64_t id) {
@@ -391,6 +488,16 @@ int lrc_server_release(lrc_server *sv, uint64_t id) {
 }
 
 lrc_batch *lrc_server_batch(lrc_server *sv) { return sv ? sv->batch : nullptr; }
+
+int lrc_server_set_wavefront(lrc_server *sv, uint32_t slots, int32_t variant) {
+    if (!sv) return LRC_E_INVALID;
+    for (lrc_server::Wave &W : sv->wave) {
+        int rc = lrc_batch_set_wavefront(W.batch, slots, variant);
+        if (rc) return rc;
+    }
+    sv->reserved_tasks = 0;                            // (the next wave sizes the buffers again)
+    return LRC_OK;
+}
 
 int lrc_server_stats(const lrc_server *sv, uint64_t *waves, uint64_t *kernels, double *gpu_ms) {
     if (!sv) return LRC_E_INVALID;

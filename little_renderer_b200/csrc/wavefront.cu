@@ -41,12 +41,12 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *ctr, bool want) {
 }
 
 // the slots emptied, the queues cleared, the task queue set to [0, limit)
-__global__ void wf_clear_kernel(WfState W, unsigned long long limit) {
+__global__ void wf_clear_kernel(WfState W) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < 8) W.ctl[i] = 0;
     if (i == 0) {
         W.next[0] = 0;
-        W.next[1] = limit;
+        W.next[1] = W.run[0];
         W.next[2] = 0;                               // (the counting closest-hit kernel's box tests
         W.next[3] = 0;                               //  and triangle tests)
     }
@@ -55,7 +55,8 @@ __global__ void wf_clear_kernel(WfState W, unsigned long long limit) {
     W.flags[i] = 0;
 }
 
-__global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *__restrict__ jobs, uint32_t njobs, WfState W) {
+__global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *__restrict__ jobs, WfState W) {
+    const uint32_t njobs = (uint32_t)W.run[1];
     const uint32_t i = blockIdx.x * ADV_BLOCK + threadIdx.x;   // (M is a multiple of the block: every lane has a slot)
     const uint32_t lane = threadIdx.x & 31;
     if (i == 0) {
@@ -204,8 +205,8 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
 // that measure the engine's algorithmic bytes launch it)
 template <int BLOCK, int MINB, bool INST, bool COUNT = false>
 __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJob *__restrict__ jobs, WfState W, uint32_t *err,
-                                                                   cudaGraphConditionalHandle cond, uint32_t max_passes,
-                                                                   int use_cond) {
+                                                                   cudaGraphConditionalHandle cond, int use_cond) {
+    const uint32_t max_passes = (uint32_t)W.run[2];
     // (the pass counter is advanced by the shadow kernel, so every block of this one and of the
     // shade kernel reads the same value)
     uint32_t count = *reinterpret_cast<volatile uint32_t *>(&W.ctl[0]);
@@ -251,7 +252,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) wf_intersect_kernel(const BatchJo
 // the rest of every queued path's bounce; its shadow rays into the shadow queue
 template <int SMINB>
 __global__ void __launch_bounds__(SHADE_BLOCK, SMINB) wf_shade_kernel(const BatchJob *__restrict__ jobs, WfState W,
-                                                                       uint32_t *err, uint32_t max_passes) {
+                                                                       uint32_t *err) {
+    const uint32_t max_passes = (uint32_t)W.run[2];
     const uint32_t count = W.ctl[4] >= max_passes ? 0u : *reinterpret_cast<volatile uint32_t *>(&W.ctl[0]);
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (SHADE_BLOCK / 32);
@@ -372,7 +374,7 @@ int wf_variant_shape(int v, int *block, int *minb) {
 size_t wf_bytes(uint32_t M) {
     const size_t m = M;
     return a256(m * 8) + 5 * a256(m * 4) + a256(m * 8) + 10 * a256(m * 16) + a256(m * 16) + a256(m * 2) + a256(m * 4) +
-           2 * a256(m * 2 * 16) + 256 + 256;
+           2 * a256(m * 2 * 16) + 256 + 256 + 256;
 }
 
 WfState wf_carve(void *base, uint32_t M) {
@@ -409,12 +411,16 @@ WfState wf_carve(void *base, uint32_t M) {
     W.sq_d = reinterpret_cast<float4 *>(take(m * 2 * 16));
     W.ctl = reinterpret_cast<uint32_t *>(take(64));
     W.next = reinterpret_cast<unsigned long long *>(take(64));
+    W.run = reinterpret_cast<unsigned long long *>(take(64));
     return W;
 }
 
-cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned long long ntasks, const WfState &W,
-                            uint32_t *d_status, int variant, bool instances, int num_sms, uint32_t max_passes,
-                            cudaStream_t st, cudaStream_t body_st) {
+cudaError_t wf_set_run(const WfState &W, const unsigned long long *h_run4, cudaStream_t st) {
+    return cudaMemcpyAsync(W.run, h_run4, 32, cudaMemcpyHostToDevice, st);
+}
+
+cudaError_t wf_capture_loop(const BatchJob *d_jobs, const WfState &W, uint32_t *d_status, int variant, bool instances,
+                            int num_sms, cudaStream_t st, cudaStream_t body_st) {
     if (variant < 0 || variant >= wf_variants() || W.M == 0 || W.M % pt::ADV_BLOCK) return cudaErrorInvalidValue;
     cudaStreamCaptureStatus cs;
     cudaGraph_t g = nullptr;
@@ -423,7 +429,7 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd);
     if (e) return e;
     if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureUnmatched;
-    pt::wf_clear_kernel<<<(W.M + 255) / 256, 256, 0, st>>>(W, ntasks);
+    pt::wf_clear_kernel<<<(W.M + 255) / 256, 256, 0, st>>>(W);
     e = cudaGetLastError();
     if (e) return e;
     e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd);
@@ -451,12 +457,12 @@ cudaError_t wf_capture_loop(const BatchJob *d_jobs, uint32_t njobs, unsigned lon
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_per_sm, V.shade, pt::SHADE_BLOCK, 0);
     const int shade_grid = std::max(shade_per_sm, 1) * num_sms;
     WfState w = W;
-    pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, body_st>>>(d_jobs, njobs, w);
+    pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, body_st>>>(d_jobs, w);
     int use_cond = 1;
-    void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
+    void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&use_cond};
     e = cudaLaunchKernel(isect, dim3(grid), dim3(V.block), iargs, 0, body_st);
     if (!e) {
-        void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&max_passes};
+        void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};
         e = cudaLaunchKernel(V.shade, dim3(shade_grid), dim3(pt::SHADE_BLOCK), hargs, 0, body_st);
     }
     if (!e) {
@@ -492,16 +498,20 @@ cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long
     WfState w = W;
     cudaGraphConditionalHandle cond = 0;
     int use_cond = 0;
-    pt::wf_clear_kernel<<<(W.M + 255) / 256, 256, 0, st>>>(w, ntasks);
-    cudaError_t e = cudaGetLastError();
+    const unsigned long long run[4] = {ntasks, njobs, max_passes, 0};
+    cudaError_t e = cudaMemcpyAsync(W.run, run, 32, cudaMemcpyHostToDevice, st);   // (pageable: staged before it returns)
+    if (!e) {
+        pt::wf_clear_kernel<<<(W.M + 255) / 256, 256, 0, st>>>(w);
+        e = cudaGetLastError();
+    }
     for (uint32_t pass = 0; !e && pass <= max_passes; pass++) {
-        pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, st>>>(d_jobs, njobs, w);
-        void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&max_passes, (void *)&use_cond};
+        pt::wf_advance_kernel<<<W.M / pt::ADV_BLOCK, pt::ADV_BLOCK, 0, st>>>(d_jobs, w);
+        void *iargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&cond, (void *)&use_cond};
         if (stats) cudaEventRecord(e0, st);
         e = cudaLaunchKernel(isect, dim3(grid), dim3(V.block), iargs, 0, st);
         if (stats) cudaEventRecord(e1, st);
         if (e) break;
-        void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status, (void *)&max_passes};
+        void *hargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};
         e = cudaLaunchKernel(V.shade, dim3(shade_grid), dim3(pt::SHADE_BLOCK), hargs, 0, st);
         if (e) break;
         void *sargs[] = {(void *)&d_jobs, (void *)&w, (void *)&d_status};

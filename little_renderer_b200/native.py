@@ -174,6 +174,7 @@ def lib():
     L.lrc_server_clock.restype = C.c_double
     L.lrc_server_batch.argtypes = [vp]
     L.lrc_server_batch.restype = vp
+    L.lrc_server_set_wavefront.argtypes = [vp, u32, C.c_int32]
     L.lrc_batch_set_engine.argtypes = [vp, C.c_int32]
     L.lrc_batch_set_wavefront.argtypes = [vp, u32, C.c_int32]
     L.lrc_batch_wavefront_shape.argtypes = [C.c_int32, vp, vp, vp]
@@ -877,7 +878,7 @@ class Server:
 
     def set_wavefront(self, slots, variant=0):
         """The waves' wavefront size (paths in flight) and closest-hit / shadow launch shape."""
-        self.ctx.check(self.ctx.L.lrc_batch_set_wavefront(C.c_void_p(self.batch_handle()), slots, variant))
+        self.ctx.check(self.ctx.L.lrc_server_set_wavefront(self.h, slots, variant))
 
 
 def clock_ms():
