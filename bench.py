@@ -82,6 +82,9 @@ def parse():
     ap.add_argument("--rays", type=int, default=16 * 1024 * 1024)
     ap.add_argument("--builder", default="ploc", choices=["ploc", "lbvh"])
     ap.add_argument("--bits", type=int, default=30, choices=[30, 63])
+    ap.add_argument("--walk", type=int, default=1, choices=[0, 1, 2],
+                    help="builder: the ray queries' walk (lrc_scene_set_walk): 0 the tree as built, 1 tight boxes, "
+                         "2 tight 8-wide quantised nodes")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="builder: the soup and its rays scaled by this (555: the reference's scene units, where the "
                          "triangles' 1e-3 box padding has its intended relative size)")
@@ -127,7 +130,8 @@ def config(a, world):
     scaled = f", scaled x{a.scale:g}" if a.scale != 1.0 else ""
     c = {"workload": f"builder+closest-hit: {a.n} triangles (soup{scaled}), {a.rays} rays, {a.builder.upper()} "
                      f"{a.bits}-bit Morton", "triangles": a.n, "rays": a.rays, "builder": a.builder,
-         "key_bits": a.bits, "parallelism": f"replicas x{world}",
+         "key_bits": a.bits, "walk": ("tree as built", "tight boxes", "8-wide quantised nodes")[a.walk],
+         "parallelism": f"replicas x{world}",
          "l2": "inputs larger than L2 (triangles 48 B x N + rays 24 B x R > 126 MB)"}
     if a.scale != 1.0:
         c["scale"] = a.scale
@@ -880,6 +884,11 @@ def run_serve(a):
     line["plain_mrays_s"] = plain_rays / plain_span / 1e6
     line["served_vs_plain"] = value / line["plain_mrays_s"]
     line["served_vs_plain_megakernel"] = r_mid["served_vs_plain_megakernel"]
+    # (the two one-job-at-a-time denominators by name: each job alone through lrc_trace as shipped,
+    # which puts large images on the wavefront engine - the best plain path - and, at the middle
+    # rate, each job alone on the one-kernel path)
+    line["plain_best_mrays_s"] = line["plain_mrays_s"]
+    line["plain_megakernel_mrays_s"] = r_mid["plain_megakernel"]["mrays_s"]
     line["denominators"] = ("plain_mrays_s: each job alone through lrc_trace as shipped (jobs of 2^20 paths and "
                             "more on the wavefront engine); served_vs_plain_megakernel: at the middle rate, each "
                             "job alone on the one-kernel path (LRC_TRACE_MEGAKERNEL)")
@@ -1641,6 +1650,7 @@ def main():
     d_t = torch.empty(a.rays, dtype=torch.float32, device=dev)
 
     scene.set_triangles(None, device_ptr=d_tris.data_ptr(), n=a.n)
+    scene.set_walk(a.walk)
 
     def step():
         scene.build(builder, a.bits)
@@ -1720,7 +1730,7 @@ def main():
                 "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
                 "algorithmic_bytes_per_launch": trace_bytes, "bytes_per_ray": bytes_per_ray,
                 "ms_per_launch": trace_ms}
-    if (a.n, a.rays, a.builder, a.bits, a.scale) == (4 << 20, 16 << 20, "ploc", 30, 1.0):
+    if (a.n, a.rays, a.builder, a.bits, a.scale, a.walk) == (4 << 20, 16 << 20, "ploc", 30, 1.0, 1):
         dram_gbs = BUILDER_CLOSEST_DRAM["bytes_per_launch"] / (BUILDER_CLOSEST_DRAM["ms_per_launch"] / 1e3) / 1e9
         rl_trace.update({"traffic": BUILDER_CLOSEST_DRAM["bytes_per_launch"],
                          "traffic_from": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4th closest_kernel "

@@ -157,14 +157,16 @@ int lrc_scene_tree_device(lrc_scene *s, const uint32_t **nodes, const uint32_t *
  * change of its shapes, replaces it. lrc_scene_tree then copies out nnodes and naux entries. */
 int lrc_scene_set_tree(lrc_scene *s, const uint32_t *nodes, uint32_t nnodes, const uint32_t *aux, uint32_t naux,
                        unsigned flags);
-/* The walk's tree of a scene of triangles alone (no primitives). tight = 1 (the default): after
- * each lrc_scene_build or lrc_scene_set_tree, the ray queries below (closest hit, any hit, walk
+/* The walk's tree of a scene of triangles alone (no primitives). mode 1 (the default): after each
+ * lrc_scene_build or lrc_scene_set_tree, the ray queries below (closest hit, any hit, walk
  * statistics) follow a copy of the tree - the same nodes and leaves - whose boxes are the
  * triangles' own bounds widened by 2^-17 of the root box's largest coordinate (at most the 1e-3
  * of triangle_bounds, scene.c:65-74), inner boxes their unions: the same hits as the padded tree,
- * fewer box tests where the padding is large beside the triangles. tight = 0: the tree as built.
+ * fewer box tests where the padding is large beside the triangles. mode 2: that tree collapsed
+ * into 8-wide nodes with their children's boxes quantised to bytes (80 bytes a node; a tree whose
+ * leaves hold more triangles than a node's slots keeps mode 1). mode 0: the tree as built.
  * lrc_scene_tree always gives the tree as built (the reference's); the path tracer walks that. */
-int lrc_scene_set_walk(lrc_scene *s, int tight);
+int lrc_scene_set_walk(lrc_scene *s, int mode);
 
 /* Closest hits of nrays rays (origins, directions: 3 floats each) in (tmin, tmax) through the
  * scene's BVH: prim = the triangle hit (-1: none), t. The reference's Moller-Trumbore arithmetic
@@ -176,7 +178,8 @@ int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint6
 int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const float *tmax, uint64_t nrays,
                        float tmin, uint8_t *out, unsigned flags);
 /* The closest-hit walk of lrc_scene_intersect, counting instead of answering: stats[0] = box tests
- * (32-byte node records read), stats[1] = triangle tests (48-byte triangles read), over all rays.
+ * (32-byte node records read; with the 8-wide walk, each 80-byte node read counts 2.5), stats[1] =
+ * triangle tests (48-byte triangles read), over all rays.
  * The traversal's algorithmic bytes (as the reference's tree statistics, LR_GPU_BVH_CHECK's cost
  * and depth, trace_gpu.c:768-805, describe a tree). stats: host. */
 int lrc_scene_trace_stats(lrc_scene *s, const float *orig, const float *dir, uint64_t nrays, float tmin, float tmax,

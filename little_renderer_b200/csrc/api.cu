@@ -31,6 +31,7 @@ int scene_build_on(lrc_scene *s, int builder, int key_bits, void **scratch, size
     if (!no_alloc) s->built_n = 0;
     s->tree_nnodes = s->tree_naux = 0;
     s->walk_ok = false;
+    s->wide_ok = false;
     if (!n) return LRC_OK;
     const size_t need_scratch = lrc::build_scratch_bytes(n, key_bits, builder);
     if (no_alloc) {
@@ -93,7 +94,8 @@ cudaError_t build_tlas_on(lrc_ctx *c, const float *d_inst, uint32_t n, Node *d_n
 // the closest- and any-hit queries; the path tracer walks the tree as built
 int make_walk(lrc_scene *s) {
     s->walk_ok = false;
-    if (!s->walk_tight || s->nprims || !s->built_n || !s->ntris) return LRC_OK;
+    s->wide_ok = false;
+    if (!s->walk_mode || s->nprims || !s->built_n || !s->ntris) return LRC_OK;
     lrc_ctx *c = s->ctx;
     const size_t nn = s->tree_nnodes ? s->tree_nnodes : 2 * (size_t)s->built_n - 1;
     const size_t na = s->tree_nnodes ? s->tree_naux : s->built_n;
@@ -112,6 +114,40 @@ int make_walk(lrc_scene *s) {
     c->timer.end(c->st);
     if (e) return cuda_status(c, e, "the walk's tree");
     s->walk_ok = true;
+    if (s->walk_mode != 2) return LRC_OK;
+    // the 8-wide nodes from it (a tree whose leaves do not fit a node's slots keeps the binary walk)
+    const size_t wcap = lrc::wide_node_cap((uint32_t)na);
+    if (s->wide_cap < wcap) {
+        cudaFree(s->d_wide);
+        s->d_wide = nullptr;
+        s->wide_cap = 0;
+        e = cudaMalloc(&s->d_wide, wcap * 80);
+        if (!e) s->wide_cap = wcap;
+    }
+    if (!e && s->wrefs_cap < wcap) {
+        cudaFree(s->d_wrefs);
+        s->d_wrefs = nullptr;
+        s->wrefs_cap = 0;
+        e = cudaMalloc(&s->d_wrefs, wcap * 4);
+        if (!e) s->wrefs_cap = wcap;
+    }
+    if (!e) e = reserve(&c->scratch, &c->scratch_cap, lrc::wide_scratch_bytes((uint32_t)na));
+    c->timer.begin(LRC_TS_HIERARCHY, c->st);
+    uint32_t nwide = 0;
+    if (!e) e = lrc::wide_build(s->d_wnodes, (uint32_t)nn, s->d_aux, (uint32_t)na, reinterpret_cast<const float *>(s->d_tris),
+                                s->ntris, s->d_wide, (uint32_t)s->wide_cap, s->d_wrefs, (uint32_t)s->wrefs_cap, c->scratch,
+                                c->scratch_cap, c->d_status, c->st, &nwide);
+    c->timer.end(c->st);
+    if (e) return cuda_status(c, e, "the walk's wide tree");
+    uint32_t status = 0;
+    e = cudaMemcpy(&status, c->d_status, 4, cudaMemcpyDeviceToHost);
+    if (e) return cuda_status(c, e, "the walk's wide tree");
+    if (status & lrc::ST_BAD_TREE) {                   // (leaves too large: the binary walk stays)
+        cudaMemset(c->d_status, 0, 4);
+        return LRC_OK;
+    }
+    s->nwide = nwide;
+    s->wide_ok = nwide > 0;
     return LRC_OK;
 }
 
@@ -302,6 +338,8 @@ void lrc_scene_destroy(lrc_scene *s) {
     cudaFree(s->d_tris);
     cudaFree(s->d_nodes);
     cudaFree(s->d_wnodes);
+    cudaFree(s->d_wide);
+    cudaFree(s->d_wrefs);
     cudaFree(s->d_aux);
     cudaFree(s->d_boxes);
     cudaFree(s->d_small);
@@ -338,6 +376,7 @@ int lrc_scene_set_triangles(lrc_scene *s, const uint32_t *tris, uint32_t n, unsi
     s->built_n = 0;
     s->tree_nnodes = s->tree_naux = 0;
     s->walk_ok = false;
+    s->wide_ok = false;
     if (!(flags & LRC_DEVICE)) return check_status(c);   // (the host array may be freed on return)
     return LRC_OK;
 }
@@ -349,10 +388,10 @@ int lrc_scene_build(lrc_scene *s, int builder, int key_bits) {
     return rc ? rc : make_walk(s);
 }
 
-int lrc_scene_set_walk(lrc_scene *s, int tight) {
-    if (!s || tight < 0 || tight > 1) return LRC_E_INVALID;
+int lrc_scene_set_walk(lrc_scene *s, int mode) {
+    if (!s || mode < 0 || mode > 2) return LRC_E_INVALID;
     DeviceGuard g(s->ctx->device);
-    s->walk_tight = tight != 0;
+    s->walk_mode = mode;
     return make_walk(s);
 }
 
@@ -392,6 +431,7 @@ int lrc_scene_set_tree(lrc_scene *s, const uint32_t *nodes, uint32_t nnodes, con
     }
     DeviceGuard g(c->device);
     s->walk_ok = false;
+    s->wide_ok = false;
     const size_t cap = std::max<size_t>(naux, ((size_t)nnodes + 1) / 2);   // (2 cap - 1 nodes, cap aux)
     cudaError_t e = cudaSuccess;
     if (s->tree_cap < cap) {
@@ -489,6 +529,7 @@ int lrc_scene_intersect(lrc_scene *s, const float *orig, const float *dir, uint6
     // a world with primitives walks shape ids (primitives, then triangles); a mesh, triangles alone
     auto run = [&](const float *o, const float *d, int32_t *p, float *tt_out) {
         if (s->nprims) return lrc::pt_intersect(pt_scene(s), o, d, nrays, tmin, tmax, p, nullptr, tt_out, c->d_status, c->st);
+        if (s->wide_ok) return lrc::wide_intersect(wide_tables(s), o, d, nrays, tmin, tmax, p, tt_out, c->d_status, c->st);
         return lrc::intersect_device(tt, o, d, nrays, tmin, tmax, p, tt_out, c->d_status, c->st, c->num_sms, sort_scratch,
                                      c->scratch_cap);
     };
@@ -536,10 +577,13 @@ int lrc_scene_trace_stats(lrc_scene *s, const float *orig, const float *dir, uin
         d_o = o;
         d_d = d;
     }
-    if (!e) e = lrc::count_device(tt, d_o, d_d, nrays, tmin, tmax, d_stats, c->d_status, c->st);
+    if (!e) e = s->wide_ok ? lrc::wide_count(wide_tables(s), d_o, d_d, nrays, tmin, tmax, d_stats, c->d_status, c->st)
+                           : lrc::count_device(tt, d_o, d_d, nrays, tmin, tmax, d_stats, c->d_status, c->st);
     if (!e) e = cudaMemcpyAsync(stats, d_stats, 16, cudaMemcpyDeviceToHost, c->st);
     if (e) return cuda_status(c, e, "lrc_scene_trace_stats");
-    return check_status(c);
+    const int rc = check_status(c);
+    if (!rc && s->wide_ok) stats[0] = (stats[0] * 5 + 1) / 2;   // (an 80-byte wide node: 2.5 records of 32 bytes)
+    return rc;
 }
 
 int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const float *tmax, uint64_t nrays, float tmin,
@@ -550,7 +594,8 @@ int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const 
     DeviceGuard g(c->device);
     lrc::TraceTables tt = tables(s);
     if (flags & LRC_DEVICE) {
-        cudaError_t e = lrc::occluded_device(tt, orig, dir, tmax, nrays, tmin, out, c->d_status, c->st);
+        cudaError_t e = s->wide_ok ? lrc::wide_occluded(wide_tables(s), orig, dir, tmax, nrays, tmin, out, c->d_status, c->st)
+                                   : lrc::occluded_device(tt, orig, dir, tmax, nrays, tmin, out, c->d_status, c->st);
         return cuda_status(c, e, "lrc_scene_occluded");
     }
     const size_t b_ray = al(nrays * 12);
@@ -563,7 +608,8 @@ int lrc_scene_occluded(lrc_scene *s, const float *orig, const float *dir, const 
     e = cudaMemcpyAsync(d_o, orig, nrays * 12, cudaMemcpyHostToDevice, c->st);
     if (!e) e = cudaMemcpyAsync(d_d, dir, nrays * 12, cudaMemcpyHostToDevice, c->st);
     if (!e) e = cudaMemcpyAsync(d_tm, tmax, nrays * 4, cudaMemcpyHostToDevice, c->st);
-    if (!e) e = lrc::occluded_device(tt, d_o, d_d, d_tm, nrays, tmin, d_out, c->d_status, c->st);
+    if (!e) e = s->wide_ok ? lrc::wide_occluded(wide_tables(s), d_o, d_d, d_tm, nrays, tmin, d_out, c->d_status, c->st)
+                           : lrc::occluded_device(tt, d_o, d_d, d_tm, nrays, tmin, d_out, c->d_status, c->st);
     if (!e) e = cudaMemcpyAsync(out, d_out, nrays, cudaMemcpyDeviceToHost, c->st);
     if (e) return cuda_status(c, e, "lrc_scene_occluded");
     return check_status(c);
@@ -583,6 +629,7 @@ int lrc_scene_set_prims(lrc_scene *s, const float *prims, uint32_t n, unsigned f
     s->built_n = 0;
     s->tree_nnodes = s->tree_naux = 0;
     s->walk_ok = false;
+    s->wide_ok = false;
     return (flags & LRC_DEVICE) ? LRC_OK : check_status(c);
 }
 

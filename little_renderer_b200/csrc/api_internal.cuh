@@ -2,6 +2,7 @@
 // behind include/lrc.h's opaque handles, status helpers and the path tracer's view of a scene.
 #pragma once
 #include "lrc_internal.cuh"
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -38,7 +39,13 @@ struct lrc_scene {
     Node *d_wnodes = nullptr;     // the walk's copy of a triangle tree with tight boxes (lrc_scene_set_walk)
     size_t wnodes_cap = 0;        // (nodes)
     bool walk_ok = false;         // d_wnodes is the current tree's
-    bool walk_tight = true;
+    int walk_mode = 1;            // 0 the tree as built, 1 tight boxes, 2 tight 8-wide nodes
+    float4 *d_wide = nullptr;     // the walk's 8-wide nodes (walk_mode 2) and their triangle entries
+    size_t wide_cap = 0;
+    uint32_t *d_wrefs = nullptr;
+    size_t wrefs_cap = 0;
+    uint32_t nwide = 0;
+    bool wide_ok = false;
     float *d_boxes = nullptr;
     size_t boxes_cap = 0;
     uint32_t *d_small = nullptr;  // 6 bound keys, 6 bounds, 6 lo/ext
@@ -240,6 +247,18 @@ inline lrc::TraceTables tables(const lrc_scene *s) {
     tt.naux = s->tree_nnodes ? s->tree_naux : s->built_n;
     tt.ntris = s->ntris;
     return tt;
+}
+
+// the wide walk's view of a scene (walk_mode 2, made)
+inline lrc::WideTables wide_tables(const lrc_scene *s) {
+    lrc::WideTables wt{};
+    wt.nodes = s->d_wide;
+    wt.refs = s->d_wrefs;
+    wt.tris = reinterpret_cast<const float4 *>(s->d_tris);
+    wt.nnodes = s->nwide;
+    wt.nrefs = (uint32_t)std::min<size_t>(s->wrefs_cap, 0xffffffffu);
+    wt.ntris = s->ntris;
+    return wt;
 }
 
 // builds the scene's world tree (triangles and primitives) on stream st with the given scratch

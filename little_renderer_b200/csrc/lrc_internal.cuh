@@ -137,6 +137,29 @@ cudaError_t refit_device(Node *d_nodes, const uint32_t *d_aux, uint32_t n, uint3
                          uint32_t stride4, uint32_t lo_at, void *scratch, size_t scratch_bytes, uint32_t *d_status,
                          cudaStream_t st);
 cudaError_t tree_cost_device(const Node *d_nodes, uint32_t n, double *d_out, cudaStream_t st);
+// the ray queries' walk over 8-wide nodes (wide.cu): 80-byte nodes (5 float4), triangle entries
+struct WideTables {
+    const float4 *nodes;
+    const uint32_t *refs;
+    const float4 *tris;      // 3 float4 per triangle
+    uint32_t nnodes, nrefs, ntris;
+};
+// capacity of wide nodes and triangle entries for a binary tree with naux leaf entries
+size_t wide_node_cap(uint32_t naux);
+size_t wide_scratch_bytes(uint32_t naux);
+// the wide tree of the binary tree d_bin (nn nodes, root 0, leaves' aux = triangle ids) into
+// d_wnodes (wcap nodes) and d_wrefs (rcap entries); *nwide: the wide nodes made. Waits for the stream
+// (one launch a level). A leaf that does not fit a node's slots: ST_BAD_TREE.
+cudaError_t wide_build(const Node *d_bin, uint32_t nn, const uint32_t *d_aux, uint32_t naux, const float *d_tris,
+                       uint32_t ntris, float4 *d_wnodes, uint32_t wcap, uint32_t *d_wrefs, uint32_t rcap, void *scratch,
+                       size_t scratch_bytes, uint32_t *d_status, cudaStream_t st, uint32_t *nwide);
+cudaError_t wide_intersect(const WideTables &wt, const float *d_orig, const float *d_dir, uint64_t nrays, float tmin,
+                           float tmax, int32_t *d_prim, float *d_t, uint32_t *d_status, cudaStream_t st);
+cudaError_t wide_occluded(const WideTables &wt, const float *d_orig, const float *d_dir, const float *d_tmax, uint64_t nrays,
+                          float tmin, uint8_t *d_out, uint32_t *d_status, cudaStream_t st);
+// totals: [0] wide nodes fetched (80 bytes each), [1] triangle tests
+cudaError_t wide_count(const WideTables &wt, const float *d_orig, const float *d_dir, uint64_t nrays, float tmin, float tmax,
+                       unsigned long long *d_stats, uint32_t *d_status, cudaStream_t st);
 // the walk's tree of a triangle tree (nn nodes, root at 0, leaves' aux = triangle ids): the same
 // nodes with each leaf's box the bounds of its triangles' corners widened by 2^-17 of the largest
 // coordinate of the source root box (at most the 1e-3 the builders pad with), inner boxes the unions

@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "liblrc.so")
-SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu", "media.cu", "textures.cu"]
+SOURCES = ["api.cu", "build.cu", "traverse.cu", "static_build.cu", "pathtrace.cu", "host_tables.cu", "batch.cu", "wavefront.cu", "refit.cu", "serve.cu", "caustics.cu", "denoise.cu", "media.cu", "textures.cu", "wide.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC"]
 OBJ_DIR = os.path.join(PKG, "_build")
@@ -419,10 +419,10 @@ class Scene:
         aux = np.ascontiguousarray(aux, np.uint32)
         self.ctx.check(self.ctx.L.lrc_scene_set_tree(self.h, _ptr(nodes), nodes.shape[0], _ptr(aux), aux.shape[0], 0))
 
-    def set_walk(self, tight):
-        """lrc_scene_set_walk: ray queries over a copy of the tree with tight boxes (1, the default)
-        or over the tree as built (0)."""
-        self.ctx.check(self.ctx.L.lrc_scene_set_walk(self.h, int(tight)))
+    def set_walk(self, mode):
+        """lrc_scene_set_walk: ray queries over a copy of the tree with tight boxes (1, the default),
+        that copy as 8-wide quantised nodes (2), or the tree as built (0)."""
+        self.ctx.check(self.ctx.L.lrc_scene_set_walk(self.h, int(mode)))
 
     def tree(self):
         nodes = np.zeros((2 * self.n - 1, 8), np.uint32)

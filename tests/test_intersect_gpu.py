@@ -40,14 +40,16 @@ def assert_hits_match(prim, t, rprim, rt):
     return int(diff.sum())
 
 
+@pytest.mark.parametrize("walk", [1, 2])
 @pytest.mark.parametrize("builder", [0, 1])
 @pytest.mark.parametrize("n", [1, 3, 1000, 100000])
-def test_closest_hits_match_scene_intersect(ctx, oracle, builder, n):
+def test_closest_hits_match_scene_intersect(ctx, oracle, builder, n, walk):
     cor, quv, ref = _scene(oracle, n, 40 + n)
     o, d = _rays(cor, 200000, 3)
     rp, _, rt = ref.intersect(o, d)
     s = L.Scene(ctx)
     s.set_triangles(L.pack_tris(quv))
+    s.set_walk(walk)
     s.build(builder, 30)
     p, t = s.intersect(o, d)
     ties = assert_hits_match(p, t, rp, rt)
@@ -66,8 +68,10 @@ def test_closest_hits_full_size(ctx, oracle):
     s.set_triangles(L.pack_tris(quv))
     for builder in (0, 1):
         s.build(builder, 30)
-        p, t = s.intersect(o, d)
-        assert assert_hits_match(p, t, rp, rt) <= 20
+        for walk in (1, 2):
+            s.set_walk(walk)
+            p, t = s.intersect(o, d)
+            assert assert_hits_match(p, t, rp, rt) <= 20
 
 
 @pytest.mark.parametrize("builder", [0, 1])
@@ -110,8 +114,8 @@ def _flat_grids(cells=32):
 @pytest.mark.parametrize("builder", [0, 1])
 def test_tight_walk_same_hits_on_flat_grids_edges_and_far_rays(ctx, oracle, builder):
     """The walk's tree (lrc_scene_set_walk 1: the triangles' own bounds widened by 2^-17 of the
-    scene's size) against the tree as built and against scene_intersect, where tight boxes are
-    thinnest: axis-aligned grids of flat triangles, rays aimed at their shared corners and edge
+    scene's size; 2: the same as 8-wide quantised nodes) against the tree as built and against
+    scene_intersect, where tight boxes are thinnest: axis-aligned grids of flat triangles, rays aimed at their shared corners and edge
     midpoints from 2 to 40 units away, and rays that graze the grids' planes."""
     cor = _flat_grids()
     ref = oracle.RefScene()
@@ -154,13 +158,17 @@ def test_tight_walk_same_hits_on_flat_grids_edges_and_far_rays(ctx, oracle, buil
     s.build(builder, 30)
     p1, t1 = s.intersect(o, d)
     b1, _ = s.trace_stats(o, d)
+    s.set_walk(2)
+    p2, t2 = s.intersect(o, d)
     s.set_walk(0)
     p0, t0 = s.intersect(o, d)
     b0, _ = s.trace_stats(o, d)
     print(f"flat grids, builder {builder}: {(rp >= 0).mean():.3f} of rays hit; box tests a ray {b1 / n:.1f} "
-          f"(tight) vs {b0 / n:.1f} (as built); differing hits {int((p1 != rp).sum())} / {int((p0 != rp).sum())}")
+          f"(tight) vs {b0 / n:.1f} (as built); differing hits {int((p1 != rp).sum())} / {int((p2 != rp).sum())} / "
+          f"{int((p0 != rp).sum())} (tight, 8-wide, as built)")
     assert (rp >= 0).mean() > 0.5
     assert_hits_match(p1, t1, rp, rt)
+    assert_hits_match(p2, t2, rp, rt)
     assert_hits_match(p0, t0, rp, rt)
     assert b1 <= b0
     s.close()

@@ -4,8 +4,9 @@ lrc_scene_set_tree, as the engine's GPU backend hands the Scene's tree over, tra
 and the device-built PLOC tree. Both give scene_intersect's hits; each tree's work per ray (box and
 triangle tests of the walk) and the closest-hit kernel's device time over the same rays are
 printed, at 1M triangles / 2M rays and at the workload's 4M triangles / 16M rays, each tree walked
-as built (its boxes padded by triangle_bounds' 1e-3) and as the walk's tree (lrc_scene_set_walk:
-the triangles' own bounds, widened by 2^-17 of the scene's size)."""
+as built (its boxes padded by triangle_bounds' 1e-3), as the walk's tree (lrc_scene_set_walk 1:
+the triangles' own bounds, widened by 2^-17 of the scene's size) and as that tree's 8-wide
+quantised nodes (2; box tests count an 80-byte node as 2.5 records of 32 bytes)."""
 import numpy as np
 import pytest
 import torch
@@ -59,11 +60,11 @@ def test_sah_and_ploc_trees_give_the_same_hits_and_their_cost(ctx, oracle, n, nr
     d_t = torch.empty(nrays, dtype=torch.float32, device=dev)
     out = {}
     for name, s in (("sah", sah), ("ploc", ploc)):
-        for tight in (0, 1):
+        for tight in (0, 1, 2):
             s.set_walk(tight)
             bpr, tpr, ms = _walk(ctx, s, d_o, d_d, nrays, d_p, d_t)
             out[name, tight] = (d_p.cpu().numpy(), d_t.cpu().numpy(), bpr, tpr, ms)
-            print(f"{n} triangles, {nrays} rays, {name.upper()} tree, {'tight' if tight else 'padded'} boxes: "
+            print(f"{n} triangles, {nrays} rays, {name.upper()} tree, {('padded', 'tight', '8-wide tight')[tight]} boxes: "
                   f"{bpr:.1f} box and {tpr:.2f} triangle tests a ray ({bpr * 32 + tpr * 48:.0f} B of nodes and "
                   f"triangles), closest-hit pass {ms:.2f} ms = {nrays / ms / 1e3:.1f} Mrays/s")
     sah.close()
