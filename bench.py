@@ -441,9 +441,12 @@ def run_batch(a):
     e2e_step()
     e2e_steps = max(1, min(a.steps, 3))
     e_ms = timed(e2e_step, e2e_steps) / e2e_steps
+    _, e2e_rays = b.rays()
     e2e = {"value": world * rays / (e_ms / 1e3) / 1e6, "unit": "Mrays/s",
            "h2d_bytes_per_step": int(sum(p.numel() * 4 for p in pins)),
-           "d2h_bytes_per_step": int(sum(o.numel() * 4 for o in outs)), "ms_per_step": e_ms}
+           "d2h_bytes_per_step": int(sum(o.numel() * 4 for o in outs)), "ms_per_step": e_ms,
+           "images_equal_plain": all(torch.equal(x, y) for x, y in zip(plain_imgs, outs)),
+           "rays_equal": bool(e2e_rays == rays)}
 
     peak, peak_kind = peaks()
     line = {"metric": METRIC_BATCH, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": a.steps,

@@ -477,7 +477,7 @@ int lrc_batch_set_wavefront(lrc_batch *b, uint32_t slots, int32_t variant);
 int lrc_batch_wavefront_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm);
 int lrc_batch_engine(const lrc_batch *b, int32_t *engine, uint32_t *slots, int32_t *wf_variant);
 /* The autotuner: times the engine's shapes on the first sample_tasks tasks of the queue (0: a
- * sixteenth) and keeps the fastest - the megakernel's launch shape (variant, grid blocks), or the
+ * sixteenth; for the wavefront at least 2^24 tasks, or all) and keeps the fastest - the megakernel's launch shape (variant, grid blocks), or the
  * wavefront's size and launch shape (variant, grid = paths in flight) - and the ns per task (each
  * optional). Changes no image. */
 int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_t *grid, double *ns_per_task);

@@ -195,8 +195,10 @@ int build_job(lrc_batch *b, const lrc_batch::Job *J, cudaStream_t st, bool captu
 
 uint32_t max_passes(const lrc_batch *b, unsigned long long limit);
 
-// the job table in queue order, the partial buffers and counters sized, the table uploaded
-int prepare(lrc_batch *b) {
+// the job table in queue order, the partial buffers and counters sized, the table uploaded; with
+// building, each job's scene as the run's builds leave it (its triangles may have been set again
+// since the last build, and builds inside a replayed graph are recorded only after the launch)
+int prepare(lrc_batch *b, bool building) {
     lrc_ctx *c = b->ctx;
     const size_t nj = b->jobs.size();
     b->order.resize(nj);
@@ -213,7 +215,7 @@ int prepare(lrc_batch *b) {
     for (size_t q = 0; q < nj; q++) {
         const lrc_batch::Job &J = b->jobs[b->order[q]];
         lrc::BatchJob &T = b->table[q];
-        T.S = view_of(J, false);
+        T.S = view_of(J, building);
         T.P = params_of(J);
         T.task0 = task;
         T.pix0 = pix;
@@ -622,7 +624,7 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
                 int rc = build_job(b, J, c->st, false);
                 if (rc) return rc;
             }
-        int rc = prepare(b);
+        int rc = prepare(b, (flags & LRC_BATCH_BUILD) != 0);
         if (!rc) rc = enqueue(b, flags, c->st, false, false, true, b->ntasks);
         return rc;
     }
@@ -640,7 +642,7 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
                 if (rc) return rc;
             }
         }
-        int rc = prepare(b);
+        int rc = prepare(b, (flags & LRC_BATCH_BUILD) != 0);
         if (rc) return rc;
         const std::vector<unsigned char> key = graph_key(b, flags);
         const bool reuse = b->exec && b->graph_flags == flags && key == b->graph_sig;
@@ -679,7 +681,7 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
             if (rc) return rc;
         }
     }
-    int rc = prepare(b);
+    int rc = prepare(b, (flags & LRC_BATCH_BUILD) != 0);
     if (rc) return rc;
     rc = enqueue(b, flags, c->st, false, false, true, b->ntasks);
     if (rc) return rc;
@@ -784,11 +786,15 @@ int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_
             if (rc) return rc;
         }
     }
-    int rc = b->prepared ? LRC_OK : prepare(b);
+    int rc = b->prepared ? LRC_OK : prepare(b, false);
     if (rc) return rc;
     // the queue's head: the most expensive tasks (the trace kernels write only per-task sums, which
     // the next run overwrites, so tuning changes no image)
-    const unsigned long long n = std::min<unsigned long long>(b->ntasks, sample_tasks ? sample_tasks : b->ntasks / 16 + 1);
+    // (the wavefront's sizes are judged on at least 2^24 tasks, or all: a sixteenth of a small queue
+    // cannot fill its larger sizes, and a size is timed only where the sample fills it)
+    const unsigned long long dflt = b->engine == 1 ? std::max<unsigned long long>(b->ntasks / 16 + 1, 1ull << 24)
+                                                   : b->ntasks / 16 + 1;
+    const unsigned long long n = std::min<unsigned long long>(b->ntasks, sample_tasks ? sample_tasks : dflt);
     if (b->engine == 1) return tune_wavefront(b, n, variant, grid, ns_per_task);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

@@ -229,6 +229,9 @@ int finish_wave(lrc_server *sv, lrc_server::Wave &W, int32_t *finished) {
             }
         }
         if (!e) e = cudaEventRecord(J->ev_done, sv->side);
+        // (work queued on the context's stream from now on - a read of lrc_server_result's image
+        // there - comes after the job's completion on the side stream)
+        if (!e) e = cudaStreamWaitEvent(c->st, J->ev_done, 0);
         if (e) return cuda_status(c, e, "server finish");
         J->state = 2;
         J->t_done = t;

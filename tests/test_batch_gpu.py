@@ -78,17 +78,22 @@ def test_graph_replay_with_builds(ctx, oracle, scenes, engine):
     b.set_engine(engine)
     for s, sc, t, bl in zip(own, scenes, imgs, builders):
         b.add(s, params(sc), sc["spp"], t.data_ptr(), builder=bl, key_bits=30)
+    refs = []
+    for sc, bl in zip(scenes, builders):
+        ref = R.world_scene(ctx, sc, min(bl, 1), blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+        refs.append(ref.trace(params(sc), sc["spp"])[0])
+        ref.close()
     used = []
-    for _ in range(3):
+    for i in range(4):
+        if i == 3:      # every scene's triangles set again (as a host copy would): the replay builds them
+            for s, sc in zip(own, scenes):
+                s.set_triangles(L.pack_tris(W.corners_to_quv(sc["corners"]), sc["tri_mats"]))
         b.run(build=True, graph=True, zero=True)
         got = host(ctx, imgs)
         used.append(b.info()["graph_used"])
-        for s, sc, g, bl in zip(own, scenes, got, builders):
-            ref = R.world_scene(ctx, sc, min(bl, 1), blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
-            acc, _ = ref.trace(params(sc), sc["spp"])
+        for g, acc in zip(got, refs):
             assert np.array_equal(g, acc)
-            ref.close()
-    assert used == [0, 1, 1]
+    assert used == [0, 1, 1, 1]
 
 
 def test_bands_and_sample_offsets_add_up(ctx, scenes, built):
