@@ -97,6 +97,9 @@ def parse():
     ap.add_argument("--budget-gb", type=float, default=24.0, help="serve: the server's HBM budget for jobs")
     ap.add_argument("--wave-paths", type=int, default=32 << 20, help="serve: paths per wave")
     ap.add_argument("--wave-slots", type=int, default=1 << 23, help="serve: the waves' paths in flight")
+    ap.add_argument("--wave-variant", type=int, default=None,
+                    help="serve: the waves' wavefront launch shape (lrc_server_set_wavefront's variant; default "
+                         "LRC_WAVEFRONT_DEFAULT_VARIANT)")
     ap.add_argument("--serve-policy", type=int, default=2, choices=[0, 1, 2],
                     help="serve: how a wave is made (lrc_server_set_policy: 0 even shares, 1 oldest first, "
                          "2 fewest paths left first)")
@@ -146,6 +149,29 @@ def max_over_ranks(ms, dist, device):
     t = torch.tensor([float(ms)], device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def library_sort_ms(n, bits, stream, device, reps=10):
+    """A library radix sort of as many keys, for comparison with the build's sort: torch.sort
+    (stable, CUB's radix sort underneath) of n uniform keys of the build's width, returning the
+    sorted keys and the permutation (int64 indices: 4 bytes a key more per pass than the build's
+    32-bit items), timed by CUDA events on the build's stream after 3 warm-up calls."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(5)
+    if bits == 63:
+        keys = torch.randint(0, 1 << 62, (n,), dtype=torch.int64, device=device, generator=g)
+    else:
+        keys = torch.randint(0, 1 << bits, (n,), dtype=torch.int32, device=device, generator=g)
+    for _ in range(3):
+        torch.sort(keys, stable=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        torch.sort(keys, stable=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return {"what": "torch.sort(stable=True) of the same number of uniform %d-bit keys, with int64 indices" % bits,
+            "ms_per_sort": e0.elapsed_time(e1) / reps}
 
 
 def whole_job_rate(units_per_rank, world, ms):
@@ -619,7 +645,8 @@ def serve_config(a, tris):
                         "{4, 16, 64}, depth 8, a tenth moving their scene's 2000 instances (top level refit), "
                         "Poisson arrivals", "rates": a.rates, "jobs_per_step": SERVE_JOBS_PER_STEP,
             "jobs_per_rate": SERVE_JOBS_PER_STEP * a.steps, "budget_gb": a.budget_gb, "wave_paths": a.wave_paths,
-            "wave_slots": a.wave_slots, "serve_policy": a.serve_policy, "parallelism": "one GPU",
+            "wave_slots": a.wave_slots, "wave_variant": a.wave_variant, "serve_policy": a.serve_policy,
+            "parallelism": "one GPU",
             "denoise_low_spp": bool(a.denoise_low_spp),
             "l2": "inputs larger than L2 (resident scenes' triangles and trees, images, wavefront state > 126 MB)"}
 
@@ -636,6 +663,8 @@ def run_serve(a):
     served again end to end (each image read back to pinned host memory inside the span)."""
     import torch
     import little_renderer_b200 as L
+    if a.wave_variant is None:
+        a.wave_variant = L.native.LRC_WAVEFRONT_DEFAULT_VARIANT
     from little_renderer_b200 import render as R, workloads as W
 
     if int(os.environ.get("RANK", "0")) != 0:
@@ -671,7 +700,7 @@ def run_serve(a):
         """lrc_server over the stream: submit each job at its arrival, step waves while any is held.
         keep: images of the first jobs kept (host); readback: every image read to pinned host memory."""
         sv = L.native.Server(ctx, int(a.budget_gb * 2**30), a.wave_paths)
-        sv.set_wavefront(a.wave_slots)
+        sv.set_wavefront(a.wave_slots, a.wave_variant)
         sv.set_policy(a.serve_policy)
         pinned = torch.empty(1920 * 1080 * 4, dtype=torch.float32).pin_memory() if readback else None
         lat, rays, ids, kept, d2h = [], 0, {}, {}, 0
@@ -838,7 +867,7 @@ def run_serve(a):
             sample_paths += j[2] * j[3] * j[4]
     imgs = [torch.zeros(j[3], j[2], 4, device=dev) for _, j in sample]
     bb = L.native.Batch(ctx)
-    bb.set_wavefront(a.wave_slots, 0)
+    bb.set_wavefront(a.wave_slots, a.wave_variant)
     for (k, j), t in zip(sample, imgs):
         bb.add(scenes[j[1]], params(j, k), j[4], t.data_ptr())
     bb.run(zero=True, stepped=True, count=True)
@@ -1744,6 +1773,7 @@ def main():
                "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
                "algorithmic_bytes_per_launch": sort_bytes, "ms_per_launch": sort_ms}
     rl_sort["frac"] = rl_sort["achieved"] / peak
+    rl_sort["library_sort"] = library_sort_ms(a.n, a.bits, stream, dev)
     dominant = rl_trace if trace_ms >= sum(v[0] for k, v in stages.items() if k != "trace") / per else rl_sort
 
     passes = 8 if a.bits == 63 else 4

@@ -456,9 +456,10 @@ int lrc_batch_passes(lrc_batch *b, uint32_t *passes, uint64_t *kernels);
 /* The last LRC_BATCH_STEPPED run of the wavefront (each optional): its closest-hit kernel's device
  * time (CUDA events around each launch) and the rays it traced; with LRC_BATCH_COUNT its walks' box
  * tests (32-byte node records read) and triangle tests (48-byte triangles read), counted by a
- * counting build of that kernel run with the default launch shape (lrc_batch_set_wavefront variant
- * 0; it tests what the plain one does: the same hits, the images the same to the bit); and the
- * kernels the run launched. */
+ * counting build of that kernel (for the launch shapes of 128 threads, registers capped for 4 or 8
+ * blocks an SM, the default's among them; with other shapes the counts are 0; it tests what the
+ * plain one does: the same hits, the images the same to the bit); and the kernels the run
+ * launched. */
 int lrc_batch_step_stats(const lrc_batch *b, double *intersect_ms, uint64_t *intersect_rays, uint64_t *box_tests,
                          uint64_t *tri_tests, uint64_t *kernels);
 /* The trace kernel's launch shapes: shape `variant`'s threads per block, the blocks per SM its
@@ -471,8 +472,13 @@ int lrc_batch_set_shape(lrc_batch *b, int32_t variant, int32_t grid);
  * persistent megakernel (one path per lane, the next sample started when a path ends). Both give
  * the same images. */
 int lrc_batch_set_engine(lrc_batch *b, int32_t engine);
-/* The wavefront's size (paths in flight: a multiple of 256) and its closest-hit / shadow kernels'
- * launch shape (lrc_batch_wavefront_shape describes them as lrc_batch_shape does). */
+/* The wavefront's size (paths in flight: a multiple of 256) and its kernels' launch shape
+ * (lrc_batch_wavefront_shape describes the closest-hit / shadow kernels' as lrc_batch_shape does;
+ * each shape also caps the shading kernel's registers). LRC_WAVEFRONT_DEFAULT_VARIANT is the shape
+ * a batch starts with, and the one lrc_trace and the server use: 128 threads a block, the
+ * closest-hit and shadow kernels' registers capped for 8 blocks an SM, the shading kernel's for 4
+ * (the fastest of the shapes on a served stream of path-traced jobs). */
+#define LRC_WAVEFRONT_DEFAULT_VARIANT 9
 int lrc_batch_set_wavefront(lrc_batch *b, uint32_t slots, int32_t variant);
 int lrc_batch_wavefront_shape(int32_t variant, int32_t *block, int32_t *minb, int32_t *per_sm);
 int lrc_batch_engine(const lrc_batch *b, int32_t *engine, uint32_t *slots, int32_t *wf_variant);

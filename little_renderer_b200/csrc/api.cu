@@ -1011,7 +1011,8 @@ int lrc_trace(lrc_scene *s, const lrc_trace_params *p, int32_t y0, int32_t rows,
             rc = lrc_batch_create(c, &c->single);
             if (rc) return rc;
         }
-        rc = lrc_batch_set_wavefront(c->single, paths >= (8u << 20) ? 1u << 22 : 1u << 20, 0);
+        rc = lrc_batch_set_wavefront(c->single, paths >= (8u << 20) ? 1u << 22 : 1u << 20,
+                                     LRC_WAVEFRONT_DEFAULT_VARIANT);
         if (!rc) rc = lrc_batch_clear(c->single);
         if (!rc) rc = guided ? lrc_batch_add_guided(c->single, s, p, y0, rows, spp0, spp, d_acc, -1, 30)
                              : lrc_batch_add(c->single, s, p, y0, rows, spp0, spp, d_acc, -1, 30);

@@ -57,7 +57,7 @@ struct lrc_batch {
     // (wf_slots paths in flight, closest-hit / shadow kernels' shape wf_variant); tuned or set
     int engine = 1;
     int variant = 0, grid = 0;
-    int wf_variant = 0;
+    int wf_variant = LRC_WAVEFRONT_DEFAULT_VARIANT;
     uint32_t wf_slots = 1u << 20;
     void *d_wf = nullptr;
     size_t wf_cap = 0;

@@ -276,7 +276,7 @@ int lrc_server_create(lrc_ctx *c, uint64_t hbm_budget_bytes, uint64_t wave_paths
     cudaError_t e = cudaSuccess;
     for (lrc_server::Wave &W : sv->wave) {
         if (!rc) rc = lrc_batch_create(c, &W.batch);
-        if (!rc) rc = lrc_batch_set_wavefront(W.batch, 1u << 22, 0);   // (4M paths in flight: a wave's tail stays short)
+        if (!rc) rc = lrc_batch_set_wavefront(W.batch, 1u << 22, LRC_WAVEFRONT_DEFAULT_VARIANT);   // (4M paths in flight: a wave's tail stays short)
         if (!rc && !e) e = cudaEventCreate(&W.ev0);
         if (!rc && !e) e = cudaEventCreate(&W.ev1);
         if (!rc && !e) e = cudaMallocHost(reinterpret_cast<void **>(&W.h_passes), 16);

@@ -355,8 +355,11 @@ struct WfVariant {
 const WfVariant kWfVariants[] = {
     LRC_WF_VARIANT(128, 4, 1), LRC_WF_VARIANT(128, 6, 1), LRC_WF_VARIANT(128, 8, 1), LRC_WF_VARIANT(256, 4, 1),
     LRC_WF_VARIANT(64, 12, 1), LRC_WF_VARIANT(128, 6, 5), LRC_WF_VARIANT(128, 8, 5), LRC_WF_VARIANT(128, 8, 6),
+    LRC_WF_VARIANT(128, 4, 4), LRC_WF_VARIANT(128, 8, 4),
 };
 #undef LRC_WF_VARIANT
+static_assert(sizeof(kWfVariants) / sizeof(kWfVariants[0]) > LRC_WAVEFRONT_DEFAULT_VARIANT &&
+              LRC_WAVEFRONT_DEFAULT_VARIANT == 9, "the default shape is (128, 8, 4)");
 size_t a256(size_t x) { return (x + 255) / 256 * 256; }
 }  // namespace
 
@@ -483,9 +486,12 @@ cudaError_t wf_run_stepped(const BatchJob *d_jobs, uint32_t njobs, unsigned long
     if (variant < 0 || variant >= wf_variants() || W.M == 0 || W.M % pt::ADV_BLOCK) return cudaErrorInvalidValue;
     const WfVariant &V = kWfVariants[variant];
     const void *isect = instances ? V.isect : V.isect_world, *shadow = instances ? V.shadow : V.shadow_world;
-    if (stats && count && V.block == 128 && V.minb == 4)   // (the counting kernels: variant 0's shape)
+    if (stats && count && V.block == 128 && V.minb == 4)   // (the counting kernels: two of the shapes)
         isect = instances ? (const void *)pt::wf_intersect_kernel<128, 4, true, true>
                           : (const void *)pt::wf_intersect_kernel<128, 4, false, true>;
+    else if (stats && count && V.block == 128 && V.minb == 8)
+        isect = instances ? (const void *)pt::wf_intersect_kernel<128, 8, true, true>
+                          : (const void *)pt::wf_intersect_kernel<128, 8, false, true>;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (stats) {
         *stats = WfStepStats{};

@@ -24,6 +24,7 @@ LRC_TRACE_GUIDED = 64
 LRC_TRACE_MEGAKERNEL = 256
 LRC_REPROJECT_EDIT = 128
 LRC_SERVE_DENOISE = 16
+LRC_WAVEFRONT_DEFAULT_VARIANT = 9      # (include/lrc.h)
 LRC_BATCH_BUILD, LRC_BATCH_GRAPH, LRC_BATCH_ZERO, LRC_BATCH_STEPPED, LRC_BATCH_COUNT = 4, 8, 16, 32, 64
 
 
@@ -758,7 +759,8 @@ class Batch:
         """0: the persistent megakernel, 1: the wavefront (the default)."""
         self.ctx.check(self.ctx.L.lrc_batch_set_engine(self.h, engine))
 
-    def set_wavefront(self, slots, variant=0):
+    def set_wavefront(self, slots, variant=None):
+        variant = LRC_WAVEFRONT_DEFAULT_VARIANT if variant is None else variant
         self.ctx.check(self.ctx.L.lrc_batch_set_wavefront(self.h, slots, variant))
 
     def engine(self):
@@ -876,8 +878,9 @@ class Server:
     def set_policy(self, policy):
         self.ctx.check(self.ctx.L.lrc_server_set_policy(self.h, policy))
 
-    def set_wavefront(self, slots, variant=0):
-        """The waves' wavefront size (paths in flight) and closest-hit / shadow launch shape."""
+    def set_wavefront(self, slots, variant=None):
+        """The waves' wavefront size (paths in flight) and launch shape (None: the default)."""
+        variant = LRC_WAVEFRONT_DEFAULT_VARIANT if variant is None else variant
         self.ctx.check(self.ctx.L.lrc_server_set_wavefront(self.h, slots, variant))
 
 
