@@ -509,7 +509,7 @@ SERVE_JOBS_PER_STEP = 5      # a serve step: 5 jobs of each rate's stream
 # launch's duration under the profiler: one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum, gpu__time_duration.sum) of launches 81-83 of wf_intersect_kernel in
 # `python bench.py --steps 2 --warmup 3 --rates 200` (the timed stepped run's full-queue passes)
-SERVE_ISECT_DRAM = {"bytes_per_launch": 474.6e6, "ms_per_launch": 3.77}
+SERVE_ISECT_DRAM = {"bytes_per_launch": 474.4e6, "ms_per_launch": 3.74}
 
 
 def serve_jobs(n, rate, seed, nscenes, inst_ids):
