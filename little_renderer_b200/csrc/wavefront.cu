@@ -29,15 +29,24 @@ constexpr int SHADE_BLOCK = 128;
 
 __device__ __forceinline__ V3 v3f(float4 a) { return v3(a.x, a.y, a.z); }
 
-// warp-aggregated append: lanes with want get consecutive positions from *ctr (all 32 lanes call)
-__device__ __forceinline__ uint32_t warp_append(uint32_t *ctr, bool want) {
-    const uint32_t lane = threadIdx.x & 31;
+// block-aggregated append (every thread of the block calls, ADV_BLOCK of them): threads with want
+// get consecutive positions from *ctr, in thread order, with one atomic per block
+__device__ __forceinline__ uint32_t block_append(uint32_t *ctr, bool want, uint32_t *s_warp, uint32_t &s_base) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t m = __ballot_sync(0xffffffffu, want);
-    uint32_t base = 0;
-    const int leader = m ? __ffs(m) - 1 : 0;
-    if (m && (int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    return base + __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) s_warp[w] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int k = 0; k < ADV_BLOCK / 32; k++) {
+            const uint32_t c = s_warp[k];
+            s_warp[k] = t;
+            t += c;
+        }
+        s_base = t ? atomicAdd(ctr, t) : 0u;
+    }
+    __syncthreads();
+    return s_base + s_warp[w] + __popc(m & ((1u << lane) - 1u));
 }
 
 // the slots emptied, the queues cleared, the task queue set to [0, limit)
@@ -182,7 +191,9 @@ __global__ void __launch_bounds__(ADV_BLOCK) wf_advance_kernel(const BatchJob *_
         path = true;
     }
     if (path) trays++;                               // its closest-hit ray
-    const uint32_t q = warp_append(&W.ctl[0], path);
+    __shared__ uint32_t s_warp[ADV_BLOCK / 32];
+    __shared__ uint32_t s_base;
+    const uint32_t q = block_append(&W.ctl[0], path, s_warp, s_base);
     if (path) W.rq[q] = i;
     W.flags[i] = path ? F_PATH : 0;
     if (new_task || task == NO_TASK) {
@@ -302,8 +313,13 @@ __global__ void __launch_bounds__(SHADE_BLOCK, SMINB) wf_shade_kernel(const Batc
             if (nee.flags & NEE_E) W.nve[s] = make_float4(nee.ve.x, nee.ve.y, nee.ve.z, 0.0f);
         }
         const bool rl = (nee.flags & NEE_RL) != 0, re = (nee.flags & NEE_RE) != 0;
-        const uint32_t ql = warp_append(&W.ctl[1], rl);
-        const uint32_t qe = warp_append(&W.ctl[1], re);
+        // (the warp's lamp rays, then its sky rays, from one atomic)
+        const uint32_t ml = __ballot_sync(0xffffffffu, rl), me = __ballot_sync(0xffffffffu, re);
+        uint32_t qb = 0;
+        if (lane == 0 && (ml | me)) qb = atomicAdd(&W.ctl[1], (uint32_t)(__popc(ml) + __popc(me)));
+        qb = __shfl_sync(0xffffffffu, qb, 0);
+        const uint32_t lt = (1u << lane) - 1u;
+        const uint32_t ql = qb + __popc(ml & lt), qe = qb + __popc(ml) + __popc(me & lt);
         if (rl) {
             W.sq_o[ql] = make_float4(nee.p.x, nee.p.y, nee.p.z, __uint_as_float(s << 1));
             W.sq_d[ql] = make_float4(nee.wl.x, nee.wl.y, nee.wl.z, nee.tl);
