@@ -43,3 +43,21 @@ def test_build_scratch_bytes_grows_with_n():
     f = L.lib().lrc_build_scratch_bytes
     assert f(1000, 30, 0) < f(100000, 30, 0) < f(100000, 63, 0)
     assert f(100000, 30, 1) > f(100000, 30, 0)
+
+
+def test_binding_constants_match_the_header():
+    """Every constant the ctypes binding restates (a name defined in include/lrc.h) has the header's
+    value."""
+    defs = {}
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", h)).read()
+            for name, val in re.findall(r"^#define\s+(LRC_[A-Z0-9_]+)\s+(.*)$", txt, flags=re.M):
+                val = re.sub(r"/\*.*", "", val).strip()
+                val = re.sub(r"(?<=[0-9a-fA-F])u\b", "", val)
+                if val and re.fullmatch(r"[0-9a-fA-Fx()<\-\s]+", val):
+                    defs[name] = int(eval(val))
+    shared = [n for n in defs if hasattr(L.native, n)]
+    assert "LRC_WAVEFRONT_DEFAULT_VARIANT" in shared and len(shared) >= 10, shared
+    wrong = {n: (getattr(L.native, n), defs[n]) for n in shared if getattr(L.native, n) != defs[n]}
+    assert not wrong, wrong
