@@ -790,7 +790,7 @@ int lrc_batch_tune(lrc_batch *b, uint64_t sample_tasks, int32_t *variant, int32_
     if (rc) return rc;
     // the queue's head: the most expensive tasks (the trace kernels write only per-task sums, which
     // the next run overwrites, so tuning changes no image)
-    // (the wavefront's sizes are judged on at least 2^24 tasks, or all: a sixteenth of a small queue
+    // (the wavefront's sizes are timed on at least 2^24 tasks, or all: a sixteenth of a small queue
     // cannot fill its larger sizes, and a size is timed only where the sample fills it)
     const unsigned long long dflt = b->engine == 1 ? std::max<unsigned long long>(b->ntasks / 16 + 1, 1ull << 24)
                                                    : b->ntasks / 16 + 1;
