@@ -68,6 +68,12 @@ struct lrc_batch {
     cudaGraphExec_t exec = nullptr;
     unsigned graph_flags = 0;
     std::vector<unsigned char> graph_sig;
+    // the wavefront's graph captured before the current one, kept: runs that alternate between two
+    // keys (a server's waves with and without instanced jobs) replay both, capturing neither again
+    cudaGraph_t alt_graph = nullptr;
+    cudaGraphExec_t alt_exec = nullptr;
+    unsigned alt_flags = 0;
+    std::vector<unsigned char> alt_sig;
     int graph_used = 0;
     cudaEvent_t ev_launch = nullptr;      // recorded right before a run's trace is launched (the server's wave timing)
     lrc::BatchJob *h_table = nullptr;     // pinned staging of the job table's upload (and the run block after it)
@@ -108,12 +114,31 @@ lrc::PtParams params_of(const lrc_batch::Job &J) {
     return P;
 }
 
-void destroy_graph(lrc_batch *b) {
+// the current graph dropped (the kept one stays)
+void drop_graph(lrc_batch *b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
     b->graph_sig.clear();
+}
+
+// both graphs dropped (their buffers may move)
+void destroy_graph(lrc_batch *b) {
+    drop_graph(b);
+    if (b->alt_exec) cudaGraphExecDestroy(b->alt_exec);
+    if (b->alt_graph) cudaGraphDestroy(b->alt_graph);
+    b->alt_exec = nullptr;
+    b->alt_graph = nullptr;
+    b->alt_sig.clear();
+}
+
+// the current graph and the kept one trade places
+void swap_graphs(lrc_batch *b) {
+    std::swap(b->graph, b->alt_graph);
+    std::swap(b->exec, b->alt_exec);
+    std::swap(b->graph_flags, b->alt_flags);
+    b->graph_sig.swap(b->alt_sig);
 }
 
 // the path tracer's view of a job's scene once the run's builds are done (a build makes the tree
@@ -380,7 +405,7 @@ int capture_exec(lrc_batch *b, unsigned flags, bool with_builds, bool with_resol
 // the run's graph, kept for replays: builds inside when GRAPH (the megakernel engine captures only
 // GRAPH runs; the wavefront's trace is always a graph, its builds plain launches without GRAPH)
 int capture(lrc_batch *b, unsigned flags, const std::vector<unsigned char> &key) {
-    destroy_graph(b);
+    drop_graph(b);
     int rc = capture_exec(b, flags, (flags & LRC_BATCH_GRAPH) != 0, true, b->ntasks, &b->graph, &b->exec);
     if (rc) return rc;
     b->graph_flags = flags;
@@ -645,8 +670,13 @@ int lrc_batch_run(lrc_batch *b, unsigned flags) {
         int rc = prepare(b, (flags & LRC_BATCH_BUILD) != 0);
         if (rc) return rc;
         const std::vector<unsigned char> key = graph_key(b, flags);
-        const bool reuse = b->exec && b->graph_flags == flags && key == b->graph_sig;
+        bool reuse = b->exec && b->graph_flags == flags && key == b->graph_sig;
+        if (!reuse && b->alt_exec && b->alt_flags == flags && key == b->alt_sig) {
+            swap_graphs(b);
+            reuse = true;
+        }
         if (!reuse) {
+            swap_graphs(b);                             // (the current graph kept, the one kept before it dropped)
             rc = capture(b, flags, key);
             if (rc) return rc;
         }
