@@ -185,3 +185,29 @@ def test_wavefront_instanced_scene_with_sky(ctx, oracle):
         assert np.array_equal(got, acc)
         assert int(b.rays()[0][0]) == rays
         b.close()
+
+
+def test_wavefront_runs_alternating_with_and_without_instances(ctx, oracle, scenes, built):
+    """Runs of one batch that alternate between jobs without instances and jobs with an instanced
+    scene (a server's waves do): each key's graph is captured once, then kept and replayed when
+    the key comes back, and every run's images are the plain ones."""
+    isc = W.instanced_box(5, n_instances=2000, width=48, height=40, spp=8)
+    inst = R.instanced_box_scene(ctx, isc, 1, blue_noise=oracle.blue_noise(), bsdf_tables=oracle.bsdf_tables())
+    sets = [list(zip(built[:3], scenes[:3])), list(zip(built[:2], scenes[:2])) + [(inst, isc)]]
+    want = [[s.trace(params(sc), sc["spp"])[0] for s, sc in js] for js in sets]
+    b = L.native.Batch(ctx)
+    b.set_engine(1)
+    used = []
+    for r in range(4):
+        js = sets[r % 2]
+        imgs = device_images([sc for _, sc in js])
+        b.clear()
+        for (s, sc), t in zip(js, imgs):
+            b.add(s, params(sc), sc["spp"], t.data_ptr())
+        b.run(graph=True)
+        got = host(ctx, imgs)
+        used.append(b.info()["graph_used"])
+        for g, acc in zip(got, want[r % 2]):
+            assert np.array_equal(g, acc)
+    assert used == [0, 0, 1, 1]
+    inst.close()
