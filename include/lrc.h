@@ -425,7 +425,9 @@ int lrc_caustics_variant(lrc_ctx *ctx, int variant);
 typedef struct lrc_batch lrc_batch;
 #define LRC_BATCH_BUILD 4u    /* build each job's scene first (its builder and key bits; once per scene) */
 #define LRC_BATCH_GRAPH 8u    /* run as one CUDA graph: captured after the first such run (which runs
-                                 uncaptured, sizing every buffer), replayed while nothing it names changed */
+                                 uncaptured, sizing every buffer), replayed while nothing it names changed
+                                 (the wavefront keeps its graph before too, and goes back to it when runs
+                                 alternate: jobs with instances, then without) */
 #define LRC_BATCH_ZERO 16u    /* clear each job's band of its image first */
 #define LRC_BATCH_STEPPED 32u /* wavefront: launch each pass's kernels from the host, no graph (slower;
                                  for profilers that cannot see into a graph's loop); not with GRAPH */
